@@ -1,0 +1,230 @@
+/*
+ * ocu_b200.h -- C ABI of the B200-native OpenCurrent projection-step library
+ * (libocu_b200.so).  Plain pointers, sizes and opaque handles; no C++ or torch types.
+ *
+ * Conventions shared by every entry point:
+ *   - Return an ocu_status; OCU_OK == 0.  ocu_last_error() gives a human-readable message for
+ *     the calling thread's most recent failure.  This replaces the reference's bool returns +
+ *     sticky ErrorHandler flag (ocuequation/error_handler.h:27-57); the C++ facade in
+ *     include/ocu/ maps it back to bool + any_error().
+ *   - Every device operation is enqueued on a caller-chosen CUDA stream (ocu_stream is
+ *     layout-compatible with cudaStream_t; NULL = legacy default stream).  The reference uses
+ *     ThreadManager::get_compute_stream() (ocuutil/thread.h:86-87).  Nothing here calls
+ *     cudaDeviceSynchronize; an entry point only blocks when it must hand a number back to the
+ *     host (norms, time steps) and says so.
+ *   - Grids follow the Grid3DDevice<T> layout contract of ocu_types.h; kernels are built for
+ *     sm_100a only and there is no CPU fallback: on a machine without a B200 every compute
+ *     entry point returns OCU_ERR_CUDA.
+ */
+#ifndef OCU_B200_H
+#define OCU_B200_H
+
+#include "ocu_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *ocu_stream; /* == cudaStream_t */
+
+typedef enum ocu_status {
+  OCU_OK = 0,
+  OCU_ERR_INVALID_VALUE = 1,  /* bad argument (NaN h, negative tolerance, bad BC type ...) */
+  OCU_ERR_LAYOUT = 2,         /* grid dimensions or padded layouts do not match */
+  OCU_ERR_CUDA = 3,           /* a CUDA runtime call or kernel launch failed */
+  OCU_ERR_NOT_CONVERGED = 4,  /* solver stopped at max_iter above tolerance */
+  OCU_ERR_NOT_INITIALIZED = 5,
+  OCU_ERR_ALLOC = 6,
+  OCU_ERR_UNSUPPORTED = 7,
+  OCU_ERR_TIMEOUT = 8         /* a bounded device-side wait gave up (status word set) */
+} ocu_status;
+
+typedef struct ocu_grid ocu_grid;
+typedef struct ocu_mg ocu_mg;
+typedef struct ocu_project ocu_project;
+typedef struct ocu_ns ocu_ns;
+
+/* ---- library ------------------------------------------------------------------------- */
+const char *ocu_last_error(void);
+/* Version string and the compute capability the kernels were built for ("sm_100a"). */
+const char *ocu_version(void);
+/* Number of kernel launches this library issued on the calling process (all streams). */
+unsigned long long ocu_kernel_launch_count(void);
+
+/* ---- grids: Grid3DDevice<T> (ocustorage/grid3d.h:219-264, grid3ddev.cu) ---------------- */
+/* Layout rule of Grid3DDevice<T>::init (grid3ddev.cu:358-400); host-only. */
+ocu_status ocu_layout_compute(int nx, int ny, int nz, int gx, int gy, int gz, int padx,
+                              int pady, int padz, ocu_layout *out);
+/* Grid3DDevice<T>::init: cudaMalloc + zero fill. */
+ocu_status ocu_grid_create(ocu_dtype dtype, int nx, int ny, int nz, int gx, int gy, int gz,
+                           int padx, int pady, int padz, ocu_grid **out);
+/* Borrow caller device memory of layout->allocated elements (e.g. a torch tensor). */
+ocu_status ocu_grid_wrap(ocu_dtype dtype, const ocu_layout *layout, void *device_buffer,
+                         ocu_grid **out);
+void ocu_grid_destroy(ocu_grid *g);
+ocu_status ocu_grid_info(const ocu_grid *g, ocu_layout *layout, ocu_dtype *dtype,
+                         void **device_buffer);
+/* copy_all_data host<->device (grid3ddev.cu:244-258; grid3dhost.cu): the whole padded
+ * buffer, synchronous with respect to the stream (the call returns after the copy). */
+ocu_status ocu_grid_upload(ocu_grid *g, const void *host_buffer, ocu_stream s);
+ocu_status ocu_grid_download(const ocu_grid *g, void *host_buffer, ocu_stream s);
+/* Same, asynchronous: host_buffer should be pinned and must stay valid until the stream
+ * reaches the copy. */
+ocu_status ocu_grid_upload_async(ocu_grid *g, const void *host_buffer, ocu_stream s);
+ocu_status ocu_grid_download_async(const ocu_grid *g, void *host_buffer, ocu_stream s);
+/* Grid3DDevice<T>::copy_all_data<S> (grid3ddev.cu:260-279): element-wise, converting. */
+ocu_status ocu_grid_copy_all_data(ocu_grid *dst, const ocu_grid *src, ocu_stream s);
+/* clear_zero / clear(T) (grid3ddev.cu:221-242). */
+ocu_status ocu_grid_clear(ocu_grid *g, double value, ocu_stream s);
+/* linear_combination (grid3ddev.cu:283-349): g2 == NULL gives this = alpha1*g1. */
+ocu_status ocu_grid_linear_combination(ocu_grid *result, double alpha1, const ocu_grid *g1,
+                                       double alpha2, const ocu_grid *g2, ocu_stream s);
+/* reduce_* (grid3dops.cu:26-130): same fold order as the reference; blocks the host. */
+ocu_status ocu_grid_reduce(const ocu_grid *g, ocu_reduce_op op, double *result, ocu_stream s);
+
+/* ---- ghost cells (ocustorage/grid3dboundary.h:26-70) --------------------------------- */
+/* apply_3d_boundary_conditions_level1 (variant OCU_BC_LEVEL1, one launch instead of three)
+ * and ..._level1_nocorners (OCU_BC_LEVEL1_NOCORNERS). */
+ocu_status ocu_apply_boundary_conditions(ocu_grid *g, const ocu_bc_set *bc, double hx,
+                                         double hy, double hz, ocu_bc_variant variant,
+                                         ocu_stream s);
+/* apply_3d_mac_boundary_conditions_level1 (grid3dboundary.cu:823-900). */
+ocu_status ocu_apply_mac_boundary_conditions(ocu_grid *u, ocu_grid *v, ocu_grid *w,
+                                             const ocu_bc_set *bc, double hx, double hy,
+                                             double hz, ocu_stream s);
+
+/* ---- stateless stencils ---------------------------------------------------------------- */
+/* Sol_Divergence3DDevice<T>::solve (sol_divergence3ddev.cu:23-88). */
+ocu_status ocu_divergence(const ocu_grid *u, const ocu_grid *v, const ocu_grid *w,
+                          ocu_grid *divergence, int nx, int ny, int nz, double hx, double hy,
+                          double hz, ocu_stream s);
+/* Sol_Gradient3DDevice<T>::solve: u += coefficient * grad(phi) (sol_gradient3ddev.cu:24-88). */
+ocu_status ocu_gradient_add(ocu_grid *u, ocu_grid *v, ocu_grid *w, const ocu_grid *phi,
+                            double coefficient, double hx, double hy, double hz, ocu_stream s);
+/* Sol_SelfAdvection3DDevice<T>::solve (sol_selfadvection3ddev.cu:584-590, kernels :135-337). */
+ocu_status ocu_advect_self(const ocu_grid *u, const ocu_grid *v, const ocu_grid *w,
+                           ocu_grid *dudt, ocu_grid *dvdt, ocu_grid *dwdt, int nx, int ny,
+                           int nz, double hx, double hy, double hz, ocu_interpolation interp,
+                           ocu_stream s);
+/* Sol_PassiveAdvection3DDevice<T>::solve (sol_passiveadvection3ddev.cu:31-136). */
+ocu_status ocu_advect_passive(const ocu_grid *u, const ocu_grid *v, const ocu_grid *w,
+                              const ocu_grid *phi, ocu_grid *dphidt, int nx, int ny, int nz,
+                              double hx, double hy, double hz, ocu_interpolation interp,
+                              ocu_stream s);
+/* Sol_LaplacianCentered3DDevice<T>::solve: dphidt += coefficient * lap(phi) over
+ * (nx,ny,nz) cells (sol_laplaciancent3ddev.cu:28-109). */
+ocu_status ocu_laplacian_add(const ocu_grid *phi, ocu_grid *dphidt, int nx, int ny, int nz,
+                             double hx, double hy, double hz, double coefficient,
+                             ocu_stream s);
+
+/* ---- multigrid pressure solver (Sol_MultigridPressure3DDevice<T>,
+ *      ocuequation/sol_mgpressure3d.h:36-248) ------------------------------------------- */
+typedef enum ocu_mg_kind {
+  OCU_MG_F32 = 0,              /* Sol_MultigridPressure3DDeviceF */
+  OCU_MG_F64 = 1,              /* Sol_MultigridPressure3DDeviceD */
+  OCU_MG_MIXED_IR = 2,         /* FP32 V-cycles inside FP64 iterative refinement (new) */
+  OCU_MG_MIXED_WARMSTART = 3   /* reference Sol_MultigridPressureMixed3DDeviceD algorithm
+                                  (sol_mgpressuremixed3ddevd.cpp:79-100) */
+} ocu_mg_kind;
+
+/* Public fields of Sol_MultigridPressure3DBase / ...Device (sol_mgpressure3d.h:86-90, 163). */
+typedef struct ocu_mg_params {
+  ocu_bc_set bc;
+  int nu1, nu2;
+  int convergence;               /* ocu_convergence */
+  int make_symmetric_operator;
+  int disable_relax_on_host;     /* kept for API parity: the coarsest level is always relaxed
+                                    on the device here; 1 = use the device colour-sweep kernel
+                                    instead of the host-order one (see DESIGN) */
+  int ir_inner_cycles;           /* OCU_MG_MIXED_IR only: FP32 fine-level cycles per
+                                    correction (0 = default 3) */
+  int store_residual_grids;      /* 1 = keep r_grid(level) filled (read_r); costs N*s */
+} ocu_mg_params;
+
+typedef struct ocu_mg_stats {
+  int num_levels;
+  int vcycles;                   /* fine-level cycles of the last do_fmg / IR inner total */
+  int outer_iterations;          /* OCU_MG_MIXED_IR: refinement steps of the last solve */
+  double last_l2, last_linf;     /* norms of the last convergence check */
+  double omega;
+} ocu_mg_stats;
+
+/* Fills the reference constructor defaults (sol_mgpressure3d.cpp:26-40). */
+void ocu_mg_params_default(ocu_mg_params *p);
+ocu_status ocu_mg_create(ocu_mg_kind kind, const ocu_mg_params *params, ocu_mg **out);
+void ocu_mg_destroy(ocu_mg *mg);
+ocu_status ocu_mg_set_params(ocu_mg *mg, const ocu_mg_params *params);
+ocu_status ocu_mg_get_params(const ocu_mg *mg, ocu_mg_params *params);
+ocu_status ocu_mg_set_stream(ocu_mg *mg, ocu_stream s);
+/* initialize_storage (sol_mgpressure3ddev.cu:376-482).  rhs is borrowed, not copied; its dtype
+ * must be F32 for OCU_MG_F32 and F64 otherwise; ghost >= 1. */
+ocu_status ocu_mg_initialize_storage(ocu_mg *mg, int nx, int ny, int nz, double hx, double hy,
+                                     double hz, ocu_grid *rhs);
+/* solve(residual, tol, max_iter) (sol_mgpressure3d.cpp:332-370): OCU_OK when converged,
+ * OCU_ERR_NOT_CONVERGED otherwise (residual still written).  Blocks the host. */
+ocu_status ocu_mg_solve(ocu_mg *mg, double *residual, double tolerance, int max_iter);
+ocu_status ocu_mg_run_vcycles(ocu_mg *mg, int count);   /* sol_mgpressure3d.cpp:372-384 */
+ocu_status ocu_mg_run_fmg(ocu_mg *mg, int count);       /* sol_mgpressure3d.cpp:386-398 */
+/* pressure() and read_u/r/b(level) (sol_mgpressure3d.h:173-179); which = 'u','r','b'.
+ * The handle is owned by the solver. */
+ocu_grid *ocu_mg_pressure(ocu_mg *mg);
+ocu_grid *ocu_mg_level_grid(ocu_mg *mg, char which, int level);
+ocu_status ocu_mg_get_stats(const ocu_mg *mg, ocu_mg_stats *stats);
+
+/* ---- projection (Sol_ProjectDivergence3DDevice<T>, sol_project3d.h:29-129) ------------- */
+ocu_status ocu_project_create(ocu_dtype dtype, ocu_project **out);
+void ocu_project_destroy(ocu_project *p);
+ocu_status ocu_project_set_stream(ocu_project *p, ocu_stream s);
+/* initialize_storage (sol_project3ddev.cu:100-135): u,v,w borrowed MAC grids of one layout. */
+ocu_status ocu_project_initialize_storage(ocu_project *p, int nx, int ny, int nz, double hx,
+                                          double hy, double hz, ocu_grid *u, ocu_grid *v,
+                                          ocu_grid *w, const ocu_bc_set *bc);
+ocu_status ocu_project_solve(ocu_project *p, double tolerance);           /* :58-71 */
+ocu_status ocu_project_solve_divergence_only(ocu_project *p);             /* :73-84 */
+ocu_grid *ocu_project_divergence(ocu_project *p);
+ocu_mg *ocu_project_pressure_solver(ocu_project *p);
+
+/* ---- incompressible Navier-Stokes / Boussinesq (Eqn_IncompressibleNS3D<T>,
+ *      ocuequation/eqn_incompressns3d.h:34-248) ------------------------------------------ */
+typedef struct ocu_ns_params {
+  int nx, ny, nz;
+  double hx, hy, hz;
+  double max_divergence;
+  ocu_bc_set temp_bc;
+  ocu_bc_set flow_bc;
+  int vertical_direction;        /* ocu_direction */
+  double gravity;                /* rounded to T, like the reference's T fields */
+  double bouyancy;
+  double thermal_diffusion;
+  double viscosity;
+  int advection_scheme;          /* ocu_interpolation */
+  int time_step;                 /* ocu_timestep */
+  double cfl_factor;
+} ocu_ns_params;
+
+/* Eqn_IncompressibleNS3DParams() defaults (eqn_incompressns3d.h:62-73). */
+void ocu_ns_params_default(ocu_ns_params *p);
+/* Layouts of Eqn_IncompressibleNS3DParams::init_grids (eqn_incompressns3d.h:75-83);
+ * which = 'u','v','w','t'. */
+ocu_status ocu_ns_init_layout(int nx, int ny, int nz, char which, ocu_layout *out);
+ocu_status ocu_ns_create(ocu_dtype dtype, ocu_ns **out);
+void ocu_ns_destroy(ocu_ns *ns);
+ocu_status ocu_ns_set_stream(ocu_ns *ns, ocu_stream s);
+/* set_parameters (eqn_incompressns3d.cu:164-298); init_* are HOST buffers in the
+ * init_grids layouts. */
+ocu_status ocu_ns_set_parameters(ocu_ns *ns, const ocu_ns_params *params, const void *init_u,
+                                 const void *init_v, const void *init_w,
+                                 const void *init_temp);
+/* get_max_stable_timestep (:301-328); blocks the host for three maxabs reductions. */
+ocu_status ocu_ns_get_max_stable_timestep(ocu_ns *ns, double *dt);
+ocu_status ocu_ns_advance_one_step(ocu_ns *ns, double dt);                  /* :331-399 */
+ocu_status ocu_ns_advance(ocu_ns *ns, double dt);       /* Equation::advance, equation.cpp:31-56 */
+/* get_u/v/w/temperature (:171-174) and the time derivatives 'U','V','W','T', pressure 'p'. */
+ocu_grid *ocu_ns_grid(ocu_ns *ns, char which);
+int ocu_ns_num_steps(const ocu_ns *ns);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OCU_B200_H */

@@ -1,0 +1,541 @@
+"""opencurrent_b200 -- B200-native (sm_100a) OpenCurrent projection-step hot path.
+
+Python mirror of the reference's C++ API over the C ABI of libocu_b200.so
+(include/ocu_b200.h).  Class and member names follow OpenCurrent (namespace ocu):
+Grid3DDevice, BoundaryCondition(Set), Sol_MultigridPressure3DDevice,
+Sol_MultigridPressureMixed3DDeviceD, Sol_ProjectDivergence3DDevice, Sol_SelfAdvection3DDevice,
+Sol_PassiveAdvection3DDevice, Sol_LaplacianCentered3DDevice, Eqn_IncompressibleNS3D.
+Where the reference returns bool and fills a double& (solve), the Python method returns
+(ok, residual).  Every compute call runs on the device; nothing falls back to the CPU.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import *  # noqa: F401,F403  (enums, structs)
+from ._capi import OcuError, check, load
+
+__all__ = [
+    "BoundaryCondition", "BoundaryConditionSet", "Grid3DDevice", "Sol_MultigridPressure3DDevice",
+    "Sol_MultigridPressure3DDeviceF", "Sol_MultigridPressure3DDeviceD",
+    "Sol_MultigridPressureMixed3DDeviceD", "Sol_ProjectDivergence3DDevice",
+    "Sol_SelfAdvection3DDevice", "Sol_PassiveAdvection3DDevice", "Sol_LaplacianCentered3DDevice",
+    "Eqn_IncompressibleNS3DParams", "Eqn_IncompressibleNS3D", "layout", "OcuError",
+    "kernel_launch_count",
+]
+
+
+def kernel_launch_count():
+    return int(load().ocu_kernel_launch_count())
+
+
+def _np_dtype(dt):
+    return np.float64 if dt == F64 else np.float32
+
+
+def layout(nx, ny, nz, gx=1, gy=1, gz=1, padx=0, pady=0, padz=0):
+    """Grid3DDevice<T>::init layout rule (ocustorage/grid3ddev.cu:358-400)."""
+    L = Layout()
+    check(load().ocu_layout_compute(nx, ny, nz, gx, gy, gz, padx, pady, padz, C.byref(L)))
+    return L
+
+
+class BoundaryCondition:
+    """ocuutil/boundary_condition.h:38-58 (value/aux_value are float32 in the reference)."""
+
+    def __init__(self, type=BC_INVALID, value=0.0, aux_value=0.0):
+        self.type, self.value, self.aux_value = int(type), float(value), float(aux_value)
+
+    def to_c(self):
+        return BC(self.type, self.value, self.aux_value)
+
+
+class BoundaryConditionSet:
+    FACES = ("xpos", "xneg", "ypos", "yneg", "zpos", "zneg")
+
+    def __init__(self, all_faces=None, **faces):
+        for f in self.FACES:
+            src = faces.get(f, all_faces)
+            if src is None:
+                src = BoundaryCondition()
+            setattr(self, f, BoundaryCondition(src.type, src.value, src.aux_value))
+
+    def to_c(self):
+        s = BCSet()
+        for f in self.FACES:
+            setattr(s, f, getattr(self, f).to_c())
+        return s
+
+    def make_homogeneous(self):
+        for f in self.FACES:
+            getattr(self, f).value = 0.0
+            getattr(self, f).aux_value = 0.0
+
+
+class Grid3DDevice:
+    """Device grid in the Grid3DDevice<T> layout; owns its buffer unless it wraps a solver's."""
+
+    def __init__(self, dtype=F32, _handle=None, _owner=None):
+        self.dtype = dtype
+        self._h = _handle
+        self._owner = _owner  # keeps a parent solver alive for borrowed handles
+        self._owned = _handle is None
+
+    @classmethod
+    def _borrow(cls, handle, owner):
+        if not handle:
+            return None
+        lib = load()
+        dt = C.c_int()
+        check(lib.ocu_grid_info(handle, None, C.byref(dt), None))
+        return cls(dt.value, _handle=handle, _owner=owner)
+
+    def init(self, nx, ny, nz, gx=1, gy=1, gz=1, padx=0, pady=0, padz=0):
+        h = C.c_void_p()
+        check(load().ocu_grid_create(self.dtype, nx, ny, nz, gx, gy, gz, padx, pady, padz, C.byref(h)))
+        self._h = h.value
+        self._owned = True
+        return True
+
+    def init_congruent(self, other):
+        L = other.layout
+        return self.init(L.nx, L.ny, L.nz, L.gx, L.gy, L.gz, L.pnx - (L.nx + 2 * L.gx),
+                         L.pny - (L.ny + 2 * L.gy), L.pnz - (L.nz + 2 * L.gz))
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def layout(self):
+        L = Layout()
+        check(load().ocu_grid_info(self._h, C.byref(L), None, None))
+        return L
+
+    @property
+    def device_ptr(self):
+        p = C.c_void_p()
+        check(load().ocu_grid_info(self._h, None, None, C.byref(p)))
+        return p.value
+
+    nx = property(lambda self: self.layout.nx)
+    ny = property(lambda self: self.layout.ny)
+    nz = property(lambda self: self.layout.nz)
+
+    def empty_host(self):
+        return np.zeros(int(self.layout.allocated), dtype=_np_dtype(self.dtype))
+
+    def copy_from_host(self, host):
+        host = np.ascontiguousarray(host, dtype=_np_dtype(self.dtype))
+        assert host.size == self.layout.allocated
+        check(load().ocu_grid_upload(self._h, host.ctypes.data_as(C.c_void_p), None))
+
+    def copy_to_host(self, out=None):
+        if out is None:
+            out = self.empty_host()
+        check(load().ocu_grid_download(self._h, out.ctypes.data_as(C.c_void_p), None))
+        return out
+
+    def clear_zero(self):
+        check(load().ocu_grid_clear(self._h, 0.0, None))
+        return True
+
+    def clear(self, value):
+        check(load().ocu_grid_clear(self._h, float(value), None))
+        return True
+
+    def copy_all_data(self, other):
+        check(load().ocu_grid_copy_all_data(self._h, other._h, None))
+        return True
+
+    def linear_combination(self, a1, g1, a2=None, g2=None):
+        check(load().ocu_grid_linear_combination(self._h, float(a1), g1._h, float(a2 or 0.0),
+                                                 g2._h if g2 is not None else None, None))
+        return True
+
+    def _reduce(self, op):
+        r = C.c_double()
+        check(load().ocu_grid_reduce(self._h, op, C.byref(r), None))
+        return r.value
+
+    def reduce_maxabs(self):
+        return self._reduce(REDUCE_MAXABS)
+
+    def reduce_max(self):
+        return self._reduce(REDUCE_MAX)
+
+    def reduce_min(self):
+        return self._reduce(REDUCE_MIN)
+
+    def reduce_sum(self):
+        return self._reduce(REDUCE_SUM)
+
+    def reduce_sqrsum(self):
+        return self._reduce(REDUCE_SQRSUM)
+
+    def reduce_checknan(self):
+        return self._reduce(REDUCE_CHECKNAN)
+
+    def apply_boundary_conditions(self, bc, hx, hy, hz, variant=BC_LEVEL1):
+        c = bc.to_c()
+        check(load().ocu_apply_boundary_conditions(self._h, C.byref(c), hx, hy, hz, variant, None))
+
+    def __del__(self):
+        try:
+            if self._owned and self._h:
+                load().ocu_grid_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+def apply_3d_mac_boundary_conditions_level1(u, v, w, bc, hx, hy, hz):
+    c = bc.to_c()
+    check(load().ocu_apply_mac_boundary_conditions(u._h, v._h, w._h, C.byref(c), hx, hy, hz, None))
+    return True
+
+
+class _MGBase:
+    kind = MG_F32
+
+    def __init__(self):
+        p = MGParams()
+        load().ocu_mg_params_default(C.byref(p))
+        self.bc = BoundaryConditionSet()
+        self.nu1 = p.nu1
+        self.nu2 = p.nu2
+        self.convergence = p.convergence
+        self.make_symmetric_operator = False
+        self.disable_relax_on_host = False
+        self.ir_inner_cycles = p.ir_inner_cycles
+        self._h = None
+        self._rhs = None
+
+    def _params(self):
+        p = MGParams()
+        p.bc = self.bc.to_c()
+        p.nu1, p.nu2, p.convergence = self.nu1, self.nu2, self.convergence
+        p.make_symmetric_operator = int(bool(self.make_symmetric_operator))
+        p.disable_relax_on_host = int(bool(self.disable_relax_on_host))
+        p.ir_inner_cycles = self.ir_inner_cycles
+        return p
+
+    def initialize_storage(self, nx, ny, nz, hx, hy, hz, rhs):
+        lib = load()
+        h = C.c_void_p()
+        p = self._params()
+        check(lib.ocu_mg_create(self.kind, C.byref(p), C.byref(h)))
+        self._h = h.value
+        self._rhs = rhs  # borrowed, as in the reference
+        check(lib.ocu_mg_initialize_storage(self._h, nx, ny, nz, hx, hy, hz, rhs._h))
+        return True
+
+    def _sync_params(self):
+        p = self._params()
+        check(load().ocu_mg_set_params(self._h, C.byref(p)))
+
+    def solve(self, tolerance=1e-6, max_iter=4):
+        """Base::solve (sol_mgpressure3d.cpp:332-370) -> (converged, residual)."""
+        self._sync_params()
+        r = C.c_double()
+        st = check(load().ocu_mg_solve(self._h, C.byref(r), tolerance, max_iter),
+                   allow=(ERR_NOT_CONVERGED,))
+        return st == OK, r.value
+
+    def run_vcycles(self, count):
+        self._sync_params()
+        check(load().ocu_mg_run_vcycles(self._h, count))
+        return True
+
+    def run_fmg(self, count):
+        self._sync_params()
+        check(load().ocu_mg_run_fmg(self._h, count))
+        return True
+
+    def pressure(self):
+        return Grid3DDevice._borrow(load().ocu_mg_pressure(self._h), self)
+
+    def read_u(self, level):
+        return Grid3DDevice._borrow(load().ocu_mg_level_grid(self._h, b"u", level), self)
+
+    def read_r(self, level):
+        return Grid3DDevice._borrow(load().ocu_mg_level_grid(self._h, b"r", level), self)
+
+    def read_b(self, level):
+        return Grid3DDevice._borrow(load().ocu_mg_level_grid(self._h, b"b", level), self)
+
+    @property
+    def stats(self):
+        s = MGStats()
+        check(load().ocu_mg_get_stats(self._h, C.byref(s)))
+        return s
+
+    def __del__(self):
+        try:
+            if self._h:
+                load().ocu_mg_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+class Sol_MultigridPressure3DDevice(_MGBase):
+    """Sol_MultigridPressure3DDevice<T> (ocuequation/sol_mgpressure3d.h:104-181)."""
+
+    def __init__(self, dtype=F32):
+        super().__init__()
+        self.kind = MG_F64 if dtype == F64 else MG_F32
+
+
+def Sol_MultigridPressure3DDeviceF():
+    return Sol_MultigridPressure3DDevice(F32)
+
+
+def Sol_MultigridPressure3DDeviceD():
+    return Sol_MultigridPressure3DDevice(F64)
+
+
+class Sol_MultigridPressureMixed3DDeviceD(_MGBase):
+    """FP64-interface mixed solver.  algorithm='ir' (default): FP32 V-cycles inside FP64
+    iterative refinement; algorithm='warmstart': the reference algorithm
+    (sol_mgpressuremixed3ddevd.cpp:79-100)."""
+
+    def __init__(self, algorithm="ir"):
+        super().__init__()
+        self.kind = MG_MIXED_IR if algorithm == "ir" else MG_MIXED_WARMSTART
+
+
+class Sol_ProjectDivergence3DDevice:
+    """Sol_ProjectDivergence3DDevice<T> (ocuequation/sol_project3d.h:74-93)."""
+
+    def __init__(self, dtype=F32):
+        self.dtype = dtype
+        self.bc = BoundaryConditionSet()
+        h = C.c_void_p()
+        check(load().ocu_project_create(dtype, C.byref(h)))
+        self._h = h.value
+        self._keep = None
+
+    def initialize_storage(self, nx, ny, nz, hx, hy, hz, u, v, w):
+        c = self.bc.to_c()
+        self._keep = (u, v, w)
+        check(load().ocu_project_initialize_storage(self._h, nx, ny, nz, hx, hy, hz, u._h, v._h, w._h,
+                                                    C.byref(c)))
+        return True
+
+    def solve(self, tolerance=1e-5):
+        st = check(load().ocu_project_solve(self._h, tolerance), allow=(ERR_NOT_CONVERGED,))
+        return st == OK
+
+    def solve_divergence_only(self):
+        check(load().ocu_project_solve_divergence_only(self._h))
+        return True
+
+    @property
+    def divergence(self):
+        return Grid3DDevice._borrow(load().ocu_project_divergence(self._h), self)
+
+    @property
+    def pressure_solver(self):
+        h = load().ocu_project_pressure_solver(self._h)
+        p = MGParams()
+        check(load().ocu_mg_get_params(h, C.byref(p)))
+        return _BorrowedMG(h, self, p)
+
+    def __del__(self):
+        try:
+            if self._h:
+                load().ocu_project_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+class _BorrowedMG(_MGBase):
+    """Pressure solver owned by a projection object (no destroy on collection)."""
+
+    def __init__(self, handle, owner, p):
+        _MGBase.__init__(self)
+        self._h = handle
+        self._owner = owner
+        self.nu1, self.nu2, self.convergence = p.nu1, p.nu2, p.convergence
+        bc = BoundaryConditionSet()
+        for f in BoundaryConditionSet.FACES:
+            b = getattr(p.bc, f)
+            setattr(bc, f, BoundaryCondition(b.type, b.value, b.aux_value))
+        self.bc = bc
+
+    def __del__(self):
+        pass
+
+
+class Sol_SelfAdvection3DDevice:
+    """Sol_SelfAdvection3DDevice<T> (sol_selfadvection3d.h:33-73)."""
+
+    def __init__(self):
+        self.interp_type = IT_FIRST_ORDER_UPWIND
+
+    def initialize_storage(self, nx, ny, nz, hx, hy, hz, u, v, w, dudt, dvdt, dwdt):
+        self.args = (nx, ny, nz, hx, hy, hz)
+        self.g = (u, v, w, dudt, dvdt, dwdt)
+        return True
+
+    def solve(self):
+        nx, ny, nz, hx, hy, hz = self.args
+        u, v, w, du, dv, dw = self.g
+        check(load().ocu_advect_self(u._h, v._h, w._h, du._h, dv._h, dw._h, nx, ny, nz, hx, hy, hz,
+                                     self.interp_type, None))
+        return True
+
+
+class Sol_PassiveAdvection3DDevice:
+    """Sol_PassiveAdvection3DDevice<T> (sol_passiveadvection3d.h:32-62)."""
+
+    def __init__(self):
+        self.interp_type = IT_FIRST_ORDER_UPWIND
+
+    def initialize_storage(self, nx, ny, nz, hx, hy, hz, u, v, w, phi, dphidt):
+        self.args = (nx, ny, nz, hx, hy, hz)
+        self.g = (u, v, w, phi, dphidt)
+        return True
+
+    def solve(self):
+        nx, ny, nz, hx, hy, hz = self.args
+        u, v, w, phi, dphi = self.g
+        check(load().ocu_advect_passive(u._h, v._h, w._h, phi._h, dphi._h, nx, ny, nz, hx, hy, hz,
+                                        self.interp_type, None))
+        return True
+
+
+class Sol_LaplacianCentered3DDevice:
+    """Sol_LaplacianCentered3DDevice<T> (sol_laplaciancent3d.h:28-58)."""
+
+    def __init__(self):
+        self.coefficient = 1.0
+
+    def initialize_storage(self, nx, ny, nz, hx, hy, hz, phi, dphidt):
+        self.args = (nx, ny, nz, hx, hy, hz)
+        self.g = (phi, dphidt)
+        return True
+
+    def solve(self):
+        nx, ny, nz, hx, hy, hz = self.args
+        phi, dphi = self.g
+        check(load().ocu_laplacian_add(phi._h, dphi._h, nx, ny, nz, hx, hy, hz, float(self.coefficient),
+                                       None))
+        return True
+
+
+class Eqn_IncompressibleNS3DParams:
+    """Eqn_IncompressibleNS3DParams<T> (eqn_incompressns3d.h:34-87); init_* are numpy host grids."""
+
+    def __init__(self, dtype=F32):
+        p = NSParams()
+        load().ocu_ns_params_default(C.byref(p))
+        self.dtype = dtype
+        self.nx = self.ny = self.nz = 0
+        self.hx = self.hy = self.hz = 0.0
+        self.max_divergence = p.max_divergence
+        self.temp_bc = BoundaryConditionSet()
+        self.flow_bc = BoundaryConditionSet()
+        self.vertical_direction = p.vertical_direction
+        self.gravity = p.gravity
+        self.bouyancy = p.bouyancy
+        self.thermal_diffusion = p.thermal_diffusion
+        self.viscosity = p.viscosity
+        self.advection_scheme = p.advection_scheme
+        self.time_step = p.time_step
+        self.cfl_factor = p.cfl_factor
+        self.init_u = self.init_v = self.init_w = self.init_temp = None
+        self.layouts = {}
+
+    def init_grids(self, nx, ny, nz):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        for c in "uvwt":
+            L = Layout()
+            check(load().ocu_ns_init_layout(nx, ny, nz, c.encode(), C.byref(L)))
+            self.layouts[c] = L
+        dt = _np_dtype(self.dtype)
+        self.init_u = np.zeros(int(self.layouts["u"].allocated), dt)
+        self.init_v = np.zeros(int(self.layouts["v"].allocated), dt)
+        self.init_w = np.zeros(int(self.layouts["w"].allocated), dt)
+        self.init_temp = np.zeros(int(self.layouts["t"].allocated), dt)
+
+    def to_c(self):
+        p = NSParams()
+        p.nx, p.ny, p.nz = self.nx, self.ny, self.nz
+        p.hx, p.hy, p.hz = self.hx, self.hy, self.hz
+        p.max_divergence = self.max_divergence
+        p.temp_bc = self.temp_bc.to_c()
+        p.flow_bc = self.flow_bc.to_c()
+        p.vertical_direction = self.vertical_direction
+        p.gravity, p.bouyancy = self.gravity, self.bouyancy
+        p.thermal_diffusion, p.viscosity = self.thermal_diffusion, self.viscosity
+        p.advection_scheme, p.time_step, p.cfl_factor = self.advection_scheme, self.time_step, self.cfl_factor
+        return p
+
+
+class Eqn_IncompressibleNS3D:
+    """Eqn_IncompressibleNS3D<T> (eqn_incompressns3d.h:138-177)."""
+
+    def __init__(self, dtype=F32):
+        self.dtype = dtype
+        h = C.c_void_p()
+        check(load().ocu_ns_create(dtype, C.byref(h)))
+        self._h = h.value
+
+    def set_parameters(self, params):
+        p = params.to_c()
+        dt = _np_dtype(self.dtype)
+        arrs = [np.ascontiguousarray(a, dtype=dt) for a in
+                (params.init_u, params.init_v, params.init_w, params.init_temp)]
+        check(load().ocu_ns_set_parameters(self._h, C.byref(p),
+                                           *[a.ctypes.data_as(C.c_void_p) for a in arrs]))
+        return True
+
+    def get_max_stable_timestep(self):
+        d = C.c_double()
+        check(load().ocu_ns_get_max_stable_timestep(self._h, C.byref(d)))
+        return d.value
+
+    def advance_one_step(self, dt):
+        check(load().ocu_ns_advance_one_step(self._h, dt))
+        return True
+
+    def advance(self, dt):
+        check(load().ocu_ns_advance(self._h, dt))
+        return True
+
+    @property
+    def num_steps(self):
+        return load().ocu_ns_num_steps(self._h)
+
+    def _grid(self, c):
+        return Grid3DDevice._borrow(load().ocu_ns_grid(self._h, c.encode()), self)
+
+    def get_u(self):
+        return self._grid("u")
+
+    def get_v(self):
+        return self._grid("v")
+
+    def get_w(self):
+        return self._grid("w")
+
+    def get_temperature(self):
+        return self._grid("t")
+
+    def get_deriv(self, c):
+        return self._grid(c.upper())
+
+    def get_pressure(self):
+        return self._grid("p")
+
+    def __del__(self):
+        try:
+            if self._h:
+                load().ocu_ns_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass

@@ -1,0 +1,329 @@
+// Projection (Sol_ProjectDivergence3DDevice<T>) and the Boussinesq Navier-Stokes stepper
+// (Eqn_IncompressibleNS3D<T>) over the sm_100a stencil kernels and the multigrid solver.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "flow_solvers.h"
+
+namespace ocub {
+
+static bool valid_mac(const ocu_grid *u, const ocu_grid *v, const ocu_grid *w, int nx, int ny, int nz) {
+  // check_valid_mac_dimensions (ocustorage/grid3dops.cpp:24-45)
+  if (u->L.nx != nx + 1 || u->L.ny != ny || u->L.nz != nz) return false;
+  if (v->L.nx != nx || v->L.ny != ny + 1 || v->L.nz != nz) return false;
+  if (w->L.nx != nx || w->L.ny != ny || w->L.nz != nz + 1) return false;
+  return layout_match(u->L, v->L) && layout_match(u->L, w->L);
+}
+
+// convert_bc_to_poisson_eqn (sol_project3d.cpp:26-43)
+static bool convert_bc(const ocu_bc &b, ocu_bc *out) {
+  out->type = OCU_BC_INVALID;
+  out->value = 0;
+  out->aux_value = 0;
+  if (b.type == OCU_BC_PERIODIC) { out->type = OCU_BC_PERIODIC; return true; }
+  if (b.type == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) { out->type = OCU_BC_NEUMANN; return true; }
+  return false;
+}
+
+ProjectSolver::~ProjectSolver() {
+  delete mg;
+  if (divergence) { cudaFree(divergence->buf); delete divergence; }
+}
+
+// initialize_storage (sol_project3ddev.cu:100-135, initialize_device_storage :28-53)
+ocu_status ProjectSolver::initialize_storage(int nx_, int ny_, int nz_, double hx_, double hy_, double hz_,
+                                             ocu_grid *u_, ocu_grid *v_, ocu_grid *w_, const ocu_bc_set &bc_) {
+  if (!u_ || !v_ || !w_) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_ProjectDivergence3DDevice::initialize_storage - null grid");
+  if (u_->dtype != dtype || v_->dtype != dtype || w_->dtype != dtype)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_ProjectDivergence3DDevice::initialize_storage - element type mismatch");
+  if (!valid_mac(u_, v_, w_, nx_, ny_, nz_))
+    return fail(OCU_ERR_LAYOUT, "[ERROR] Sol_ProjectDivergence3DBase::initialize_base_storage - u,v,w grid dimensions mismatch");
+  if (!check_float((float)hx_) || !check_float((float)hy_) || !check_float((float)hz_))
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_ProjectDivergence3DBase::initialize_base_storage - garbage hx,hy,hz value");
+  if (u_->L.gx < 1 || u_->L.gy < 1 || u_->L.gz < 1)
+    return fail(OCU_ERR_LAYOUT, "[ERROR] Sol_Divergence3DDevice::initialize_storage - must have at least one ghost cell on all sides");
+  nx = nx_; ny = ny_; nz = nz_;
+  hx = hx_; hy = hy_; hz = hz_;
+  u = u_; v = v_; w = w_;
+  bc = bc_;
+  ocu_mg_params p;
+  ocu_mg_params_default(&p);
+  if (!convert_bc(bc.xneg, &p.bc.xneg) || !convert_bc(bc.xpos, &p.bc.xpos) || !convert_bc(bc.yneg, &p.bc.yneg) ||
+      !convert_bc(bc.ypos, &p.bc.ypos) || !convert_bc(bc.zneg, &p.bc.zneg) || !convert_bc(bc.zpos, &p.bc.zpos))
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_ProjectDivergence3DBase::convert_bc_to_poisson_eqn - invalid boundary condition type");
+  ocu_layout Ld;
+  layout_compute(nx, ny, nz, 1, 1, 1, u->L.pnx - (nx + 2), u->L.pny - (ny + 2), u->L.pnz - (nz + 2), &Ld);
+  if (!layout_match(Ld, u->L))
+    return fail(OCU_ERR_LAYOUT, "[ERROR] Sol_ProjectDivergence3DDevice::initialize_device_storage - divergence layout mismatch");
+  divergence = new ocu_grid{dtype, Ld, nullptr, true};
+  OCU_TRY(check_cuda(cudaMalloc(&divergence->buf, dtype_size(dtype) * Ld.allocated), "cudaMalloc(divergence)"));
+  OCU_TRY(check_cuda(cudaMemset(divergence->buf, 0, dtype_size(dtype) * Ld.allocated), "cudaMemset(divergence)"));
+  mg = new ocu_mg(dtype == OCU_F64 ? OCU_MG_F64 : OCU_MG_F32, p);
+  mg->s.set_stream(stream);
+  OCU_TRY(mg->s.initialize_storage(nx, ny, nz, hx, hy, hz, divergence));
+  if (!layout_match(u->L, mg->s.pressure->L))
+    return fail(OCU_ERR_LAYOUT, "[ERROR] Sol_ProjectDivergence3DDevice::initialize_storage - pressure layout mismatch");
+  // pressure().clear_zero(); convergence = CONVERGENCE_LINF (sol_project3ddev.cu:131-132)
+  OCU_TRY(check_cuda(cudaMemsetAsync(mg->s.pressure->buf, 0, dtype_size(dtype) * Ld.allocated, stream), "clear_zero"));
+  p.convergence = OCU_CONVERGENCE_LINF;
+  mg->s.set_params(p);
+  initialized = true;
+  return OCU_OK;
+}
+
+template <typename T>
+ocu_status ProjectSolver::divergence_only_t() {
+  OCU_TRY(launch_mac_bc_level1<T>(origin<T>(u), origin<T>(v), origin<T>(w), u->L, nx, ny, nz, bc, stream));
+  return launch_divergence<T>(origin<T>(u), origin<T>(v), origin<T>(w), origin<T>(divergence), u->L, nx, ny, nz, hx,
+                              hy, hz, stream);
+}
+
+template <typename T>
+ocu_status ProjectSolver::solve_t(double tolerance) {
+  OCU_TRY(divergence_only_t<T>());
+  double residual = 0;
+  ocu_status st = mg->s.solve(&residual, tolerance, 15);
+  if (st != OCU_OK && st != OCU_ERR_NOT_CONVERGED) return st;
+  OCU_TRY(launch_gradient<T>(origin<T>(u), origin<T>(v), origin<T>(w), origin<T>(mg->s.pressure), u->L, nx, ny, nz,
+                             hx, hy, hz, (T)-1, stream));
+  OCU_TRY(launch_mac_bc_level1<T>(origin<T>(u), origin<T>(v), origin<T>(w), u->L, nx, ny, nz, bc, stream));
+  return st;
+}
+
+// solve (sol_project3ddev.cu:58-71): MAC ghosts, divergence, pressure solve (max_iter 15),
+// u -= grad p, MAC ghosts.  A pressure solve that stops above tolerance makes the whole call
+// report OCU_ERR_NOT_CONVERGED, as the reference returns false.
+ocu_status ProjectSolver::solve(double tolerance) {
+  if (!initialized) return fail(OCU_ERR_NOT_INITIALIZED, "[ERROR] Sol_ProjectDivergence3DDevice::solve - not initialized");
+  return dtype == OCU_F64 ? solve_t<double>(tolerance) : solve_t<float>(tolerance);
+}
+
+ocu_status ProjectSolver::solve_divergence_only() {
+  if (!initialized) return fail(OCU_ERR_NOT_INITIALIZED, "[ERROR] solve_divergence_only - not initialized");
+  OCU_TRY(dtype == OCU_F64 ? divergence_only_t<double>() : divergence_only_t<float>());
+  return check_cuda(cudaStreamSynchronize(stream), "solve_divergence_only");
+}
+
+void ProjectSolver::set_stream(cudaStream_t s) {
+  stream = s;
+  if (mg) mg->s.set_stream(s);
+}
+
+// ------------------------------------------------------------------------------------------
+// Eqn_IncompressibleNS3D<T>
+// ------------------------------------------------------------------------------------------
+static double round_t(ocu_dtype dt, double x) { return dt == OCU_F64 ? x : (double)(float)x; }
+
+NSSolver::~NSSolver() {
+  for (ocu_grid *g : {u, v, w, t, du, dv, dw, dt, ldu, ldv, ldw, ldt}) {
+    if (g) { cudaFree(g->buf); delete g; }
+  }
+  if (scratch) cudaFree(scratch);
+  if (d_red) cudaFree(d_red);
+  if (h_red) cudaFreeHost(h_red);
+}
+
+static ocu_status make_grid(ocu_dtype dt, const ocu_layout &L, ocu_grid **out) {
+  ocu_grid *g = new ocu_grid{dt, L, nullptr, true};
+  cudaError_t e = cudaMalloc(&g->buf, dtype_size(dt) * L.allocated);
+  if (e != cudaSuccess) { delete g; return check_cuda(e, "cudaMalloc"); }
+  e = cudaMemset(g->buf, 0, dtype_size(dt) * L.allocated);
+  *out = g;
+  return check_cuda(e, "cudaMemset");
+}
+
+ocu_status ns_init_layout(int nx, int ny, int nz, char which, ocu_layout *L) {
+  // Eqn_IncompressibleNS3DParams::init_grids (eqn_incompressns3d.h:75-83)
+  switch (which) {
+    case 'u': layout_compute(nx + 1, ny, nz, 1, 1, 1, 0, 1, 1, L); return OCU_OK;
+    case 'v': layout_compute(nx, ny + 1, nz, 1, 1, 1, 1, 0, 1, L); return OCU_OK;
+    case 'w': layout_compute(nx, ny, nz + 1, 1, 1, 1, 1, 1, 0, L); return OCU_OK;
+    case 't': layout_compute(nx, ny, nz, 1, 1, 1, 1, 1, 1, L); return OCU_OK;
+    default: return fail(OCU_ERR_INVALID_VALUE, "[ERROR] init_grids - unknown grid '%c'", which);
+  }
+}
+
+// set_parameters (eqn_incompressns3d.cu:164-298, set_base_parameters :67-117)
+ocu_status NSSolver::set_parameters(const ocu_ns_params &p, const void *iu, const void *iv, const void *iw,
+                                    const void *it) {
+  if (!check_float((float)p.max_divergence) || p.max_divergence < 0 || p.max_divergence > 1)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - invalid max_divergence %f", p.max_divergence);
+  if (p.cfl_factor < 0)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - invalid cfl_factor %f", p.cfl_factor);
+  if (p.time_step != OCU_TS_ADAMS_BASHFORD2 && p.time_step != OCU_TS_FORWARD_EULER)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - unknown timestep type %d", p.time_step);
+  const int vd = p.vertical_direction;
+  if (vd != OCU_DIR_XPOS && vd != OCU_DIR_XNEG && vd != OCU_DIR_YPOS && vd != OCU_DIR_YNEG && vd != OCU_DIR_ZPOS &&
+      vd != OCU_DIR_ZNEG)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - bad vertical_direction %d", vd);
+  if (!check_float((float)p.hx) || !check_float((float)p.hy) || !check_float((float)p.hz) || p.hx <= 0 || p.hy <= 0 ||
+      p.hz <= 0)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - bad hx, hy, hz (%f, %f, %f)", p.hx, p.hy, p.hz);
+  if (!check_float((float)p.thermal_diffusion) || p.thermal_diffusion < 0)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - invalid thermal diffusion %f", p.thermal_diffusion);
+  if (!check_float((float)p.viscosity) || p.viscosity < 0)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - invalid viscosity %f", p.viscosity);
+  if (p.advection_scheme != OCU_IT_FIRST_ORDER_UPWIND && p.advection_scheme != OCU_IT_SECOND_ORDER_CENTERED)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - invalid interpolation type %d", p.advection_scheme);
+  if (!bc_check_scalar(p.temp_bc) || !bc_check_mac(p.flow_bc))
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - invalid boundary condition types");
+  prm = p;
+  T_gravity = round_t(dtype, p.gravity);
+  T_bouyancy = round_t(dtype, p.bouyancy);
+  T_kappa = round_t(dtype, p.thermal_diffusion);
+  T_nu = round_t(dtype, p.viscosity);
+  lastdt = 0;
+  num_steps = 0;
+  ocu_layout Lu, Lv, Lw, Lt;
+  ns_init_layout(p.nx, p.ny, p.nz, 'u', &Lu);
+  ns_init_layout(p.nx, p.ny, p.nz, 'v', &Lv);
+  ns_init_layout(p.nx, p.ny, p.nz, 'w', &Lw);
+  ns_init_layout(p.nx, p.ny, p.nz, 't', &Lt);
+  OCU_TRY(make_grid(dtype, Lu, &u)); OCU_TRY(make_grid(dtype, Lu, &du)); OCU_TRY(make_grid(dtype, Lu, &ldu));
+  OCU_TRY(make_grid(dtype, Lv, &v)); OCU_TRY(make_grid(dtype, Lv, &dv)); OCU_TRY(make_grid(dtype, Lv, &ldv));
+  OCU_TRY(make_grid(dtype, Lw, &w)); OCU_TRY(make_grid(dtype, Lw, &dw)); OCU_TRY(make_grid(dtype, Lw, &ldw));
+  OCU_TRY(make_grid(dtype, Lt, &t)); OCU_TRY(make_grid(dtype, Lt, &dt)); OCU_TRY(make_grid(dtype, Lt, &ldt));
+  const size_t es = dtype_size(dtype);
+  OCU_TRY(check_cuda(cudaMemcpy(u->buf, iu, es * Lu.allocated, cudaMemcpyHostToDevice), "copy init_u"));
+  OCU_TRY(check_cuda(cudaMemcpy(v->buf, iv, es * Lv.allocated, cudaMemcpyHostToDevice), "copy init_v"));
+  OCU_TRY(check_cuda(cudaMemcpy(w->buf, iw, es * Lw.allocated, cudaMemcpyHostToDevice), "copy init_w"));
+  OCU_TRY(check_cuda(cudaMemcpy(t->buf, it, es * Lt.allocated, cudaMemcpyHostToDevice), "copy init_temp"));
+  proj.dtype = dtype;
+  proj.set_stream(stream);
+  OCU_TRY(proj.initialize_storage(p.nx, p.ny, p.nz, p.hx, p.hy, p.hz, u, v, w, p.flow_bc));
+  if (dtype == OCU_F64) {
+    OCU_TRY(launch_mac_bc_level1<double>(origin<double>(u), origin<double>(v), origin<double>(w), Lu, p.nx, p.ny, p.nz, p.flow_bc, stream));
+    OCU_TRY(launch_bc_level1<double>(origin<double>(t), Lt, p.temp_bc, p.hx, p.hy, p.hz, stream));
+  } else {
+    OCU_TRY(launch_mac_bc_level1<float>(origin<float>(u), origin<float>(v), origin<float>(w), Lu, p.nx, p.ny, p.nz, p.flow_bc, stream));
+    OCU_TRY(launch_bc_level1<float>(origin<float>(t), Lt, p.temp_bc, p.hx, p.hy, p.hz, stream));
+  }
+  for (ocu_grid *g : {du, dv, dw, dt})
+    OCU_TRY(check_cuda(cudaMemsetAsync(g->buf, 0, es * g->L.allocated, stream), "clear derivatives"));
+  if (!scratch) {
+    OCU_TRY(check_cuda(cudaMalloc(&scratch, reduce_scratch_bytes(Lu, 8) * 3), "cudaMalloc(ns scratch)"));
+    OCU_TRY(check_cuda(cudaMemset(scratch, 0, reduce_scratch_bytes(Lu, 8) * 3), "cudaMemset"));
+    OCU_TRY(check_cuda(cudaMalloc(&d_red, 4 * sizeof(double)), "cudaMalloc"));
+    OCU_TRY(check_cuda(cudaMallocHost(&h_red, 4 * sizeof(double)), "cudaMallocHost"));
+  }
+  initialized = true;
+  return check_cuda(cudaStreamSynchronize(stream), "set_parameters");
+}
+
+// get_max_stable_timestep (eqn_incompressns3d.cu:301-328)
+ocu_status NSSolver::get_max_stable_timestep(double *out) {
+  if (!initialized) return fail(OCU_ERR_NOT_INITIALIZED, "[ERROR] get_max_stable_timestep - not initialized");
+  if (dtype == OCU_F64) {
+    OCU_TRY(launch_reduce<double>(origin<double>(u), u->L, OCU_REDUCE_MAXABS, scratch, d_red, stream));
+    OCU_TRY(launch_reduce<double>(origin<double>(v), v->L, OCU_REDUCE_MAXABS, scratch, d_red + 1, stream));
+    OCU_TRY(launch_reduce<double>(origin<double>(w), w->L, OCU_REDUCE_MAXABS, scratch, d_red + 2, stream));
+  } else {
+    OCU_TRY(launch_reduce<float>(origin<float>(u), u->L, OCU_REDUCE_MAXABS, scratch, d_red, stream));
+    OCU_TRY(launch_reduce<float>(origin<float>(v), v->L, OCU_REDUCE_MAXABS, scratch, d_red + 1, stream));
+    OCU_TRY(launch_reduce<float>(origin<float>(w), w->L, OCU_REDUCE_MAXABS, scratch, d_red + 2, stream));
+  }
+  OCU_TRY(check_cuda(cudaMemcpyAsync(h_red, d_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream), "maxabs"));
+  OCU_TRY(check_cuda(cudaStreamSynchronize(stream), "maxabs"));
+  double ut = prm.hx / h_red[0], vt = prm.hy / h_red[1], wt = prm.hz / h_red[2];
+  if (!check_float((float)ut)) ut = 1e10;
+  if (!check_float((float)vt)) vt = 1e10;
+  if (!check_float((float)wt)) wt = 1e10;
+  auto min3 = [](double a, double b, double c) { return a < b ? (a < c ? a : c) : (b < c ? b : c); };
+  double step = prm.cfl_factor * min3(ut, vt, wt);
+  const double minh = min3(prm.hx, prm.hy, prm.hz);
+  if (T_kappa > 0) step = std::min(step, (minh * minh) / round_t(dtype, 6 * T_kappa));
+  if (T_nu > 0) step = std::min(step, (minh * minh) / round_t(dtype, 6 * T_nu));
+  *out = step;
+  return OCU_OK;
+}
+
+template <typename T>
+ocu_status NSSolver::step_t(double dtv) {
+  const int nx = prm.nx, ny = prm.ny, nz = prm.nz;
+  const int vd = prm.vertical_direction;
+  const ocu_layout &Lu = u->L;
+  const T dm = (vd & OCU_DIR_NEGATIVE_FLAG) ? (T)1 : (T)-1;
+  const T coef = dm * (T)T_gravity * (T)T_bouyancy;
+  ocu_grid *vert = (vd & OCU_DIR_XAXIS_FLAG) ? du : (vd & OCU_DIR_YAXIS_FLAG) ? dv : dw;
+  const int nbr = (vd & OCU_DIR_XAXIS_FLAG) ? t->L.xstride : (vd & OCU_DIR_YAXIS_FLAG) ? t->L.ystride : 1;
+  const T ab = (T)(-dtv * dtv / (2 * lastdt));
+  const bool ab2 = prm.time_step == OCU_TS_ADAMS_BASHFORD2 && lastdt > 0;
+  num_steps++;
+  OCU_TRY(launch_advect_self<T>(origin<T>(u), origin<T>(v), origin<T>(w), origin<T>(du), origin<T>(dv), origin<T>(dw),
+                                Lu, nx, ny, nz, prm.hx, prm.hy, prm.hz, prm.advection_scheme, stream));
+  if (T_nu > 0) {
+    OCU_TRY(launch_laplacian<T>(origin<T>(u), origin<T>(du), Lu, nx + 1, ny, nz, prm.hx, prm.hy, prm.hz, (T)T_nu, stream));
+    OCU_TRY(launch_laplacian<T>(origin<T>(v), origin<T>(dv), Lu, nx, ny + 1, nz, prm.hx, prm.hy, prm.hz, (T)T_nu, stream));
+    OCU_TRY(launch_laplacian<T>(origin<T>(w), origin<T>(dw), Lu, nx, ny, nz + 1, prm.hx, prm.hy, prm.hz, (T)T_nu, stream));
+  }
+  OCU_TRY(launch_thermal_force<T>(origin<T>(vert), coef, origin<T>(t), t->L, nbr, nx, ny, nz, stream));
+  OCU_TRY(launch_advect_passive<T>(origin<T>(u), origin<T>(v), origin<T>(w), origin<T>(t), origin<T>(dt), t->L, nx, ny,
+                                   nz, prm.hx, prm.hy, prm.hz, prm.advection_scheme, stream));
+  if (T_kappa > 0)
+    OCU_TRY(launch_laplacian<T>(origin<T>(t), origin<T>(dt), t->L, nx, ny, nz, prm.hx, prm.hy, prm.hz, (T)T_kappa, stream));
+  T *tb = (T *)t->buf;
+  if (ab2) {
+    OCU_TRY(launch_lincomb2<T>(tb, t->L, (T)1.0, tb, (T)(dtv - ab), (const T *)dt->buf, stream));
+    OCU_TRY(launch_lincomb2<T>(tb, t->L, (T)1.0, tb, ab, (const T *)ldt->buf, stream));
+  } else {
+    OCU_TRY(launch_lincomb2<T>(tb, t->L, (T)1.0, tb, (T)dtv, (const T *)dt->buf, stream));
+  }
+  OCU_TRY(launch_bc_nocorners_dev<T>(origin<T>(t), t->L, prm.temp_bc, prm.hx, prm.hy, prm.hz, stream));
+  ocu_grid *st[3] = {u, v, w}, *ds[3] = {du, dv, dw}, *ls[3] = {ldu, ldv, ldw};
+  for (int c = 0; c < 3; c++) {
+    T *x = (T *)st[c]->buf;
+    if (ab2) {
+      OCU_TRY(launch_lincomb2<T>(x, st[c]->L, (T)1.0, x, (T)(dtv - ab), (const T *)ds[c]->buf, stream));
+      OCU_TRY(launch_lincomb2<T>(x, st[c]->L, (T)1.0, x, ab, (const T *)ls[c]->buf, stream));
+    } else {
+      OCU_TRY(launch_lincomb2<T>(x, st[c]->L, (T)1.0, x, (T)dtv, (const T *)ds[c]->buf, stream));
+    }
+  }
+  if (prm.time_step == OCU_TS_ADAMS_BASHFORD2) {
+    lastdt = dtv;
+    const size_t es = sizeof(T);
+    OCU_TRY(check_cuda(cudaMemcpyAsync(ldt->buf, dt->buf, es * dt->L.allocated, cudaMemcpyDeviceToDevice, stream), "AB2 copy"));
+    for (int c = 0; c < 3; c++)
+      OCU_TRY(check_cuda(cudaMemcpyAsync(ls[c]->buf, ds[c]->buf, es * ds[c]->L.allocated, cudaMemcpyDeviceToDevice, stream), "AB2 copy"));
+  }
+  return proj.solve(prm.max_divergence);
+}
+
+// advance_one_step (eqn_incompressns3d.cu:331-399)
+ocu_status NSSolver::advance_one_step(double dtv) {
+  if (!initialized) return fail(OCU_ERR_NOT_INITIALIZED, "[ERROR] advance_one_step - not initialized");
+  return dtype == OCU_F64 ? step_t<double>(dtv) : step_t<float>(dtv);
+}
+
+// Equation::advance (equation.cpp:31-56)
+ocu_status NSSolver::advance(double dtv) {
+  if (!check_float((float)dtv)) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Equation::advance - bad dt value");
+  double dtleft = dtv;
+  while (dtleft > 0) {
+    double maxdt;
+    OCU_TRY(get_max_stable_timestep(&maxdt));
+    const int subds = (int)std::ceil(dtleft / maxdt);
+    const double subdt = dtleft / subds;
+    ocu_status st = advance_one_step(subdt);
+    if (st != OCU_OK) return st;
+    dtleft -= subdt;
+  }
+  return OCU_OK;
+}
+
+void NSSolver::set_stream(cudaStream_t s) {
+  stream = s;
+  proj.set_stream(s);
+}
+
+ocu_grid *NSSolver::grid(char which) {
+  switch (which) {
+    case 'u': return u; case 'v': return v; case 'w': return w; case 't': return t;
+    case 'U': return du; case 'V': return dv; case 'W': return dw; case 'T': return dt;
+    case 'p': return proj.mg ? proj.mg->s.pressure : nullptr;
+    default: return nullptr;
+  }
+}
+
+}  // namespace ocub

@@ -1,0 +1,66 @@
+// Projection and Navier-Stokes classes behind the ocu_project_* / ocu_ns_* entry points.
+#pragma once
+
+#include "mg_solver.h"
+
+namespace ocub {
+
+struct ProjectSolver {
+  ocu_dtype dtype = OCU_F32;
+  ocu_bc_set bc{};
+  int nx = 0, ny = 0, nz = 0;
+  double hx = 0, hy = 0, hz = 0;
+  ocu_grid *u = nullptr, *v = nullptr, *w = nullptr;  // borrowed
+  ocu_grid *divergence = nullptr;                     // owned
+  ocu_mg *mg = nullptr;                               // owned pressure solver
+  cudaStream_t stream = nullptr;
+  bool initialized = false;
+
+  ~ProjectSolver();
+  ocu_status initialize_storage(int nx, int ny, int nz, double hx, double hy, double hz, ocu_grid *u,
+                                ocu_grid *v, ocu_grid *w, const ocu_bc_set &bc);
+  ocu_status solve(double tolerance);
+  ocu_status solve_divergence_only();
+  void set_stream(cudaStream_t s);
+  template <typename T> ocu_status solve_t(double tolerance);
+  template <typename T> ocu_status divergence_only_t();
+};
+
+ocu_status ns_init_layout(int nx, int ny, int nz, char which, ocu_layout *L);
+
+struct NSSolver {
+  ocu_dtype dtype = OCU_F32;
+  ocu_ns_params prm{};
+  double T_gravity = 0, T_bouyancy = 0, T_kappa = 0, T_nu = 0;
+  ocu_grid *u = nullptr, *v = nullptr, *w = nullptr, *t = nullptr;
+  ocu_grid *du = nullptr, *dv = nullptr, *dw = nullptr, *dt = nullptr;
+  ocu_grid *ldu = nullptr, *ldv = nullptr, *ldw = nullptr, *ldt = nullptr;
+  ProjectSolver proj;
+  double lastdt = 0;
+  int num_steps = 0;
+  bool initialized = false;
+  cudaStream_t stream = nullptr;
+  void *scratch = nullptr;
+  double *d_red = nullptr;
+  double *h_red = nullptr;
+
+  ~NSSolver();
+  ocu_status set_parameters(const ocu_ns_params &p, const void *iu, const void *iv, const void *iw,
+                            const void *it);
+  ocu_status get_max_stable_timestep(double *dt);
+  ocu_status advance_one_step(double dt);
+  ocu_status advance(double dt);
+  void set_stream(cudaStream_t s);
+  ocu_grid *grid(char which);
+  template <typename T> ocu_status step_t(double dt);
+};
+
+}  // namespace ocub
+
+struct ocu_project {
+  ocub::ProjectSolver s;
+};
+
+struct ocu_ns {
+  ocub::NSSolver s;
+};

@@ -1,0 +1,110 @@
+// Multigrid solver classes behind the ocu_mg_* C entry points.
+#pragma once
+
+#include <array>
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "ocu_internal.h"
+
+namespace ocub {
+
+int mg_num_levels(int nx, int ny, int nz);
+double mg_optimal_omega(double fx, double fy, double fz);
+
+// The virtual level operations of Sol_MultigridPressure3DBase (sol_mgpressure3d.h:76-80).
+struct CoreOps {
+  virtual ~CoreOps() {}
+  virtual ocu_status relax(int level, int iterations, int order) = 0;
+  virtual ocu_status clear_zero(int level) = 0;
+  virtual ocu_status apply_bc(int level) = 0;
+  virtual ocu_status restrict_residuals(int fine, int coarse, double *l2, double *linf) = 0;
+  virtual ocu_status prolong(int coarse, int fine) = 0;
+  virtual ocu_grid *grid(char which, int level) = 0;
+};
+
+// Level hierarchy of one precision (Sol_MultigridPressure3DDevice<T> storage).
+template <typename T>
+struct MGCore : CoreOps {
+  int num_levels = 0;
+  std::vector<double> h;
+  std::vector<std::array<int, 3>> dim;
+  double omega = 1, fx = 1, fy = 1, fz = 1;
+  std::vector<ocu_layout> lay;
+  std::vector<ocu_grid *> grids_u, grids_b, grids_r;  // u[0] = pressure, b[0] = caller rhs
+  std::vector<void *> diag;                           // FP64 diagonal tables
+  ocu_bc_set bc{};
+  bool update_bc_between_colors = false;
+  bool disable_relax_on_host = false;
+  cudaStream_t stream = nullptr;
+  void *red_scratch = nullptr;
+  double *d_norms = nullptr;
+  double *h_norms = nullptr;
+
+  ~MGCore();
+  ocu_status init(const ocu_bc_set &bc, bool disable_host, int nx, int ny, int nz, double hx, double hy,
+                  double hz, ocu_grid *rhs, ocu_grid *pressure, cudaStream_t s);
+  ocu_bc_set bc_at_level(int level) const;
+  RelaxParams relax_params(int level) const;
+  double hx(int l) const { return h[l] / std::sqrt(fx); }
+  double hy(int l) const { return h[l] / std::sqrt(fy); }
+  double hz(int l) const { return h[l] / std::sqrt(fz); }
+  T *u0(int l) { return origin<T>(grids_u[l]); }
+  T *b0(int l) { return origin<T>(grids_b[l]); }
+  T *r0(int l) { return origin<T>(grids_r[l]); }
+
+  ocu_status relax(int level, int iterations, int order) override;
+  ocu_status clear_zero(int level) override;
+  ocu_status apply_bc(int level) override;
+  ocu_status restrict_residuals(int fine, int coarse, double *l2, double *linf) override;
+  ocu_status prolong(int coarse, int fine) override;
+  ocu_grid *grid(char which, int level) override {
+    return which == 'u' ? grids_u[level] : which == 'b' ? grids_b[level] : which == 'r' ? grids_r[level] : nullptr;
+  }
+};
+
+struct MGSolver {
+  ocu_mg_kind kind;
+  ocu_mg_params prm;
+  MGCore<float> cf;
+  MGCore<double> cd;
+  bool double_mode = false;
+  bool initialized = false;
+  int num_levels = 0;
+  ocu_grid *pressure = nullptr;   // u0 of the interface precision
+  ocu_grid *rhs_f = nullptr;      // FP32 rhs of the mixed solvers
+  struct GridDeleter {
+    void operator()(ocu_grid *g) const {
+      if (g) { cudaFree(g->buf); delete g; }
+    }
+  };
+  std::unique_ptr<ocu_grid, GridDeleter> pressure_f;  // FP32 u0 of the mixed solvers
+  cudaStream_t stream = nullptr;
+  ocu_mg_stats stats{};
+
+  explicit MGSolver(ocu_mg_kind k, const ocu_mg_params &p) : kind(k), prm(p) {}
+  ~MGSolver();
+
+  CoreOps *active();
+  int coarse_iters() const;
+  ocu_status initialize_storage(int nx, int ny, int nz, double hx, double hy, double hz, ocu_grid *rhs);
+  ocu_status set_params(const ocu_mg_params &p);
+  void set_stream(cudaStream_t s);
+  ocu_status do_fmg(double tol, int max_iter, double *l2, double *linf);
+  ocu_status do_vcycle(double tol, int max_iter, double *l2, double *linf);
+  ocu_status mixed_warmstart_fmg(double tol, int max_iter, double *l2, double *linf);
+  ocu_status ir_solve(double tol, int max_outer, double *l2, double *linf);
+  ocu_status fmg_dispatch(double tol, int max_iter, double *l2, double *linf);
+  ocu_status solve(double *residual, double tol, int max_iter);
+  ocu_status run_vcycles(int count);
+  ocu_status run_fmg(int count);
+  ocu_grid *level_grid(char which, int level);
+};
+
+}  // namespace ocub
+
+struct ocu_mg {
+  ocub::MGSolver s;
+  ocu_mg(ocu_mg_kind k, const ocu_mg_params &p) : s(k, p) {}
+};

@@ -1,0 +1,147 @@
+// Internal declarations shared by the CUDA translation units of libocu_b200.so.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/ocu_b200.h"
+
+struct ocu_grid {
+  ocu_dtype dtype;
+  ocu_layout L;
+  void *buf;
+  bool owned;
+};
+
+namespace ocub {
+
+// ---- error reporting (thread-local message behind ocu_last_error) ----------------------
+void set_error(const char *fmt, ...);
+ocu_status fail(ocu_status st, const char *fmt, ...);
+ocu_status check_cuda(cudaError_t e, const char *what);
+ocu_status check_launch(const char *what);
+void count_launch(int n = 1);
+unsigned long long launch_count();
+const char *last_error_text();
+
+inline size_t dtype_size(ocu_dtype d) { return d == OCU_F64 ? 8 : 4; }
+
+template <typename T> inline T *origin(ocu_grid *g) { return static_cast<T *>(g->buf) + g->L.shift; }
+template <typename T> inline const T *origin(const ocu_grid *g) { return static_cast<const T *>(g->buf) + g->L.shift; }
+
+inline bool layout_match(const ocu_layout &a, const ocu_layout &b) {
+  return a.pnx == b.pnx && a.pny == b.pny && a.pnz == b.pnz;
+}
+
+void layout_compute(int nx, int ny, int nz, int gx, int gy, int gz, int padx, int pady, int padz,
+                    ocu_layout *L);
+
+// Face-by-face view of a BoundaryConditionSet for kernels (passed by value).
+struct BCDev {
+  int type[6];     // xpos, xneg, ypos, yneg, zpos, zneg
+  float value[6];
+  float aux[6];
+};
+BCDev to_dev(const ocu_bc_set &bc);
+bool bc_check_scalar(const ocu_bc_set &bc);
+bool bc_check_mac(const ocu_bc_set &bc);
+bool bc_any_periodic(const ocu_bc_set &bc);
+void bc_make_homogeneous(ocu_bc_set *bc);
+double bc_diag_mod(const ocu_bc &b, double factor);
+bool check_float(float f);
+
+// ---- launchers (kernels_*.cu) -----------------------------------------------------------
+// Every launcher enqueues on stream s and returns OCU_OK or an error from the launch.
+template <typename T>
+ocu_status launch_bc_level1(T *origin, const ocu_layout &L, const ocu_bc_set &bc, double hx,
+                            double hy, double hz, cudaStream_t s);
+template <typename T>
+ocu_status launch_bc_nocorners_dev(T *origin, const ocu_layout &L, const ocu_bc_set &bc,
+                                   double hx, double hy, double hz, cudaStream_t s);
+template <typename T>
+ocu_status launch_mac_bc_level1(T *u, T *v, T *w, const ocu_layout &L, int nx, int ny, int nz,
+                                const ocu_bc_set &bc, cudaStream_t s);
+
+template <typename T>
+ocu_status launch_clear(T *buf, long long n, T value, cudaStream_t s);
+template <typename T, typename S>
+ocu_status launch_convert(T *dst, const S *src, long long n, cudaStream_t s);
+template <typename T>
+ocu_status launch_lincomb1(T *res, T a1, const T *g1, long long n, cudaStream_t s);
+template <typename T>
+ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, T a2, const T *g2,
+                           cudaStream_t s);
+
+// Reduction in the reference fold order over the interior of a grid; the T result is stored
+// as double at *d_result (device pointer).  d_scratch: >= reduce_scratch_elems(L) elements of
+// T plus one unsigned counter (see kernels_grid.cu).
+size_t reduce_scratch_bytes(const ocu_layout &L, size_t elem);
+template <typename T>
+ocu_status launch_reduce(const T *origin, const ocu_layout &L, int op, void *d_scratch,
+                         double *d_result, cudaStream_t s);
+
+// ---- multigrid level operations (kernels_mg.cu) ------------------------------------------
+struct RelaxParams {
+  double omega, h, fx, fy, fz;
+  ocu_bc_set bc;   // bc at this level
+};
+template <typename T>
+ocu_status launch_relax_color(T *u, const T *b, const ocu_layout &L, const T *diag, int color,
+                              const RelaxParams &p, cudaStream_t s);
+template <typename T>
+ocu_status launch_init_diag(T *diag, int nx, int ny, const RelaxParams &p, cudaStream_t s);
+// Coarsest-level relaxation with the host routine's arithmetic and ghost handling
+// (sol_mgpressure3ddev.cu:82-188), as one single-CTA kernel.
+template <typename T>
+ocu_status launch_coarse_relax(T *u, const T *b, const ocu_layout &L, int iterations, int order,
+                               const RelaxParams &p, double hx, double hy, double hz,
+                               cudaStream_t s);
+template <typename T>
+ocu_status launch_residual(const T *u, const T *b, T *r, const ocu_layout &L, double h,
+                           double fx, double fy, double fz, cudaStream_t s);
+template <typename T>
+ocu_status launch_restrict(const T *r, const ocu_layout &Lf, T *bc_, const ocu_layout &Lc,
+                           cudaStream_t s);
+template <typename T>
+ocu_status launch_prolong(const T *uc, const ocu_layout &Lc, T *uf, const ocu_layout &Lf,
+                          cudaStream_t s);
+// IR helpers: r32 = (float) r64 on the interior; x64 += (double) e32 on the interior.
+ocu_status launch_downcast_interior(const double *r, float *b32, const ocu_layout &L,
+                                    cudaStream_t s);
+ocu_status launch_add_correction(double *x, const float *e, const ocu_layout &L,
+                                 cudaStream_t s);
+
+// ---- flow stencils (kernels_flow.cu) ---------------------------------------------------------
+template <typename T>
+ocu_status launch_divergence(const T *u, const T *v, const T *w, T *div, const ocu_layout &L,
+                             int nx, int ny, int nz, double hx, double hy, double hz,
+                             cudaStream_t s);
+template <typename T>
+ocu_status launch_gradient(T *u, T *v, T *w, const T *phi, const ocu_layout &L, int nx, int ny,
+                           int nz, double hx, double hy, double hz, T coefficient,
+                           cudaStream_t s);
+template <typename T>
+ocu_status launch_laplacian(const T *phi, T *dphidt, const ocu_layout &L, int nx, int ny,
+                            int nz, double hx, double hy, double hz, T coefficient,
+                            cudaStream_t s);
+template <typename T>
+ocu_status launch_advect_self(const T *u, const T *v, const T *w, T *du, T *dv, T *dw,
+                              const ocu_layout &L, int nx, int ny, int nz, double hx, double hy,
+                              double hz, int interp, cudaStream_t s);
+template <typename T>
+ocu_status launch_advect_passive(const T *u, const T *v, const T *w, const T *phi, T *dphi,
+                                 const ocu_layout &L, int nx, int ny, int nz, double hx,
+                                 double hy, double hz, int interp, cudaStream_t s);
+template <typename T>
+ocu_status launch_thermal_force(T *dvdt, T coefficient, const T *temp, const ocu_layout &L,
+                                int nbr_stride, int nx, int ny, int nz, cudaStream_t s);
+
+}  // namespace ocub
+
+#define OCU_TRY(...)                         \
+  do {                                       \
+    ocu_status _st = (__VA_ARGS__);          \
+    if (_st != OCU_OK) return _st;           \
+  } while (0)
