@@ -1,0 +1,441 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 projection-step hot path.
+
+Headline workload (one "step" = one pressure solve from a zero initial guess):
+  256^3 cell-centred Poisson, h = 1/256, homogeneous Neumann on all faces, RHS = sum of 16 cosine
+  modes cos(kx pi x) cos(ky pi y) cos(kz pi z) at cell centres x = (i+1/2)h with integer
+  wavenumbers in 1..16 and N(0,1) amplitudes (seeded), mean removed; solved to a 1e-10
+  relative RMS residual by FP32 V-cycles inside FP64 iterative refinement.  The plain FP64
+  multigrid solve of the same system is timed beside it.  Synthetic data (no dataset).
+Secondary lines in the same JSON object: the 64^3 FP32 solve to 1e-6 and 100 steps of the
+128x128x64 FP32 Boussinesq (Rayleigh-Benard) flow.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Prints one JSON line on rank 0.  --impl reference times the CPU restatement of the
+reference algorithm (FP32 FMG warm start + FP64 FMG, sol_mgpressuremixed3ddevd.cpp:79-100) on
+the host cores instead.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms to 1e-10 rel residual @256^3 (mixed vs FP64 MG), HBM GB/s, NS steps/s"
+N_CFG3 = 256
+TOL_REL = 1e-10
+
+
+from opencurrent_b200.workloads import config1_rhs, fourier_rhs, interior, padded, rayleigh_benard  # noqa: E402
+
+
+# --------------------------------------------------------------------------- clocks -----
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------- helpers ----
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch recorded from an ncu capture in profiles/<name>.md."""
+    p = os.path.join(ROOT, "profiles", name)
+    try:
+        txt = open(p).read()
+    except OSError:
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) if m else None
+
+
+def dist_setup(gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------- GPU arm ----
+def run_gpu(args):
+    import torch
+    import opencurrent_b200 as ocu
+    from opencurrent_b200 import _capi
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    lib = ocu.load()
+    stream = torch.cuda.Stream()
+    sh = C.c_void_p(stream.cuda_stream)
+
+    n = N_CFG3
+    h = 1.0 / n
+    L = ocu.layout(n, n, n)
+    b = fourier_rhs(n)
+    rms_b = float(np.sqrt(np.mean(b ** 2)))
+    tol = TOL_REL * rms_b
+    host_rhs = torch.from_numpy(padded(b, L, np.float64)).pin_memory()
+    host_out = torch.empty(int(L.allocated), dtype=torch.float64).pin_memory()
+
+    rhs = ocu.Grid3DDevice(ocu.F64)
+    rhs.init(n, n, n)
+    rhs.copy_from_host(host_rhs.numpy())
+
+    def make_solver(kind):
+        s = ocu.Sol_MultigridPressureMixed3DDeviceD("ir") if kind == "ir" else ocu.Sol_MultigridPressure3DDevice(ocu.F64)
+        s.bc = ocu.BoundaryConditionSet(ocu.BoundaryCondition(ocu.BC_NEUMANN, 0.0))
+        s.ir_inner_cycles = args.ir_inner
+        s.initialize_storage(n, n, n, h, h, h, rhs)
+        _capi.check(lib.ocu_mg_set_stream(s._h, sh))
+        return s
+
+    mixed = make_solver("ir")
+    fp64 = make_solver("fp64")
+
+    def one_solve(s):
+        _capi.check(lib.ocu_grid_clear(s.pressure().handle, 0.0, sh))
+        ok, res = s.solve(tol, 30)
+        if not ok:
+            raise RuntimeError(f"solve did not reach tolerance: residual {res / rms_b:.3e}")
+        return res
+
+    def timed(fn, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        n0 = ocu.kernel_launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        if sampler:
+            sampler.__enter__()
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if sampler:
+            sampler.__exit__(None, None, None)
+        barrier(world)
+        ms = e0.elapsed_time(e1) / steps
+        return max_over_ranks(ms, world), ocu.kernel_launch_count() - n0
+
+    sampler = ClockSampler(local)
+    res_holder = {}
+
+    def mixed_step():
+        res_holder["mixed"] = one_solve(mixed)
+
+    ms_mixed, launches = timed(mixed_step, args.steps, args.warmup, sampler)
+    st_mixed = mixed.stats
+    ms_fp64, _ = timed(lambda: res_holder.__setitem__("fp64", one_solve(fp64)), args.steps, args.warmup)
+    st_fp64 = fp64.stats
+
+    # error of the mixed result against the plain FP64 solution (both mean-removed)
+    x_mixed = mixed.pressure().copy_to_host()
+    x_fp64 = fp64.pressure().copy_to_host()
+    xm, xd = interior(x_mixed, L).copy(), interior(x_fp64, L).copy()
+    xm -= xm.mean()
+    xd -= xd.mean()
+    err_vs_fp64 = float(np.abs(xm - xd).max() / np.abs(xd).max())
+
+    # end to end through the public API with host buffers: H2D rhs, solve, D2H pressure
+    def e2e_step():
+        _capi.check(lib.ocu_grid_upload_async(rhs.handle, C.c_void_p(host_rhs.data_ptr()), sh))
+        one_solve(mixed)
+        _capi.check(lib.ocu_grid_download_async(mixed.pressure().handle, C.c_void_p(host_out.data_ptr()), sh))
+        stream.synchronize()
+
+    ms_e2e, _ = timed(e2e_step, max(1, args.steps // 2), 1)
+    bytes_grid = int(L.allocated) * 8
+
+    # dominant kernel: level-0 FP32 colour sweep of the refinement solver's inner hierarchy
+    reps = 40
+    for c in range(4):
+        mixed.relax_sweep(0, c & 1, core=1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for c in range(reps):
+        mixed.relax_sweep(0, c & 1, core=1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sweep_ms = e0.elapsed_time(e1) / reps
+    ncell = n ** 3
+    alg_bytes = 2.0 * ncell * 4  # read u, read b (own colour), write u (own colour)
+    achieved = alg_bytes / (sweep_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profile_traffic("relax_color_f32_256cube.md")
+
+    secondary = {}
+    if rank == 0 and not args.skip_secondary:
+        secondary = run_secondary(torch, ocu, _capi, lib, stream, sh)
+
+    clocks = sampler.summary()
+    if rank != 0:
+        return None
+    cpu = cpu_baseline_sample(args) if not args.skip_cpu else None
+    line = {
+        "metric": METRIC,
+        "value": round(ms_mixed, 4),
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_mixed, 4),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32 V-cycles in fp64 refinement",
+        "data": "synthetic",
+        "config": {"workload": "mixed-precision Poisson solve 256^3 Neumann, 16 cosine modes, to 1e-10 rel RMS residual",
+                   "grid": [n, n, n], "tolerance_rel": TOL_REL, "ir_inner_cycles": args.ir_inner,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2_policy": "inputs larger than L2 (rhs 145 MB FP64, levels 217 MB)"},
+        "fp64_mg_ms": round(ms_fp64, 4),
+        "speedup_mixed_vs_fp64": round(ms_fp64 / ms_mixed, 3),
+        "mixed": {"outer_iterations": st_mixed.outer_iterations, "fp32_vcycles": st_mixed.vcycles,
+                  "rel_residual": res_holder["mixed"] / rms_b, "max_rel_err_vs_fp64_mg": err_vs_fp64},
+        "fp64": {"vcycles": st_fp64.vcycles, "rel_residual": res_holder["fp64"] / rms_b},
+        "roofline": {"bound": "hbm", "kernel": "k_relax_color<float> level 0 (256^3)",
+                     "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": round(sweep_ms, 5)},
+        "e2e": {"value": round(ms_e2e, 4), "unit": "ms", "h2d_bytes_per_step": bytes_grid,
+                "d2h_bytes_per_step": bytes_grid},
+        "gpu_launches": int(launches),
+        "gpu_launches_per_step": round(launches / args.steps, 1),
+        "clocks": clocks,
+        "secondary": secondary,
+        "cpu_baseline": cpu,
+    }
+    return line
+
+
+def run_secondary(torch, ocu, _capi, lib, stream, sh):
+    out = {}
+    # 64^3 FP32 pressure solve to 1e-6 relative (U[-1,1] seed 0)
+    n = 64
+    L = ocu.layout(n, n, n)
+    b = config1_rhs(n)
+    buf = padded(b, L, np.float32)
+    rms = float(np.sqrt(np.mean(b.astype(np.float32).astype(np.float64) ** 2)))
+    g = ocu.Grid3DDevice(ocu.F32)
+    g.init(n, n, n)
+    g.copy_from_host(buf)
+    s = ocu.Sol_MultigridPressure3DDevice(ocu.F32)
+    s.bc = ocu.BoundaryConditionSet(ocu.BoundaryCondition(ocu.BC_NEUMANN, 0.0))
+    s.initialize_storage(n, n, n, 1 / n, 1 / n, 1 / n, g)
+    _capi.check(lib.ocu_mg_set_stream(s._h, sh))
+
+    def solve64():
+        _capi.check(lib.ocu_grid_clear(s.pressure().handle, 0.0, sh))
+        ok, res = s.solve(1e-6 * rms, 20)
+        assert ok
+    for _ in range(3):
+        solve64()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 10
+    e0.record(stream)
+    for _ in range(reps):
+        solve64()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    out["fp32_64cube_solve_ms"] = round(e0.elapsed_time(e1) / reps, 4)
+    out["fp32_64cube_vcycles"] = s.stats.vcycles
+
+    # 100 steps of the 128x128x64 FP32 Boussinesq flow
+    pp = rayleigh_benard(ocu, 128, 128, 64)
+    eq = ocu.Eqn_IncompressibleNS3D(ocu.F32)
+    eq.set_parameters(pp)
+    _capi.check(lib.ocu_ns_set_stream(eq._h, sh))
+    for _ in range(3):
+        eq.advance_one_step(eq.get_max_stable_timestep())
+    torch.cuda.synchronize()
+    e0.record(stream)
+    steps = 100
+    unconverged = 0
+    for _ in range(steps):
+        unconverged += 0 if eq.advance_one_step(eq.get_max_stable_timestep()) else 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    out["ns_128x128x64_fp32_steps_per_s"] = round(steps / (ms * 1e-3), 2)
+    out["ns_ms_per_step"] = round(ms / steps, 4)
+    out["ns_steps_projection_above_tol"] = unconverged
+    return out
+
+
+# --------------------------------------------------------------------------- CPU arms ---
+def cpu_threads():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
+def cpu_solve_once(kind="mixed"):
+    """One 256^3 solve by the oracle's restatement of the reference algorithm."""
+    from oracle import oracle_ctypes as O
+    n = N_CFG3
+    L = O.layout(n, n, n)
+    b = fourier_rhs(n)
+    rms = float(np.sqrt(np.mean(b ** 2)))
+    rhs = padded(b, L, np.float64)
+    prm = O.MGParams()
+    prm.bc = O.bcset_all(4, 0.0)
+    prm.nu1 = prm.nu2 = 2
+    prm.convergence = 0x05
+    O.lib().orc_ns_set_omp_threads(cpu_threads())
+    m = O.OracleMG(kind, prm, n, n, n, 1 / n, 1 / n, 1 / n, rhs, L)
+    t0 = time.perf_counter()
+    ok, res = m.solve(TOL_REL * rms, 30)
+    ms = (time.perf_counter() - t0) * 1e3
+    return ms, ok, res / rms
+
+
+def cpu_baseline_sample(args):
+    ms, ok, rel = cpu_solve_once("mixed")
+    return {"value": round(ms, 1), "unit": "ms", "cores": cpu_threads(), "kind": "port",
+            "sample": f"one full 256^3 solve to 1e-10 by the oracle's restatement of the reference mixed "
+                      f"solver (FP32 FMG warm start + FP64 FMG), OpenMP, converged={bool(ok)}, rel={rel:.2e}"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    for _ in range(args.warmup):
+        cpu_solve_once("mixed")
+    times = []
+    for _ in range(args.steps):
+        ms, ok, rel = cpu_solve_once("mixed")
+        times.append(ms)
+    v = float(np.mean(times))
+    return {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": round(v, 1),
+        "unit": "ms",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(v, 1),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "fp32 warm start + fp64 FMG",
+        "data": "synthetic",
+        "config": {"workload": "mixed-precision Poisson solve 256^3 Neumann, 16 cosine modes, to 1e-10 rel RMS residual",
+                   "grid": [N_CFG3] * 3, "tolerance_rel": TOL_REL},
+        "cpu_baseline": {"value": round(v, 1), "unit": "ms", "cores": cpu_threads(), "kind": "port",
+                         "sample": "full 256^3 solve per step, oracle restatement of the reference mixed solver"},
+        "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--ir-inner", type=int, default=3)
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-secondary", action="store_true")
+    args = ap.parse_args()
+    line = run_reference(args) if args.impl == "reference" else run_gpu(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

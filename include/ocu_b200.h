@@ -139,6 +139,11 @@ typedef struct ocu_mg_params {
   int ir_inner_cycles;           /* OCU_MG_MIXED_IR only: FP32 fine-level cycles per
                                     correction (0 = default 3) */
   int store_residual_grids;      /* 1 = keep r_grid(level) filled (read_r); costs N*s */
+  int unfused;                   /* 1 = one launch per reference operation (no fused ghost
+                                    writes, no fused residual+restriction, no tail kernel);
+                                    same results, for A/B timing */
+  int tail_cells;                /* levels with at most this many cells run in one single-CTA
+                                    kernel per cycle; 0 = default (4096), < 0 = off */
 } ocu_mg_params;
 
 typedef struct ocu_mg_stats {
@@ -170,6 +175,22 @@ ocu_status ocu_mg_run_fmg(ocu_mg *mg, int count);       /* sol_mgpressure3d.cpp:
 ocu_grid *ocu_mg_pressure(ocu_mg *mg);
 ocu_grid *ocu_mg_level_grid(ocu_mg *mg, char which, int level);
 ocu_status ocu_mg_get_stats(const ocu_mg *mg, ocu_mg_stats *stats);
+/* The level operations the cycle is built from (protected in the reference,
+ * sol_mgpressure3d.h:76-80), exposed for testing and kernel timing.  core = 0 acts on the
+ * interface precision, core = 1 on the FP32 hierarchy of a mixed solver.  They enqueue work and
+ * return without waiting, except restrict_residuals when a norm is requested. */
+/* relax(level, iterations, order): order 0 red-black, 1 black-red, 2 symmetric
+ * (sol_mgpressure3ddev.cu:190-248). */
+ocu_status ocu_mg_relax(ocu_mg *mg, int core, int level, int iterations, int order);
+/* One colour-sweep launch, no ghost refresh (sol_mgpressure3ddevf.cu:200-252). */
+ocu_status ocu_mg_relax_sweep(ocu_mg *mg, int core, int level, int color);
+/* restrict_residuals(fine, coarse, l2, linf) (sol_mgpressure3ddev.cu:250-279); NULL skips a norm. */
+ocu_status ocu_mg_restrict_residuals(ocu_mg *mg, int core, int fine, int coarse, double *l2,
+                                     double *linf);
+/* prolong(coarse, fine) + ghost refresh (sol_mgpressure3ddev.cu:284-297). */
+ocu_status ocu_mg_prolong(ocu_mg *mg, int core, int coarse, int fine);
+/* Wait for all work the solver enqueued. */
+ocu_status ocu_mg_synchronize(ocu_mg *mg);
 
 /* ---- projection (Sol_ProjectDivergence3DDevice<T>, sol_project3d.h:29-129) ------------- */
 ocu_status ocu_project_create(ocu_dtype dtype, ocu_project **out);

@@ -209,6 +209,9 @@ class _MGBase:
         self.make_symmetric_operator = False
         self.disable_relax_on_host = False
         self.ir_inner_cycles = p.ir_inner_cycles
+        self.store_residual_grids = False
+        self.unfused = False
+        self.tail_cells = 0
         self._h = None
         self._rhs = None
 
@@ -219,6 +222,9 @@ class _MGBase:
         p.make_symmetric_operator = int(bool(self.make_symmetric_operator))
         p.disable_relax_on_host = int(bool(self.disable_relax_on_host))
         p.ir_inner_cycles = self.ir_inner_cycles
+        p.store_residual_grids = int(bool(self.store_residual_grids))
+        p.unfused = int(bool(self.unfused))
+        p.tail_cells = int(self.tail_cells)
         return p
 
     def initialize_storage(self, nx, ny, nz, hx, hy, hz, rhs):
@@ -270,6 +276,26 @@ class _MGBase:
         s = MGStats()
         check(load().ocu_mg_get_stats(self._h, C.byref(s)))
         return s
+
+    # level operations (protected in the reference; exposed for tests and kernel timing)
+    def relax(self, level, iterations, order=0, core=0):
+        check(load().ocu_mg_relax(self._h, core, level, iterations, order))
+
+    def relax_sweep(self, level, color, core=0):
+        check(load().ocu_mg_relax_sweep(self._h, core, level, color))
+
+    def restrict_residuals(self, fine, coarse, norms=False, core=0):
+        l2, linf = C.c_double(), C.c_double()
+        check(load().ocu_mg_restrict_residuals(self._h, core, fine, coarse,
+                                               C.byref(l2) if norms else None,
+                                               C.byref(linf) if norms else None))
+        return (l2.value, linf.value) if norms else None
+
+    def prolong(self, coarse, fine, core=0):
+        check(load().ocu_mg_prolong(self._h, core, coarse, fine))
+
+    def synchronize(self):
+        check(load().ocu_mg_synchronize(self._h))
 
     def __del__(self):
         try:
@@ -500,12 +526,17 @@ class Eqn_IncompressibleNS3D:
         return d.value
 
     def advance_one_step(self, dt):
-        check(load().ocu_ns_advance_one_step(self._h, dt))
-        return True
+        """advance_one_step (eqn_incompressns3d.cu:331-399).  Returns False, like the reference,
+        when the projection's pressure solve stops above max_divergence; the state has still
+        been advanced and projected with the last pressure iterate."""
+        st = check(load().ocu_ns_advance_one_step(self._h, dt), allow=(ERR_NOT_CONVERGED,))
+        return st == OK
 
     def advance(self, dt):
-        check(load().ocu_ns_advance(self._h, dt))
-        return True
+        """Equation::advance (equation.cpp:31-56): sub-steps at the stable time step; stops and
+        returns False at the first sub-step that fails."""
+        st = check(load().ocu_ns_advance(self._h, dt), allow=(ERR_NOT_CONVERGED,))
+        return st == OK
 
     @property
     def num_steps(self):

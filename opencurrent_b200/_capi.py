@@ -52,7 +52,8 @@ class BCSet(C.Structure):
 class MGParams(C.Structure):
     _fields_ = [("bc", BCSet), ("nu1", C.c_int), ("nu2", C.c_int), ("convergence", C.c_int),
                 ("make_symmetric_operator", C.c_int), ("disable_relax_on_host", C.c_int),
-                ("ir_inner_cycles", C.c_int), ("store_residual_grids", C.c_int)]
+                ("ir_inner_cycles", C.c_int), ("store_residual_grids", C.c_int),
+                ("unfused", C.c_int), ("tail_cells", C.c_int)]
 
 
 class MGStats(C.Structure):
@@ -111,6 +112,11 @@ SIGNATURES = {
     "ocu_mg_pressure": (P, [P]),
     "ocu_mg_level_grid": (P, [P, C.c_char, I]),
     "ocu_mg_get_stats": (I, [P, C.POINTER(MGStats)]),
+    "ocu_mg_relax": (I, [P, I, I, I, I]),
+    "ocu_mg_relax_sweep": (I, [P, I, I, I]),
+    "ocu_mg_restrict_residuals": (I, [P, I, I, I, C.POINTER(D), C.POINTER(D)]),
+    "ocu_mg_prolong": (I, [P, I, I, I]),
+    "ocu_mg_synchronize": (I, [P]),
     "ocu_project_create": (I, [I, PP]),
     "ocu_project_destroy": (None, [P]),
     "ocu_project_set_stream": (I, [P, P]),

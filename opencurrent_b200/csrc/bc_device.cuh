@@ -71,4 +71,37 @@ struct Level1Compose {
   }
 };
 
+// The whole level1 fill executed by one thread block (the composition reads interior values
+// only, so every ghost can be written in the same phase).
+template <typename T>
+__device__ void level1_fill_block(T *u, long long xs, long long ys, int nx, int ny, int nz, const BCDev &bc, T hx,
+                                  T hy, T hz) {
+  Level1Compose<T> lc;
+  lc.p = u; lc.xs = xs; lc.ys = ys; lc.nx = nx; lc.ny = ny; lc.nz = nz; lc.bc = bc;
+  lc.hx = hx; lc.hy = hy; lc.hz = hz;
+  const int zr = 2 * (nx + 2) * (ny + 2), yr = 2 * (nx + 2) * nz, xr = 2 * ny * nz;
+  for (int q = threadIdx.x; q < zr + yr + xr; q += blockDim.x) {
+    int r = q;
+    if (r < zr) {
+      const int per = (nx + 2) * (ny + 2), side = r / per, i = (r % per) / (ny + 2) - 1, j = (r % per) % (ny + 2) - 1;
+      if (Level1Compose<T>::writes(bc.type[side ? FZ_POS : FZ_NEG]))
+        u[(long long)i * xs + (long long)j * ys + (side ? nz : -1)] = lc.az(i, j, side ? nz : -1);
+      continue;
+    }
+    r -= zr;
+    if (r < yr) {
+      const int per = (nx + 2) * nz, side = r / per, i = (r % per) / nz - 1, k = (r % per) % nz;
+      if (Level1Compose<T>::writes(bc.type[side ? FY_POS : FY_NEG]))
+        u[(long long)i * xs + (long long)(side ? ny : -1) * ys + k] = lc.ay(i, side ? ny : -1, k);
+      continue;
+    }
+    r -= yr;
+    {
+      const int per = ny * nz, side = r / per, j = (r % per) / nz, k = (r % per) % nz;
+      if (Level1Compose<T>::writes(bc.type[side ? FX_POS : FX_NEG]))
+        u[(long long)(side ? nx : -1) * xs + (long long)j * ys + k] = lc.ax(side ? nx : -1, j, k);
+    }
+  }
+}
+
 }  // namespace ocub

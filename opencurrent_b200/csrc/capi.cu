@@ -146,11 +146,13 @@ ocu_status ocu_grid_reduce(const ocu_grid *g, ocu_reduce_op op, double *result, 
   OCU_NOT_NULL(result, "result");
   if (op < OCU_REDUCE_MAXABS || op > OCU_REDUCE_CHECKNAN) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] reduce - bad op");
   cudaStream_t st = (cudaStream_t)s;
-  const size_t bytes = reduce_scratch_bytes(g->L, dtype_size(g->dtype)) + 64;
+  // [counter | block partials | result]: the result slot starts on a 64-byte boundary
+  const size_t base = ((reduce_scratch_bytes(g->L, dtype_size(g->dtype)) + 63) / 64) * 64;
+  const size_t bytes = base + 64;
   char *scratch = nullptr;
   OCU_TRY(check_cuda(cudaMallocAsync((void **)&scratch, bytes, st), "cudaMallocAsync(reduce)"));
   ocu_status rs = check_cuda(cudaMemsetAsync(scratch, 0, bytes, st), "cudaMemsetAsync(reduce)");
-  double *d_res = (double *)(scratch + bytes - 64);
+  double *d_res = (double *)(scratch + base);
   if (rs == OCU_OK) {
     if (g->dtype == OCU_F64) rs = launch_reduce<double>(origin<double>(g), g->L, op, scratch, d_res, st);
     else rs = launch_reduce<float>(origin<float>(g), g->L, op, scratch, d_res, st);
@@ -336,6 +338,57 @@ ocu_status ocu_mg_run_fmg(ocu_mg *mg, int count) {
 ocu_grid *ocu_mg_pressure(ocu_mg *mg) { return mg ? mg->s.pressure : nullptr; }
 
 ocu_grid *ocu_mg_level_grid(ocu_mg *mg, char which, int level) { return mg ? mg->s.level_grid(which, level) : nullptr; }
+
+static ocu_status pick_core(ocu_mg *mg, int core, int level, CoreOps **out) {
+  OCU_NOT_NULL(mg, "solver");
+  if (!mg->s.initialized) return fail(OCU_ERR_NOT_INITIALIZED, "[ERROR] level operation - not initialized");
+  CoreOps *c;
+  if (core == 1) {
+    if (mg->s.kind != OCU_MG_MIXED_IR && mg->s.kind != OCU_MG_MIXED_WARMSTART && mg->s.kind != OCU_MG_F32)
+      return fail(OCU_ERR_INVALID_VALUE, "[ERROR] level operation - solver has no FP32 hierarchy");
+    c = &mg->s.cf;
+  } else if (core == 0) {
+    c = mg->s.kind == OCU_MG_F32 ? (CoreOps *)&mg->s.cf : (CoreOps *)&mg->s.cd;
+  } else {
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] level operation - bad core %d", core);
+  }
+  if (level < 0 || level >= c->levels()) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] level operation - bad level %d", level);
+  *out = c;
+  return OCU_OK;
+}
+
+ocu_status ocu_mg_relax(ocu_mg *mg, int core, int level, int iterations, int order) {
+  CoreOps *c;
+  OCU_TRY(pick_core(mg, core, level, &c));
+  if (iterations < 0 || order < 0 || order > 2) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] relax - bad arguments");
+  return c->relax(level, iterations, order);
+}
+
+ocu_status ocu_mg_relax_sweep(ocu_mg *mg, int core, int level, int color) {
+  CoreOps *c;
+  OCU_TRY(pick_core(mg, core, level, &c));
+  return c->relax_sweep(level, color & 1);
+}
+
+ocu_status ocu_mg_restrict_residuals(ocu_mg *mg, int core, int fine, int coarse, double *l2, double *linf) {
+  CoreOps *c;
+  OCU_TRY(pick_core(mg, core, fine, &c));
+  if (coarse != fine && coarse != fine + 1) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] restrict_residuals - bad levels");
+  if (coarse >= c->levels()) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] restrict_residuals - bad coarse level");
+  return c->restrict_residuals(fine, coarse, l2, linf);
+}
+
+ocu_status ocu_mg_prolong(ocu_mg *mg, int core, int coarse, int fine) {
+  CoreOps *c;
+  OCU_TRY(pick_core(mg, core, fine, &c));
+  if (coarse != fine + 1 || coarse >= c->levels()) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] prolong - bad levels");
+  return c->prolong(coarse, fine);
+}
+
+ocu_status ocu_mg_synchronize(ocu_mg *mg) {
+  OCU_NOT_NULL(mg, "solver");
+  return check_cuda(cudaStreamSynchronize(mg->s.stream), "synchronize");
+}
 
 ocu_status ocu_mg_get_stats(const ocu_mg *mg, ocu_mg_stats *stats) {
   OCU_NOT_NULL(mg, "solver"); OCU_NOT_NULL(stats, "stats");

@@ -38,9 +38,21 @@ ocu_status check_launch(const char *what) {
   return check_cuda(cudaGetLastError(), what);
 }
 
-void count_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
+// Launches recorded while a stream capture is open do not run; they are counted separately and
+// credited to the global count each time the captured graph is launched.
+static thread_local bool g_capturing = false;
+static thread_local unsigned long long g_captured = 0;
+
+void count_launch(int n) {
+  if (g_capturing) g_captured += (unsigned long long)n;
+  else g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed);
+}
 
 unsigned long long launch_count() { return g_launches.load(); }
+
+void set_capturing(bool on) { g_capturing = on; }
+
+unsigned long long launch_count_captured() { return g_captured; }
 
 const char *last_error_text() { return g_last_error; }
 

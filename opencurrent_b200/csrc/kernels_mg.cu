@@ -4,6 +4,7 @@
 // Arithmetic follows the reference kernels operation by operation (file:line at each kernel);
 // the library is built with --fmad=false, so results are bit-identical to the CPU oracle.
 #include "bc_device.cuh"
+#include "mg_fused.h"
 #include "ocu_internal.h"
 
 namespace ocub {
@@ -112,116 +113,14 @@ ocu_status launch_init_diag(T *diag, int nx, int ny, const RelaxParams &p, cudaS
 // ------------------------------------------------------------------------------------------
 // Coarsest level.  The reference copies u and b to the host, runs do_cpu_solve with host ghost
 // fills after every colour, copies back and re-applies the device ghost fill
-// (sol_mgpressure3ddev.cu:82-188).  Here the same sequence runs as ONE single-CTA kernel:
-// do_cpu_solve's arithmetic (the _fz*(...) products in double, accumulated into a T residual),
-// the host faces-only fill in T, then the device level1 fill.  No PCIe round trip.
+// (sol_mgpressure3ddev.cu:82-188).  Here the same sequence runs as ONE single-CTA kernel
+// (coarse_relax_block in mg_fused.h).  No PCIe round trip.
 // ------------------------------------------------------------------------------------------
-template <typename T>
-struct CoarseCoef {
-  double fx, fy, fz;
-  T omega, ld, h;
-  T xp, xn, yp, yn, zp, zn;
-};
-
-template <typename T>
-__device__ __forceinline__ T host_face(const BCDev &bc, int f, T src, T h, bool neg) {
-  const int t = bc.type[f];
-  if (t == OCU_BC_DIRICHELET) return -src + (T)2 * (T)bc.value[f];
-  if (t == OCU_BC_NEUMANN) return neg ? src - h * (T)bc.value[f] : src + h * (T)bc.value[f];
-  return src;
-}
-
 template <typename T>
 __global__ void __launch_bounds__(512) k_coarse_relax(T *u, const T *b, long long xs, long long ys, int nx, int ny,
                                                       int nz, int iterations, int order, CoarseCoef<T> c,
                                                       BCDev bc, T hx, T hy, T hz) {
-  const int ncell = nx * ny * nz;
-  auto at = [&](int i, int j, int k) -> T & { return u[(long long)i * xs + (long long)j * ys + k]; };
-  for (int it = 0; it < iterations; it++) {
-    for (int rb = 0; rb < 2; rb++) {
-      int color = rb;
-      if (order == 1 || (order == 2 && it >= iterations / 2)) color = !rb;
-      for (int q = threadIdx.x; q < ncell; q += blockDim.x) {
-        const int i = q / (ny * nz), j = (q / nz) % ny, k = q % nz;
-        if (((i + j + color) & 1) != (k & 1)) continue;
-        const long long id = (long long)i * xs + (long long)j * ys + k;
-        const T x_mod = (i == 0) ? c.xn : (i == nx - 1) ? c.xp : (T)0;
-        const T y_mod = (j == 0) ? c.yn : (j == ny - 1) ? c.yp : (T)0;
-        const T z_mod = (k == 0) ? c.zn : (k == nz - 1) ? c.zp : (T)0;
-        T residual = (-c.h * c.h * b[id] - c.ld * u[id]);
-        residual = (T)((double)residual + c.fz * (double)(u[id - 1] + u[id + 1]));
-        residual = (T)((double)residual + c.fy * (double)(u[id + ys] + u[id - ys]));
-        residual = (T)((double)residual + c.fx * (double)(u[id + xs] + u[id - xs]));
-        u[id] = u[id] + c.omega * residual / (c.ld + x_mod + y_mod + z_mod);
-      }
-      __syncthreads();
-      // host faces-only fill (grid3dboundary.cu:1018-1111); faces depend on interior only
-      const int nzf = nx * ny, nyf = nx * nz, nxf = ny * nz;
-      for (int q = threadIdx.x; q < 2 * (nzf + nyf + nxf); q += blockDim.x) {
-        int r = q;
-        if (r < 2 * nzf) {
-          const int side = r / nzf, i = (r % nzf) / ny, j = (r % nzf) % ny;
-          const int f = side ? FZ_POS : FZ_NEG, t = bc.type[f];
-          if (t == OCU_BC_PERIODIC) at(i, j, side ? nz : -1) = at(i, j, side ? 0 : nz - 1);
-          else if (t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN)
-            at(i, j, side ? nz : -1) = host_face<T>(bc, f, at(i, j, side ? nz - 1 : 0), hz, !side);
-          continue;
-        }
-        r -= 2 * nzf;
-        if (r < 2 * nyf) {
-          const int side = r / nyf, i = (r % nyf) / nz, k = (r % nyf) % nz;
-          const int f = side ? FY_POS : FY_NEG, t = bc.type[f];
-          if (t == OCU_BC_PERIODIC) at(i, side ? ny : -1, k) = at(i, side ? 0 : ny - 1, k);
-          else if (t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN)
-            at(i, side ? ny : -1, k) = host_face<T>(bc, f, at(i, side ? ny - 1 : 0, k), hy, !side);
-          continue;
-        }
-        r -= 2 * nyf;
-        {
-          const int side = r / nxf, j = (r % nxf) / nz, k = (r % nxf) % nz;
-          const int f = side ? FX_POS : FX_NEG, t = bc.type[f];
-          if (t == OCU_BC_PERIODIC) at(side ? nx : -1, j, k) = at(side ? 0 : nx - 1, j, k);
-          else if (t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN)
-            at(side ? nx : -1, j, k) = host_face<T>(bc, f, at(side ? nx - 1 : 0, j, k), hx, !side);
-        }
-      }
-      __syncthreads();
-    }
-  }
-  // device level1 fill after the copy back (sol_mgpressure3ddev.cu:187)
-  Level1Compose<T> lc;
-  lc.p = u; lc.xs = xs; lc.ys = ys; lc.nx = nx; lc.ny = ny; lc.nz = nz; lc.bc = bc;
-  lc.hx = hx; lc.hy = hy; lc.hz = hz;
-  const int zr = 2 * (nx + 2) * (ny + 2), yr = 2 * (nx + 2) * nz, xr = 2 * ny * nz;
-  // the composition reads interior values only, so all ghosts can be written in one phase
-  for (int q = threadIdx.x; q < zr + yr + xr; q += blockDim.x) {
-    int r = q;
-    if (r < zr) {
-      const int per = (nx + 2) * (ny + 2), side = r / per, i = (r % per) / (ny + 2) - 1, j = (r % per) % (ny + 2) - 1;
-      if (Level1Compose<T>::writes(bc.type[side ? FZ_POS : FZ_NEG])) {
-        const T v = lc.az(i, j, side ? nz : -1);
-        at(i, j, side ? nz : -1) = v;
-      }
-      continue;
-    }
-    r -= zr;
-    if (r < yr) {
-      const int per = (nx + 2) * nz, side = r / per, i = (r % per) / nz - 1, k = (r % per) % nz;
-      if (Level1Compose<T>::writes(bc.type[side ? FY_POS : FY_NEG])) {
-        const T v = lc.ay(i, side ? ny : -1, k);
-        at(i, side ? ny : -1, k) = v;
-      }
-      continue;
-    }
-    r -= yr;
-    {
-      const int per = ny * nz, side = r / per, j = (r % per) / nz, k = (r % per) % nz;
-      if (Level1Compose<T>::writes(bc.type[side ? FX_POS : FX_NEG])) {
-        const T v = lc.ax(side ? nx : -1, j, k);
-        at(side ? nx : -1, j, k) = v;
-      }
-    }
-  }
+  coarse_relax_block<T>(u, b, xs, ys, nx, ny, nz, iterations, order, c, bc, hx, hy, hz);
 }
 
 template <typename T>
@@ -230,14 +129,7 @@ ocu_status launch_coarse_relax(T *u, const T *b, const ocu_layout &L, int iterat
                                cudaStream_t s) {
   if (!bc_check_scalar(p.bc))
     return fail(OCU_ERR_INVALID_VALUE, "[ERROR] relax_on_host - invalid boundary condition types");
-  CoarseCoef<T> c;
-  c.fx = p.fx; c.fy = p.fy; c.fz = p.fz;
-  c.omega = (T)p.omega;
-  c.ld = (T)(2 * p.fx + 2 * p.fy + 2 * p.fz);
-  c.h = (T)p.h;
-  c.xp = (T)bc_diag_mod(p.bc.xpos, p.fx); c.xn = (T)bc_diag_mod(p.bc.xneg, p.fx);
-  c.yp = (T)bc_diag_mod(p.bc.ypos, p.fy); c.yn = (T)bc_diag_mod(p.bc.yneg, p.fy);
-  c.zp = (T)bc_diag_mod(p.bc.zpos, p.fz); c.zn = (T)bc_diag_mod(p.bc.zneg, p.fz);
+  const CoarseCoef<T> c = make_coarse_coef<T>(p);
   // RO_SYMMETRIC needs an even iteration count of at least 4 (sol_mgpressure3ddev.cu:159-163)
   if (order == 2) {
     if (iterations % 2 == 1) iterations++;

@@ -1,0 +1,498 @@
+// Fused multigrid kernels (same arithmetic as kernels_mg.cu, fewer launches and bytes):
+//   - colour sweep and prolongation that also write the ghosts of the cells they update;
+//   - residual + 8-cell restriction + norm partials in one pass (r is never written);
+//   - residual + norms (+ optional FP32 down-cast) for the level-0 checks and the refinement
+//     solver;
+//   - a single-CTA kernel that runs the coarse end of a V-cycle (all levels at or below a few
+//     thousand cells) with __syncthreads between phases instead of one launch per operation.
+// Norm partials follow the reference fold order exactly (grid3dops.cu:26-130): for each fine
+// (i,j) row, lane t folds k = t, t+32, ... and the 32 lanes fold 16/8/4/2/1; rows are folded by
+// 256-wide trees (grid1dops.cu:33-115) in k_fold_rows.
+#include "bc_device.cuh"
+#include "ghost_emit.cuh"
+#include "mg_fused.h"
+#include "ocu_internal.h"
+
+namespace ocub {
+
+template <typename T>
+__device__ __forceinline__ T relax_point(const T *__restrict__ u, const T *__restrict__ b, long long id, long long xs,
+                                         long long ys, int i, int j, int k, int nx, int ny, int nz,
+                                         const RelaxCoefD<T> &c, const T *__restrict__ diag) {
+  const T uc = u[id];
+  T res, dg;
+  if (sizeof(T) == 4) {
+    const T bv = b[id];
+    res = (-c.hsq * bv - c.ld * uc);
+    res += c.fz * (u[id - 1] + u[id + 1]);
+    res += c.fy * (u[id - ys] + u[id + ys]);
+    res += c.fx * (u[id - xs] + u[id + xs]);
+    dg = c.ld;
+    if (i == nx - 1) dg += c.xp;
+    if (i == 0) dg += c.xn;
+    if (j == ny - 1) dg += c.yp;
+    if (j == 0) dg += c.yn;
+    if (k == nz - 1) dg += c.zp;
+    if (k == 0) dg += c.zn;
+  } else {
+    res = -c.ld * uc;
+    res += c.fz * (u[id - 1] + u[id + 1]);
+    res += c.fy * (u[id - ys] + u[id + ys]);
+    res += c.fx * (u[id - xs] + u[id + xs]);
+    res += c.hsq * b[id];
+    if (diag) {
+      dg = diag[(long long)i * ny + j];
+    } else {  // same sequence the 2D table is built with (sol_mgpressure3ddev.cu:36-41)
+      dg = c.ld;
+      if (i == nx - 1) dg += c.xp;
+      if (i == 0) dg += c.xn;
+      if (j == ny - 1) dg += c.yp;
+      if (j == 0) dg += c.yn;
+    }
+    if (k == nz - 1) dg += c.zp;
+    if (k == 0) dg += c.zn;
+  }
+  return uc + c.omega * res / dg;
+}
+
+// Colour sweep + ghost writes: thread (t, j, i), k = 2t + parity.
+template <typename T>
+__global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, const T *__restrict__ b, long long xs,
+                                                          long long ys, int nx, int ny, int nz, int color,
+                                                          RelaxCoefD<T> c, const T *__restrict__ diag,
+                                                          GhostEmit<T> ge) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z * blockDim.z + threadIdx.z;
+  if (i >= nx || j >= ny || t >= nz / 2) return;
+  const int k = 2 * t + ((i + j + color) & 1);
+  const long long id = (long long)i * xs + (long long)j * ys + k;
+  const T nv = relax_point<T>(u, b, id, xs, ys, i, j, k, nx, ny, nz, c, diag);
+  u[id] = nv;
+  ge.emit(i, j, k, nv);
+}
+
+template <typename T>
+ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const T *diag, int color,
+                                   const RelaxParams &p, double hx, double hy, double hz, cudaStream_t s) {
+  const RelaxCoefD<T> c = make_relax_coef_d<T>(p);
+  const int half = L.nz / 2;
+  if (half == 0) return OCU_OK;
+  dim3 block(half >= 32 ? 32 : (half >= 16 ? 16 : (half >= 8 ? 8 : 4)), 4, 2);
+  block.y = 256 / (block.x * block.z) > 8 ? 8 : 256 / (block.x * block.z);
+  dim3 grid((half + block.x - 1) / block.x, (L.ny + block.y - 1) / block.y, (L.nx + block.z - 1) / block.z);
+  GhostEmit<T> ge{nullptr, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(p.bc), (T)hx, (T)hy, (T)hz};
+  ge.p = u;
+  k_relax_color_emit<T><<<grid, block, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c, diag, ge);
+  return check_launch("k_relax_color_emit");
+}
+
+// Prolongation + correction + ghost writes (devf.cu:94-197 then the level1 fill).
+template <typename T>
+__device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, long long tc, long long cx, long long cy,
+                                             T *__restrict__ uf, long long f, long long fxs, long long fys, int ic,
+                                             int jc, int kc, const GhostEmit<T> *ge) {
+  const T w1 = (T)0.421875, w2 = (T)0.140625, w3 = (T)0.046875, w4 = (T)0.015625;
+  const T c000 = uc[tc];
+  const T cp00 = uc[tc + cx], c0p0 = uc[tc + cy], cpp0 = uc[tc + cx + cy];
+  const T c00p = uc[tc + 1], cp0p = uc[tc + cx + 1], c0pp = uc[tc + cy + 1], cppp = uc[tc + cx + cy + 1];
+  const T cm00 = uc[tc - cx], c0m0 = uc[tc - cy], cmm0 = uc[tc - cx - cy], c00m = uc[tc - 1];
+  const T cm0m = uc[tc - cx - 1], c0mm = uc[tc - cy - 1], cmmm = uc[tc - cx - cy - 1];
+  const T cmp0 = uc[tc - cx + cy], cm0p = uc[tc - cx + 1], cpm0 = uc[tc + cx - cy];
+  const T c0mp = uc[tc - cy + 1], cp0m = uc[tc + cx - 1], c0pm = uc[tc + cy - 1];
+  const T cpmm = uc[tc + cx - cy - 1], cmpm = uc[tc - cx + cy - 1], cmmp = uc[tc - cx - cy + 1];
+  const T cppm = uc[tc + cx + cy - 1], cpmp = uc[tc + cx - cy + 1];
+  const int i = 2 * ic + 1, j = 2 * jc + 1, k = 2 * kc + 1;
+  T v;
+  v = uf[f] + w1 * c000 + w2 * (cp00 + c0p0 + c00p) + w3 * (cpp0 + cp0p + c0pp) + w4 * cppp;
+  uf[f] = v; if (ge) ge->emit(i, j, k, v);
+  v = uf[f - fxs] + w1 * c000 + w2 * (cm00 + c0p0 + c00p) + w3 * (cmp0 + cm0p + c0pp) + w4 * cppp;
+  uf[f - fxs] = v; if (ge) ge->emit(i - 1, j, k, v);
+  v = uf[f - fys] + w1 * c000 + w2 * (cp00 + c0m0 + c00p) + w3 * (cpm0 + cp0p + c0mp) + w4 * cpmp;
+  uf[f - fys] = v; if (ge) ge->emit(i, j - 1, k, v);
+  v = uf[f - 1] + w1 * c000 + w2 * (cp00 + c0p0 + c00m) + w3 * (cpp0 + cp0m + c0pm) + w4 * cppm;
+  uf[f - 1] = v; if (ge) ge->emit(i, j, k - 1, v);
+  v = uf[f - fxs - fys] + w1 * c000 + w2 * (cm00 + c0m0 + c00p) + w3 * (cmm0 + cm0p + c0mp) + w4 * cmmp;
+  uf[f - fxs - fys] = v; if (ge) ge->emit(i - 1, j - 1, k, v);
+  v = uf[f - fxs - 1] + w1 * c000 + w2 * (cm00 + c0p0 + c00m) + w3 * (cmp0 + cm0m + c0pm) + w4 * cmpm;
+  uf[f - fxs - 1] = v; if (ge) ge->emit(i - 1, j, k - 1, v);
+  v = uf[f - fys - 1] + w1 * c000 + w2 * (cp00 + c0m0 + c00m) + w3 * (cpm0 + cp0m + c0mm) + w4 * cpmm;
+  uf[f - fys - 1] = v; if (ge) ge->emit(i, j - 1, k - 1, v);
+  v = uf[f - fxs - fys - 1] + w1 * c000 + w2 * (cm00 + c0m0 + c00m) + w3 * (cmm0 + cm0m + c0mm) + w4 * cmmm;
+  uf[f - fxs - fys - 1] = v; if (ge) ge->emit(i - 1, j - 1, k - 1, v);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong_emit(const T *__restrict__ uc, long long cx, long long cy, int cnx,
+                                                      int cny, int cnz, T *__restrict__ uf, long long fxs,
+                                                      long long fys, GhostEmit<T> ge) {
+  const int kc = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jc = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ic = blockIdx.z;
+  if (kc >= cnz || jc >= cny || ic >= cnx) return;
+  const long long tc = (long long)ic * cx + (long long)jc * cy + kc;
+  const long long f = (long long)(2 * ic + 1) * fxs + (long long)(2 * jc + 1) * fys + (2 * kc + 1);
+  prolong_cell<T>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, &ge);
+}
+
+template <typename T>
+ocu_status launch_prolong_emit(const T *uc, const ocu_layout &Lc, T *uf, const ocu_layout &Lf,
+                               const ocu_bc_set &bc_fine, double hx, double hy, double hz, cudaStream_t s) {
+  dim3 block(Lc.nz >= 32 ? 32 : 16, 8);
+  dim3 grid((Lc.nz + block.x - 1) / block.x, (Lc.ny + block.y - 1) / block.y, Lc.nx);
+  GhostEmit<T> ge{uf, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, to_dev(bc_fine), (T)hx, (T)hy, (T)hz};
+  k_prolong_emit<T><<<grid, block, 0, s>>>(uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf, Lf.xstride,
+                                           Lf.ystride, ge);
+  return check_launch("k_prolong_emit");
+}
+
+// ------------------------------------------------------------------------------------------
+// Residual helpers
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T residual_at(const T *__restrict__ u, const T *__restrict__ b, long long id, long long xs,
+                                         long long ys, const ResCoefT<T> &c) {
+  return b[id] - (c.fzh * (u[id - 1] + u[id + 1]) + c.fyh * (u[id - ys] + u[id + ys]) +
+                  c.fxh * (u[id - xs] + u[id + xs]) - c.dg * u[id]);
+}
+
+// Fold one 64-wide chunk of a fine row into the lane accumulators in reference order:
+// this lane holds r at k = base + 2*lane (+1); virtual lane t needs k = base + t and
+// base + 32 + t, held by lanes t/2 and 16 + t/2.
+template <typename T>
+__device__ __forceinline__ void fold_chunk(T e0, T e1, int base, int nz, int lane, T &acc2, T &accinf,
+                                           bool want2, bool wantinf) {
+  const int src1 = lane >> 1, src2 = 16 + (lane >> 1);
+  const T a0 = __shfl_sync(0xffffffffu, e0, src1), a1 = __shfl_sync(0xffffffffu, e1, src1);
+  const T b0 = __shfl_sync(0xffffffffu, e0, src2), b1 = __shfl_sync(0xffffffffu, e1, src2);
+  const T x1 = (lane & 1) ? a1 : a0;
+  const T x2 = (lane & 1) ? b1 : b0;
+  if (base + lane < nz) {
+    if (want2) acc2 = x1 * x1 + acc2;
+    if (wantinf) accinf = fmax(fabs(x1), accinf);
+  }
+  if (base + 32 + lane < nz) {
+    if (want2) acc2 = x2 * x2 + acc2;
+    if (wantinf) accinf = fmax(fabs(x2), accinf);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_tree(T v, bool is_max) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const T other = __shfl_down_sync(0xffffffffu, v, o);
+    v = is_max ? fmax(v, other) : v + other;
+  }
+  return v;
+}
+
+// Residual over one fine row per warp (chunks of 64 along k): optional outputs r (T), r as
+// float (the refinement solver's FP32 right-hand side), and per-row norm partials.
+template <typename T>
+__global__ void __launch_bounds__(256) k_residual_rows(const T *__restrict__ u, const T *__restrict__ b,
+                                                       T *__restrict__ r, float *__restrict__ r32, long long xs,
+                                                       long long ys, int nx, int ny, int nz, ResCoefT<T> c,
+                                                       T *__restrict__ rows2, T *__restrict__ rowsinf) {
+  const int lane = threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (j >= ny) return;  // whole warp exits together
+  const bool want2 = rows2 != nullptr, wantinf = rowsinf != nullptr;
+  T acc2 = 0, accinf = 0;
+  const long long row = (long long)i * xs + (long long)j * ys;
+  for (int base = 0; base < nz; base += 64) {
+    const int k0 = base + 2 * lane;
+    T e0 = 0, e1 = 0;
+    if (k0 < nz) {
+      e0 = residual_at<T>(u, b, row + k0, xs, ys, c);
+      if (r) r[row + k0] = e0;
+      if (r32) r32[row + k0] = (float)e0;
+    }
+    if (k0 + 1 < nz) {
+      e1 = residual_at<T>(u, b, row + k0 + 1, xs, ys, c);
+      if (r) r[row + k0 + 1] = e1;
+      if (r32) r32[row + k0 + 1] = (float)e1;
+    }
+    if (want2 || wantinf) fold_chunk<T>(e0, e1, base, nz, lane, acc2, accinf, want2, wantinf);
+  }
+  if (want2) {
+    const T v = warp_tree<T>(acc2, false);
+    if (lane == 0) rows2[(long long)i * ny + j] = v;
+  }
+  if (wantinf) {
+    const T v = warp_tree<T>(accinf, true);
+    if (lane == 0) rowsinf[(long long)i * ny + j] = v;
+  }
+}
+
+// Residual at the 8 children of each coarse cell + restriction, one coarse row per warp.
+// The children's residuals are never stored; norm partials (level 0 only) fold the 4 fine rows
+// (2ic+di, 2jc+dj) of the warp.
+template <typename T, bool NORM>
+__global__ void __launch_bounds__(256) k_residual_restrict(const T *__restrict__ u, const T *__restrict__ b,
+                                                           long long xs, long long ys, int nx, int ny, int nz,
+                                                           ResCoefT<T> c, T *__restrict__ bc_, long long bxs,
+                                                           long long bys, int cnx, int cny, int cnz,
+                                                           T *__restrict__ rows2, T *__restrict__ rowsinf) {
+  const int lane = threadIdx.x;
+  const int jc = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ic = blockIdx.z;
+  if (jc >= cny) return;
+  const bool want2 = NORM && rows2 != nullptr, wantinf = NORM && rowsinf != nullptr;
+  T acc2[4] = {0, 0, 0, 0}, accinf[4] = {0, 0, 0, 0};
+  const long long frow = (long long)(2 * ic) * xs + (long long)(2 * jc) * ys;
+  for (int cbase = 0; cbase < cnz; cbase += 32) {
+    const int kc = cbase + lane;
+    T r[8];
+    if (kc < cnz) {
+      const long long ri = frow + 2 * kc;
+      r[0] = residual_at<T>(u, b, ri, xs, ys, c);
+      r[1] = residual_at<T>(u, b, ri + 1, xs, ys, c);
+      r[2] = residual_at<T>(u, b, ri + ys, xs, ys, c);
+      r[3] = residual_at<T>(u, b, ri + 1 + ys, xs, ys, c);
+      r[4] = residual_at<T>(u, b, ri + xs, xs, ys, c);
+      r[5] = residual_at<T>(u, b, ri + 1 + xs, xs, ys, c);
+      r[6] = residual_at<T>(u, b, ri + ys + xs, xs, ys, c);
+      r[7] = residual_at<T>(u, b, ri + 1 + ys + xs, xs, ys, c);
+      bc_[(long long)ic * bxs + (long long)jc * bys + kc] =
+          (T)0.125 * (r[0] + r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 8; q++) r[q] = 0;
+    }
+    if (NORM && (want2 || wantinf)) {
+      // fine rows: (di,dj) = (0,0): r0,r1 ; (0,1): r2,r3 ; (1,0): r4,r5 ; (1,1): r6,r7
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        fold_chunk<T>(r[2 * q], r[2 * q + 1], 2 * cbase, nz, lane, acc2[q], accinf[q], want2, wantinf);
+    }
+  }
+  if (NORM) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * ic + (q >> 1), j = 2 * jc + (q & 1);
+      if (want2) {
+        const T v = warp_tree<T>(acc2[q], false);
+        if (lane == 0) rows2[(long long)i * ny + j] = v;
+      }
+      if (wantinf) {
+        const T v = warp_tree<T>(accinf[q], true);
+        if (lane == 0) rowsinf[(long long)i * ny + j] = v;
+      }
+    }
+  }
+}
+
+// 256-wide fold of row values (grid1dops.cu:33-115), one launch: block b folds rows
+// [256b, 256b+256), the last block folds the block partials.  Writes the T result as double.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fold_rows(const T *__restrict__ rows, long long nrows, int is_max,
+                                                   T *partial, unsigned *counter, double *result) {
+  __shared__ T sh[256];
+  __shared__ bool last;
+  const long long idx = (long long)blockIdx.x * 256 + threadIdx.x;
+  sh[threadIdx.x] = idx < nrows ? rows[idx] : (T)0;
+  __syncthreads();
+  for (int stride = 128; stride > 0; stride >>= 1) {
+    if (threadIdx.x < stride)
+      sh[threadIdx.x] = is_max ? fmax(sh[threadIdx.x], sh[threadIdx.x + stride]) : sh[threadIdx.x] + sh[threadIdx.x + stride];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = sh[0];
+    __threadfence();
+    last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  volatile T *vp = partial;
+  long long count = gridDim.x;
+  while (count > 1) {
+    const long long nb = (count + 255) / 256;
+    for (long long bb = 0; bb < nb; bb++) {
+      const long long q = bb * 256 + threadIdx.x;
+      sh[threadIdx.x] = q < count ? vp[q] : (T)0;
+      __syncthreads();
+      for (int stride = 128; stride > 0; stride >>= 1) {
+        if (threadIdx.x < stride)
+          sh[threadIdx.x] = is_max ? fmax(sh[threadIdx.x], sh[threadIdx.x + stride]) : sh[threadIdx.x] + sh[threadIdx.x + stride];
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) vp[bb] = sh[0];
+      __syncthreads();
+    }
+    count = nb;
+  }
+  if (threadIdx.x == 0) {
+    *result = (double)vp[0];
+    *counter = 0;
+  }
+}
+
+template <typename T>
+static ResCoefT<T> res_coef(double h, double fx, double fy, double fz) {
+  ResCoefT<T> c;
+  c.fxh = (T)(fx / (h * h));
+  c.fyh = (T)(fy / (h * h));
+  c.fzh = (T)(fz / (h * h));
+  c.dg = (T)(2 * (fx + fy + fz) / (h * h));
+  return c;
+}
+
+template <typename T>
+ocu_status launch_residual_rows(const T *u, const T *b, T *r, float *r32, const ocu_layout &L, double h, double fx,
+                                double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s) {
+  dim3 block(32, 8), grid(1, (L.ny + 7) / 8, L.nx);
+  k_residual_rows<T><<<grid, block, 0, s>>>(u, b, r, r32, L.xstride, L.ystride, L.nx, L.ny, L.nz,
+                                            res_coef<T>(h, fx, fy, fz), rows2, rowsinf);
+  return check_launch("k_residual_rows");
+}
+
+template <typename T>
+ocu_status launch_residual_restrict(const T *u, const T *b, const ocu_layout &Lf, T *bc_, const ocu_layout &Lc,
+                                    double h, double fx, double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s) {
+  dim3 block(32, 8), grid(1, (Lc.ny + 7) / 8, Lc.nx);
+  const ResCoefT<T> c = res_coef<T>(h, fx, fy, fz);
+  if (rows2 || rowsinf)
+    k_residual_restrict<T, true><<<grid, block, 0, s>>>(u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
+                                                        Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf);
+  else
+    k_residual_restrict<T, false><<<grid, block, 0, s>>>(u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
+                                                         Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr);
+  return check_launch("k_residual_restrict");
+}
+
+template <typename T>
+ocu_status launch_fold_rows(const T *rows, long long nrows, bool is_max, void *scratch, double *result,
+                            cudaStream_t s) {
+  const long long blocks = (nrows + 255) / 256;
+  unsigned *counter = reinterpret_cast<unsigned *>(scratch);
+  T *partial = reinterpret_cast<T *>(reinterpret_cast<char *>(scratch) + 64);
+  k_fold_rows<T><<<(unsigned)blocks, 256, 0, s>>>(rows, nrows, is_max ? 1 : 0, partial, counter, result);
+  return check_launch("k_fold_rows");
+}
+
+// ------------------------------------------------------------------------------------------
+// Single-CTA coarse tail: levels s..L-1 of one V-cycle (down: relax nu1, clear, residual +
+// restrict; coarsest: relax with the host routine's arithmetic; up: prolong + ghosts, relax
+// nu2), phases separated by __syncthreads.  Identical operation sequence and arithmetic to the
+// per-level kernels.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__device__ void tail_relax(const TailLevel<T> &lv, int iterations, int order, int nt) {
+  GhostEmit<T> ge{lv.u, lv.xs, lv.ys, lv.nx, lv.ny, lv.nz, lv.bc, lv.hx, lv.hy, lv.hz};
+  if (order == 2) {
+    if (iterations % 2 == 1) iterations++;
+    if (iterations < 4) iterations = 4;
+  }
+  const int half = lv.nz / 2;
+  const int nwork = lv.nx * lv.ny * half;
+  for (int it = 0; it < iterations; it++) {
+    for (int rb = 0; rb < 2; rb++) {
+      int color = rb;
+      if (order == 1 || (order == 2 && it >= iterations / 2)) color = !rb;
+      for (int q = threadIdx.x; q < nwork; q += nt) {
+        const int i = q / (lv.ny * half), rem = q % (lv.ny * half), j = rem / half, t = rem % half;
+        const int k = 2 * t + ((i + j + color) & 1);
+        const long long id = (long long)i * lv.xs + (long long)j * lv.ys + k;
+        const T nv = relax_point<T>(lv.u, lv.b, id, lv.xs, lv.ys, i, j, k, lv.nx, lv.ny, lv.nz, lv.rc, nullptr);
+        lv.u[id] = nv;
+        if (lv.emit_ok) ge.emit(i, j, k, nv);
+      }
+      __syncthreads();
+      // without fused ghost writes: refresh between colours when periodic, else after both
+      // (sol_mgpressure3ddev.cu:235-241)
+      if (!lv.emit_ok && (lv.periodic || rb == 1)) {
+        level1_fill_block<T>(lv.u, lv.xs, lv.ys, lv.nx, lv.ny, lv.nz, lv.bc, lv.hx, lv.hy, lv.hz);
+        __syncthreads();
+      }
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(1024) k_coarse_tail(TailParams<T> P) {
+  const int nt = blockDim.x;
+  const int L = P.nlev;  // levels in the tail: P.lv[0] = level s ... P.lv[L-1] = coarsest
+  for (int l = 0; l < L - 1; l++) {
+    const TailLevel<T> &f = P.lv[l];
+    const TailLevel<T> &c = P.lv[l + 1];
+    tail_relax<T>(f, P.nu1, 0, nt);
+    // clear_zero(coarse) + homogeneous ghost fill == zero every cell of the shell and interior
+    const int cz = c.nz + 2, cy = c.ny + 2, cx = c.nx + 2;
+    for (int q = threadIdx.x; q < cx * cy * cz; q += nt) {
+      const int i = q / (cy * cz) - 1, j = (q / cz) % cy - 1, k = q % cz - 1;
+      c.u[(long long)i * c.xs + (long long)j * c.ys + k] = (T)0;
+    }
+    // residual + restriction into b of the coarse level
+    for (int q = threadIdx.x; q < c.nx * c.ny * c.nz; q += nt) {
+      const int ic = q / (c.ny * c.nz), jc = (q / c.nz) % c.ny, kc = q % c.nz;
+      const long long ri = (long long)(2 * ic) * f.xs + (long long)(2 * jc) * f.ys + 2 * kc;
+      const T r0 = residual_at<T>(f.u, f.b, ri, f.xs, f.ys, f.res);
+      const T r1 = residual_at<T>(f.u, f.b, ri + 1, f.xs, f.ys, f.res);
+      const T r2 = residual_at<T>(f.u, f.b, ri + f.ys, f.xs, f.ys, f.res);
+      const T r3 = residual_at<T>(f.u, f.b, ri + 1 + f.ys, f.xs, f.ys, f.res);
+      const T r4 = residual_at<T>(f.u, f.b, ri + f.xs, f.xs, f.ys, f.res);
+      const T r5 = residual_at<T>(f.u, f.b, ri + 1 + f.xs, f.xs, f.ys, f.res);
+      const T r6 = residual_at<T>(f.u, f.b, ri + f.ys + f.xs, f.xs, f.ys, f.res);
+      const T r7 = residual_at<T>(f.u, f.b, ri + 1 + f.ys + f.xs, f.xs, f.ys, f.res);
+      c.b[(long long)ic * c.xs + (long long)jc * c.ys + kc] = (T)0.125 * (r0 + r1 + r2 + r3 + r4 + r5 + r6 + r7);
+    }
+    __syncthreads();
+  }
+  // coarsest level
+  {
+    const TailLevel<T> &cl = P.lv[L - 1];
+    if (P.host_coarse) {
+      coarse_relax_block<T>(cl.u, cl.b, cl.xs, cl.ys, cl.nx, cl.ny, cl.nz, P.coarse_iters, P.coarse_order, P.cc,
+                            cl.bc, cl.hx, cl.hy, cl.hz);
+    } else {
+      tail_relax<T>(cl, P.coarse_iters, P.coarse_order, nt);
+    }
+    __syncthreads();
+  }
+  for (int l = L - 2; l >= 0; l--) {
+    const TailLevel<T> &f = P.lv[l];
+    const TailLevel<T> &c = P.lv[l + 1];
+    GhostEmit<T> ge{f.u, f.xs, f.ys, f.nx, f.ny, f.nz, f.bc, f.hx, f.hy, f.hz};
+    for (int q = threadIdx.x; q < c.nx * c.ny * c.nz; q += nt) {
+      const int ic = q / (c.ny * c.nz), jc = (q / c.nz) % c.ny, kc = q % c.nz;
+      const long long tc = (long long)ic * c.xs + (long long)jc * c.ys + kc;
+      const long long fi = (long long)(2 * ic + 1) * f.xs + (long long)(2 * jc + 1) * f.ys + (2 * kc + 1);
+      prolong_cell<T>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, f.emit_ok ? &ge : nullptr);
+    }
+    __syncthreads();
+    if (!f.emit_ok) {
+      level1_fill_block<T>(f.u, f.xs, f.ys, f.nx, f.ny, f.nz, f.bc, f.hx, f.hy, f.hz);
+      __syncthreads();
+    }
+    if (P.first_level + l > 0) {
+      tail_relax<T>(f, P.nu2, P.post_order, nt);
+    }
+  }
+}
+
+template <typename T>
+ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s) {
+  k_coarse_tail<T><<<1, 1024, 0, s>>>(P);
+  return check_launch("k_coarse_tail");
+}
+
+#define INST(T)                                                                                                \
+  template ocu_status launch_relax_color_emit<T>(T *, const T *, const ocu_layout &, const T *, int,           \
+                                                 const RelaxParams &, double, double, double, cudaStream_t);  \
+  template ocu_status launch_prolong_emit<T>(const T *, const ocu_layout &, T *, const ocu_layout &,           \
+                                             const ocu_bc_set &, double, double, double, cudaStream_t);       \
+  template ocu_status launch_residual_rows<T>(const T *, const T *, T *, float *, const ocu_layout &, double,   \
+                                              double, double, double, T *, T *, cudaStream_t);                 \
+  template ocu_status launch_residual_restrict<T>(const T *, const T *, const ocu_layout &, T *,                \
+                                                  const ocu_layout &, double, double, double, double, T *, T *, \
+                                                  cudaStream_t);                                               \
+  template ocu_status launch_fold_rows<T>(const T *, long long, bool, void *, double *, cudaStream_t);          \
+  template ocu_status launch_coarse_tail<T>(const TailParams<T> &, cudaStream_t);
+INST(float)
+INST(double)
+#undef INST
+
+}  // namespace ocub

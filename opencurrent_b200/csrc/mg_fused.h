@@ -1,0 +1,179 @@
+// Shared device-side pieces of the multigrid kernels (coefficients, coarsest-level block
+// relaxation, single-CTA tail parameters) and the fused-kernel launchers.
+#pragma once
+
+#include "bc_device.cuh"
+#include "ocu_internal.h"
+
+namespace ocub {
+
+// Colour-sweep coefficients rounded to T the way the reference launcher rounds them
+// (sol_mgpressure3ddevf.cu:390-393 float, sol_mgpressure3ddevd.cu:1262-1268 double).
+template <typename T>
+struct RelaxCoefD {
+  T omega, hsq, fx, fy, fz, ld;  // hsq = (T)(h*h) for float, (-h)*h for double
+  T xp, xn, yp, yn, zp, zn;
+};
+
+template <typename T>
+inline RelaxCoefD<T> make_relax_coef_d(const RelaxParams &p) {
+  RelaxCoefD<T> c;
+  c.omega = (T)p.omega;
+  c.hsq = sizeof(T) == 4 ? (T)(p.h * p.h) : (T)(-p.h * p.h);
+  c.fx = (T)p.fx; c.fy = (T)p.fy; c.fz = (T)p.fz;
+  c.ld = (T)(2 * p.fx + 2 * p.fy + 2 * p.fz);
+  c.xp = (T)bc_diag_mod(p.bc.xpos, p.fx); c.xn = (T)bc_diag_mod(p.bc.xneg, p.fx);
+  c.yp = (T)bc_diag_mod(p.bc.ypos, p.fy); c.yn = (T)bc_diag_mod(p.bc.yneg, p.fy);
+  c.zp = (T)bc_diag_mod(p.bc.zpos, p.fz); c.zn = (T)bc_diag_mod(p.bc.zneg, p.fz);
+  return c;
+}
+
+// do_cpu_solve coefficients (sol_mgpressure3ddev.cu:82-125)
+template <typename T>
+struct CoarseCoef {
+  double fx, fy, fz;
+  T omega, ld, h;
+  T xp, xn, yp, yn, zp, zn;
+};
+
+template <typename T>
+inline CoarseCoef<T> make_coarse_coef(const RelaxParams &p) {
+  CoarseCoef<T> c;
+  c.fx = p.fx; c.fy = p.fy; c.fz = p.fz;
+  c.omega = (T)p.omega;
+  c.ld = (T)(2 * p.fx + 2 * p.fy + 2 * p.fz);
+  c.h = (T)p.h;
+  c.xp = (T)bc_diag_mod(p.bc.xpos, p.fx); c.xn = (T)bc_diag_mod(p.bc.xneg, p.fx);
+  c.yp = (T)bc_diag_mod(p.bc.ypos, p.fy); c.yn = (T)bc_diag_mod(p.bc.yneg, p.fy);
+  c.zp = (T)bc_diag_mod(p.bc.zpos, p.fz); c.zn = (T)bc_diag_mod(p.bc.zneg, p.fz);
+  return c;
+}
+
+template <typename T>
+__device__ __forceinline__ T host_face(const BCDev &bc, int f, T src, T h, bool neg) {
+  const int t = bc.type[f];
+  if (t == OCU_BC_DIRICHELET) return -src + (T)2 * (T)bc.value[f];
+  if (t == OCU_BC_NEUMANN) return neg ? src - h * (T)bc.value[f] : src + h * (T)bc.value[f];
+  return src;
+}
+
+// Coarsest-level relaxation as the reference runs it on the host: do_cpu_solve per colour
+// (the _fz*(...) products in double, accumulated into a T residual), the host faces-only ghost
+// fill in T after every colour (grid3dboundary.cu:1018-1111), and the device level1 fill at the
+// end (sol_mgpressure3ddev.cu:134-188).  Executed by one thread block, phases separated by
+// __syncthreads; the caller has already adjusted `iterations` for RO_SYMMETRIC.
+template <typename T>
+__device__ void coarse_relax_block(T *u, const T *b, long long xs, long long ys, int nx, int ny, int nz,
+                                   int iterations, int order, const CoarseCoef<T> &c, const BCDev &bc, T hx,
+                                   T hy, T hz) {
+  const int nt = blockDim.x;
+  const int ncell = nx * ny * nz;
+  auto at = [&](int i, int j, int k) -> T & { return u[(long long)i * xs + (long long)j * ys + k]; };
+  for (int it = 0; it < iterations; it++) {
+    for (int rb = 0; rb < 2; rb++) {
+      int color = rb;
+      if (order == 1 || (order == 2 && it >= iterations / 2)) color = !rb;
+      for (int q = threadIdx.x; q < ncell; q += nt) {
+        const int i = q / (ny * nz), j = (q / nz) % ny, k = q % nz;
+        if (((i + j + color) & 1) != (k & 1)) continue;
+        const long long id = (long long)i * xs + (long long)j * ys + k;
+        const T x_mod = (i == 0) ? c.xn : (i == nx - 1) ? c.xp : (T)0;
+        const T y_mod = (j == 0) ? c.yn : (j == ny - 1) ? c.yp : (T)0;
+        const T z_mod = (k == 0) ? c.zn : (k == nz - 1) ? c.zp : (T)0;
+        T residual = (-c.h * c.h * b[id] - c.ld * u[id]);
+        residual = (T)((double)residual + c.fz * (double)(u[id - 1] + u[id + 1]));
+        residual = (T)((double)residual + c.fy * (double)(u[id + ys] + u[id - ys]));
+        residual = (T)((double)residual + c.fx * (double)(u[id + xs] + u[id - xs]));
+        u[id] = u[id] + c.omega * residual / (c.ld + x_mod + y_mod + z_mod);
+      }
+      __syncthreads();
+      const int nzf = nx * ny, nyf = nx * nz, nxf = ny * nz;
+      for (int q = threadIdx.x; q < 2 * (nzf + nyf + nxf); q += nt) {
+        int r = q;
+        if (r < 2 * nzf) {
+          const int side = r / nzf, i = (r % nzf) / ny, j = (r % nzf) % ny;
+          const int f = side ? FZ_POS : FZ_NEG, t = bc.type[f];
+          if (t == OCU_BC_PERIODIC) at(i, j, side ? nz : -1) = at(i, j, side ? 0 : nz - 1);
+          else if (t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN)
+            at(i, j, side ? nz : -1) = host_face<T>(bc, f, at(i, j, side ? nz - 1 : 0), hz, !side);
+          continue;
+        }
+        r -= 2 * nzf;
+        if (r < 2 * nyf) {
+          const int side = r / nyf, i = (r % nyf) / nz, k = (r % nyf) % nz;
+          const int f = side ? FY_POS : FY_NEG, t = bc.type[f];
+          if (t == OCU_BC_PERIODIC) at(i, side ? ny : -1, k) = at(i, side ? 0 : ny - 1, k);
+          else if (t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN)
+            at(i, side ? ny : -1, k) = host_face<T>(bc, f, at(i, side ? ny - 1 : 0, k), hy, !side);
+          continue;
+        }
+        r -= 2 * nyf;
+        {
+          const int side = r / nxf, j = (r % nxf) / nz, k = (r % nxf) % nz;
+          const int f = side ? FX_POS : FX_NEG, t = bc.type[f];
+          if (t == OCU_BC_PERIODIC) at(side ? nx : -1, j, k) = at(side ? 0 : nx - 1, j, k);
+          else if (t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN)
+            at(side ? nx : -1, j, k) = host_face<T>(bc, f, at(side ? nx - 1 : 0, j, k), hx, !side);
+        }
+      }
+      __syncthreads();
+    }
+  }
+  level1_fill_block<T>(u, xs, ys, nx, ny, nz, bc, hx, hy, hz);
+  __syncthreads();
+}
+
+template <typename T>
+struct ResCoefT {
+  T fxh, fyh, fzh, dg;
+};
+
+// One level of the single-CTA tail.
+template <typename T>
+struct TailLevel {
+  T *u;
+  T *b;
+  long long xs, ys;
+  int nx, ny, nz;
+  int emit_ok;  // ghosts may be written by the sweeping threads (no BC_NONE, even periodic axes)
+  int periodic; // any periodic face (ghost refresh between colours when emit_ok == 0)
+  BCDev bc;
+  T hx, hy, hz;
+  RelaxCoefD<T> rc;
+  ResCoefT<T> res;
+};
+
+constexpr int kMaxTailLevels = 8;
+
+template <typename T>
+struct TailParams {
+  TailLevel<T> lv[kMaxTailLevels];
+  int nlev;          // levels in the tail; lv[nlev-1] is the coarsest
+  int first_level;   // absolute level number of lv[0]
+  int nu1, nu2;
+  int post_order;    // relax order of the up-leg (RO_BLACK_RED when symmetric)
+  int coarse_iters;  // already adjusted for RO_SYMMETRIC when host_coarse
+  int coarse_order;
+  int host_coarse;   // 1: coarsest relaxed with the host routine's arithmetic
+  CoarseCoef<T> cc;
+};
+
+template <typename T>
+ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const T *diag, int color,
+                                   const RelaxParams &p, double hx, double hy, double hz, cudaStream_t s);
+template <typename T>
+ocu_status launch_prolong_emit(const T *uc, const ocu_layout &Lc, T *uf, const ocu_layout &Lf,
+                               const ocu_bc_set &bc_fine, double hx, double hy, double hz, cudaStream_t s);
+template <typename T>
+ocu_status launch_residual_rows(const T *u, const T *b, T *r, float *r32, const ocu_layout &L, double h, double fx,
+                                double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s);
+template <typename T>
+ocu_status launch_residual_restrict(const T *u, const T *b, const ocu_layout &Lf, T *bc_, const ocu_layout &Lc,
+                                    double h, double fx, double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s);
+template <typename T>
+ocu_status launch_fold_rows(const T *rows, long long nrows, bool is_max, void *scratch, double *result,
+                            cudaStream_t s);
+template <typename T>
+ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s);
+
+}  // namespace ocub

@@ -14,6 +14,8 @@
 #include <memory>
 #include <vector>
 
+#include "ghost_emit.cuh"
+#include "mg_fused.h"
 #include "mg_solver.h"
 
 namespace ocub {
@@ -56,6 +58,7 @@ MGCore<T>::~MGCore() {
   }
   for (auto p : diag) cudaFree(p);
   if (red_scratch) cudaFree(red_scratch);
+  if (rows) cudaFree(rows);
   if (d_norms) cudaFree(d_norms);
   if (h_norms) cudaFreeHost(h_norms);
 }
@@ -129,6 +132,8 @@ ocu_status MGCore<T>::init(const ocu_bc_set &bc_, bool disable_host, int nx, int
   }
   OCU_TRY(check_cuda(cudaMalloc(&red_scratch, reduce_scratch_bytes(lay[0], sizeof(T))), "cudaMalloc(reduce)"));
   OCU_TRY(check_cuda(cudaMemset(red_scratch, 0, reduce_scratch_bytes(lay[0], sizeof(T))), "cudaMemset(reduce)"));
+  rows_stride = ((long long)dim[0][0] * dim[0][1] + 63) / 64 * 64;
+  OCU_TRY(check_cuda(cudaMalloc(&rows, 2 * sizeof(T) * rows_stride), "cudaMalloc(norm rows)"));
   OCU_TRY(check_cuda(cudaMalloc(&d_norms, 2 * sizeof(double)), "cudaMalloc(norms)"));
   OCU_TRY(check_cuda(cudaMallocHost(&h_norms, 2 * sizeof(double)), "cudaMallocHost(norms)"));
   return check_cuda(cudaStreamSynchronize(stream), "initialize_storage");
@@ -161,6 +166,29 @@ ocu_status MGCore<T>::clear_zero(int level) {
   return check_cuda(cudaMemsetAsync(grids_u[level]->buf, 0, sizeof(T) * lay[level].allocated, stream), "clear_zero");
 }
 
+// clear_zero(level) followed by apply_boundary_conditions(level).  Below level 0 the boundary
+// values are homogeneous, so every ghost rule maps the zero interior to +0 -- the same bits the
+// memset wrote -- and the ghost launch is skipped.
+template <typename T>
+ocu_status MGCore<T>::clear_level(int level) {
+  OCU_TRY(clear_zero(level));
+  return level == 0 ? apply_bc(level) : OCU_OK;
+}
+
+// Ghost writes can ride along with the kernels that update interior cells when no face is
+// BC_NONE and every periodic axis has an even cell count (otherwise a colour sweep would read
+// a ghost written in the same sweep).
+template <typename T>
+bool MGCore<T>::emit_ok(int level) const {
+  if (!fused) return false;
+  const ocu_bc_set b = bc_at_level(level);
+  if (bc_has_none(b)) return false;
+  if ((b.xpos.type == OCU_BC_PERIODIC || b.xneg.type == OCU_BC_PERIODIC) && (dim[level][0] & 1)) return false;
+  if ((b.ypos.type == OCU_BC_PERIODIC || b.yneg.type == OCU_BC_PERIODIC) && (dim[level][1] & 1)) return false;
+  if ((b.zpos.type == OCU_BC_PERIODIC || b.zneg.type == OCU_BC_PERIODIC) && (dim[level][2] & 1)) return false;
+  return true;
+}
+
 // relax (sol_mgpressure3ddev.cu:190-248)
 template <typename T>
 ocu_status MGCore<T>::relax(int level, int iterations, int order) {
@@ -173,46 +201,157 @@ ocu_status MGCore<T>::relax(int level, int iterations, int order) {
     if (iterations < 4) iterations = 4;
   }
   const T *dg = diag.empty() ? nullptr : (const T *)diag[level];
+  const bool emit = emit_ok(level);
   for (int it = 0; it < iterations; it++) {
     for (int rb = 0; rb < 2; rb++) {
       int color = rb;
       if (order == RO_BLACK_RED || (order == RO_SYMMETRIC && it >= iterations / 2)) color = !rb;
-      OCU_TRY(launch_relax_color<T>(u0(level), b0(level), lay[level], dg, color, p, stream));
-      if (update_bc_between_colors) OCU_TRY(apply_bc(level));
+      if (emit) {
+        OCU_TRY(launch_relax_color_emit<T>(u0(level), b0(level), lay[level], dg, color, p, hx(level), hy(level),
+                                           hz(level), stream));
+      } else {
+        OCU_TRY(launch_relax_color<T>(u0(level), b0(level), lay[level], dg, color, p, stream));
+        if (update_bc_between_colors) OCU_TRY(apply_bc(level));
+      }
     }
-    if (!update_bc_between_colors) OCU_TRY(apply_bc(level));
+    if (!emit && !update_bc_between_colors) OCU_TRY(apply_bc(level));
   }
   return OCU_OK;
 }
 
-// restrict_residuals (sol_mgpressure3ddev.cu:250-279): the squared-residual sum is folded in
-// T, divided by the cell count in T and square-rooted in T.
+// restrict_residuals, enqueue part (sol_mgpressure3ddev.cu:250-279).  The fused path computes
+// the residual, the restriction and the norm partials in one pass without storing r; with
+// store_residuals the reference's separate kernels run and r_grid(level) is kept.  Requested
+// norms are folded on the device and copied to pinned host memory; finish_norms() waits.
 template <typename T>
-ocu_status MGCore<T>::restrict_residuals(int fine, int coarse, double *l2, double *linf) {
+ocu_status MGCore<T>::enqueue_restrict_residuals(int fine, int coarse, bool want_l2, bool want_linf) {
   const double hf = h[fine];
-  OCU_TRY(launch_residual<T>(u0(fine), b0(fine), r0(fine), lay[fine], hf, fx, fy, fz, stream));
-  if (coarse != fine) OCU_TRY(launch_restrict<T>(r0(fine), lay[fine], b0(coarse), lay[coarse], stream));
-  if (l2 || linf) {
-    if (l2) OCU_TRY(launch_reduce<T>(r0(fine), lay[fine], OCU_REDUCE_SQRSUM, red_scratch, d_norms, stream));
-    if (linf) OCU_TRY(launch_reduce<T>(r0(fine), lay[fine], OCU_REDUCE_MAXABS, red_scratch, d_norms + 1, stream));
+  const bool norms = want_l2 || want_linf;
+  if (!fused || store_residuals) {
+    OCU_TRY(launch_residual<T>(u0(fine), b0(fine), r0(fine), lay[fine], hf, fx, fy, fz, stream));
+    if (coarse != fine) OCU_TRY(launch_restrict<T>(r0(fine), lay[fine], b0(coarse), lay[coarse], stream));
+    if (want_l2) OCU_TRY(launch_reduce<T>(r0(fine), lay[fine], OCU_REDUCE_SQRSUM, red_scratch, d_norms, stream));
+    if (want_linf) OCU_TRY(launch_reduce<T>(r0(fine), lay[fine], OCU_REDUCE_MAXABS, red_scratch, d_norms + 1, stream));
+  } else {
+    T *rows2 = want_l2 ? (T *)rows : nullptr;
+    T *rowsinf = want_linf ? (T *)rows + rows_stride : nullptr;
+    if (coarse != fine) {
+      OCU_TRY(launch_residual_restrict<T>(u0(fine), b0(fine), lay[fine], b0(coarse), lay[coarse], hf, fx, fy, fz,
+                                          rows2, rowsinf, stream));
+    } else if (norms) {
+      OCU_TRY(launch_residual_rows<T>(u0(fine), b0(fine), nullptr, nullptr, lay[fine], hf, fx, fy, fz, rows2, rowsinf,
+                                      stream));
+    }
+    const long long nrows = (long long)dim[fine][0] * dim[fine][1];
+    if (want_l2) OCU_TRY(launch_fold_rows<T>(rows2, nrows, false, red_scratch, d_norms, stream));
+    if (want_linf) OCU_TRY(launch_fold_rows<T>(rowsinf, nrows, true, red_scratch, d_norms + 1, stream));
+  }
+  if (norms)
     OCU_TRY(check_cuda(cudaMemcpyAsync(h_norms, d_norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream),
                        "norm readback"));
-    OCU_TRY(check_cuda(cudaStreamSynchronize(stream), "norm readback"));
-    if (l2) {
-      T rn = (T)h_norms[0];
-      rn /= (T)(dim[fine][0] * dim[fine][1] * dim[fine][2]);
-      *l2 = (double)std::sqrt(rn);
-    }
-    if (linf) *linf = h_norms[1];
+  return OCU_OK;
+}
+
+// The squared-residual sum is folded in T, divided by the cell count in T and square-rooted in
+// T (sol_mgpressure3ddev.cu:263-268).
+template <typename T>
+ocu_status MGCore<T>::finish_norms(int fine, double *l2, double *linf) {
+  OCU_TRY(check_cuda(cudaStreamSynchronize(stream), "norm readback"));
+  if (l2) {
+    T rn = (T)h_norms[0];
+    rn /= (T)(dim[fine][0] * dim[fine][1] * dim[fine][2]);
+    *l2 = (double)std::sqrt(rn);
   }
+  if (linf) *linf = h_norms[1];
+  return OCU_OK;
+}
+
+template <typename T>
+ocu_status MGCore<T>::restrict_residuals(int fine, int coarse, double *l2, double *linf) {
+  OCU_TRY(enqueue_restrict_residuals(fine, coarse, l2 != nullptr, linf != nullptr));
+  if (l2 || linf) return finish_norms(fine, l2, linf);
   return OCU_OK;
 }
 
 // prolong (sol_mgpressure3ddev.cu:284-297)
 template <typename T>
 ocu_status MGCore<T>::prolong(int coarse, int fine) {
+  if (emit_ok(fine))
+    return launch_prolong_emit<T>(u0(coarse), lay[coarse], u0(fine), lay[fine], bc_at_level(fine), hx(fine), hy(fine),
+                                  hz(fine), stream);
   OCU_TRY(launch_prolong<T>(u0(coarse), lay[coarse], u0(fine), lay[fine], stream));
   return apply_bc(fine);
+}
+
+// First level handled by the single-CTA tail: the finest level >= 1 from which every level has
+// at most tail_cells cells.  num_levels-1 means "coarsest only" (the plain coarse kernel).
+template <typename T>
+int MGCore<T>::tail_start() const {
+  const int coarse = num_levels - 1;
+  if (!fused || tail_cells <= 0) return coarse;
+  int s = coarse;
+  while (s - 1 >= 1 && (long long)dim[s - 1][0] * dim[s - 1][1] * dim[s - 1][2] <= tail_cells &&
+         coarse - (s - 1) + 1 <= kMaxTailLevels)
+    s--;
+  return s;
+}
+
+// Levels s..L-1 of a V-cycle: down (relax nu1, clear, residual+restrict), coarsest relax,
+// up (prolong + ghosts, relax nu2 where the absolute level is > 0).
+template <typename T>
+ocu_status MGCore<T>::cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool symmetric) {
+  const int coarse = num_levels - 1;
+  if (s >= coarse) return relax(coarse, coarse_iters, symmetric ? RO_SYMMETRIC : RO_RED_BLACK);
+  for (int l = s; l <= coarse; l++)
+    if (!emit_ok(l) && l != coarse) {
+      // ghost writes cannot be fused on this hierarchy: run the per-level kernels
+      for (int q = s; q < coarse; q++) {
+        OCU_TRY(relax(q, nu1, RO_RED_BLACK));
+        OCU_TRY(clear_level(q + 1));
+        OCU_TRY(enqueue_restrict_residuals(q, q + 1, false, false));
+      }
+      OCU_TRY(relax(coarse, coarse_iters, symmetric ? RO_SYMMETRIC : RO_RED_BLACK));
+      for (int q = coarse - 1; q >= s; q--) {
+        OCU_TRY(prolong(q + 1, q));
+        if (q > 0) OCU_TRY(relax(q, nu2, symmetric ? RO_BLACK_RED : RO_RED_BLACK));
+      }
+      return OCU_OK;
+    }
+  TailParams<T> P;
+  std::memset(&P, 0, sizeof(P));
+  P.nlev = coarse - s + 1;
+  P.first_level = s;
+  P.nu1 = nu1;
+  P.nu2 = nu2;
+  P.post_order = symmetric ? RO_BLACK_RED : RO_RED_BLACK;
+  P.host_coarse = disable_relax_on_host ? 0 : 1;
+  P.coarse_order = symmetric ? RO_SYMMETRIC : RO_RED_BLACK;
+  int ci = coarse_iters;
+  if (P.host_coarse && P.coarse_order == RO_SYMMETRIC) {
+    if (ci % 2 == 1) ci++;
+    if (ci < 4) ci = 4;
+  }
+  P.coarse_iters = ci;
+  P.cc = make_coarse_coef<T>(relax_params(coarse));
+  for (int l = s; l <= coarse; l++) {
+    TailLevel<T> &v = P.lv[l - s];
+    v.u = u0(l);
+    v.b = b0(l);
+    v.xs = lay[l].xstride;
+    v.ys = lay[l].ystride;
+    v.nx = dim[l][0]; v.ny = dim[l][1]; v.nz = dim[l][2];
+    v.emit_ok = emit_ok(l) ? 1 : 0;
+    v.periodic = bc_any_periodic(bc) ? 1 : 0;
+    v.bc = to_dev(bc_at_level(l));
+    v.hx = (T)hx(l); v.hy = (T)hy(l); v.hz = (T)hz(l);
+    v.rc = make_relax_coef_d<T>(relax_params(l));
+    const double hh = h[l];
+    v.res.fxh = (T)(fx / (hh * hh));
+    v.res.fyh = (T)(fy / (hh * hh));
+    v.res.fzh = (T)(fz / (hh * hh));
+    v.res.dg = (T)(2 * (fx + fy + fz) / (hh * hh));
+  }
+  return launch_coarse_tail<T>(P, stream);
 }
 
 template struct MGCore<float>;
@@ -237,7 +376,180 @@ static double pick(int conv, double l2, double linf) {
 
 // do_fmg (sol_mgpressure3d.cpp:113-251); returns OCU_OK (converged), OCU_ERR_NOT_CONVERGED, or
 // an error.
+// ------------------------------------------------------------------------------------------
+// CUDA-graph replay.  The schedule between two host decisions is fixed for a given solver
+// configuration, so each such segment is captured once (stream capture of the same enqueue
+// code) and replayed with one cudaGraphLaunch:
+//   INIT   ghost fill of u0 + residual norms of level 0 (read back, then decide)
+//   RAMP   restriction chain + the FMG cycles from the coarsest level up to level 1
+//   PRE0   pre-smooth at level 0, clear level 1, residual+restriction+norms (read back)
+//   REST0  the rest of a level-0 cycle (levels 1.. down, tail kernel, up to level 0)
+//   FINAL  ghost fill of u0 after convergence
+// With CONVERGENCE_NONE nothing is read back, so a whole fixed-schedule FMG (the refinement
+// solver's inner solve) runs as a chain of graph launches without a host wait.
+// ------------------------------------------------------------------------------------------
+MGSolver::~MGSolver() {
+  clear_graphs();
+  if (pressure) { cudaFree(pressure->buf); delete pressure; }
+  if (rhs_f) { cudaFree(rhs_f->buf); delete rhs_f; }
+}
+
+void MGSolver::clear_graphs() {
+  for (auto &kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+  graphs.clear();
+}
+
+template <typename F>
+ocu_status MGSolver::run_segment(const void *core, int seg, F &&enqueue) {
+  if (!use_graphs) return enqueue();
+  const auto key = std::make_pair(core, seg);
+  auto it = graphs.find(key);
+  if (it == graphs.end()) {
+    OCU_TRY(check_cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture"));
+    set_capturing(true);
+    const unsigned long long n0 = launch_count_captured();
+    ocu_status st = enqueue();
+    const int kernels = (int)(launch_count_captured() - n0);
+    set_capturing(false);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    if (st != OCU_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    OCU_TRY(check_cuda(e, "cudaStreamEndCapture"));
+    GraphEntry ent;
+    e = cudaGraphInstantiate(&ent.exec, g, 0);
+    cudaGraphDestroy(g);
+    OCU_TRY(check_cuda(e, "cudaGraphInstantiate"));
+    ent.kernels = kernels;
+    it = graphs.emplace(key, ent).first;
+  }
+  OCU_TRY(check_cuda(cudaGraphLaunch(it->second.exec, stream), "cudaGraphLaunch"));
+  count_launch(it->second.kernels);
+  return OCU_OK;
+}
+
+enum { SEG_INIT = 0, SEG_RAMP = 8, SEG_PRE0 = 16, SEG_REST0 = 24, SEG_FINAL = 32 };
+
+// levels [a, b) of a down-leg without norm checks
+ocu_status MGSolver::enq_down(CoreOps *c, int a, int b) {
+  for (int level = a; level < b; level++) {
+    OCU_TRY(c->relax(level, prm.nu1, RO_RED_BLACK));
+    OCU_TRY(c->clear_level(level + 1));
+    OCU_TRY(c->enqueue_restrict_residuals(level, level + 1, false, false));
+  }
+  return OCU_OK;
+}
+
+// tail from level s, then the up-leg from s-1 to f
+ocu_status MGSolver::enq_tail_up(CoreOps *c, int s, int f) {
+  const bool sym = prm.make_symmetric_operator != 0;
+  OCU_TRY(c->cycle_tail(s, prm.nu1, prm.nu2, coarse_iters(), sym));
+  for (int level = s - 1; level >= f; level--) {
+    OCU_TRY(c->prolong(level + 1, level));
+    if (level > 0) OCU_TRY(c->relax(level, prm.nu2, sym ? RO_BLACK_RED : RO_RED_BLACK));
+  }
+  return OCU_OK;
+}
+
+ocu_status MGSolver::do_fmg_graph(double tolerance, int max_iter, double *rl2, double *rlinf) {
+  const int conv = prm.convergence;
+  const bool wl2 = conv & OCU_CONVERGENCE_CALC_L2, wlinf = conv & OCU_CONVERGENCE_CALC_LINF;
+  const int nv = (wl2 ? 1 : 0) + (wlinf ? 2 : 0);
+  CoreOps *c = active();
+  const int ts = c->tail_start();
+  double orig_l2 = 0, orig_linf = 0;
+  *rl2 = *rlinf = 0;
+  OCU_TRY(run_segment(c, SEG_INIT + nv, [&]() -> ocu_status {
+    OCU_TRY(c->apply_bc(0));
+    return c->enqueue_restrict_residuals(0, 0, wl2, wlinf);
+  }));
+  if (wl2 || wlinf) OCU_TRY(c->finish_norms(0, wl2 ? &orig_l2 : nullptr, wlinf ? &orig_linf : nullptr));
+  if (pick(conv, orig_l2, orig_linf) < tolerance) {
+    if (wl2) *rl2 = orig_l2;
+    if (wlinf) *rlinf = orig_linf;
+    stats.vcycles = 0;
+    return OCU_OK;
+  }
+  OCU_TRY(run_segment(c, SEG_RAMP, [&]() -> ocu_status {
+    for (int level = 0; level < num_levels - 1; level++) {
+      OCU_TRY(c->clear_level(level + 1));
+      OCU_TRY(c->enqueue_restrict_residuals(level, level + 1, false, false));
+    }
+    for (int f = num_levels - 1; f >= 1; f--) {
+      const int s = ts > f ? ts : f;
+      OCU_TRY(enq_down(c, f, s));
+      OCU_TRY(enq_tail_up(c, s, f));
+      OCU_TRY(c->prolong(f, f - 1));
+    }
+    return OCU_OK;
+  }));
+  int num_vcyc = 0;
+  for (int i_cyc = 0; i_cyc < max_iter + 1; i_cyc++) {
+    num_vcyc++;
+    OCU_TRY(run_segment(c, SEG_PRE0 + nv, [&]() -> ocu_status {
+      OCU_TRY(c->relax(0, prm.nu1, RO_RED_BLACK));
+      OCU_TRY(c->clear_level(1));
+      return c->enqueue_restrict_residuals(0, 1, wl2, wlinf);
+    }));
+    if (wl2 || wlinf) {
+      OCU_TRY(c->finish_norms(0, wl2 ? rl2 : nullptr, wlinf ? rlinf : nullptr));
+      stats.last_l2 = *rl2;
+      stats.last_linf = *rlinf;
+    }
+    if (pick(conv, *rl2, *rlinf) < tolerance) {
+      OCU_TRY(run_segment(c, SEG_FINAL, [&]() -> ocu_status { return c->apply_bc(0); }));
+      stats.vcycles = num_vcyc;
+      return OCU_OK;
+    }
+    OCU_TRY(run_segment(c, SEG_REST0, [&]() -> ocu_status {
+      OCU_TRY(enq_down(c, 1, ts));
+      return enq_tail_up(c, ts, 0);
+    }));
+  }
+  stats.vcycles = num_vcyc;
+  return OCU_ERR_NOT_CONVERGED;
+}
+
+ocu_status MGSolver::do_vcycle_graph(double tolerance, int max_iter, double *rl2, double *rlinf) {
+  const int conv = prm.convergence;
+  const bool wl2 = conv & OCU_CONVERGENCE_CALC_L2, wlinf = conv & OCU_CONVERGENCE_CALC_LINF;
+  const int nv = (wl2 ? 1 : 0) + (wlinf ? 2 : 0);
+  CoreOps *c = active();
+  const int ts = c->tail_start();
+  double orig_l2 = 0, orig_linf = 0;
+  OCU_TRY(run_segment(c, SEG_INIT + nv, [&]() -> ocu_status {
+    OCU_TRY(c->apply_bc(0));
+    return c->enqueue_restrict_residuals(0, 0, wl2, wlinf);
+  }));
+  if (wl2 || wlinf) OCU_TRY(c->finish_norms(0, wl2 ? &orig_l2 : nullptr, wlinf ? &orig_linf : nullptr));
+  if (pick(conv, orig_l2, orig_linf) < tolerance) {
+    if (wl2) *rl2 = orig_l2;
+    if (wlinf) *rlinf = orig_linf;
+    return OCU_OK;
+  }
+  for (int i_cyc = 0; i_cyc < max_iter; i_cyc++) {
+    OCU_TRY(run_segment(c, SEG_PRE0 + nv, [&]() -> ocu_status {
+      OCU_TRY(c->relax(0, prm.nu1, RO_RED_BLACK));
+      OCU_TRY(c->clear_level(1));
+      return c->enqueue_restrict_residuals(0, 1, wl2, wlinf);
+    }));
+    if (wl2 || wlinf) OCU_TRY(c->finish_norms(0, wl2 ? rl2 : nullptr, wlinf ? rlinf : nullptr));
+    if (pick(conv, *rl2, *rlinf) < tolerance) {
+      OCU_TRY(run_segment(c, SEG_FINAL, [&]() -> ocu_status { return c->apply_bc(0); }));
+      return OCU_OK;
+    }
+    OCU_TRY(run_segment(c, SEG_REST0, [&]() -> ocu_status {
+      OCU_TRY(enq_down(c, 1, ts));
+      return enq_tail_up(c, ts, 0);
+    }));
+  }
+  return OCU_ERR_NOT_CONVERGED;
+}
+
 ocu_status MGSolver::do_fmg(double tolerance, int max_iter, double *rl2, double *rlinf) {
+  if (use_graphs && num_levels >= 2) return do_fmg_graph(tolerance, max_iter, rl2, rlinf);
   const int conv = prm.convergence;
   const int coarse_level = num_levels - 1;
   int num_vcyc = 0;
@@ -254,37 +566,18 @@ ocu_status MGSolver::do_fmg(double tolerance, int max_iter, double *rl2, double 
     return OCU_OK;
   }
   for (int level = 0; level < num_levels - 1; level++) {
-    OCU_TRY(c->clear_zero(level + 1));
-    OCU_TRY(c->apply_bc(level + 1));
-    OCU_TRY(c->restrict_residuals(level, level + 1, nullptr, nullptr));
+    OCU_TRY(c->clear_level(level + 1));
+    OCU_TRY(c->enqueue_restrict_residuals(level, level + 1, false, false));
   }
   for (int fine_level = num_levels - 1; fine_level >= 0; fine_level--) {
     const int level_ncyc = (fine_level == 0) ? max_iter + 1 : 1;
     for (int i_cyc = 0; i_cyc < level_ncyc; i_cyc++) {
       if (fine_level == 0) num_vcyc++;
-      for (int level = fine_level; level < coarse_level; level++) {
-        OCU_TRY(c->relax(level, prm.nu1, RO_RED_BLACK));
-        OCU_TRY(c->clear_zero(level + 1));
-        OCU_TRY(c->apply_bc(level + 1));
-        if (level == 0) {
-          OCU_TRY(c->restrict_residuals(0, 1, (conv & OCU_CONVERGENCE_CALC_L2) ? rl2 : nullptr,
-                                        (conv & OCU_CONVERGENCE_CALC_LINF) ? rlinf : nullptr));
-          stats.last_l2 = *rl2;
-          stats.last_linf = *rlinf;
-          if (pick(conv, *rl2, *rlinf) < tolerance) {
-            OCU_TRY(c->apply_bc(0));
-            stats.vcycles = num_vcyc;
-            return OCU_OK;
-          }
-        } else {
-          OCU_TRY(c->restrict_residuals(level, level + 1, nullptr, nullptr));
-        }
-      }
-      OCU_TRY(c->relax(coarse_level, coarse_iters(), prm.make_symmetric_operator ? RO_SYMMETRIC : RO_RED_BLACK));
-      for (int level = coarse_level - 1; level >= fine_level; level--) {
-        OCU_TRY(c->prolong(level + 1, level));
-        if (level > 0)
-          OCU_TRY(c->relax(level, prm.nu2, prm.make_symmetric_operator ? RO_BLACK_RED : RO_RED_BLACK));
+      bool converged = false;
+      OCU_TRY(cycle(c, fine_level, tolerance, rl2, rlinf, &converged));
+      if (converged) {
+        stats.vcycles = num_vcyc;
+        return OCU_OK;
       }
     }
     if (fine_level > 0) OCU_TRY(c->prolong(fine_level, fine_level - 1));
@@ -293,10 +586,49 @@ ocu_status MGSolver::do_fmg(double tolerance, int max_iter, double *rl2, double 
   return OCU_ERR_NOT_CONVERGED;
 }
 
-// do_vcycle (sol_mgpressure3d.cpp:253-329)
-ocu_status MGSolver::do_vcycle(double tolerance, int max_iter, double *rl2, double *rlinf) {
+// One V-cycle from fine_level (the body of the cycle loops of do_fmg and do_vcycle).  The
+// levels from tail_start() down are handed to the single-CTA tail kernel; at level 0 the
+// residual norm is read back after the pre-smooth and the cycle stops when it is below the
+// tolerance, after refreshing the level-0 ghosts (sol_mgpressure3d.cpp:186-236).
+ocu_status MGSolver::cycle(CoreOps *c, int fine_level, double tolerance, double *rl2, double *rlinf,
+                           bool *converged) {
   const int conv = prm.convergence;
   const int coarse_level = num_levels - 1;
+  const bool sym = prm.make_symmetric_operator != 0;
+  const int s = c->tail_start() > fine_level ? c->tail_start() : fine_level;
+  *converged = false;
+  for (int level = fine_level; level < s; level++) {
+    OCU_TRY(c->relax(level, prm.nu1, RO_RED_BLACK));
+    OCU_TRY(c->clear_level(level + 1));
+    if (level == 0) {
+      double *l2 = (conv & OCU_CONVERGENCE_CALC_L2) ? rl2 : nullptr;
+      double *linf = (conv & OCU_CONVERGENCE_CALC_LINF) ? rlinf : nullptr;
+      OCU_TRY(c->enqueue_restrict_residuals(0, 1, l2 != nullptr, linf != nullptr));
+      if (l2 || linf) OCU_TRY(c->finish_norms(0, l2, linf));
+      stats.last_l2 = *rl2;
+      stats.last_linf = *rlinf;
+      if (pick(conv, *rl2, *rlinf) < tolerance) {
+        OCU_TRY(c->apply_bc(0));
+        *converged = true;
+        return OCU_OK;
+      }
+    } else {
+      OCU_TRY(c->enqueue_restrict_residuals(level, level + 1, false, false));
+    }
+  }
+  OCU_TRY(c->cycle_tail(s, prm.nu1, prm.nu2, coarse_iters(), sym));
+  (void)coarse_level;
+  for (int level = s - 1; level >= fine_level; level--) {
+    OCU_TRY(c->prolong(level + 1, level));
+    if (level > 0) OCU_TRY(c->relax(level, prm.nu2, sym ? RO_BLACK_RED : RO_RED_BLACK));
+  }
+  return OCU_OK;
+}
+
+// do_vcycle (sol_mgpressure3d.cpp:253-329)
+ocu_status MGSolver::do_vcycle(double tolerance, int max_iter, double *rl2, double *rlinf) {
+  if (use_graphs && num_levels >= 2) return do_vcycle_graph(tolerance, max_iter, rl2, rlinf);
+  const int conv = prm.convergence;
   double orig_l2 = 0, orig_linf = 0;
   CoreOps *c = active();
   OCU_TRY(c->apply_bc(0));
@@ -308,27 +640,9 @@ ocu_status MGSolver::do_vcycle(double tolerance, int max_iter, double *rl2, doub
     return OCU_OK;
   }
   for (int i_cyc = 0; i_cyc < max_iter; i_cyc++) {
-    for (int level = 0; level < coarse_level; level++) {
-      OCU_TRY(c->relax(level, prm.nu1, RO_RED_BLACK));
-      OCU_TRY(c->clear_zero(level + 1));
-      OCU_TRY(c->apply_bc(level + 1));
-      if (level == 0) {
-        OCU_TRY(c->restrict_residuals(0, 1, (conv & OCU_CONVERGENCE_CALC_L2) ? rl2 : nullptr,
-                                      (conv & OCU_CONVERGENCE_CALC_LINF) ? rlinf : nullptr));
-        if (pick(conv, *rl2, *rlinf) < tolerance) {
-          OCU_TRY(c->apply_bc(0));
-          return OCU_OK;
-        }
-      } else {
-        OCU_TRY(c->restrict_residuals(level, level + 1, nullptr, nullptr));
-      }
-    }
-    OCU_TRY(c->relax(coarse_level, coarse_iters(), prm.make_symmetric_operator ? RO_SYMMETRIC : RO_RED_BLACK));
-    for (int level = coarse_level - 1; level >= 0; level--) {
-      OCU_TRY(c->prolong(level + 1, level));
-      if (level > 0)
-        OCU_TRY(c->relax(level, prm.nu2, prm.make_symmetric_operator ? RO_BLACK_RED : RO_RED_BLACK));
-    }
+    bool converged = false;
+    OCU_TRY(cycle(c, 0, tolerance, rl2, rlinf, &converged));
+    if (converged) return OCU_OK;
   }
   return OCU_ERR_NOT_CONVERGED;
 }
@@ -364,15 +678,15 @@ ocu_status MGSolver::ir_solve(double tolerance, int max_outer, double *rl2, doub
   stats.vcycles = 0;
   double_mode = true;
   OCU_TRY(cd.apply_bc(0));
-  OCU_TRY(cd.restrict_residuals(0, 0, &l2, &linf));
+  OCU_TRY(ir_residual(&l2, &linf));
   *rl2 = l2; *rlinf = linf;
   stats.last_l2 = l2; stats.last_linf = linf;
   if (pick(conv, l2, linf) < tolerance) return OCU_OK;
   const int inner = prm.ir_inner_cycles > 0 ? prm.ir_inner_cycles : 3;
   ocu_mg_params saved = prm;
   int total_inner = 0;
+  (void)L;
   for (int outer = 1; outer <= max_outer; outer++) {
-    OCU_TRY(launch_downcast_interior((const double *)cd.r0(0), (float *)cf.b0(0), L, stream));
     OCU_TRY(cf.clear_zero(0));
     prm.convergence = OCU_CONVERGENCE_NONE;
     double_mode = false;
@@ -384,7 +698,7 @@ ocu_status MGSolver::ir_solve(double tolerance, int max_outer, double *rl2, doub
     if (st != OCU_OK && st != OCU_ERR_NOT_CONVERGED) return st;
     OCU_TRY(launch_add_correction((double *)cd.u0(0), (const float *)cf.u0(0), L, stream));
     OCU_TRY(cd.apply_bc(0));
-    OCU_TRY(cd.restrict_residuals(0, 0, &l2, &linf));
+    OCU_TRY(ir_residual(&l2, &linf));
     stats.outer_iterations = outer;
     stats.vcycles = total_inner;
     *rl2 = l2; *rlinf = linf;
@@ -392,6 +706,25 @@ ocu_status MGSolver::ir_solve(double tolerance, int max_outer, double *rl2, doub
     if (pick(conv, l2, linf) < tolerance) return OCU_OK;
   }
   return OCU_ERR_NOT_CONVERGED;
+}
+
+// FP64 residual of the refinement step, with both norms, written to the FP32 hierarchy's
+// right-hand side as float in the same pass.
+ocu_status MGSolver::ir_residual(double *l2, double *linf) {
+  const ocu_layout &L = cd.lay[0];
+  if (!cd.fused || cd.store_residuals) {
+    OCU_TRY(cd.restrict_residuals(0, 0, l2, linf));
+    return launch_downcast_interior((const double *)cd.r0(0), (float *)cf.b0(0), L, stream);
+  }
+  double *rows2 = (double *)cd.rows, *rowsinf = (double *)cd.rows + cd.rows_stride;
+  OCU_TRY(launch_residual_rows<double>(cd.u0(0), cd.b0(0), nullptr, (float *)cf.b0(0), L, cd.h[0], cd.fx, cd.fy,
+                                       cd.fz, rows2, rowsinf, stream));
+  const long long nrows = (long long)L.nx * L.ny;
+  OCU_TRY(launch_fold_rows<double>(rows2, nrows, false, cd.red_scratch, cd.d_norms, stream));
+  OCU_TRY(launch_fold_rows<double>(rowsinf, nrows, true, cd.red_scratch, cd.d_norms + 1, stream));
+  OCU_TRY(check_cuda(cudaMemcpyAsync(cd.h_norms, cd.d_norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                     "norm readback"));
+  return cd.finish_norms(0, l2, linf);
 }
 
 ocu_status MGSolver::fmg_dispatch(double tol, int max_iter, double *l2, double *linf) {
@@ -444,11 +777,6 @@ ocu_status MGSolver::run_fmg(int count) {
   return st;
 }
 
-MGSolver::~MGSolver() {
-  if (pressure) { cudaFree(pressure->buf); delete pressure; }
-  if (rhs_f) { cudaFree(rhs_f->buf); delete rhs_f; }
-}
-
 ocu_status MGSolver::initialize_storage(int nx, int ny, int nz, double hx, double hy, double hz, ocu_grid *rhs) {
   if (initialized) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] initialize_storage - already initialized");
   if (!check_float((float)hx) || !check_float((float)hy) || !check_float((float)hz))
@@ -486,8 +814,16 @@ ocu_status MGSolver::initialize_storage(int nx, int ny, int nz, double hx, doubl
     }
   }
   stats.num_levels = num_levels;
+  apply_knobs();
   initialized = true;
   return OCU_OK;
+}
+
+void MGSolver::apply_knobs() {
+  const int tc = prm.tail_cells == 0 ? 4096 : (prm.tail_cells < 0 ? 0 : prm.tail_cells);
+  cf.fused = cd.fused = prm.unfused == 0;
+  cf.store_residuals = cd.store_residuals = prm.store_residual_grids != 0;
+  cf.tail_cells = cd.tail_cells = tc;
 }
 
 ocu_status MGSolver::set_params(const ocu_mg_params &p) {
@@ -496,6 +832,8 @@ ocu_status MGSolver::set_params(const ocu_mg_params &p) {
   cd.bc = p.bc;
   if (kind == OCU_MG_MIXED_IR) bc_make_homogeneous(&cf.bc);
   cf.disable_relax_on_host = cd.disable_relax_on_host = p.disable_relax_on_host != 0;
+  apply_knobs();
+  clear_graphs();  // captured schedules depend on every parameter
   return OCU_OK;
 }
 

@@ -3,6 +3,8 @@
 
 #include <array>
 #include <cmath>
+#include <cstdlib>
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -21,7 +23,17 @@ struct CoreOps {
   virtual ocu_status apply_bc(int level) = 0;
   virtual ocu_status restrict_residuals(int fine, int coarse, double *l2, double *linf) = 0;
   virtual ocu_status prolong(int coarse, int fine) = 0;
+  virtual ocu_status relax_sweep(int level, int color) = 0;
   virtual ocu_grid *grid(char which, int level) = 0;
+  virtual int levels() const = 0;
+  // clear_zero + apply_boundary_conditions
+  virtual ocu_status clear_level(int level) = 0;
+  // restrict_residuals split at the host wait: enqueue, then finish_norms for the numbers
+  virtual ocu_status enqueue_restrict_residuals(int fine, int coarse, bool want_l2, bool want_linf) = 0;
+  virtual ocu_status finish_norms(int fine, double *l2, double *linf) = 0;
+  // levels tail_start()..L-1 of a V-cycle in one launch
+  virtual int tail_start() const = 0;
+  virtual ocu_status cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool symmetric) = 0;
 };
 
 // Level hierarchy of one precision (Sol_MultigridPressure3DDevice<T> storage).
@@ -41,8 +53,19 @@ struct MGCore : CoreOps {
   void *red_scratch = nullptr;
   double *d_norms = nullptr;
   double *h_norms = nullptr;
+  void *rows = nullptr;           // per-row norm partials of level 0 (l2 then linf)
+  long long rows_stride = 0;
+  bool fused = true;              // fused kernels (ghost writes, residual+restrict, tail)
+  bool store_residuals = false;   // keep r_grid filled (reference kernels) for read_r
+  int tail_cells = 4096;          // levels with at most this many cells run in the tail kernel
 
   ~MGCore();
+  ocu_status clear_level(int level) override;
+  bool emit_ok(int level) const;
+  ocu_status enqueue_restrict_residuals(int fine, int coarse, bool want_l2, bool want_linf) override;
+  ocu_status finish_norms(int fine, double *l2, double *linf) override;
+  int tail_start() const override;
+  ocu_status cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool symmetric) override;
   ocu_status init(const ocu_bc_set &bc, bool disable_host, int nx, int ny, int nz, double hx, double hy,
                   double hz, ocu_grid *rhs, ocu_grid *pressure, cudaStream_t s);
   ocu_bc_set bc_at_level(int level) const;
@@ -59,6 +82,11 @@ struct MGCore : CoreOps {
   ocu_status apply_bc(int level) override;
   ocu_status restrict_residuals(int fine, int coarse, double *l2, double *linf) override;
   ocu_status prolong(int coarse, int fine) override;
+  ocu_status relax_sweep(int level, int color) override {
+    const T *dg = diag.empty() ? nullptr : (const T *)diag[level];
+    return launch_relax_color<T>(u0(level), b0(level), lay[level], dg, color, relax_params(level), stream);
+  }
+  int levels() const override { return num_levels; }
   ocu_grid *grid(char which, int level) override {
     return which == 'u' ? grids_u[level] : which == 'b' ? grids_b[level] : which == 'r' ? grids_r[level] : nullptr;
   }
@@ -82,17 +110,36 @@ struct MGSolver {
   std::unique_ptr<ocu_grid, GridDeleter> pressure_f;  // FP32 u0 of the mixed solvers
   cudaStream_t stream = nullptr;
   ocu_mg_stats stats{};
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;
+  };
+  std::map<std::pair<const void *, int>, GraphEntry> graphs;
+  bool use_graphs = true;
 
-  explicit MGSolver(ocu_mg_kind k, const ocu_mg_params &p) : kind(k), prm(p) {}
+  // OCU_B200_GRAPHS=0 in the environment replays nothing (every launch issued by the host)
+  explicit MGSolver(ocu_mg_kind k, const ocu_mg_params &p) : kind(k), prm(p) {
+    const char *g = std::getenv("OCU_B200_GRAPHS");
+    use_graphs = !(g && g[0] == '0');
+  }
   ~MGSolver();
+  void clear_graphs();
+  template <typename F> ocu_status run_segment(const void *core, int seg, F &&enqueue);
+  ocu_status enq_down(CoreOps *c, int a, int b);
+  ocu_status enq_tail_up(CoreOps *c, int s, int f);
+  ocu_status do_fmg_graph(double tol, int max_iter, double *l2, double *linf);
+  ocu_status do_vcycle_graph(double tol, int max_iter, double *l2, double *linf);
 
   CoreOps *active();
   int coarse_iters() const;
   ocu_status initialize_storage(int nx, int ny, int nz, double hx, double hy, double hz, ocu_grid *rhs);
   ocu_status set_params(const ocu_mg_params &p);
+  void apply_knobs();
   void set_stream(cudaStream_t s);
   ocu_status do_fmg(double tol, int max_iter, double *l2, double *linf);
   ocu_status do_vcycle(double tol, int max_iter, double *l2, double *linf);
+  ocu_status cycle(CoreOps *c, int fine_level, double tol, double *l2, double *linf, bool *converged);
+  ocu_status ir_residual(double *l2, double *linf);
   ocu_status mixed_warmstart_fmg(double tol, int max_iter, double *l2, double *linf);
   ocu_status ir_solve(double tol, int max_outer, double *l2, double *linf);
   ocu_status fmg_dispatch(double tol, int max_iter, double *l2, double *linf);

@@ -24,6 +24,8 @@ ocu_status check_cuda(cudaError_t e, const char *what);
 ocu_status check_launch(const char *what);
 void count_launch(int n = 1);
 unsigned long long launch_count();
+void set_capturing(bool on);
+unsigned long long launch_count_captured();
 const char *last_error_text();
 
 inline size_t dtype_size(ocu_dtype d) { return d == OCU_F64 ? 8 : 4; }

@@ -460,6 +460,37 @@ int orc_mg_run_fmg(orc_mg *m, int count)
   return 1;
 }
 
+/* Level operations on one hierarchy (core 0 = interface precision, 1 = FP32 hierarchy). */
+static int core_is_f(const orc_mg *m, int core) { return core == 1 || m->kind == ORC_KIND_F; }
+
+int orc_mg_relax(orc_mg *m, int core, int level, int iterations, int order)
+{
+  if (core_is_f(m, core)) core_relax_f(m->cf, level, iterations, order);
+  else core_relax_d(m->cd, level, iterations, order);
+  return 1;
+}
+
+int orc_mg_relax_sweep(orc_mg *m, int core, int level, int color)
+{
+  if (core_is_f(m, core)) core_relax_color_f(m->cf, level, color & 1);
+  else core_relax_color_d(m->cd, level, color & 1);
+  return 1;
+}
+
+int orc_mg_restrict_residuals(orc_mg *m, int core, int fine, int coarse, double *l2, double *linf)
+{
+  if (core_is_f(m, core)) core_restrict_residuals_f(m->cf, fine, coarse, l2, linf);
+  else core_restrict_residuals_d(m->cd, fine, coarse, l2, linf);
+  return 1;
+}
+
+int orc_mg_prolong(orc_mg *m, int core, int coarse, int fine)
+{
+  if (core_is_f(m, core)) core_prolong_bc_f(m->cf, coarse, fine);
+  else core_prolong_bc_d(m->cd, coarse, fine);
+  return 1;
+}
+
 int orc_mg_num_levels(const orc_mg *m) { return m->num_levels; }
 int orc_mg_vcycles(const orc_mg *m) { return m->last_vcycles; }
 int orc_mgir_outer_iterations(const orc_mg *m) { return m->outer_iters; }

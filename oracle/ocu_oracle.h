@@ -90,6 +90,12 @@ int orc_mg_solve(orc_mg *mg, double *residual, double tolerance, int max_iter);
 int orc_mg_run_vcycles(orc_mg *mg, int count);  /* sol_mgpressure3d.cpp:372-384 */
 int orc_mg_run_fmg(orc_mg *mg, int count);      /* sol_mgpressure3d.cpp:386-398 */
 int orc_mg_num_levels(const orc_mg *mg);
+/* Level operations (relax, one colour sweep, restrict_residuals, prolong+BC) on the interface
+ * hierarchy (core 0) or the FP32 hierarchy of a mixed solver (core 1). */
+int orc_mg_relax(orc_mg *mg, int core, int level, int iterations, int order);
+int orc_mg_relax_sweep(orc_mg *mg, int core, int level, int color);
+int orc_mg_restrict_residuals(orc_mg *mg, int core, int fine, int coarse, double *l2, double *linf);
+int orc_mg_prolong(orc_mg *mg, int core, int coarse, int fine);
 /* which: 'u', 'b', 'r'.  Returns the level's buffer (host memory owned by the oracle). */
 void *orc_mg_grid(orc_mg *mg, char which, int level, ocu_layout *layout_out);
 int orc_mg_vcycles(const orc_mg *mg); /* fine-level cycles run by the last do_fmg */

@@ -101,6 +101,10 @@ def _setup(L):
     L.orc_mg_run_vcycles.argtypes = [P, i]
     L.orc_mg_run_fmg.argtypes = [P, i]
     L.orc_mg_num_levels.argtypes = [P]
+    L.orc_mg_relax.argtypes = [P, i, i, i, i]
+    L.orc_mg_relax_sweep.argtypes = [P, i, i, i]
+    L.orc_mg_restrict_residuals.argtypes = [P, i, i, i, C.POINTER(d), C.POINTER(d)]
+    L.orc_mg_prolong.argtypes = [P, i, i, i]
     L.orc_mg_grid.argtypes = [P, C.c_char, i, LP]
     L.orc_mg_grid.restype = P
     L.orc_mg_vcycles.argtypes = [P]

@@ -384,8 +384,10 @@ def test_ns_steps(dt, scheme, ts):
         dt_o = O.lib().orc_ns_get_max_stable_timestep(on)
         dt_d = eq.get_max_stable_timestep()
         assert dt_o == dt_d
-        O.lib().orc_ns_advance_one_step(on, dt_o)
-        eq.advance_one_step(dt_d)
+        ok_o = bool(O.lib().orc_ns_advance_one_step(on, dt_o))
+        ok_d = eq.advance_one_step(dt_d)
+        # FP32 cannot always reach an absolute 1e-5 divergence; both sides must agree on it
+        assert ok_o == ok_d
     for c, get in zip("uvwt", (eq.get_u, eq.get_v, eq.get_w, eq.get_temperature)):
         ref = O.wrap(O.lib().orc_ns_grid(on, c.encode()), Ls[c], dt)
         assert_same(get().copy_to_host(), ref, f"ns {c}")
