@@ -55,7 +55,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -195,20 +195,22 @@ def run_gpu(args):
         torch.cuda.synchronize()
         barrier(world)
         torch.cuda.synchronize()
+        if sampler:
+            sampler.__enter__()
+            time.sleep(0.25)  # let the sampler emit before the timed region starts
         n0 = ocu.kernel_launch_count()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        if sampler:
-            sampler.__enter__()
         for _ in range(steps):
             fn()
         e1.record(stream)
         torch.cuda.synchronize()
+        n1 = ocu.kernel_launch_count()
         if sampler:
             sampler.__exit__(None, None, None)
         barrier(world)
         ms = e0.elapsed_time(e1) / steps
-        return max_over_ranks(ms, world), ocu.kernel_launch_count() - n0
+        return max_over_ranks(ms, world), n1 - n0
 
     sampler = ClockSampler(local)
     res_holder = {}
@@ -425,7 +427,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ir-inner", type=int, default=3)

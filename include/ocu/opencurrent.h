@@ -351,6 +351,9 @@ class Sol_ProjectDivergence3DDevice : public ErrorHandler {
   Grid3DDevice<T> &divergence() { return _div; }
 };
 
+typedef Sol_ProjectDivergence3DDevice<float> Sol_ProjectDivergence3DDeviceF;
+typedef Sol_ProjectDivergence3DDevice<double> Sol_ProjectDivergence3DDeviceD;
+
 template <typename T>
 class Sol_SelfAdvection3DDevice : public ErrorHandler {
   int _nx = 0, _ny = 0, _nz = 0;

@@ -390,8 +390,10 @@ static double pick(int conv, double l2, double linf) {
 // ------------------------------------------------------------------------------------------
 MGSolver::~MGSolver() {
   clear_graphs();
+  if (stream) cudaStreamSynchronize(stream);
   if (pressure) { cudaFree(pressure->buf); delete pressure; }
   if (rhs_f) { cudaFree(rhs_f->buf); delete rhs_f; }
+  if (own_stream) cudaStreamDestroy(own_stream);
 }
 
 void MGSolver::clear_graphs() {
@@ -779,6 +781,7 @@ ocu_status MGSolver::run_fmg(int count) {
 
 ocu_status MGSolver::initialize_storage(int nx, int ny, int nz, double hx, double hy, double hz, ocu_grid *rhs) {
   if (initialized) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] initialize_storage - already initialized");
+  if (!stream) set_stream(nullptr);
   if (!check_float((float)hx) || !check_float((float)hy) || !check_float((float)hz))
     return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_MultigridPressure3DBase::initialize_storage - garbage hx,hy,hz value %f %f %f", hx, hy, hz);
   if (!rhs) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] initialize_storage - null rhs");
@@ -837,7 +840,14 @@ ocu_status MGSolver::set_params(const ocu_mg_params &p) {
   return OCU_OK;
 }
 
+// Work runs on the caller's stream.  The legacy default stream (NULL) cannot be captured into a
+// graph, so for NULL the solver uses a private blocking stream, which the legacy stream orders
+// against implicitly in both directions -- the same semantics as issuing on NULL.
 void MGSolver::set_stream(cudaStream_t s) {
+  if (!s) {
+    if (!own_stream) cudaStreamCreate(&own_stream);
+    s = own_stream;
+  }
   stream = s;
   cf.stream = s;
   cd.stream = s;

@@ -109,6 +109,7 @@ struct MGSolver {
   };
   std::unique_ptr<ocu_grid, GridDeleter> pressure_f;  // FP32 u0 of the mixed solvers
   cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;  // used when the caller's stream is the legacy NULL stream
   ocu_mg_stats stats{};
   struct GraphEntry {
     cudaGraphExec_t exec = nullptr;

@@ -1,0 +1,176 @@
+// The reference's own test flow, written against the C++ drop-in facade (include/ocu/opencurrent.h):
+//   - run_all_dirichelet_test (tests/mgdoubletest.cpp:199-227): zero RHS, Dirichlet v => p == v
+//   - run_neumann_test (tests/mgtest.cpp): FP32 Neumann solve reaches the tolerance
+//   - ProjectTest (tests/projecttest.cpp:27-136): sine velocity field, max |div| <= 2e-4 after
+//     projection
+//   - NSTest-style smoke (tests/nstest.cpp): a few Boussinesq steps stay finite
+// Prints "FACADE OK" and exits 0 when every check passes.
+#include <cmath>
+#include <cstdio>
+
+#include "ocu/opencurrent.h"
+
+using namespace ocu;
+
+static int failures = 0;
+#define REQUIRE(c)                                                \
+  do {                                                            \
+    if (!(c)) {                                                   \
+      std::printf("REQUIRE FAILED %s:%d: %s\n", __FILE__, __LINE__, #c); \
+      failures++;                                                 \
+      return;                                                     \
+    }                                                             \
+  } while (0)
+#define CHECK(c)                                                  \
+  do {                                                            \
+    if (!(c)) {                                                   \
+      std::printf("CHECK FAILED %s:%d: %s\n", __FILE__, __LINE__, #c); \
+      failures++;                                                 \
+    }                                                             \
+  } while (0)
+
+static void all_dirichlet(double value) {
+  const int n = 32;
+  Grid3DDeviceD rhs;
+  REQUIRE(rhs.init(n, n, n, 1, 1, 1));
+  CHECK(rhs.clear_zero());
+  Sol_MultigridPressure3DDeviceD solver;
+  BoundaryCondition d;
+  d.type = BC_DIRICHELET;
+  d.value = (float)value;
+  solver.bc = BoundaryConditionSet(d);
+  REQUIRE(solver.initialize_storage(n, n, n, 4.0 / n, 4.0 / n, 4.0 / n, &rhs));
+  Grid3DHostD init;
+  init.init_congruent(solver.pressure());
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+      for (int k = 0; k < n; k++) init.at(i, j, k) = 0.5 - std::fmod(0.618033988749 * (i * n * n + j * n + k), 1.0);
+  CHECK(solver.pressure().copy_all_data(init));
+  double residual = 0;
+  CHECK(solver.solve(residual, 1e-8, 15));
+  CHECK(residual < 1e-8);
+  double mx = 0, mn = 0;
+  CHECK(solver.pressure().reduce_max(mx));
+  CHECK(solver.pressure().reduce_min(mn));
+  CHECK(std::fabs(mx - value) < 1e-7 && std::fabs(mn - value) < 1e-7);
+}
+
+static void neumann_fp32() {
+  const int n = 64;
+  Grid3DHostF h;
+  h.init(n, n, n, 1, 1, 1);
+  double mean = 0;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+      for (int k = 0; k < n; k++) {
+        const double x = (i + 0.5) / n, y = (j + 0.5) / n, z = (k + 0.5) / n;
+        mean += std::cos(M_PI * x) * std::cos(2 * M_PI * y) * std::cos(3 * M_PI * z);
+      }
+  mean /= (double)n * n * n;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+      for (int k = 0; k < n; k++) {
+        const double x = (i + 0.5) / n, y = (j + 0.5) / n, z = (k + 0.5) / n;
+        h.at(i, j, k) = (float)(std::cos(M_PI * x) * std::cos(2 * M_PI * y) * std::cos(3 * M_PI * z) - mean);
+      }
+  Grid3DDeviceF rhs;
+  REQUIRE(rhs.init_congruent(h));
+  CHECK(rhs.copy_all_data(h));
+  Sol_MultigridPressure3DDeviceF solver;
+  BoundaryCondition neu;
+  neu.type = BC_NEUMANN;
+  solver.bc = BoundaryConditionSet(neu);
+  REQUIRE(solver.initialize_storage(n, n, n, 1.0 / n, 1.0 / n, 1.0 / n, &rhs));
+  double residual = 0;
+  CHECK(solver.solve(residual, 1e-4, 10));
+  CHECK(residual < 1e-4);
+  CHECK(!solver.any_error());
+}
+
+static void projection() {
+  const int nx = 64, ny = 32, nz = 32;
+  const double hx = .5, hy = .5, hz = 1;
+  Grid3DDeviceF u, v, w;
+  REQUIRE(u.init(nx + 1, ny, nz, 1, 1, 1, 0, 1, 1));
+  REQUIRE(v.init(nx, ny + 1, nz, 1, 1, 1, 1, 0, 1));
+  REQUIRE(w.init(nx, ny, nz + 1, 1, 1, 1, 1, 1, 0));
+  Grid3DHostF hu, hv, hw;
+  hu.init_congruent(u);
+  hv.init_congruent(v);
+  hw.init_congruent(w);
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++)
+      for (int k = 0; k < nz; k++) {
+        hu.at(i, j, k) = std::sin(((float)k) / nz * 4 * M_PI) + std::sin(((float)j) / ny * 4 * M_PI);
+        hv.at(i, j, k) = std::sin(((float)k) / nz * 8 * M_PI) + std::sin(((float)i) / nx * 6 * M_PI);
+        hw.at(i, j, k) = std::cos(((float)j) / ny * 8 * M_PI) + std::sin(((float)k) / nz * 6 * M_PI);
+      }
+  CHECK(u.copy_all_data(hu));
+  CHECK(v.copy_all_data(hv));
+  CHECK(w.copy_all_data(hw));
+  Sol_ProjectDivergence3DDeviceF project;
+  BoundaryCondition closed;
+  closed.type = BC_FORCED_INFLOW_VARIABLE_SLIP;
+  BoundaryCondition periodic;
+  periodic.type = BC_PERIODIC;
+  project.bc = BoundaryConditionSet(periodic);
+  project.bc.zpos = closed;
+  project.bc.zneg = closed;
+  CHECK(apply_3d_mac_boundary_conditions_level1(u, v, w, project.bc, hx, hy, hz));
+  CHECK(project.initialize_storage(nx, ny, nz, hx, hy, hz, &u, &v, &w));
+  CHECK(project.solve(2e-4));
+  CHECK(project.solve_divergence_only());
+  float max_div = 1;
+  CHECK(project.divergence().reduce_maxabs(max_div));
+  CHECK(max_div <= 2e-4f);
+}
+
+static void ns_smoke() {
+  Eqn_IncompressibleNS3DParamsD params;
+  params.init_grids(32, 32, 16);
+  params.hx = params.hy = params.hz = 1.0 / 16;
+  BoundaryCondition periodic, wall, hot, cold;
+  periodic.type = BC_PERIODIC;
+  wall.type = BC_FORCED_INFLOW_VARIABLE_SLIP;
+  wall.aux_value = 1;
+  hot.type = BC_DIRICHELET;
+  hot.value = 1;
+  cold.type = BC_DIRICHELET;
+  params.flow_bc = BoundaryConditionSet(periodic);
+  params.flow_bc.zpos = wall;
+  params.flow_bc.zneg = wall;
+  params.temp_bc = BoundaryConditionSet(periodic);
+  params.temp_bc.zpos = cold;
+  params.temp_bc.zneg = hot;
+  params.vertical_direction = DIR_ZPOS;
+  params.gravity = -1;
+  params.bouyancy = 2000;
+  params.viscosity = 1;
+  params.thermal_diffusion = 1;
+  params.max_divergence = 1e-9;
+  for (int i = 0; i < 32; i++)
+    for (int j = 0; j < 32; j++)
+      for (int k = 0; k < 16; k++)
+        params.init_temp.at(i, j, k) = 1 - (k + .5) / 16 + 1e-3 * std::sin(0.7 * i + 1.3 * j);
+  Eqn_IncompressibleNS3DD eqn;
+  REQUIRE(eqn.set_parameters(params));
+  for (int s = 0; s < 5; s++) CHECK(eqn.advance_one_step(eqn.get_max_stable_timestep()));
+  double tmax = 0;
+  CHECK(eqn.get_temperature().reduce_maxabs(tmax));
+  CHECK(std::isfinite(tmax) && tmax <= 1.0 + 1e-2);
+  CHECK(eqn.num_steps() == 5);
+}
+
+int main() {
+  all_dirichlet(0.0);
+  all_dirichlet(0.5);
+  neumann_fp32();
+  projection();
+  ns_smoke();
+  if (failures) {
+    std::printf("FACADE FAILED (%d)\n", failures);
+    return 1;
+  }
+  std::printf("FACADE OK\n");
+  return 0;
+}
