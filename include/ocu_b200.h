@@ -82,6 +82,23 @@ ocu_status ocu_grid_linear_combination(ocu_grid *result, double alpha1, const oc
 /* reduce_* (grid3dops.cu:26-130): same fold order as the reference; blocks the host. */
 ocu_status ocu_grid_reduce(const ocu_grid *g, ocu_reduce_op op, double *result, ocu_stream s);
 
+/* Largest number of 256-row blocks ocu_grid_reduce_noalloc can fold: grids with
+ * nx*ny <= 256 * OCU_REDUCE_NOALLOC_MAX_BLOCKS (1,048,576 rows, e.g. 1024 x 1024 planes). */
+#define OCU_REDUCE_NOALLOC_MAX_BLOCKS 4096
+/* ocu_grid_reduce without any device allocation.  (No counterpart in the reference: it exists
+ * for callers that must not allocate device memory when they ask for a norm -- a host whose
+ * allocator already owns the whole device, a plugin host that reserves all memory up front and
+ * forbids later allocations, or a latency-critical loop that must stay off the allocator.)
+ * Same result as ocu_grid_reduce, bit for bit.  Its scratch is one static array in the
+ * library's device image (about 33 KB, held on every GPU that loads the library until the
+ * process exits); larger grids than the limit above are rejected with OCU_ERR_INVALID_VALUE.
+ * All calls on a device share that array and it keeps the previous call's contents (each call
+ * clears what must start at zero), so calls that overlap on the GPU -- other streams or host
+ * threads without ordering between them -- race and must be serialised by the caller.  The
+ * first call on a device looks up the array's device address while that device is current;
+ * make that first call before any stream capture.  Blocks the host until the result is back. */
+ocu_status ocu_grid_reduce_noalloc(const ocu_grid *g, ocu_reduce_op op, double *result, ocu_stream s);
+
 /* ---- ghost cells (ocustorage/grid3dboundary.h:26-70) --------------------------------- */
 /* apply_3d_boundary_conditions_level1 (variant OCU_BC_LEVEL1, one launch instead of three)
  * and ..._level1_nocorners (OCU_BC_LEVEL1_NOCORNERS). */

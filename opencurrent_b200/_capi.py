@@ -92,6 +92,7 @@ SIGNATURES = {
     "ocu_grid_clear": (I, [P, D, P]),
     "ocu_grid_linear_combination": (I, [P, D, P, D, P, P]),
     "ocu_grid_reduce": (I, [P, I, C.POINTER(D), P]),
+    "ocu_grid_reduce_noalloc": (I, [P, I, C.POINTER(D), P]),
     "ocu_apply_boundary_conditions": (I, [P, BP, D, D, D, I, P]),
     "ocu_apply_mac_boundary_conditions": (I, [P, P, P, BP, D, D, D, P]),
     "ocu_divergence": (I, [P, P, P, P, I, I, I, D, D, D, P]),
