@@ -38,8 +38,8 @@ struct Level1Compose {
     if (i >= 0 && i < nx) return mem(i, j, k);
     const bool neg = i < 0;
     const int f = neg ? FX_NEG : FX_POS;
-    const int t = bc.type[f];
-    const float v = bc.value[f];
+    const int t = bc.ty(f);
+    const float v = bc.val(f);
     if (t == OCU_BC_PERIODIC) return mem(neg ? nx - 1 : 0, j, k);
     if (t == OCU_BC_DIRICHELET) return dir(mem(neg ? 0 : nx - 1, j, k), v);
     if (t == OCU_BC_NEUMANN) return neg ? mem(0, j, k) - hx * (T)v : mem(nx - 1, j, k) + hx * (T)v;
@@ -50,8 +50,8 @@ struct Level1Compose {
     if (j >= 0 && j < ny) return ax(i, j, k);
     const bool neg = j < 0;
     const int f = neg ? FY_NEG : FY_POS;
-    const int t = bc.type[f];
-    const float v = bc.value[f];
+    const int t = bc.ty(f);
+    const float v = bc.val(f);
     if (t == OCU_BC_PERIODIC) return ax(i, neg ? ny - 1 : 0, k);
     if (t == OCU_BC_DIRICHELET) return dir(ax(i, neg ? 0 : ny - 1, k), v);
     if (t == OCU_BC_NEUMANN) return neg ? ax(i, 0, k) - hy * (T)v : ax(i, ny - 1, k) + hy * (T)v;
@@ -62,8 +62,8 @@ struct Level1Compose {
     if (k >= 0 && k < nz) return ay(i, j, k);
     const bool neg = k < 0;
     const int f = neg ? FZ_NEG : FZ_POS;
-    const int t = bc.type[f];
-    const float v = bc.value[f];
+    const int t = bc.ty(f);
+    const float v = bc.val(f);
     if (t == OCU_BC_PERIODIC) return ay(i, j, neg ? nz - 1 : 0);
     if (t == OCU_BC_DIRICHELET) return dir(ay(i, j, neg ? 0 : nz - 1), v);
     if (t == OCU_BC_NEUMANN) return neg ? ay(i, j, 0) - hz * (T)v : ay(i, j, nz - 1) + hz * (T)v;
@@ -84,21 +84,21 @@ __device__ void level1_fill_block(T *u, long long xs, long long ys, int nx, int 
     int r = q;
     if (r < zr) {
       const int per = (nx + 2) * (ny + 2), side = r / per, i = (r % per) / (ny + 2) - 1, j = (r % per) % (ny + 2) - 1;
-      if (Level1Compose<T>::writes(bc.type[side ? FZ_POS : FZ_NEG]))
+      if (Level1Compose<T>::writes(bc.ty(side ? FZ_POS : FZ_NEG)))
         u[(long long)i * xs + (long long)j * ys + (side ? nz : -1)] = lc.az(i, j, side ? nz : -1);
       continue;
     }
     r -= zr;
     if (r < yr) {
       const int per = (nx + 2) * nz, side = r / per, i = (r % per) / nz - 1, k = (r % per) % nz;
-      if (Level1Compose<T>::writes(bc.type[side ? FY_POS : FY_NEG]))
+      if (Level1Compose<T>::writes(bc.ty(side ? FY_POS : FY_NEG)))
         u[(long long)i * xs + (long long)(side ? ny : -1) * ys + k] = lc.ay(i, side ? ny : -1, k);
       continue;
     }
     r -= yr;
     {
       const int per = ny * nz, side = r / per, j = (r % per) / nz, k = (r % per) % nz;
-      if (Level1Compose<T>::writes(bc.type[side ? FX_POS : FX_NEG]))
+      if (Level1Compose<T>::writes(bc.ty(side ? FX_POS : FX_NEG)))
         u[(long long)(side ? nx : -1) * xs + (long long)j * ys + k] = lc.ax(side ? nx : -1, j, k);
     }
   }

@@ -25,41 +25,49 @@ struct GhostEmit {
   BCDev bc;
   T hx, hy, hz;
 
-  __device__ __forceinline__ int targets(int c, int n, int fneg, int fpos, int *idx, int *face) const {
-    int m = 0;
-    const int tn = bc.type[fneg], tp = bc.type[fpos];
-    if ((tn == OCU_BC_DIRICHELET || tn == OCU_BC_NEUMANN) && c == 0) { idx[m] = -1; face[m] = fneg; m++; }
-    else if (tn == OCU_BC_PERIODIC && c == n - 1) { idx[m] = -1; face[m] = fneg; m++; }
-    if ((tp == OCU_BC_DIRICHELET || tp == OCU_BC_NEUMANN) && c == n - 1) { idx[m] = n; face[m] = fpos; m++; }
-    else if (tp == OCU_BC_PERIODIC && c == 0) { idx[m] = n; face[m] = fpos; m++; }
-    return m;
+  // Does the negative (resp. positive) face of an axis take coordinate c as a ghost source?
+  __device__ __forceinline__ bool src_neg(int t, int c, int n) const {
+    return ((t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN) && c == 0) || (t == OCU_BC_PERIODIC && c == n - 1);
+  }
+  __device__ __forceinline__ bool src_pos(int t, int c, int n) const {
+    return ((t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN) && c == n - 1) || (t == OCU_BC_PERIODIC && c == 0);
   }
 
   // face ids: odd = negative side (FX_NEG = 1, FY_NEG = 3, FZ_NEG = 5)
-  __device__ __forceinline__ T rule(int f, T src, T h) const {
-    const int t = bc.type[f];
-    const float v = bc.value[f];
+  template <int F>
+  __device__ __forceinline__ T rule(T src, T h) const {
+    const int t = bc.type[F];
+    const float v = bc.value[F];
     if (t == OCU_BC_PERIODIC) return src;
     if (t == OCU_BC_DIRICHELET) return -src + (T)(2 * v);
-    return (f & 1) ? src - h * (T)v : src + h * (T)v;
+    return (F & 1) ? src - h * (T)v : src + h * (T)v;
   }
 
+  // Writes every ghost whose source is (i,j,k): per axis the candidates are the cell itself,
+  // the negative-face ghost and the positive-face ghost, composed x -> y -> z.  The loops are
+  // fully unrolled so every face index is a constant (per-thread local arrays, or a face index
+  // known only at run time, would put the struct in local memory for every thread).
   __device__ __forceinline__ void emit(int i, int j, int k, T val) const {
     if (i > 0 && i < nx - 1 && j > 0 && j < ny - 1 && k > 0 && k < nz - 1) return;
-    int xi[3], xf[3], yi[3], yf[3], zi[3], zf[3];
-    xi[0] = i; yi[0] = j; zi[0] = k;
-    xf[0] = yf[0] = zf[0] = 0;
-    const int mx = 1 + targets(i, nx, FX_NEG, FX_POS, xi + 1, xf + 1);
-    const int my = 1 + targets(j, ny, FY_NEG, FY_POS, yi + 1, yf + 1);
-    const int mz = 1 + targets(k, nz, FZ_NEG, FZ_POS, zi + 1, zf + 1);
-    for (int a = 0; a < mx; a++) {
-      const T vx = a ? rule(xf[a], val, hx) : val;
-      for (int b = 0; b < my; b++) {
-        const T vy = b ? rule(yf[b], vx, hy) : vx;
-        for (int c = 0; c < mz; c++) {
+    const bool x1 = src_neg(bc.type[FX_NEG], i, nx), x2 = src_pos(bc.type[FX_POS], i, nx);
+    const bool y1 = src_neg(bc.type[FY_NEG], j, ny), y2 = src_pos(bc.type[FY_POS], j, ny);
+    const bool z1 = src_neg(bc.type[FZ_NEG], k, nz), z2 = src_pos(bc.type[FZ_POS], k, nz);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      if ((a == 1 && !x1) || (a == 2 && !x2)) continue;
+      const T vx = a == 0 ? val : a == 1 ? rule<FX_NEG>(val, hx) : rule<FX_POS>(val, hx);
+      const long long ox = (long long)(a == 0 ? i : a == 1 ? -1 : nx) * xs;
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        if ((b == 1 && !y1) || (b == 2 && !y2)) continue;
+        const T vy = b == 0 ? vx : b == 1 ? rule<FY_NEG>(vx, hy) : rule<FY_POS>(vx, hy);
+        const long long oy = ox + (long long)(b == 0 ? j : b == 1 ? -1 : ny) * ys;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
           if (a == 0 && b == 0 && c == 0) continue;
-          const T vz = c ? rule(zf[c], vy, hz) : vy;
-          p[(long long)xi[a] * xs + (long long)yi[b] * ys + zi[c]] = vz;
+          if ((c == 1 && !z1) || (c == 2 && !z2)) continue;
+          const T vz = c == 0 ? vy : c == 1 ? rule<FZ_NEG>(vy, hz) : rule<FZ_POS>(vy, hz);
+          p[oy + (c == 0 ? k : c == 1 ? -1 : nz)] = vz;
         }
       }
     }

@@ -20,7 +20,7 @@ __global__ void __launch_bounds__(256) k_bc_level1(Level1Compose<T> c, long long
     const long long r = t - side * per;
     const int i = (int)(r / (ny + 2)) - 1, j = (int)(r % (ny + 2)) - 1;
     const int k = side ? nz : -1;
-    if (Level1Compose<T>::writes(c.bc.type[side ? FZ_POS : FZ_NEG]))
+    if (Level1Compose<T>::writes(c.bc.ty(side ? FZ_POS : FZ_NEG)))
       c.p[(long long)i * c.xs + (long long)j * c.ys + k] = c.az(i, j, k);
     return;
   }
@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(256) k_bc_level1(Level1Compose<T> c, long long
     const long long r = t - side * per;
     const int i = (int)(r / nz) - 1, k = (int)(r % nz);
     const int j = side ? ny : -1;
-    if (Level1Compose<T>::writes(c.bc.type[side ? FY_POS : FY_NEG]))
+    if (Level1Compose<T>::writes(c.bc.ty(side ? FY_POS : FY_NEG)))
       c.p[(long long)i * c.xs + (long long)j * c.ys + k] = c.ay(i, j, k);
     return;
   }
@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(256) k_bc_level1(Level1Compose<T> c, long long
     const long long r = t - side * per;
     const int j = (int)(r / nz), k = (int)(r % nz);
     const int i = side ? nx : -1;
-    if (Level1Compose<T>::writes(c.bc.type[side ? FX_POS : FX_NEG]))
+    if (Level1Compose<T>::writes(c.bc.ty(side ? FX_POS : FX_NEG)))
       c.p[(long long)i * c.xs + (long long)j * c.ys + k] = c.ax(i, j, k);
   }
 }
@@ -78,9 +78,9 @@ ocu_status launch_bc_level1(T *origin, const ocu_layout &L, const ocu_bc_set &bc
 // ------------------------------------------------------------------------------------------
 template <typename T>
 __device__ __forceinline__ T nocorner_rule(const BCDev &bc, int f, T src, T h, bool neg) {
-  const int t = bc.type[f];
-  if (t == OCU_BC_DIRICHELET) return (T)((double)(-src) + 2.0 * (double)(T)bc.value[f]);
-  if (t == OCU_BC_NEUMANN) return neg ? src - h * (T)bc.value[f] : src + h * (T)bc.value[f];
+  const int t = bc.ty(f);
+  if (t == OCU_BC_DIRICHELET) return (T)((double)(-src) + 2.0 * (double)(T)bc.val(f));
+  if (t == OCU_BC_NEUMANN) return neg ? src - h * (T)bc.val(f) : src + h * (T)bc.val(f);
   return src;  // periodic: the caller passed the wrapped source
 }
 
@@ -95,7 +95,7 @@ __global__ void __launch_bounds__(256) k_bc_nocorners(T *p, long long xs, long l
     const long long r = t - side * (long long)nx * ny;
     const int i = (int)(r / ny), j = (int)(r % ny);
     const int f = side ? FZ_POS : FZ_NEG;
-    const int ty = bc.type[f];
+    const int ty = bc.ty(f);
     if (ty == OCU_BC_PERIODIC) at(i, j, side ? nz : -1) = at(i, j, side ? 0 : nz - 1);
     else if (ty == OCU_BC_DIRICHELET || ty == OCU_BC_NEUMANN)
       at(i, j, side ? nz : -1) = nocorner_rule<T>(bc, f, at(i, j, side ? nz - 1 : 0), hz, !side);
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(256) k_bc_nocorners(T *p, long long xs, long l
     const long long r = t - side * (long long)nx * nz;
     const int i = (int)(r / nz), k = (int)(r % nz);
     const int f = side ? FY_POS : FY_NEG;
-    const int ty = bc.type[f];
+    const int ty = bc.ty(f);
     if (ty == OCU_BC_PERIODIC) at(i, side ? ny : -1, k) = at(i, side ? 0 : ny - 1, k);
     else if (ty == OCU_BC_DIRICHELET || ty == OCU_BC_NEUMANN)
       at(i, side ? ny : -1, k) = nocorner_rule<T>(bc, f, at(i, side ? ny - 1 : 0, k), hy, !side);
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(256) k_bc_nocorners(T *p, long long xs, long l
     const long long r = t - side * (long long)ny * nz;
     const int j = (int)(r / nz), k = (int)(r % nz);
     const int f = side ? FX_POS : FX_NEG;
-    const int ty = bc.type[f];
+    const int ty = bc.ty(f);
     if (ty == OCU_BC_PERIODIC) at(side ? nx : -1, j, k) = at(side ? 0 : nx - 1, j, k);
     else if (ty == OCU_BC_DIRICHELET || ty == OCU_BC_NEUMANN)
       at(side ? nx : -1, j, k) = nocorner_rule<T>(bc, f, at(side ? nx - 1 : 0, j, k), hx, !side);
@@ -152,26 +152,26 @@ __global__ void k_mac_bc_x(T *u, T *v, T *w, BCDev bc, long long xs, long long y
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (j >= ny || k >= nz) return;
   auto I = [&](int i) { return (long long)i * xs + (long long)j * ys + k; };
-  if (bc.type[FX_NEG] == OCU_BC_PERIODIC) {
+  if (bc.ty(FX_NEG) == OCU_BC_PERIODIC) {
     u[I(-1)] = u[I(nx - 1)];
     v[I(-1)] = v[I(nx - 1)];
     w[I(-1)] = w[I(nx - 1)];
-  } else if (bc.type[FX_NEG] == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
-    const float f = 1.0f - 2.0f * bc.aux[FX_NEG];
-    u[I(-1)] = (T)bc.value[FX_NEG];
-    u[I(0)] = (T)bc.value[FX_NEG];
+  } else if (bc.ty(FX_NEG) == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
+    const float f = 1.0f - 2.0f * bc.auxv(FX_NEG);
+    u[I(-1)] = (T)bc.val(FX_NEG);
+    u[I(0)] = (T)bc.val(FX_NEG);
     v[I(-1)] = v[I(0)] * (T)f;
     w[I(-1)] = w[I(0)] * (T)f;
   }
-  if (bc.type[FX_POS] == OCU_BC_PERIODIC) {
+  if (bc.ty(FX_POS) == OCU_BC_PERIODIC) {
     u[I(nx)] = u[I(0)];
     u[I(nx + 1)] = u[I(1)];
     v[I(nx)] = v[I(0)];
     w[I(nx)] = w[I(0)];
-  } else if (bc.type[FX_POS] == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
-    const float f = 1.0f - 2.0f * bc.aux[FX_POS];
-    u[I(nx)] = (T)bc.value[FX_POS];
-    u[I(nx + 1)] = (T)bc.value[FX_POS];
+  } else if (bc.ty(FX_POS) == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
+    const float f = 1.0f - 2.0f * bc.auxv(FX_POS);
+    u[I(nx)] = (T)bc.val(FX_POS);
+    u[I(nx + 1)] = (T)bc.val(FX_POS);
     v[I(nx)] = v[I(nx - 1)] * (T)f;
     w[I(nx)] = w[I(nx - 1)] * (T)f;
   }
@@ -183,26 +183,26 @@ __global__ void k_mac_bc_y(T *u, T *v, T *w, BCDev bc, long long xs, long long y
   const int i = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 1;
   if (i > nx || k >= nz) return;
   auto J = [&](int j) { return (long long)i * xs + (long long)j * ys + k; };
-  if (bc.type[FY_NEG] == OCU_BC_PERIODIC) {
+  if (bc.ty(FY_NEG) == OCU_BC_PERIODIC) {
     v[J(-1)] = v[J(ny - 1)];
     u[J(-1)] = u[J(ny - 1)];
     w[J(-1)] = w[J(ny - 1)];
-  } else if (bc.type[FY_NEG] == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
-    const float f = 1.0f - 2.0f * bc.aux[FY_NEG];
-    v[J(-1)] = (T)bc.value[FY_NEG];
-    v[J(0)] = (T)bc.value[FY_NEG];
+  } else if (bc.ty(FY_NEG) == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
+    const float f = 1.0f - 2.0f * bc.auxv(FY_NEG);
+    v[J(-1)] = (T)bc.val(FY_NEG);
+    v[J(0)] = (T)bc.val(FY_NEG);
     u[J(-1)] = u[J(0)] * (T)f;
     w[J(-1)] = w[J(0)] * (T)f;
   }
-  if (bc.type[FY_POS] == OCU_BC_PERIODIC) {
+  if (bc.ty(FY_POS) == OCU_BC_PERIODIC) {
     v[J(ny)] = v[J(0)];
     v[J(ny + 1)] = v[J(1)];
     u[J(ny)] = u[J(0)];
     w[J(ny)] = w[J(0)];
-  } else if (bc.type[FY_POS] == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
-    const float f = 1.0f - 2.0f * bc.aux[FY_POS];
-    v[J(ny)] = (T)bc.value[FY_POS];
-    v[J(ny + 1)] = (T)bc.value[FY_POS];
+  } else if (bc.ty(FY_POS) == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
+    const float f = 1.0f - 2.0f * bc.auxv(FY_POS);
+    v[J(ny)] = (T)bc.val(FY_POS);
+    v[J(ny + 1)] = (T)bc.val(FY_POS);
     u[J(ny)] = u[J(ny - 1)] * (T)f;
     w[J(ny)] = w[J(ny - 1)] * (T)f;
   }
@@ -214,26 +214,26 @@ __global__ void k_mac_bc_z(T *u, T *v, T *w, BCDev bc, long long xs, long long y
   const int i = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 1;
   if (i > nx || j > ny) return;
   auto K = [&](int k) { return (long long)i * xs + (long long)j * ys + k; };
-  if (bc.type[FZ_NEG] == OCU_BC_PERIODIC) {
+  if (bc.ty(FZ_NEG) == OCU_BC_PERIODIC) {
     w[K(-1)] = w[K(nz - 1)];
     u[K(-1)] = u[K(nz - 1)];
     v[K(-1)] = v[K(nz - 1)];
-  } else if (bc.type[FZ_NEG] == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
-    const float f = 1.0f - 2.0f * bc.aux[FZ_NEG];
-    w[K(-1)] = (T)bc.value[FZ_NEG];
-    w[K(0)] = (T)bc.value[FZ_NEG];
+  } else if (bc.ty(FZ_NEG) == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
+    const float f = 1.0f - 2.0f * bc.auxv(FZ_NEG);
+    w[K(-1)] = (T)bc.val(FZ_NEG);
+    w[K(0)] = (T)bc.val(FZ_NEG);
     u[K(-1)] = u[K(0)] * (T)f;
     v[K(-1)] = v[K(0)] * (T)f;
   }
-  if (bc.type[FZ_POS] == OCU_BC_PERIODIC) {
+  if (bc.ty(FZ_POS) == OCU_BC_PERIODIC) {
     w[K(nz)] = w[K(0)];
     w[K(nz + 1)] = w[K(1)];
     u[K(nz)] = u[K(0)];
     v[K(nz)] = v[K(0)];
-  } else if (bc.type[FZ_POS] == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
-    const float f = 1.0f - 2.0f * bc.aux[FZ_POS];
-    w[K(nz)] = (T)bc.value[FZ_POS];
-    w[K(nz + 1)] = (T)bc.value[FZ_POS];
+  } else if (bc.ty(FZ_POS) == OCU_BC_FORCED_INFLOW_VARIABLE_SLIP) {
+    const float f = 1.0f - 2.0f * bc.auxv(FZ_POS);
+    w[K(nz)] = (T)bc.val(FZ_POS);
+    w[K(nz + 1)] = (T)bc.val(FZ_POS);
     u[K(nz)] = u[K(nz - 1)] * (T)f;
     v[K(nz)] = v[K(nz - 1)] * (T)f;
   }

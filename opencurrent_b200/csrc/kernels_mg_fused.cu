@@ -4,56 +4,20 @@
 //   - residual + norms (+ optional FP32 down-cast) for the level-0 checks and the refinement
 //     solver;
 //   - a single-CTA kernel that runs the coarse end of a V-cycle (all levels at or below a few
-//     thousand cells) with __syncthreads between phases instead of one launch per operation.
+//     thousand cells) with __syncthreads between phases instead of one launch per operation,
+//     staged in shared memory when the levels fit (about 200 KB).
 // Norm partials follow the reference fold order exactly (grid3dops.cu:26-130): for each fine
 // (i,j) row, lane t folds k = t, t+32, ... and the 32 lanes fold 16/8/4/2/1; rows are folded by
 // 256-wide trees (grid1dops.cu:33-115) in k_fold_rows.
+#include <atomic>
+
 #include "bc_device.cuh"
 #include "ghost_emit.cuh"
 #include "mg_fused.h"
 #include "ocu_internal.h"
+#include "relax_math.cuh"
 
 namespace ocub {
-
-template <typename T>
-__device__ __forceinline__ T relax_point(const T *__restrict__ u, const T *__restrict__ b, long long id, long long xs,
-                                         long long ys, int i, int j, int k, int nx, int ny, int nz,
-                                         const RelaxCoefD<T> &c, const T *__restrict__ diag) {
-  const T uc = u[id];
-  T res, dg;
-  if (sizeof(T) == 4) {
-    const T bv = b[id];
-    res = (-c.hsq * bv - c.ld * uc);
-    res += c.fz * (u[id - 1] + u[id + 1]);
-    res += c.fy * (u[id - ys] + u[id + ys]);
-    res += c.fx * (u[id - xs] + u[id + xs]);
-    dg = c.ld;
-    if (i == nx - 1) dg += c.xp;
-    if (i == 0) dg += c.xn;
-    if (j == ny - 1) dg += c.yp;
-    if (j == 0) dg += c.yn;
-    if (k == nz - 1) dg += c.zp;
-    if (k == 0) dg += c.zn;
-  } else {
-    res = -c.ld * uc;
-    res += c.fz * (u[id - 1] + u[id + 1]);
-    res += c.fy * (u[id - ys] + u[id + ys]);
-    res += c.fx * (u[id - xs] + u[id + xs]);
-    res += c.hsq * b[id];
-    if (diag) {
-      dg = diag[(long long)i * ny + j];
-    } else {  // same sequence the 2D table is built with (sol_mgpressure3ddev.cu:36-41)
-      dg = c.ld;
-      if (i == nx - 1) dg += c.xp;
-      if (i == 0) dg += c.xn;
-      if (j == ny - 1) dg += c.yp;
-      if (j == 0) dg += c.yn;
-    }
-    if (k == nz - 1) dg += c.zp;
-    if (k == 0) dg += c.zn;
-  }
-  return uc + c.omega * res / dg;
-}
 
 // Colour sweep + ghost writes: thread (t, j, i), k = 2t + parity.
 template <typename T>
@@ -93,37 +57,49 @@ __device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, long long
                                              T *__restrict__ uf, long long f, long long fxs, long long fys, int ic,
                                              int jc, int kc, const GhostEmit<T> *ge) {
   const T w1 = (T)0.421875, w2 = (T)0.140625, w3 = (T)0.046875, w4 = (T)0.015625;
-  const T c000 = uc[tc];
-  const T cp00 = uc[tc + cx], c0p0 = uc[tc + cy], cpp0 = uc[tc + cx + cy];
-  const T c00p = uc[tc + 1], cp0p = uc[tc + cx + 1], c0pp = uc[tc + cy + 1], cppp = uc[tc + cx + cy + 1];
-  const T cm00 = uc[tc - cx], c0m0 = uc[tc - cy], cmm0 = uc[tc - cx - cy], c00m = uc[tc - 1];
-  const T cm0m = uc[tc - cx - 1], c0mm = uc[tc - cy - 1], cmmm = uc[tc - cx - cy - 1];
-  const T cmp0 = uc[tc - cx + cy], cm0p = uc[tc - cx + 1], cpm0 = uc[tc + cx - cy];
-  const T c0mp = uc[tc - cy + 1], cp0m = uc[tc + cx - 1], c0pm = uc[tc + cy - 1];
-  const T cpmm = uc[tc + cx - cy - 1], cmpm = uc[tc - cx + cy - 1], cmmp = uc[tc - cx - cy + 1];
-  const T cppm = uc[tc + cx + cy - 1], cpmp = uc[tc + cx - cy + 1];
   const int i = 2 * ic + 1, j = 2 * jc + 1, k = 2 * kc + 1;
+  // all eight fine values are loaded before the first store: the ghost writes go through
+  // another pointer, so loads placed after a store could not be issued until it completed
+  const T f000 = uf[f], f100 = uf[f - fxs], f010 = uf[f - fys], f001 = uf[f - 1];
+  const T f110 = uf[f - fxs - fys], f101 = uf[f - fxs - 1], f011 = uf[f - fys - 1], f111 = uf[f - fxs - fys - 1];
+  const T c000 = uc[tc];
+  const T c0p0 = uc[tc + cy], c00p = uc[tc + 1], c0pp = uc[tc + cy + 1];
+  const T c0m0 = uc[tc - cy], c00m = uc[tc - 1], c0mm = uc[tc - cy - 1];
+  const T c0mp = uc[tc - cy + 1], c0pm = uc[tc + cy - 1];
   T v;
-  v = uf[f] + w1 * c000 + w2 * (cp00 + c0p0 + c00p) + w3 * (cpp0 + cp0p + c0pp) + w4 * cppp;
-  uf[f] = v; if (ge) ge->emit(i, j, k, v);
-  v = uf[f - fxs] + w1 * c000 + w2 * (cm00 + c0p0 + c00p) + w3 * (cmp0 + cm0p + c0pp) + w4 * cppp;
-  uf[f - fxs] = v; if (ge) ge->emit(i - 1, j, k, v);
-  v = uf[f - fys] + w1 * c000 + w2 * (cp00 + c0m0 + c00p) + w3 * (cpm0 + cp0p + c0mp) + w4 * cpmp;
-  uf[f - fys] = v; if (ge) ge->emit(i, j - 1, k, v);
-  v = uf[f - 1] + w1 * c000 + w2 * (cp00 + c0p0 + c00m) + w3 * (cpp0 + cp0m + c0pm) + w4 * cppm;
-  uf[f - 1] = v; if (ge) ge->emit(i, j, k - 1, v);
-  v = uf[f - fxs - fys] + w1 * c000 + w2 * (cm00 + c0m0 + c00p) + w3 * (cmm0 + cm0p + c0mp) + w4 * cmmp;
-  uf[f - fxs - fys] = v; if (ge) ge->emit(i - 1, j - 1, k, v);
-  v = uf[f - fxs - 1] + w1 * c000 + w2 * (cm00 + c0p0 + c00m) + w3 * (cmp0 + cm0m + c0pm) + w4 * cmpm;
-  uf[f - fxs - 1] = v; if (ge) ge->emit(i - 1, j, k - 1, v);
-  v = uf[f - fys - 1] + w1 * c000 + w2 * (cp00 + c0m0 + c00m) + w3 * (cpm0 + cp0m + c0mm) + w4 * cpmm;
-  uf[f - fys - 1] = v; if (ge) ge->emit(i, j - 1, k - 1, v);
-  v = uf[f - fxs - fys - 1] + w1 * c000 + w2 * (cm00 + c0m0 + c00m) + w3 * (cmm0 + cm0m + c0mm) + w4 * cmmm;
-  uf[f - fxs - fys - 1] = v; if (ge) ge->emit(i - 1, j - 1, k - 1, v);
+  {  // children on the +x side of the coarse centre (coarse plane x+1)
+    const T cp00 = uc[tc + cx], cpp0 = uc[tc + cx + cy], cp0p = uc[tc + cx + 1], cppp = uc[tc + cx + cy + 1];
+    const T cpm0 = uc[tc + cx - cy], cp0m = uc[tc + cx - 1], cpmm = uc[tc + cx - cy - 1];
+    const T cppm = uc[tc + cx + cy - 1], cpmp = uc[tc + cx - cy + 1];
+    v = f000 + w1 * c000 + w2 * (cp00 + c0p0 + c00p) + w3 * (cpp0 + cp0p + c0pp) + w4 * cppp;
+    uf[f] = v; if (ge) ge->emit(i, j, k, v);
+    v = f010 + w1 * c000 + w2 * (cp00 + c0m0 + c00p) + w3 * (cpm0 + cp0p + c0mp) + w4 * cpmp;
+    uf[f - fys] = v; if (ge) ge->emit(i, j - 1, k, v);
+    v = f001 + w1 * c000 + w2 * (cp00 + c0p0 + c00m) + w3 * (cpp0 + cp0m + c0pm) + w4 * cppm;
+    uf[f - 1] = v; if (ge) ge->emit(i, j, k - 1, v);
+    v = f011 + w1 * c000 + w2 * (cp00 + c0m0 + c00m) + w3 * (cpm0 + cp0m + c0mm) + w4 * cpmm;
+    uf[f - fys - 1] = v; if (ge) ge->emit(i, j - 1, k - 1, v);
+    // the -x child with (0,0) y/z offsets takes its corner weight from cppp, as the reference
+    // kernel does (devf.cu:94-197)
+    const T cm00 = uc[tc - cx], cmp0 = uc[tc - cx + cy], cm0p = uc[tc - cx + 1];
+    v = f100 + w1 * c000 + w2 * (cm00 + c0p0 + c00p) + w3 * (cmp0 + cm0p + c0pp) + w4 * cppp;
+    uf[f - fxs] = v; if (ge) ge->emit(i - 1, j, k, v);
+  }
+  {  // remaining children on the -x side (coarse plane x-1)
+    const T cm00 = uc[tc - cx], cmm0 = uc[tc - cx - cy], cm0p = uc[tc - cx + 1], cm0m = uc[tc - cx - 1];
+    const T cmmm = uc[tc - cx - cy - 1], cmp0 = uc[tc - cx + cy], cmpm = uc[tc - cx + cy - 1];
+    const T cmmp = uc[tc - cx - cy + 1];
+    v = f110 + w1 * c000 + w2 * (cm00 + c0m0 + c00p) + w3 * (cmm0 + cm0p + c0mp) + w4 * cmmp;
+    uf[f - fxs - fys] = v; if (ge) ge->emit(i - 1, j - 1, k, v);
+    v = f101 + w1 * c000 + w2 * (cm00 + c0p0 + c00m) + w3 * (cmp0 + cm0m + c0pm) + w4 * cmpm;
+    uf[f - fxs - 1] = v; if (ge) ge->emit(i - 1, j, k - 1, v);
+    v = f111 + w1 * c000 + w2 * (cm00 + c0m0 + c00m) + w3 * (cmm0 + cm0m + c0mm) + w4 * cmmm;
+    uf[f - fxs - fys - 1] = v; if (ge) ge->emit(i - 1, j - 1, k - 1, v);
+  }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_prolong_emit(const T *__restrict__ uc, long long cx, long long cy, int cnx,
+__global__ void __launch_bounds__(256, 3) k_prolong_emit(const T *__restrict__ uc, long long cx, long long cy, int cnx,
                                                       int cny, int cnz, T *__restrict__ uf, long long fxs,
                                                       long long fys, GhostEmit<T> ge) {
   const int kc = blockIdx.x * blockDim.x + threadIdx.x;
@@ -411,13 +387,14 @@ __device__ void tail_relax(const TailLevel<T> &lv, int iterations, int order, in
   }
 }
 
+// The tail schedule on level descriptors lv[0..nlev-1] (lv[0] = level s), held in shared
+// memory.  Works on global memory or on a shared-memory copy; the arithmetic is the same.
 template <typename T>
-__global__ void __launch_bounds__(1024) k_coarse_tail(TailParams<T> P) {
-  const int nt = blockDim.x;
-  const int L = P.nlev;  // levels in the tail: P.lv[0] = level s ... P.lv[L-1] = coarsest
+__device__ void tail_body(const TailLevel<T> *lv, const TailParams<T> &P, int nt) {
+  const int L = P.nlev;
   for (int l = 0; l < L - 1; l++) {
-    const TailLevel<T> &f = P.lv[l];
-    const TailLevel<T> &c = P.lv[l + 1];
+    const TailLevel<T> &f = lv[l];
+    const TailLevel<T> &c = lv[l + 1];
     tail_relax<T>(f, P.nu1, 0, nt);
     // clear_zero(coarse) + homogeneous ghost fill == zero every cell of the shell and interior
     const int cz = c.nz + 2, cy = c.ny + 2, cx = c.nx + 2;
@@ -441,9 +418,8 @@ __global__ void __launch_bounds__(1024) k_coarse_tail(TailParams<T> P) {
     }
     __syncthreads();
   }
-  // coarsest level
-  {
-    const TailLevel<T> &cl = P.lv[L - 1];
+  {  // coarsest level
+    const TailLevel<T> &cl = lv[L - 1];
     if (P.host_coarse) {
       coarse_relax_block<T>(cl.u, cl.b, cl.xs, cl.ys, cl.nx, cl.ny, cl.nz, P.coarse_iters, P.coarse_order, P.cc,
                             cl.bc, cl.hx, cl.hy, cl.hz);
@@ -453,8 +429,8 @@ __global__ void __launch_bounds__(1024) k_coarse_tail(TailParams<T> P) {
     __syncthreads();
   }
   for (int l = L - 2; l >= 0; l--) {
-    const TailLevel<T> &f = P.lv[l];
-    const TailLevel<T> &c = P.lv[l + 1];
+    const TailLevel<T> &f = lv[l];
+    const TailLevel<T> &c = lv[l + 1];
     GhostEmit<T> ge{f.u, f.xs, f.ys, f.nx, f.ny, f.nz, f.bc, f.hx, f.hy, f.hz};
     for (int q = threadIdx.x; q < c.nx * c.ny * c.nz; q += nt) {
       const int ic = q / (c.ny * c.nz), jc = (q / c.nz) % c.ny, kc = q % c.nz;
@@ -474,7 +450,91 @@ __global__ void __launch_bounds__(1024) k_coarse_tail(TailParams<T> P) {
 }
 
 template <typename T>
+__global__ void __launch_bounds__(1024) k_coarse_tail(const __grid_constant__ TailParams<T> P) {
+  __shared__ TailLevel<T> lv[kMaxTailLevels];
+  if (threadIdx.x < P.nlev) lv[threadIdx.x] = P.lv[threadIdx.x];
+  __syncthreads();
+  tail_body<T>(lv, P, blockDim.x);
+}
+
+// Shared-memory variant: every tail level's u and b (interior + ghost shell, compact strides)
+// is staged in dynamic shared memory, the schedule runs there, and u (shell included) and the
+// interior of b are written back.  Only level s is read: the lower levels are zeroed /
+// restricted inside the schedule before they are used.
+template <typename T>
+__global__ void __launch_bounds__(512) k_coarse_tail_smem(const __grid_constant__ TailParams<T> P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ TailLevel<T> lv[kMaxTailLevels];
+  const int L = P.nlev;
+  if (threadIdx.x == 0) {
+    T *cur = reinterpret_cast<T *>(smem_raw);
+    for (int l = 0; l < L; l++) {
+      TailLevel<T> d = P.lv[l];
+      const long long sys = d.nz + 2, sxs = (long long)(d.ny + 2) * (d.nz + 2);
+      const long long cells = (long long)(d.nx + 2) * sxs;
+      d.xs = sxs;
+      d.ys = sys;
+      d.u = cur + sxs + sys + 1;
+      cur += cells;
+      d.b = cur + sxs + sys + 1;
+      cur += cells;
+      lv[l] = d;
+    }
+  }
+  __syncthreads();
+  const int nt = blockDim.x;
+  {  // stage level s
+    const TailLevel<T> &g = P.lv[0];
+    const TailLevel<T> &sh = lv[0];
+    const int cz = g.nz + 2, cy = g.ny + 2, cx = g.nx + 2;
+    for (int q = threadIdx.x; q < cx * cy * cz; q += nt) {
+      const int i = q / (cy * cz) - 1, j = (q / cz) % cy - 1, k = q % cz - 1;
+      sh.u[(long long)i * sh.xs + (long long)j * sh.ys + k] = g.u[(long long)i * g.xs + (long long)j * g.ys + k];
+      sh.b[(long long)i * sh.xs + (long long)j * sh.ys + k] = g.b[(long long)i * g.xs + (long long)j * g.ys + k];
+    }
+  }
+  __syncthreads();
+  tail_body<T>(lv, P, nt);
+  __syncthreads();
+  for (int l = 0; l < L; l++) {  // write back: u with its ghost shell, b interior below level s
+    const TailLevel<T> &g = P.lv[l];
+    const TailLevel<T> &sh = lv[l];
+    const int cz = g.nz + 2, cy = g.ny + 2, cx = g.nx + 2;
+    for (int q = threadIdx.x; q < cx * cy * cz; q += nt) {
+      const int i = q / (cy * cz) - 1, j = (q / cz) % cy - 1, k = q % cz - 1;
+      const long long gi = (long long)i * g.xs + (long long)j * g.ys + k;
+      const long long si = (long long)i * sh.xs + (long long)j * sh.ys + k;
+      g.u[gi] = sh.u[si];
+      if (l > 0 && i >= 0 && i < g.nx && j >= 0 && j < g.ny && k >= 0 && k < g.nz) g.b[gi] = sh.b[si];
+    }
+  }
+}
+
+template <typename T>
+size_t tail_smem_bytes(const TailParams<T> &P) {
+  size_t cells = 0;
+  for (int l = 0; l < P.nlev; l++) cells += 2 * (size_t)(P.lv[l].nx + 2) * (P.lv[l].ny + 2) * (P.lv[l].nz + 2);
+  return cells * sizeof(T);
+}
+
+template <typename T>
 ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s) {
+  const size_t bytes = tail_smem_bytes<T>(P);
+  constexpr size_t kMaxSmem = 200 * 1024;
+  if (bytes <= kMaxSmem) {
+    static std::atomic<unsigned long long> attr_set{0};  // one bit per device, per instance
+    int dev = 0;
+    OCU_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr_set.load() & bit)) {
+      OCU_TRY(check_cuda(cudaFuncSetAttribute(k_coarse_tail_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)kMaxSmem),
+                         "cudaFuncSetAttribute(k_coarse_tail_smem)"));
+      attr_set.fetch_or(bit);
+    }
+    k_coarse_tail_smem<T><<<1, 512, bytes, s>>>(P);
+    return check_launch("k_coarse_tail_smem");
+  }
   k_coarse_tail<T><<<1, 1024, 0, s>>>(P);
   return check_launch("k_coarse_tail");
 }

@@ -51,9 +51,9 @@ inline CoarseCoef<T> make_coarse_coef(const RelaxParams &p) {
 
 template <typename T>
 __device__ __forceinline__ T host_face(const BCDev &bc, int f, T src, T h, bool neg) {
-  const int t = bc.type[f];
-  if (t == OCU_BC_DIRICHELET) return -src + (T)2 * (T)bc.value[f];
-  if (t == OCU_BC_NEUMANN) return neg ? src - h * (T)bc.value[f] : src + h * (T)bc.value[f];
+  const int t = bc.ty(f);
+  if (t == OCU_BC_DIRICHELET) return -src + (T)2 * (T)bc.val(f);
+  if (t == OCU_BC_NEUMANN) return neg ? src - h * (T)bc.val(f) : src + h * (T)bc.val(f);
   return src;
 }
 
@@ -92,7 +92,7 @@ __device__ void coarse_relax_block(T *u, const T *b, long long xs, long long ys,
         int r = q;
         if (r < 2 * nzf) {
           const int side = r / nzf, i = (r % nzf) / ny, j = (r % nzf) % ny;
-          const int f = side ? FZ_POS : FZ_NEG, t = bc.type[f];
+          const int f = side ? FZ_POS : FZ_NEG, t = bc.ty(f);
           if (t == OCU_BC_PERIODIC) at(i, j, side ? nz : -1) = at(i, j, side ? 0 : nz - 1);
           else if (t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN)
             at(i, j, side ? nz : -1) = host_face<T>(bc, f, at(i, j, side ? nz - 1 : 0), hz, !side);
@@ -101,7 +101,7 @@ __device__ void coarse_relax_block(T *u, const T *b, long long xs, long long ys,
         r -= 2 * nzf;
         if (r < 2 * nyf) {
           const int side = r / nyf, i = (r % nyf) / nz, k = (r % nyf) % nz;
-          const int f = side ? FY_POS : FY_NEG, t = bc.type[f];
+          const int f = side ? FY_POS : FY_NEG, t = bc.ty(f);
           if (t == OCU_BC_PERIODIC) at(i, side ? ny : -1, k) = at(i, side ? 0 : ny - 1, k);
           else if (t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN)
             at(i, side ? ny : -1, k) = host_face<T>(bc, f, at(i, side ? ny - 1 : 0, k), hy, !side);
@@ -110,7 +110,7 @@ __device__ void coarse_relax_block(T *u, const T *b, long long xs, long long ys,
         r -= 2 * nyf;
         {
           const int side = r / nxf, j = (r % nxf) / nz, k = (r % nxf) % nz;
-          const int f = side ? FX_POS : FX_NEG, t = bc.type[f];
+          const int f = side ? FX_POS : FX_NEG, t = bc.ty(f);
           if (t == OCU_BC_PERIODIC) at(side ? nx : -1, j, k) = at(side ? 0 : nx - 1, j, k);
           else if (t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN)
             at(side ? nx : -1, j, k) = host_face<T>(bc, f, at(side ? nx - 1 : 0, j, k), hx, !side);

@@ -45,6 +45,17 @@ struct BCDev {
   int type[6];     // xpos, xneg, ypos, yneg, zpos, zneg
   float value[6];
   float aux[6];
+  // Per-face reads by a run-time face index, as select chains: indexing the arrays directly
+  // with a non-constant index makes every thread copy the struct to local memory.
+  __host__ __device__ __forceinline__ int ty(int f) const {
+    return f == 0 ? type[0] : f == 1 ? type[1] : f == 2 ? type[2] : f == 3 ? type[3] : f == 4 ? type[4] : type[5];
+  }
+  __host__ __device__ __forceinline__ float val(int f) const {
+    return f == 0 ? value[0] : f == 1 ? value[1] : f == 2 ? value[2] : f == 3 ? value[3] : f == 4 ? value[4] : value[5];
+  }
+  __host__ __device__ __forceinline__ float auxv(int f) const {
+    return f == 0 ? aux[0] : f == 1 ? aux[1] : f == 2 ? aux[2] : f == 3 ? aux[3] : f == 4 ? aux[4] : aux[5];
+  }
 };
 BCDev to_dev(const ocu_bc_set &bc);
 bool bc_check_scalar(const ocu_bc_set &bc);
