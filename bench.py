@@ -241,23 +241,29 @@ def run_gpu(args):
     ms_e2e, _ = timed(e2e_step, max(1, args.steps // 2), 1)
     bytes_grid = int(L.allocated) * 8
 
-    # dominant kernel: level-0 FP32 colour sweep of the refinement solver's inner hierarchy
-    reps = 40
-    for c in range(4):
-        mixed.relax_sweep(0, c & 1, core=1)
+    # dominant kernel: the level-0 FP32 relaxation of the refinement solver's inner hierarchy, as
+    # the V-cycles issue it -- one two-colour TMA pass per iteration when the level qualifies
+    # (reads u and b, writes u: 3N values), else two colour launches (each 2N values: all of u,
+    # half of b, half of u written)
+    iters = 20
+    mixed.relax(0, 2, 0, core=1)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0 = ocu.kernel_launch_count()
     e0.record(stream)
-    for c in range(reps):
-        mixed.relax_sweep(0, c & 1, core=1)
+    mixed.relax(0, iters, 0, core=1)
     e1.record(stream)
     torch.cuda.synchronize()
-    sweep_ms = e0.elapsed_time(e1) / reps
+    per_iter = (ocu.kernel_launch_count() - c0) // iters
     ncell = n ** 3
-    alg_bytes = 2.0 * ncell * 4  # read u, read b (own colour), write u (own colour)
+    if per_iter == 1:
+        kernel_name, alg_bytes = "k_relax_sweep2<float> level 0 (256^3)", 3.0 * ncell * 4
+    else:
+        kernel_name, alg_bytes = "k_relax_color_emit<float> level 0 (256^3)", 2.0 * ncell * 4
+    sweep_ms = e0.elapsed_time(e1) / (iters * per_iter)
     achieved = alg_bytes / (sweep_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profile_traffic("relax_color_f32_256cube.md")
+    traffic = profile_traffic("relax_sweep2_f32_256cube.md" if per_iter == 1 else "relax_color_f32_256cube.md")
 
     secondary = {}
     if rank == 0 and not args.skip_secondary:
@@ -289,7 +295,7 @@ def run_gpu(args):
         "mixed": {"outer_iterations": st_mixed.outer_iterations, "fp32_vcycles": st_mixed.vcycles,
                   "rel_residual": res_holder["mixed"] / rms_b, "max_rel_err_vs_fp64_mg": err_vs_fp64},
         "fp64": {"vcycles": st_fp64.vcycles, "rel_residual": res_holder["fp64"] / rms_b},
-        "roofline": {"bound": "hbm", "kernel": "k_relax_color<float> level 0 (256^3)",
+        "roofline": {"bound": "hbm", "kernel": kernel_name,
                      "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": round(sweep_ms, 5)},
@@ -424,6 +430,33 @@ def run_reference(args):
     }
 
 
+def run_kernel_case(args):
+    """A few launches of one hot kernel on a 256^3 FP32 hierarchy, for focused profiler captures
+    (ncu -k <kernel> -c 1..3).  Level 1 is filled by a restriction first, so no FMG runs."""
+    import torch
+    import opencurrent_b200 as ocu
+
+    n = N_CFG3
+    h = 1.0 / n
+    L = ocu.layout(n, n, n)
+    rhs = ocu.Grid3DDevice(ocu.F32)
+    rhs.init(n, n, n)
+    rhs.copy_from_host(padded(fourier_rhs(n), L, np.float32))
+    s = ocu.Sol_MultigridPressure3DDevice(ocu.F32)
+    s.bc = ocu.BoundaryConditionSet(ocu.BoundaryCondition(ocu.BC_NEUMANN, 0.0))
+    s.initialize_storage(n, n, n, h, h, h, rhs)
+    if args.kernel_case == "relax":
+        s.relax(0, 3, 0)          # one pair of two-colour passes + one iteration of colour launches
+    elif args.kernel_case == "prolong":
+        s.relax(1, 1, 0)
+        s.prolong(1, 0)
+    elif args.kernel_case == "restrict":
+        s.restrict_residuals(0, 1, norms=True)
+    s.synchronize()
+    torch.cuda.synchronize()
+    print(json.dumps({"kernel_case": args.kernel_case, "grid": [n] * 3, "ok": True}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -433,7 +466,12 @@ def main():
     ap.add_argument("--ir-inner", type=int, default=3)
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-secondary", action="store_true")
+    ap.add_argument("--kernel-case", choices=["relax", "prolong", "restrict"],
+                    help="run a few launches of one kernel on the 256^3 FP32 hierarchy (profiling)")
     args = ap.parse_args()
+    if args.kernel_case:
+        run_kernel_case(args)
+        return
     line = run_reference(args) if args.impl == "reference" else run_gpu(args)
     if line is not None:
         print(json.dumps(line), flush=True)

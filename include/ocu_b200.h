@@ -160,7 +160,10 @@ typedef struct ocu_mg_params {
                                     writes, no fused residual+restriction, no tail kernel);
                                     same results, for A/B timing */
   int tail_cells;                /* levels with at most this many cells run in one single-CTA
-                                    kernel per cycle; 0 = default (4096), < 0 = off */
+                                    kernel per cycle; 0 = default (512), < 0 = off */
+  int sweep_cells;               /* levels with at least this many cells relax both colours in
+                                    one TMA-fed pass (out of place, same results; Dirichlet and
+                                    Neumann faces only); 0 = default (1048576), < 0 = off */
 } ocu_mg_params;
 
 typedef struct ocu_mg_stats {

@@ -212,6 +212,7 @@ class _MGBase:
         self.store_residual_grids = False
         self.unfused = False
         self.tail_cells = 0
+        self.sweep_cells = 0
         self._h = None
         self._rhs = None
 
@@ -225,6 +226,7 @@ class _MGBase:
         p.store_residual_grids = int(bool(self.store_residual_grids))
         p.unfused = int(bool(self.unfused))
         p.tail_cells = int(self.tail_cells)
+        p.sweep_cells = int(self.sweep_cells)
         return p
 
     def initialize_storage(self, nx, ny, nz, hx, hy, hz, rhs):

@@ -176,4 +176,19 @@ ocu_status launch_fold_rows(const T *rows, long long nrows, bool is_max, void *s
 template <typename T>
 ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s);
 
+// Opaque copy of a CUtensorMap (128 bytes, 64-byte aligned) so host headers need no cuda.h.
+struct alignas(64) SweepTmap {
+  unsigned char bytes[128];
+};
+// Two-colour sweep (kernels_relax_tma.cu): supported layouts/BCs, the tensor map of one grid
+// buffer, and the launch u_in (through its map) -> u_out.  err: device word set to 1 when a
+// bounded wait inside the kernel gives up.
+bool sweep2_supported(const ocu_layout &L, const ocu_bc_set &bc);
+template <typename T>
+ocu_status make_sweep_tmap(const void *buf, const ocu_layout &L, SweepTmap *out);
+template <typename T>
+ocu_status launch_relax_sweep2(const SweepTmap &tm_u_in, const SweepTmap &tm_b, T *u_out, const ocu_layout &L,
+                               const T *diag, int first_color, const RelaxParams &p, double hx, double hy, double hz,
+                               int *err, cudaStream_t s);
+
 }  // namespace ocub

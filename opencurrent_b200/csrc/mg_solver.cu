@@ -56,6 +56,8 @@ MGCore<T>::~MGCore() {
     if (l > 0 && grids_b[l]) { cudaFree(grids_b[l]->buf); delete grids_b[l]; }
     if (grids_r[l]) { cudaFree(grids_r[l]->buf); delete grids_r[l]; }
   }
+  for (auto g : grids_u2)
+    if (g) { cudaFree(g->buf); delete g; }
   for (auto p : diag) cudaFree(p);
   if (red_scratch) cudaFree(red_scratch);
   if (rows) cudaFree(rows);
@@ -134,8 +136,26 @@ ocu_status MGCore<T>::init(const ocu_bc_set &bc_, bool disable_host, int nx, int
   OCU_TRY(check_cuda(cudaMemset(red_scratch, 0, reduce_scratch_bytes(lay[0], sizeof(T))), "cudaMemset(reduce)"));
   rows_stride = ((long long)dim[0][0] * dim[0][1] + 63) / 64 * 64;
   OCU_TRY(check_cuda(cudaMalloc(&rows, 2 * sizeof(T) * rows_stride), "cudaMalloc(norm rows)"));
-  OCU_TRY(check_cuda(cudaMalloc(&d_norms, 2 * sizeof(double)), "cudaMalloc(norms)"));
-  OCU_TRY(check_cuda(cudaMallocHost(&h_norms, 2 * sizeof(double)), "cudaMallocHost(norms)"));
+  // norms[0..1] = l2, linf; norms[2] holds the kernels' timeout word (read back with the norms)
+  OCU_TRY(check_cuda(cudaMalloc(&d_norms, 4 * sizeof(double)), "cudaMalloc(norms)"));
+  OCU_TRY(check_cuda(cudaMemset(d_norms, 0, 4 * sizeof(double)), "cudaMemset(norms)"));
+  OCU_TRY(check_cuda(cudaMallocHost(&h_norms, 4 * sizeof(double)), "cudaMallocHost(norms)"));
+  std::memset(h_norms, 0, 4 * sizeof(double));
+  d_err = reinterpret_cast<int *>(d_norms + 2);
+  // second u buffer + TMA maps for every level the two-colour pass may run on
+  grids_u2.assign(num_levels, nullptr);
+  tm_u.resize(num_levels);
+  tm_u2.resize(num_levels);
+  tm_b.resize(num_levels);
+  for (int l = 0; l < num_levels; l++) {
+    if (!sweep2_supported(lay[l], bc_at_level(l))) continue;
+    if ((long long)dim[l][0] * dim[l][1] * dim[l][2] < 512) continue;
+    grids_u2[l] = alloc_grid(dt, lay[l], &st);
+    if (!grids_u2[l]) return st;
+    OCU_TRY(make_sweep_tmap<T>(grids_u[l]->buf, lay[l], &tm_u[l]));
+    OCU_TRY(make_sweep_tmap<T>(grids_u2[l]->buf, lay[l], &tm_u2[l]));
+    OCU_TRY(make_sweep_tmap<T>(grids_b[l]->buf, lay[l], &tm_b[l]));
+  }
   return check_cuda(cudaStreamSynchronize(stream), "initialize_storage");
 }
 
@@ -202,6 +222,7 @@ ocu_status MGCore<T>::relax(int level, int iterations, int order) {
   }
   const T *dg = diag.empty() ? nullptr : (const T *)diag[level];
   const bool emit = emit_ok(level);
+  if (emit && sweep2_ok(level)) return relax_pairs(level, iterations, order);
   for (int it = 0; it < iterations; it++) {
     for (int rb = 0; rb < 2; rb++) {
       int color = rb;
@@ -216,6 +237,35 @@ ocu_status MGCore<T>::relax(int level, int iterations, int order) {
     }
     if (!emit && !update_bc_between_colors) OCU_TRY(apply_bc(level));
   }
+  return OCU_OK;
+}
+
+template <typename T>
+bool MGCore<T>::sweep2_ok(int level) const {
+  if (!fused || sweep_cells <= 0 || level >= (int)grids_u2.size() || !grids_u2[level]) return false;
+  return (long long)dim[level][0] * dim[level][1] * dim[level][2] >= sweep_cells;
+}
+
+// Iterations in pairs through the two-colour pass (u -> u2 -> u, so the result stays in u);
+// an odd last iteration runs as two colour launches.  Same colour order as relax().
+template <typename T>
+ocu_status MGCore<T>::relax_pairs(int level, int iterations, int order) {
+  const RelaxParams p = relax_params(level);
+  const T *dg = diag.empty() ? nullptr : (const T *)diag[level];
+  auto first = [&](int it) {
+    return (order == RO_BLACK_RED || (order == RO_SYMMETRIC && it >= iterations / 2)) ? 1 : 0;
+  };
+  int it = 0;
+  for (; it + 1 < iterations; it += 2) {
+    OCU_TRY(launch_relax_sweep2<T>(tm_u[level], tm_b[level], origin<T>(grids_u2[level]), lay[level], dg, first(it), p,
+                                   hx(level), hy(level), hz(level), d_err, stream));
+    OCU_TRY(launch_relax_sweep2<T>(tm_u2[level], tm_b[level], u0(level), lay[level], dg, first(it + 1), p, hx(level),
+                                   hy(level), hz(level), d_err, stream));
+  }
+  for (; it < iterations; it++)
+    for (int rb = 0; rb < 2; rb++)
+      OCU_TRY(launch_relax_color_emit<T>(u0(level), b0(level), lay[level], dg, first(it) ? !rb : rb, p, hx(level),
+                                         hy(level), hz(level), stream));
   return OCU_OK;
 }
 
@@ -247,7 +297,7 @@ ocu_status MGCore<T>::enqueue_restrict_residuals(int fine, int coarse, bool want
     if (want_linf) OCU_TRY(launch_fold_rows<T>(rowsinf, nrows, true, red_scratch, d_norms + 1, stream));
   }
   if (norms)
-    OCU_TRY(check_cuda(cudaMemcpyAsync(h_norms, d_norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream),
+    OCU_TRY(check_cuda(cudaMemcpyAsync(h_norms, d_norms, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream),
                        "norm readback"));
   return OCU_OK;
 }
@@ -257,6 +307,11 @@ ocu_status MGCore<T>::enqueue_restrict_residuals(int fine, int coarse, bool want
 template <typename T>
 ocu_status MGCore<T>::finish_norms(int fine, double *l2, double *linf) {
   OCU_TRY(check_cuda(cudaStreamSynchronize(stream), "norm readback"));
+  if (*reinterpret_cast<const int *>(h_norms + 2) != 0) {
+    cudaMemsetAsync(d_err, 0, sizeof(int), stream);
+    *reinterpret_cast<int *>(h_norms + 2) = 0;
+    return fail(OCU_ERR_TIMEOUT, "[ERROR] multigrid - a kernel's bounded wait for its TMA loads gave up");
+  }
   if (l2) {
     T rn = (T)h_norms[0];
     rn /= (T)(dim[fine][0] * dim[fine][1] * dim[fine][2]);
@@ -724,7 +779,7 @@ ocu_status MGSolver::ir_residual(double *l2, double *linf) {
   const long long nrows = (long long)L.nx * L.ny;
   OCU_TRY(launch_fold_rows<double>(rows2, nrows, false, cd.red_scratch, cd.d_norms, stream));
   OCU_TRY(launch_fold_rows<double>(rowsinf, nrows, true, cd.red_scratch, cd.d_norms + 1, stream));
-  OCU_TRY(check_cuda(cudaMemcpyAsync(cd.h_norms, cd.d_norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream),
+  OCU_TRY(check_cuda(cudaMemcpyAsync(cd.h_norms, cd.d_norms, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream),
                      "norm readback"));
   return cd.finish_norms(0, l2, linf);
 }
@@ -814,6 +869,7 @@ ocu_status MGSolver::initialize_storage(int nx, int ny, int nz, double hx, doubl
       ocu_bc_set fbc = prm.bc;
       if (kind == OCU_MG_MIXED_IR) bc_make_homogeneous(&fbc);
       OCU_TRY(cf.init(fbc, dis, nx, ny, nz, hx, hy, hz, rhs_f, pf, stream));
+      cf.d_err = cd.d_err;  // one timeout word, read back with the FP64 norms
     }
   }
   stats.num_levels = num_levels;
@@ -823,10 +879,12 @@ ocu_status MGSolver::initialize_storage(int nx, int ny, int nz, double hx, doubl
 }
 
 void MGSolver::apply_knobs() {
-  const int tc = prm.tail_cells == 0 ? 4096 : (prm.tail_cells < 0 ? 0 : prm.tail_cells);
+  const int tc = prm.tail_cells == 0 ? kDefaultTailCells : (prm.tail_cells < 0 ? 0 : prm.tail_cells);
   cf.fused = cd.fused = prm.unfused == 0;
   cf.store_residuals = cd.store_residuals = prm.store_residual_grids != 0;
   cf.tail_cells = cd.tail_cells = tc;
+  cf.sweep_cells = cd.sweep_cells =
+      prm.sweep_cells == 0 ? kDefaultSweepCells : (prm.sweep_cells < 0 ? 0 : prm.sweep_cells);
 }
 
 ocu_status MGSolver::set_params(const ocu_mg_params &p) {

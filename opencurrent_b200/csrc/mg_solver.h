@@ -8,11 +8,19 @@
 #include <memory>
 #include <vector>
 
+#include "mg_fused.h"
 #include "ocu_internal.h"
 
 namespace ocub {
 
 int mg_num_levels(int nx, int ny, int nz);
+
+// One CTA runs the coarse end of a cycle up to 8^3 cells (a 16^3 level already keeps one SM
+// busy longer than its separate launches take).
+constexpr int kDefaultTailCells = 512;
+// The two-colour TMA pass needs enough (tile, plane) steps to fill every SM; below about a
+// million cells the colour launches finish sooner.
+constexpr int kDefaultSweepCells = 1 << 20;
 double mg_optimal_omega(double fx, double fy, double fz);
 
 // The virtual level operations of Sol_MultigridPressure3DBase (sol_mgpressure3d.h:76-80).
@@ -57,11 +65,18 @@ struct MGCore : CoreOps {
   long long rows_stride = 0;
   bool fused = true;              // fused kernels (ghost writes, residual+restrict, tail)
   bool store_residuals = false;   // keep r_grid filled (reference kernels) for read_r
-  int tail_cells = 4096;          // levels with at most this many cells run in the tail kernel
+  int tail_cells = kDefaultTailCells;    // levels with at most this many cells run in the tail kernel
+  int sweep_cells = kDefaultSweepCells;  // levels with at least this many cells use the two-colour pass
+  // two-colour pass: per level a second u buffer (ping-pong) and the TMA maps of u, u2 and b
+  std::vector<ocu_grid *> grids_u2;
+  std::vector<SweepTmap> tm_u, tm_u2, tm_b;
+  int *d_err = nullptr;           // set by kernels whose bounded waits gave up (inside d_norms)
 
   ~MGCore();
   ocu_status clear_level(int level) override;
   bool emit_ok(int level) const;
+  bool sweep2_ok(int level) const;
+  ocu_status relax_pairs(int level, int iterations, int order);
   ocu_status enqueue_restrict_residuals(int fine, int coarse, bool want_l2, bool want_linf) override;
   ocu_status finish_norms(int fine, double *l2, double *linf) override;
   int tail_start() const override;

@@ -9,42 +9,51 @@ namespace ocub {
 
 // One red-black SOR update from the cell's value, its right-hand side and its six neighbours
 // (z-, z+, y-, y+, x-, x+); arithmetic of the reference's colour kernels
-// (sol_mgpressure3ddev.cu:145-230).
+// (sol_mgpressure3ddev.cu:145-230): residual sequence, boundary-aware diagonal, then
+// u + omega * res / diag.
 template <typename T>
-__device__ __forceinline__ T relax_value(T uc, T bv, T zm, T zp, T ym, T yp, T xm, T xp, int i, int j, int k,
-                                         int nx, int ny, int nz, const RelaxCoefD<T> &c,
-                                         const T *__restrict__ diag) {
-  T res, dg;
+__device__ __forceinline__ T relax_res(T uc, T bv, T zm, T zp, T ym, T yp, T xm, T xp, const RelaxCoefD<T> &c) {
+  T res;
   if (sizeof(T) == 4) {
     res = (-c.hsq * bv - c.ld * uc);
     res += c.fz * (zm + zp);
     res += c.fy * (ym + yp);
     res += c.fx * (xm + xp);
-    dg = c.ld;
-    if (i == nx - 1) dg += c.xp;
-    if (i == 0) dg += c.xn;
-    if (j == ny - 1) dg += c.yp;
-    if (j == 0) dg += c.yn;
-    if (k == nz - 1) dg += c.zp;
-    if (k == 0) dg += c.zn;
   } else {
     res = -c.ld * uc;
     res += c.fz * (zm + zp);
     res += c.fy * (ym + yp);
     res += c.fx * (xm + xp);
     res += c.hsq * bv;
-    if (diag) {
-      dg = diag[(long long)i * ny + j];
-    } else {  // same sequence the 2D table is built with (sol_mgpressure3ddev.cu:36-41)
-      dg = c.ld;
-      if (i == nx - 1) dg += c.xp;
-      if (i == 0) dg += c.xn;
-      if (j == ny - 1) dg += c.yp;
-      if (j == 0) dg += c.yn;
-    }
-    if (k == nz - 1) dg += c.zp;
-    if (k == 0) dg += c.zn;
   }
+  return res;
+}
+
+// Diagonal of cell (i,j,k); away from every face it is c.ld exactly (nothing is added).
+template <typename T>
+__device__ __forceinline__ T relax_dg(int i, int j, int k, int nx, int ny, int nz, const RelaxCoefD<T> &c,
+                                      const T *__restrict__ diag) {
+  T dg;
+  if (sizeof(T) == 4 || !diag) {  // FP64: same sequence the 2D table is built with (sol_mgpressure3ddev.cu:36-41)
+    dg = c.ld;
+    if (i == nx - 1) dg += c.xp;
+    if (i == 0) dg += c.xn;
+    if (j == ny - 1) dg += c.yp;
+    if (j == 0) dg += c.yn;
+  } else {
+    dg = diag[(long long)i * ny + j];
+  }
+  if (k == nz - 1) dg += c.zp;
+  if (k == 0) dg += c.zn;
+  return dg;
+}
+
+template <typename T>
+__device__ __forceinline__ T relax_value(T uc, T bv, T zm, T zp, T ym, T yp, T xm, T xp, int i, int j, int k,
+                                         int nx, int ny, int nz, const RelaxCoefD<T> &c,
+                                         const T *__restrict__ diag) {
+  const T res = relax_res<T>(uc, bv, zm, zp, ym, yp, xm, xp, c);
+  const T dg = relax_dg<T>(i, j, k, nx, ny, nz, c, diag);
   return uc + c.omega * res / dg;
 }
 

@@ -35,6 +35,8 @@ SCALAR_BCS = {
                    "zpos": (NEU, 0.0), "zneg": (NEU, 0.0)},
     "mixed_all": {"xpos": (DIR, -1.0), "xneg": (NEU, 0.5), "ypos": (PER, 0), "yneg": (PER, 0),
                   "zpos": (NONE, 0), "zneg": (DIR, 0.25)},
+    "mixed_dn": {"xpos": (DIR, 0.5), "xneg": (NEU, -0.25), "ypos": (NEU, 0.75), "yneg": (DIR, -0.125),
+                 "zpos": (DIR, 1.5), "zneg": (NEU, 0.375)},
 }
 
 MAC_BCS = {

@@ -44,14 +44,18 @@ def pair(dt, shape, h, bcname, seed=0, sym=0, disable_host=0, conv=0x05, **knobs
     return om, dm, g
 
 
-KNOBS = [dict(), dict(unfused=True), dict(tail_cells=-1), dict(tail_cells=40000), dict(store_residual_grids=True)]
+KNOBS = [dict(), dict(unfused=True), dict(tail_cells=-1), dict(tail_cells=40000), dict(tail_cells=4096),
+         dict(store_residual_grids=True), dict(sweep_cells=1), dict(sweep_cells=-1)]
 
 
 @pytest.mark.parametrize("dt", [F32, F64])
-@pytest.mark.parametrize("bcname", ["neumann", "periodic", "mixed_all", "neumann_inhom"])
+@pytest.mark.parametrize("bcname", ["neumann", "periodic", "mixed_all", "neumann_inhom", "dirichlet", "mixed_dn"])
 @pytest.mark.parametrize("order", [0, 1, 2])
-def test_relax_levels(dt, bcname, order):
-    om, dm, _ = pair(dt, (32, 32, 32), (0.03, 0.03, 0.03), bcname, seed=1)
+@pytest.mark.parametrize("sweep", [1, -1])
+def test_relax_levels(dt, bcname, order, sweep):
+    """Every level, both relax paths: the two-colour TMA pass (sweep_cells=1 puts every
+    eligible level on it) and the per-colour launches."""
+    om, dm, _ = pair(dt, (32, 32, 32), (0.03, 0.03, 0.03), bcname, seed=1, sweep_cells=sweep)
     lib = O.lib()
     for lev in range(om.num_levels):
         it = 3
@@ -85,7 +89,8 @@ def test_restrict_and_prolong(dt, knobs):
 @pytest.mark.parametrize("dt", [F32, F64])
 @pytest.mark.parametrize("knobs", range(len(KNOBS)))
 @pytest.mark.parametrize("case", [((64, 64, 64), "neumann", 0, 0), ((48, 32, 64), "periodic", 1, 0),
-                                  ((32, 64, 32), "mixed_xdir", 0, 1), ((96, 48, 48), "mixed_all", 1, 1)])
+                                  ((32, 64, 32), "mixed_xdir", 0, 1), ((96, 48, 48), "mixed_all", 1, 1),
+                                  ((40, 24, 48), "mixed_dn", 1, 0), ((64, 48, 56), "dirichlet", 0, 0)])
 def test_kernel_paths_match_oracle(dt, knobs, case):
     shape, bcname, sym, disable_host = case
     om, dm, _ = pair(dt, shape, (0.02, 0.025, 0.02), bcname, seed=3, sym=sym, disable_host=disable_host,
