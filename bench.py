@@ -175,6 +175,7 @@ def run_gpu(args):
         s = ocu.Sol_MultigridPressureMixed3DDeviceD("ir") if kind == "ir" else ocu.Sol_MultigridPressure3DDevice(ocu.F64)
         s.bc = ocu.BoundaryConditionSet(ocu.BoundaryCondition(ocu.BC_NEUMANN, 0.0))
         s.ir_inner_cycles = args.ir_inner
+        s.sweep_cells = args.sweep_cells
         s.initialize_storage(n, n, n, h, h, h, rhs)
         _capi.check(lib.ocu_mg_set_stream(s._h, sh))
         return s
@@ -464,6 +465,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--ir-inner", type=int, default=3)
+    ap.add_argument("--sweep-cells", type=int, default=0,
+                    help="levels with at least this many cells use the two-colour TMA pass (0 = library "
+                         "default, -1 = never)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-secondary", action="store_true")
     ap.add_argument("--kernel-case", choices=["relax", "prolong", "restrict"],

@@ -28,12 +28,16 @@ __global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, con
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z * blockDim.z + threadIdx.z;
+  // blocks that hold no cell of the outer layer skip the ghost code entirely
+  const bool edge_block = blockIdx.x == 0 || (blockIdx.x + 1) * blockDim.x * 2 >= (unsigned)nz || blockIdx.y == 0 ||
+                          (blockIdx.y + 1) * blockDim.y >= (unsigned)ny || blockIdx.z == 0 ||
+                          (blockIdx.z + 1) * blockDim.z >= (unsigned)nx;
   if (i >= nx || j >= ny || t >= nz / 2) return;
   const int k = 2 * t + ((i + j + color) & 1);
   const long long id = (long long)i * xs + (long long)j * ys + k;
   const T nv = relax_point<T>(u, b, id, xs, ys, i, j, k, nx, ny, nz, c, diag);
   u[id] = nv;
-  ge.emit(i, j, k, nv);
+  if (edge_block) ge.emit(i, j, k, nv);
 }
 
 template <typename T>
@@ -52,7 +56,8 @@ ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const 
 }
 
 // Prolongation + correction + ghost writes (devf.cu:94-197 then the level1 fill).
-template <typename T>
+// EMIT = false compiles the ghost writes out (children that touch no face, or no fusable BCs).
+template <typename T, bool EMIT>
 __device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, long long tc, long long cx, long long cy,
                                              T *__restrict__ uf, long long f, long long fxs, long long fys, int ic,
                                              int jc, int kc, const GhostEmit<T> *ge) {
@@ -72,43 +77,47 @@ __device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, long long
     const T cpm0 = uc[tc + cx - cy], cp0m = uc[tc + cx - 1], cpmm = uc[tc + cx - cy - 1];
     const T cppm = uc[tc + cx + cy - 1], cpmp = uc[tc + cx - cy + 1];
     v = f000 + w1 * c000 + w2 * (cp00 + c0p0 + c00p) + w3 * (cpp0 + cp0p + c0pp) + w4 * cppp;
-    uf[f] = v; if (ge) ge->emit(i, j, k, v);
+    uf[f] = v; if (EMIT) ge->emit(i, j, k, v);
     v = f010 + w1 * c000 + w2 * (cp00 + c0m0 + c00p) + w3 * (cpm0 + cp0p + c0mp) + w4 * cpmp;
-    uf[f - fys] = v; if (ge) ge->emit(i, j - 1, k, v);
+    uf[f - fys] = v; if (EMIT) ge->emit(i, j - 1, k, v);
     v = f001 + w1 * c000 + w2 * (cp00 + c0p0 + c00m) + w3 * (cpp0 + cp0m + c0pm) + w4 * cppm;
-    uf[f - 1] = v; if (ge) ge->emit(i, j, k - 1, v);
+    uf[f - 1] = v; if (EMIT) ge->emit(i, j, k - 1, v);
     v = f011 + w1 * c000 + w2 * (cp00 + c0m0 + c00m) + w3 * (cpm0 + cp0m + c0mm) + w4 * cpmm;
-    uf[f - fys - 1] = v; if (ge) ge->emit(i, j - 1, k - 1, v);
+    uf[f - fys - 1] = v; if (EMIT) ge->emit(i, j - 1, k - 1, v);
     // the -x child with (0,0) y/z offsets takes its corner weight from cppp, as the reference
     // kernel does (devf.cu:94-197)
     const T cm00 = uc[tc - cx], cmp0 = uc[tc - cx + cy], cm0p = uc[tc - cx + 1];
     v = f100 + w1 * c000 + w2 * (cm00 + c0p0 + c00p) + w3 * (cmp0 + cm0p + c0pp) + w4 * cppp;
-    uf[f - fxs] = v; if (ge) ge->emit(i - 1, j, k, v);
+    uf[f - fxs] = v; if (EMIT) ge->emit(i - 1, j, k, v);
   }
   {  // remaining children on the -x side (coarse plane x-1)
     const T cm00 = uc[tc - cx], cmm0 = uc[tc - cx - cy], cm0p = uc[tc - cx + 1], cm0m = uc[tc - cx - 1];
     const T cmmm = uc[tc - cx - cy - 1], cmp0 = uc[tc - cx + cy], cmpm = uc[tc - cx + cy - 1];
     const T cmmp = uc[tc - cx - cy + 1];
     v = f110 + w1 * c000 + w2 * (cm00 + c0m0 + c00p) + w3 * (cmm0 + cm0p + c0mp) + w4 * cmmp;
-    uf[f - fxs - fys] = v; if (ge) ge->emit(i - 1, j - 1, k, v);
+    uf[f - fxs - fys] = v; if (EMIT) ge->emit(i - 1, j - 1, k, v);
     v = f101 + w1 * c000 + w2 * (cm00 + c0p0 + c00m) + w3 * (cmp0 + cm0m + c0pm) + w4 * cmpm;
-    uf[f - fxs - 1] = v; if (ge) ge->emit(i - 1, j, k - 1, v);
+    uf[f - fxs - 1] = v; if (EMIT) ge->emit(i - 1, j, k - 1, v);
     v = f111 + w1 * c000 + w2 * (cm00 + c0m0 + c00m) + w3 * (cmm0 + cm0m + c0mm) + w4 * cmmm;
-    uf[f - fxs - fys - 1] = v; if (ge) ge->emit(i - 1, j - 1, k - 1, v);
+    uf[f - fxs - fys - 1] = v; if (EMIT) ge->emit(i - 1, j - 1, k - 1, v);
   }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256, 3) k_prolong_emit(const T *__restrict__ uc, long long cx, long long cy, int cnx,
                                                       int cny, int cnz, T *__restrict__ uf, long long fxs,
-                                                      long long fys, GhostEmit<T> ge) {
+                                                      long long fys, const __grid_constant__ GhostEmit<T> ge) {
   const int kc = blockIdx.x * blockDim.x + threadIdx.x;
   const int jc = blockIdx.y * blockDim.y + threadIdx.y;
   const int ic = blockIdx.z;
   if (kc >= cnz || jc >= cny || ic >= cnx) return;
   const long long tc = (long long)ic * cx + (long long)jc * cy + kc;
   const long long f = (long long)(2 * ic + 1) * fxs + (long long)(2 * jc + 1) * fys + (2 * kc + 1);
-  prolong_cell<T>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, &ge);
+  // only children on the fine grid's outer layer are ghost sources
+  if (ic == 0 || ic == cnx - 1 || jc == 0 || jc == cny - 1 || kc == 0 || kc == cnz - 1)
+    prolong_cell<T, true>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, &ge);
+  else
+    prolong_cell<T, false>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, nullptr);
 }
 
 template <typename T>
@@ -436,7 +445,10 @@ __device__ void tail_body(const TailLevel<T> *lv, const TailParams<T> &P, int nt
       const int ic = q / (c.ny * c.nz), jc = (q / c.nz) % c.ny, kc = q % c.nz;
       const long long tc = (long long)ic * c.xs + (long long)jc * c.ys + kc;
       const long long fi = (long long)(2 * ic + 1) * f.xs + (long long)(2 * jc + 1) * f.ys + (2 * kc + 1);
-      prolong_cell<T>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, f.emit_ok ? &ge : nullptr);
+      if (f.emit_ok)
+        prolong_cell<T, true>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, &ge);
+      else
+        prolong_cell<T, false>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, nullptr);
     }
     __syncthreads();
     if (!f.emit_ok) {

@@ -116,7 +116,7 @@ __device__ __forceinline__ T sweep_update(const T *uc, const T *um, const T *up,
 }
 
 template <typename T>
-__global__ void __launch_bounds__(SweepTile<T>::THREADS) k_relax_sweep2(
+__global__ void __launch_bounds__(SweepTile<T>::THREADS, 3) k_relax_sweep2(
     const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_b, T *__restrict__ u_out,
     long long xs, long long ys, SweepArgs a, RelaxCoefD<T> c, const T *__restrict__ diag, GhostEmit<T> ge,
     int *__restrict__ err) {
@@ -244,13 +244,27 @@ __global__ void __launch_bounds__(SweepTile<T>::THREADS) k_relax_sweep2(
           const uint4 v = *reinterpret_cast<const uint4 *>(uc + (jr + 2) * S::W + S::H + kv);
           *reinterpret_cast<uint4 *>(dst_plane + (long long)j * ys + k) = v;
         }
-        const bool edge = s == 0 || s == a.nx - 1 || j0 == 0 || j0 + S::TJ >= a.ny || k0 == 0 || k0 + S::TK >= a.nz;
-        if (edge) {
+        if (s == 0 || s == a.nx - 1) {  // a face plane: every cell is a ghost source
           for (int q = threadIdx.x; q < S::TJ * S::TK; q += S::THREADS) {
             const int jr = q / S::TK, kk = q % S::TK;
             const int j = j0 + jr, k = k0 + kk;
             if (j >= a.ny || k >= a.nz) continue;
             ge.emit(s, j, k, uc[(jr + 2) * S::W + S::H + kk]);
+          }
+        } else if (j0 == 0 || j0 + S::TJ >= a.ny || k0 == 0 || k0 + S::TK >= a.nz) {
+          // rows j = 0, ny-1 and columns k = 0, nz-1 that fall in this tile
+          for (int q = threadIdx.x; q < 2 * S::TK + 2 * S::TJ; q += S::THREADS) {
+            int j, k;
+            if (q < 2 * S::TK) {
+              j = q < S::TK ? 0 : a.ny - 1;
+              k = k0 + (q % S::TK);
+            } else {
+              const int r = q - 2 * S::TK;
+              k = r < S::TJ ? 0 : a.nz - 1;
+              j = j0 + (r % S::TJ);
+            }
+            if (j < j0 || j >= j0 + S::TJ || j >= a.ny || k < k0 || k >= k0 + S::TK || k >= a.nz) continue;
+            ge.emit(s, j, k, uc[(j - j0 + 2) * S::W + S::H + (k - k0)]);
           }
         }
       }
