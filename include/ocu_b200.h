@@ -163,7 +163,7 @@ typedef struct ocu_mg_params {
                                     kernel per cycle; 0 = default (512), < 0 = off */
   int sweep_cells;               /* levels with at least this many cells relax both colours in
                                     one TMA-fed pass (out of place, same results; Dirichlet and
-                                    Neumann faces only); 0 = default (1048576), < 0 = off */
+                                    Neumann faces only); <= 0 = off (the default) */
 } ocu_mg_params;
 
 typedef struct ocu_mg_stats {

@@ -10,6 +10,7 @@
 // (i,j) row, lane t folds k = t, t+32, ... and the 32 lanes fold 16/8/4/2/1; rows are folded by
 // 256-wide trees (grid1dops.cu:33-115) in k_fold_rows.
 #include <atomic>
+#include <cstring>
 
 #include "bc_device.cuh"
 #include "ghost_emit.cuh"
@@ -461,10 +462,24 @@ __device__ void tail_body(const TailLevel<T> *lv, const TailParams<T> &P, int nt
   }
 }
 
+// Member of this CTA, or -1 when its state does not select it (single grid: member 0).
+__device__ __forceinline__ int batch_member(const BatchSel &sel, int m) {
+  if (!sel.state) return 0;
+  return sel.state[m] == sel.want ? m : -1;
+}
+
 template <typename T>
-__global__ void __launch_bounds__(1024) k_coarse_tail(const __grid_constant__ TailParams<T> P) {
+__global__ void __launch_bounds__(1024) k_coarse_tail(const __grid_constant__ TailParams<T> P,
+                                                      const __grid_constant__ TailBatch tb) {
   __shared__ TailLevel<T> lv[kMaxTailLevels];
-  if (threadIdx.x < P.nlev) lv[threadIdx.x] = P.lv[threadIdx.x];
+  const int m = batch_member(tb.sel, blockIdx.x);
+  if (m < 0) return;
+  if (threadIdx.x < P.nlev) {
+    TailLevel<T> d = P.lv[threadIdx.x];
+    d.u += m * tb.ms[threadIdx.x];
+    d.b += m * tb.ms[threadIdx.x];
+    lv[threadIdx.x] = d;
+  }
   __syncthreads();
   tail_body<T>(lv, P, blockDim.x);
 }
@@ -474,14 +489,25 @@ __global__ void __launch_bounds__(1024) k_coarse_tail(const __grid_constant__ Ta
 // interior of b are written back.  Only level s is read: the lower levels are zeroed /
 // restricted inside the schedule before they are used.
 template <typename T>
-__global__ void __launch_bounds__(512) k_coarse_tail_smem(const __grid_constant__ TailParams<T> P) {
+__global__ void __launch_bounds__(512) k_coarse_tail_smem(const __grid_constant__ TailParams<T> P,
+                                                           const __grid_constant__ TailBatch tb) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ TailLevel<T> lv[kMaxTailLevels];
+  __shared__ TailLevel<T> gl[kMaxTailLevels];  // this member's levels in global memory
+  const int m = batch_member(tb.sel, blockIdx.x);
+  if (m < 0) return;
   const int L = P.nlev;
+  if (threadIdx.x < L) {
+    TailLevel<T> d = P.lv[threadIdx.x];
+    d.u += m * tb.ms[threadIdx.x];
+    d.b += m * tb.ms[threadIdx.x];
+    gl[threadIdx.x] = d;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
     T *cur = reinterpret_cast<T *>(smem_raw);
     for (int l = 0; l < L; l++) {
-      TailLevel<T> d = P.lv[l];
+      TailLevel<T> d = gl[l];
       const long long sys = d.nz + 2, sxs = (long long)(d.ny + 2) * (d.nz + 2);
       const long long cells = (long long)(d.nx + 2) * sxs;
       d.xs = sxs;
@@ -496,7 +522,7 @@ __global__ void __launch_bounds__(512) k_coarse_tail_smem(const __grid_constant_
   __syncthreads();
   const int nt = blockDim.x;
   {  // stage level s
-    const TailLevel<T> &g = P.lv[0];
+    const TailLevel<T> &g = gl[0];
     const TailLevel<T> &sh = lv[0];
     const int cz = g.nz + 2, cy = g.ny + 2, cx = g.nx + 2;
     for (int q = threadIdx.x; q < cx * cy * cz; q += nt) {
@@ -509,7 +535,7 @@ __global__ void __launch_bounds__(512) k_coarse_tail_smem(const __grid_constant_
   tail_body<T>(lv, P, nt);
   __syncthreads();
   for (int l = 0; l < L; l++) {  // write back: u with its ghost shell, b interior below level s
-    const TailLevel<T> &g = P.lv[l];
+    const TailLevel<T> &g = gl[l];
     const TailLevel<T> &sh = lv[l];
     const int cz = g.nz + 2, cy = g.ny + 2, cx = g.nx + 2;
     for (int q = threadIdx.x; q < cx * cy * cz; q += nt) {
@@ -530,7 +556,7 @@ size_t tail_smem_bytes(const TailParams<T> &P) {
 }
 
 template <typename T>
-ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s) {
+ocu_status launch_coarse_tail_batch(const TailParams<T> &P, const TailBatch &tb, int members, cudaStream_t s) {
   const size_t bytes = tail_smem_bytes<T>(P);
   constexpr size_t kMaxSmem = 200 * 1024;
   if (bytes <= kMaxSmem) {
@@ -544,12 +570,348 @@ ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s) {
                          "cudaFuncSetAttribute(k_coarse_tail_smem)"));
       attr_set.fetch_or(bit);
     }
-    k_coarse_tail_smem<T><<<1, 512, bytes, s>>>(P);
+    k_coarse_tail_smem<T><<<members, 512, bytes, s>>>(P, tb);
     return check_launch("k_coarse_tail_smem");
   }
-  k_coarse_tail<T><<<1, 1024, 0, s>>>(P);
+  k_coarse_tail<T><<<members, 1024, 0, s>>>(P, tb);
   return check_launch("k_coarse_tail");
 }
+
+template <typename T>
+ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s) {
+  TailBatch tb;
+  std::memset(&tb, 0, sizeof(tb));
+  return launch_coarse_tail_batch<T>(P, tb, 1, s);
+}
+
+// ------------------------------------------------------------------------------------------
+// Ensemble (batched) kernels: the same cell arithmetic as the single-grid kernels above, over
+// `members` congruent grids laid out at base + m * ms.  blockIdx.z carries (member, z block);
+// members whose state differs from sel.want return at once.  Each member's result is
+// bit-identical to the single-grid kernel applied to that member alone.
+// ------------------------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_relax_color_emit_b(T *__restrict__ u, const T *__restrict__ b, long long xs,
+                                                            long long ys, int nx, int ny, int nz, int color,
+                                                            RelaxCoefD<T> c, const T *__restrict__ diag,
+                                                            const __grid_constant__ GhostEmit<T> ge, BatchSel sel,
+                                                            long long ms, int zb) {
+  const int m = batch_member(sel, blockIdx.z / zb);
+  if (m < 0) return;
+  const int bz = blockIdx.z % zb;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = bz * blockDim.z + threadIdx.z;
+  const bool edge_block = blockIdx.x == 0 || (blockIdx.x + 1) * blockDim.x * 2 >= (unsigned)nz || blockIdx.y == 0 ||
+                          (blockIdx.y + 1) * blockDim.y >= (unsigned)ny || bz == 0 ||
+                          (bz + 1) * blockDim.z >= (unsigned)nx;
+  if (i >= nx || j >= ny || t >= nz / 2) return;
+  u += m * ms;
+  b += m * ms;
+  const int k = 2 * t + ((i + j + color) & 1);
+  const long long id = (long long)i * xs + (long long)j * ys + k;
+  const T nv = relax_point<T>(u, b, id, xs, ys, i, j, k, nx, ny, nz, c, diag);
+  u[id] = nv;
+  if (edge_block) {
+    GhostEmit<T> g = ge;
+    g.p = u;
+    g.emit(i, j, k, nv);
+  }
+}
+
+template <typename T>
+ocu_status launch_relax_color_emit_b(T *u, const T *b, const ocu_layout &L, const T *diag, int color,
+                                     const RelaxParams &p, double hx, double hy, double hz, const BatchSel &sel,
+                                     long long ms, int members, const int block[3], cudaStream_t s) {
+  const RelaxCoefD<T> c = make_relax_coef_d<T>(p);
+  const int half = L.nz / 2;
+  if (half == 0) return OCU_OK;
+  dim3 bl(block[0], block[1], block[2]);
+  if ((int)bl.x > half) bl.x = half >= 16 ? 16 : (half >= 8 ? 8 : (half >= 4 ? 4 : half));
+  const int zb = (L.nx + bl.z - 1) / bl.z;
+  dim3 grid((half + bl.x - 1) / bl.x, (L.ny + bl.y - 1) / bl.y, (unsigned)(zb * members));
+  GhostEmit<T> ge{u, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(p.bc), (T)hx, (T)hy, (T)hz};
+  k_relax_color_emit_b<T><<<grid, bl, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c, diag, ge, sel,
+                                              ms, zb);
+  return check_launch("k_relax_color_emit_b");
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 3) k_prolong_emit_b(const T *__restrict__ uc, long long cx, long long cy,
+                                                           int cnx, int cny, int cnz, T *__restrict__ uf,
+                                                           long long fxs, long long fys,
+                                                           const __grid_constant__ GhostEmit<T> ge, BatchSel sel,
+                                                           long long cms, long long fms) {
+  const int m = batch_member(sel, blockIdx.z / cnx);
+  if (m < 0) return;
+  const int ic = blockIdx.z % cnx;
+  const int kc = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jc = blockIdx.y * blockDim.y + threadIdx.y;
+  if (kc >= cnz || jc >= cny) return;
+  uc += m * cms;
+  uf += m * fms;
+  const long long tc = (long long)ic * cx + (long long)jc * cy + kc;
+  const long long f = (long long)(2 * ic + 1) * fxs + (long long)(2 * jc + 1) * fys + (2 * kc + 1);
+  if (ic == 0 || ic == cnx - 1 || jc == 0 || jc == cny - 1 || kc == 0 || kc == cnz - 1) {
+    GhostEmit<T> g = ge;
+    g.p = uf;
+    prolong_cell<T, true>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, &g);
+  } else {
+    prolong_cell<T, false>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, nullptr);
+  }
+}
+
+template <typename T>
+ocu_status launch_prolong_emit_b(const T *uc, const ocu_layout &Lc, T *uf, const ocu_layout &Lf,
+                                 const ocu_bc_set &bc_fine, double hx, double hy, double hz, const BatchSel &sel,
+                                 long long cms, long long fms, int members, cudaStream_t s) {
+  dim3 block(Lc.nz >= 32 ? 32 : 16, 8);
+  dim3 grid((Lc.nz + block.x - 1) / block.x, (Lc.ny + block.y - 1) / block.y, (unsigned)(Lc.nx * members));
+  GhostEmit<T> ge{uf, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, to_dev(bc_fine), (T)hx, (T)hy, (T)hz};
+  k_prolong_emit_b<T><<<grid, block, 0, s>>>(uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf, Lf.xstride,
+                                             Lf.ystride, ge, sel, cms, fms);
+  return check_launch("k_prolong_emit_b");
+}
+
+// Residual + restriction (+ level-0 norm partials) per member; rows of member m at
+// rows + m * nrows (nrows = fine nx * ny).
+template <typename T, bool NORM>
+__global__ void __launch_bounds__(256) k_residual_restrict_b(const T *__restrict__ u, const T *__restrict__ b,
+                                                             long long xs, long long ys, int nx, int ny, int nz,
+                                                             ResCoefT<T> c, T *__restrict__ bc_, long long bxs,
+                                                             long long bys, int cnx, int cny, int cnz,
+                                                             T *__restrict__ rows2, BatchSel sel, long long fms,
+                                                             long long cms) {
+  const int m = batch_member(sel, blockIdx.z / cnx);
+  if (m < 0) return;
+  const int ic = blockIdx.z % cnx;
+  const int lane = threadIdx.x;
+  const int jc = blockIdx.y * blockDim.y + threadIdx.y;
+  if (jc >= cny) return;
+  u += m * fms;
+  b += m * fms;
+  bc_ += m * cms;
+  T acc2[4] = {0, 0, 0, 0}, accinf[4] = {0, 0, 0, 0};
+  const long long frow = (long long)(2 * ic) * xs + (long long)(2 * jc) * ys;
+  for (int cbase = 0; cbase < cnz; cbase += 32) {
+    const int kc = cbase + lane;
+    T r[8];
+    if (kc < cnz) {
+      const long long ri = frow + 2 * kc;
+      r[0] = residual_at<T>(u, b, ri, xs, ys, c);
+      r[1] = residual_at<T>(u, b, ri + 1, xs, ys, c);
+      r[2] = residual_at<T>(u, b, ri + ys, xs, ys, c);
+      r[3] = residual_at<T>(u, b, ri + 1 + ys, xs, ys, c);
+      r[4] = residual_at<T>(u, b, ri + xs, xs, ys, c);
+      r[5] = residual_at<T>(u, b, ri + 1 + xs, xs, ys, c);
+      r[6] = residual_at<T>(u, b, ri + ys + xs, xs, ys, c);
+      r[7] = residual_at<T>(u, b, ri + 1 + ys + xs, xs, ys, c);
+      bc_[(long long)ic * bxs + (long long)jc * bys + kc] =
+          (T)0.125 * (r[0] + r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7]);
+    } else {
+#pragma unroll
+      for (int q = 0; q < 8; q++) r[q] = 0;
+    }
+    if (NORM) {
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        fold_chunk<T>(r[2 * q], r[2 * q + 1], 2 * cbase, nz, lane, acc2[q], accinf[q], true, false);
+    }
+  }
+  if (NORM) {
+    T *rows = rows2 + (long long)m * nx * ny;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * ic + (q >> 1), j = 2 * jc + (q & 1);
+      const T v = warp_tree<T>(acc2[q], false);
+      if (lane == 0) rows[(long long)i * ny + j] = v;
+    }
+  }
+}
+
+template <typename T>
+ocu_status launch_residual_restrict_b(const T *u, const T *b, const ocu_layout &Lf, T *bc_, const ocu_layout &Lc,
+                                      double h, double fx, double fy, double fz, T *rows2, const BatchSel &sel,
+                                      long long fms, long long cms, int members, cudaStream_t s) {
+  dim3 block(32, 8), grid(1, (Lc.ny + 7) / 8, (unsigned)(Lc.nx * members));
+  const ResCoefT<T> c = res_coef<T>(h, fx, fy, fz);
+  if (rows2)
+    k_residual_restrict_b<T, true><<<grid, block, 0, s>>>(u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
+                                                          Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, sel,
+                                                          fms, cms);
+  else
+    k_residual_restrict_b<T, false><<<grid, block, 0, s>>>(u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c,
+                                                           bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr,
+                                                           sel, fms, cms);
+  return check_launch("k_residual_restrict_b");
+}
+
+// Residual norm partials of level 0 (no restriction), per member.
+template <typename T>
+__global__ void __launch_bounds__(256) k_residual_rows_b(const T *__restrict__ u, const T *__restrict__ b,
+                                                         long long xs, long long ys, int nx, int ny, int nz,
+                                                         ResCoefT<T> c, T *__restrict__ rows2, BatchSel sel,
+                                                         long long ms) {
+  const int m = batch_member(sel, blockIdx.z / nx);
+  if (m < 0) return;
+  const int i = blockIdx.z % nx;
+  const int lane = threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (j >= ny) return;
+  u += m * ms;
+  b += m * ms;
+  T acc2 = 0, accinf = 0;
+  const long long row = (long long)i * xs + (long long)j * ys;
+  for (int base = 0; base < nz; base += 64) {
+    const int k0 = base + 2 * lane;
+    T e0 = 0, e1 = 0;
+    if (k0 < nz) e0 = residual_at<T>(u, b, row + k0, xs, ys, c);
+    if (k0 + 1 < nz) e1 = residual_at<T>(u, b, row + k0 + 1, xs, ys, c);
+    fold_chunk<T>(e0, e1, base, nz, lane, acc2, accinf, true, false);
+  }
+  const T v = warp_tree<T>(acc2, false);
+  if (lane == 0) rows2[(long long)m * nx * ny + (long long)i * ny + j] = v;
+}
+
+template <typename T>
+ocu_status launch_residual_rows_b(const T *u, const T *b, const ocu_layout &L, double h, double fx, double fy,
+                                  double fz, T *rows2, const BatchSel &sel, long long ms, int members,
+                                  cudaStream_t s) {
+  dim3 block(32, 8), grid(1, (L.ny + 7) / 8, (unsigned)(L.nx * members));
+  k_residual_rows_b<T><<<grid, block, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz,
+                                              res_coef<T>(h, fx, fy, fz), rows2, sel, ms);
+  return check_launch("k_residual_rows_b");
+}
+
+// Per-member fold of the row sums, one CTA per member, in exactly k_fold_rows' order: 256-row
+// blocks folded by a 256-wide tree into partials, then the partials folded 256 at a time.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fold_rows_b(const T *__restrict__ rows, long long nrows, T *partial,
+                                                     long long pstride, double *sums, BatchSel sel) {
+  __shared__ T sh[256];
+  const int m = batch_member(sel, blockIdx.x);
+  if (m < 0) return;
+  rows += (long long)m * nrows;
+  T *part = partial + (long long)m * pstride;
+  const long long nb = (nrows + 255) / 256;
+  for (long long bb = 0; bb < nb; bb++) {
+    const long long idx = bb * 256 + threadIdx.x;
+    sh[threadIdx.x] = idx < nrows ? rows[idx] : (T)0;
+    __syncthreads();
+    for (int stride = 128; stride > 0; stride >>= 1) {
+      if (threadIdx.x < stride) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + stride];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) part[bb] = sh[0];
+    __syncthreads();
+  }
+  long long count = nb;
+  while (count > 1) {
+    const long long nb2 = (count + 255) / 256;
+    for (long long bb = 0; bb < nb2; bb++) {
+      const long long q = bb * 256 + threadIdx.x;
+      sh[threadIdx.x] = q < count ? part[q] : (T)0;
+      __syncthreads();
+      for (int stride = 128; stride > 0; stride >>= 1) {
+        if (threadIdx.x < stride) sh[threadIdx.x] = sh[threadIdx.x] + sh[threadIdx.x + stride];
+        __syncthreads();
+      }
+      if (threadIdx.x == 0) part[bb] = sh[0];
+      __syncthreads();
+    }
+    count = nb2;
+  }
+  if (threadIdx.x == 0) sums[m] = (double)part[0];
+}
+
+template <typename T>
+ocu_status launch_fold_rows_b(const T *rows, long long nrows, T *partial, long long pstride, double *sums,
+                              const BatchSel &sel, int members, cudaStream_t s) {
+  k_fold_rows_b<T><<<members, 256, 0, s>>>(rows, nrows, partial, pstride, sums, sel);
+  return check_launch("k_fold_rows_b");
+}
+
+// Level-1 ghost fill of each selected member (one CTA per member); with `retire` the member's
+// state is set to 0 afterwards (members that converged this cycle get their final fill).
+template <typename T>
+__global__ void __launch_bounds__(512) k_bc_fill_b(T *u, long long xs, long long ys, int nx, int ny, int nz,
+                                                   const __grid_constant__ BCDev bc, T hx, T hy, T hz, BatchSel sel,
+                                                   long long ms, int *state, int retire) {
+  const int m = batch_member(sel, blockIdx.x);
+  if (m < 0) return;
+  level1_fill_block<T>(u + m * ms, xs, ys, nx, ny, nz, bc, hx, hy, hz);
+  if (retire && threadIdx.x == 0) state[m] = 0;
+}
+
+template <typename T>
+ocu_status launch_bc_fill_b(T *u, const ocu_layout &L, const ocu_bc_set &bc, double hx, double hy, double hz,
+                            const BatchSel &sel, long long ms, int members, int *state, bool retire,
+                            cudaStream_t s) {
+  k_bc_fill_b<T><<<members, 512, 0, s>>>(u, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(bc), (T)hx, (T)hy,
+                                         (T)hz, sel, ms, state, retire ? 1 : 0);
+  return check_launch("k_bc_fill_b");
+}
+
+// Convergence decision of every active member, as the host driver makes it: l2 = sqrt(sum / N)
+// in T, converged when l2 < tol (sol_mgpressure3d.cpp:186-236).  initial: the check before any
+// cycle (converged members are done: state 0); otherwise a counted cycle (converged: state 2,
+// so the final ghost fill runs).  Writes the number of members still active to *active.
+template <typename T>
+__global__ void __launch_bounds__(1024) k_converge_b(const double *sums, long long ncell, const double *tol,
+                                                     int *state, int *vcycles, double *last_l2, int *active,
+                                                     int members, int initial) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int m = threadIdx.x; m < members; m += blockDim.x) {
+    if (state[m] != 1) continue;
+    T rn = (T)sums[m];
+    rn /= (T)ncell;
+    const double l2 = (double)sqrt(rn);
+    last_l2[m] = l2;
+    if (!initial) vcycles[m] += 1;
+    if (l2 < tol[m]) {
+      state[m] = initial ? 0 : 2;
+    } else {
+      mine++;
+    }
+  }
+  atomicAdd(&cnt, mine);
+  __syncthreads();
+  if (threadIdx.x == 0) *active = cnt;
+}
+
+template <typename T>
+ocu_status launch_converge_b(const double *sums, long long ncell, const double *tol, int *state, int *vcycles,
+                             double *last_l2, int *active, int members, bool initial, cudaStream_t s) {
+  k_converge_b<T><<<1, 1024, 0, s>>>(sums, ncell, tol, state, vcycles, last_l2, active, members, initial ? 1 : 0);
+  return check_launch("k_converge_b");
+}
+
+#define INST_B(T)                                                                                              \
+  template ocu_status launch_relax_color_emit_b<T>(T *, const T *, const ocu_layout &, const T *, int,         \
+                                                   const RelaxParams &, double, double, double,                \
+                                                   const BatchSel &, long long, int, const int[3],             \
+                                                   cudaStream_t);                                              \
+  template ocu_status launch_prolong_emit_b<T>(const T *, const ocu_layout &, T *, const ocu_layout &,         \
+                                               const ocu_bc_set &, double, double, double, const BatchSel &,   \
+                                               long long, long long, int, cudaStream_t);                       \
+  template ocu_status launch_residual_restrict_b<T>(const T *, const T *, const ocu_layout &, T *,              \
+                                                    const ocu_layout &, double, double, double, double, T *,    \
+                                                    const BatchSel &, long long, long long, int, cudaStream_t); \
+  template ocu_status launch_residual_rows_b<T>(const T *, const T *, const ocu_layout &, double, double,       \
+                                                double, double, T *, const BatchSel &, long long, int,          \
+                                                cudaStream_t);                                                 \
+  template ocu_status launch_fold_rows_b<T>(const T *, long long, T *, long long, double *, const BatchSel &,    \
+                                            int, cudaStream_t);                                                \
+  template ocu_status launch_bc_fill_b<T>(T *, const ocu_layout &, const ocu_bc_set &, double, double, double,  \
+                                          const BatchSel &, long long, int, int *, bool, cudaStream_t);        \
+  template ocu_status launch_converge_b<T>(const double *, long long, const double *, int *, int *, double *,    \
+                                           int *, int, bool, cudaStream_t);
+INST_B(float)
+INST_B(double)
+#undef INST_B
 
 #define INST(T)                                                                                                \
   template ocu_status launch_relax_color_emit<T>(T *, const T *, const ocu_layout &, const T *, int,           \
@@ -562,7 +924,8 @@ ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s) {
                                                   const ocu_layout &, double, double, double, double, T *, T *, \
                                                   cudaStream_t);                                               \
   template ocu_status launch_fold_rows<T>(const T *, long long, bool, void *, double *, cudaStream_t);          \
-  template ocu_status launch_coarse_tail<T>(const TailParams<T> &, cudaStream_t);
+  template ocu_status launch_coarse_tail<T>(const TailParams<T> &, cudaStream_t);                               \
+  template ocu_status launch_coarse_tail_batch<T>(const TailParams<T> &, const TailBatch &, int, cudaStream_t);
 INST(float)
 INST(double)
 #undef INST

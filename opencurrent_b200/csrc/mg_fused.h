@@ -158,6 +158,18 @@ struct TailParams {
   CoarseCoef<T> cc;
 };
 
+// Member selection of the ensemble (batched) launches: member m of a level lives at
+// base + m * stride; a launch processes the members whose state equals `want`.  state ==
+// nullptr: a single grid (member 0 only).
+struct BatchSel {
+  const int *state;
+  int want;
+};
+struct TailBatch {
+  BatchSel sel;
+  long long ms[kMaxTailLevels];  // member stride of each tail level (elements)
+};
+
 template <typename T>
 ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const T *diag, int color,
                                    const RelaxParams &p, double hx, double hy, double hz, cudaStream_t s);
@@ -175,6 +187,9 @@ ocu_status launch_fold_rows(const T *rows, long long nrows, bool is_max, void *s
                             cudaStream_t s);
 template <typename T>
 ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s);
+// The same schedule for `members` grids at once, one CTA per member.
+template <typename T>
+ocu_status launch_coarse_tail_batch(const TailParams<T> &P, const TailBatch &tb, int members, cudaStream_t s);
 
 // Opaque copy of a CUtensorMap (128 bytes, 64-byte aligned) so host headers need no cuda.h.
 struct alignas(64) SweepTmap {

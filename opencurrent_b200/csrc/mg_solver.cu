@@ -142,13 +142,21 @@ ocu_status MGCore<T>::init(const ocu_bc_set &bc_, bool disable_host, int nx, int
   OCU_TRY(check_cuda(cudaMallocHost(&h_norms, 4 * sizeof(double)), "cudaMallocHost(norms)"));
   std::memset(h_norms, 0, 4 * sizeof(double));
   d_err = reinterpret_cast<int *>(d_norms + 2);
-  // second u buffer + TMA maps for every level the two-colour pass may run on
   grids_u2.assign(num_levels, nullptr);
   tm_u.resize(num_levels);
   tm_u2.resize(num_levels);
   tm_b.resize(num_levels);
+  return check_cuda(cudaStreamSynchronize(stream), "initialize_storage");
+}
+
+// Second u buffer + TMA maps for every level the two-colour pass may run on; allocated when the
+// pass is first enabled (never inside a stream capture: set_params / initialize_storage only).
+template <typename T>
+ocu_status MGCore<T>::ensure_sweep_buffers() {
+  const ocu_dtype dt = sizeof(T) == 8 ? OCU_F64 : OCU_F32;
+  ocu_status st = OCU_OK;
   for (int l = 0; l < num_levels; l++) {
-    if (!sweep2_supported(lay[l], bc_at_level(l))) continue;
+    if (grids_u2[l] || !sweep2_supported(lay[l], bc_at_level(l))) continue;
     if ((long long)dim[l][0] * dim[l][1] * dim[l][2] < 512) continue;
     grids_u2[l] = alloc_grid(dt, lay[l], &st);
     if (!grids_u2[l]) return st;
@@ -156,7 +164,7 @@ ocu_status MGCore<T>::init(const ocu_bc_set &bc_, bool disable_host, int nx, int
     OCU_TRY(make_sweep_tmap<T>(grids_u2[l]->buf, lay[l], &tm_u2[l]));
     OCU_TRY(make_sweep_tmap<T>(grids_b[l]->buf, lay[l], &tm_b[l]));
   }
-  return check_cuda(cudaStreamSynchronize(stream), "initialize_storage");
+  return OCU_OK;
 }
 
 template <typename T>
@@ -243,6 +251,7 @@ ocu_status MGCore<T>::relax(int level, int iterations, int order) {
 template <typename T>
 bool MGCore<T>::sweep2_ok(int level) const {
   if (!fused || sweep_cells <= 0 || level >= (int)grids_u2.size() || !grids_u2[level]) return false;
+  if (!sweep2_supported(lay[level], bc_at_level(level))) return false;  // the BCs may have changed
   return (long long)dim[level][0] * dim[level][1] * dim[level][2] >= sweep_cells;
 }
 
@@ -873,18 +882,20 @@ ocu_status MGSolver::initialize_storage(int nx, int ny, int nz, double hx, doubl
     }
   }
   stats.num_levels = num_levels;
-  apply_knobs();
+  OCU_TRY(apply_knobs());
   initialized = true;
   return OCU_OK;
 }
 
-void MGSolver::apply_knobs() {
+ocu_status MGSolver::apply_knobs() {
   const int tc = prm.tail_cells == 0 ? kDefaultTailCells : (prm.tail_cells < 0 ? 0 : prm.tail_cells);
   cf.fused = cd.fused = prm.unfused == 0;
   cf.store_residuals = cd.store_residuals = prm.store_residual_grids != 0;
   cf.tail_cells = cd.tail_cells = tc;
-  cf.sweep_cells = cd.sweep_cells =
-      prm.sweep_cells == 0 ? kDefaultSweepCells : (prm.sweep_cells < 0 ? 0 : prm.sweep_cells);
+  cf.sweep_cells = cd.sweep_cells = prm.sweep_cells <= 0 ? kDefaultSweepCells : prm.sweep_cells;
+  if (cf.sweep_cells > 0 && cf.num_levels > 0) OCU_TRY(cf.ensure_sweep_buffers());
+  if (cd.sweep_cells > 0 && cd.num_levels > 0) OCU_TRY(cd.ensure_sweep_buffers());
+  return OCU_OK;
 }
 
 ocu_status MGSolver::set_params(const ocu_mg_params &p) {
@@ -893,9 +904,8 @@ ocu_status MGSolver::set_params(const ocu_mg_params &p) {
   cd.bc = p.bc;
   if (kind == OCU_MG_MIXED_IR) bc_make_homogeneous(&cf.bc);
   cf.disable_relax_on_host = cd.disable_relax_on_host = p.disable_relax_on_host != 0;
-  apply_knobs();
   clear_graphs();  // captured schedules depend on every parameter
-  return OCU_OK;
+  return apply_knobs();
 }
 
 // Work runs on the caller's stream.  The legacy default stream (NULL) cannot be captured into a

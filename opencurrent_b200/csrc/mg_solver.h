@@ -18,9 +18,10 @@ int mg_num_levels(int nx, int ny, int nz);
 // One CTA runs the coarse end of a cycle up to 8^3 cells (a 16^3 level already keeps one SM
 // busy longer than its separate launches take).
 constexpr int kDefaultTailCells = 512;
-// The two-colour TMA pass needs enough (tile, plane) steps to fill every SM; below about a
-// million cells the colour launches finish sooner.
-constexpr int kDefaultSweepCells = 1 << 20;
+// The two-colour TMA pass is off unless asked for: at 256^3 FP32 it takes 110 us per sweep
+// against 124 us for the two colour launches, but it is instruction-bound, slower in FP64, and a
+// whole solve is not faster with it yet.
+constexpr int kDefaultSweepCells = 0;
 double mg_optimal_omega(double fx, double fy, double fz);
 
 // The virtual level operations of Sol_MultigridPressure3DBase (sol_mgpressure3d.h:76-80).
@@ -76,6 +77,7 @@ struct MGCore : CoreOps {
   ocu_status clear_level(int level) override;
   bool emit_ok(int level) const;
   bool sweep2_ok(int level) const;
+  ocu_status ensure_sweep_buffers();
   ocu_status relax_pairs(int level, int iterations, int order);
   ocu_status enqueue_restrict_residuals(int fine, int coarse, bool want_l2, bool want_linf) override;
   ocu_status finish_norms(int fine, double *l2, double *linf) override;
@@ -150,7 +152,7 @@ struct MGSolver {
   int coarse_iters() const;
   ocu_status initialize_storage(int nx, int ny, int nz, double hx, double hy, double hz, ocu_grid *rhs);
   ocu_status set_params(const ocu_mg_params &p);
-  void apply_knobs();
+  ocu_status apply_knobs();
   void set_stream(cudaStream_t s);
   ocu_status do_fmg(double tol, int max_iter, double *l2, double *linf);
   ocu_status do_vcycle(double tol, int max_iter, double *l2, double *linf);
