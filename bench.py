@@ -36,7 +36,8 @@ N_CFG3 = 256
 TOL_REL = 1e-10
 
 
-from opencurrent_b200.workloads import config1_rhs, fourier_rhs, interior, padded, rayleigh_benard  # noqa: E402
+from opencurrent_b200 import _capi  # noqa: E402
+from opencurrent_b200.workloads import config1_rhs, ensemble_sizes, fourier_rhs, interior, padded, rayleigh_benard  # noqa: E402
 
 
 # --------------------------------------------------------------------------- clocks -----
@@ -363,7 +364,54 @@ def run_secondary(torch, ocu, _capi, lib, stream, sh):
     out["ns_128x128x64_fp32_steps_per_s"] = round(steps / (ms * 1e-3), 2)
     out["ns_ms_per_step"] = round(ms / steps, 4)
     out["ns_steps_projection_above_tol"] = unconverged
+    out.update(run_ensemble(torch, ocu, stream, sh))
     return out
+
+
+def run_ensemble(torch, ocu, stream, sh, count=512):
+    """512 independent FP32 Neumann solves, sizes from {32,48,64,96}^3 (seed 1), rhs U[-1,1]
+    mean-removed (seed 1000 + index), each to 1e-6 relative L2, as one ensemble: autotuned
+    first (not timed), then timed from a zero guess."""
+    sizes = ensemble_sizes(count, 1)
+    dims = [(n, n, n) for n in sizes]
+    ens = ocu.PressureEnsemble(ocu.F32, dims, [(1.0 / n,) * 3 for n in sizes])
+    ens.set_stream(stream.cuda_stream)
+    tols = []
+    for m, n in enumerate(sizes):
+        b = np.random.default_rng(1000 + m).uniform(-1.0, 1.0, (n, n, n))
+        b -= b.mean()
+        L = ocu.layout(n, n, n)
+        ens.rhs(m).copy_from_host(padded(b, L, np.float32))
+        tols.append(1e-6 * float(np.sqrt(np.mean(b ** 2))))
+    ens.autotune(tols, 30)
+    pressures = [ens.pressure(m) for m in range(count)]
+
+    def zero():
+        for g in pressures:
+            _capi.check(ocu.load().ocu_grid_clear(g.handle, 0.0, sh))
+
+    zero()
+    ens.solve(tols, 30)  # graphs recorded
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps, total = 3, 0.0
+    for _ in range(reps):
+        zero()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        conv = ens.solve(tols, 30)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total += e0.elapsed_time(e1)
+    ms = total / reps
+    cycles = [ens.member_stats(m).vcycles for m in range(count)]
+    # per member: (cycles + FMG ramp ~ 1/7 cycle) x 12.57 N s (one V-cycle's compulsory bytes)
+    alg = sum((c + 1.0 / 7.0) * 12.57 * n ** 3 * 4 for c, n in zip(cycles, sizes))
+    return {"ensemble_512_ms": round(ms, 3), "ensemble_members_converged": conv,
+            "ensemble_alg_gbs": round(alg / (ms * 1e-3) / 1e9, 1),
+            "ensemble_vcycles_mean": round(float(np.mean(cycles)), 2),
+            "ensemble_classes": [{"n": c["dims"][0], "members": c["members"], "nu": [c["nu1"], c["nu2"]],
+                                  "relax_block": list(c["relax_block"]), "tuned_ms": round(c["ms"], 3)}
+                                 for c in ens.classes()]}
 
 
 # --------------------------------------------------------------------------- CPU arms ---

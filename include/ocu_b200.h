@@ -212,6 +212,45 @@ ocu_status ocu_mg_prolong(ocu_mg *mg, int core, int coarse, int fine);
 /* Wait for all work the solver enqueued. */
 ocu_status ocu_mg_synchronize(ocu_mg *mg);
 
+/* ---- ensembles of independent pressure solves ---------------------------------------------
+ * No single counterpart in the reference: many Sol_MultigridPressure3DDevice<T>::solve calls
+ * (sol_mgpressure3d.cpp:332-370) on right-hand sides of uneven sizes, run together.  Members
+ * with equal dimensions and spacings form a size class; every multigrid step of a class is one
+ * launch over all its members, convergence is decided per member on the device, and each class
+ * replays one CUDA graph per V-cycle.  Each member's pressure is bit-identical to a single
+ * solver's with the same parameters (convergence must be OCU_CONVERGENCE_L2; every face BC must
+ * allow fused ghost writes: no BC_NONE, even periodic axes). */
+typedef struct ocu_ens ocu_ens;
+typedef struct ocu_ens_tuning {
+  int nu1, nu2;          /* smoothing counts of the class's V-cycles */
+  int relax_block[3];    /* colour-sweep CTA shape: k pairs, j, i (product <= 256) */
+  double ms;             /* autotuner: measured solve time of the class with this setting */
+} ocu_ens_tuning;
+/* dims: 3 ints per member (nx, ny, nz); h: 3 doubles per member (hx, hy, hz); params as for
+ * ocu_mg_create (bc, nu1, nu2, make_symmetric_operator, disable_relax_on_host are used). */
+ocu_status ocu_ens_create(ocu_dtype dtype, int members, const int *dims, const double *h,
+                          const ocu_mg_params *params, ocu_ens **out);
+void ocu_ens_destroy(ocu_ens *e);
+/* Solves start after prior work on this stream; ocu_ens_solve returns when all is done. */
+ocu_status ocu_ens_set_stream(ocu_ens *e, ocu_stream s);
+/* Views of one member's right-hand side and pressure (standard layout of its dimensions,
+ * ghost 1); owned by the ensemble, valid until ocu_ens_destroy, never ocu_grid_destroy'ed. */
+ocu_status ocu_ens_rhs(ocu_ens *e, int member, ocu_grid **out);
+ocu_status ocu_ens_pressure(ocu_ens *e, int member, ocu_grid **out);
+/* tol: one absolute L2 tolerance per member; each member runs the FMG + V-cycle schedule of
+ * solve() from its current pressure, at most max_iter + 1 level-0 cycles.  *converged gets the
+ * number of members that reached their tolerance; OCU_ERR_NOT_CONVERGED if some did not. */
+ocu_status ocu_ens_solve(ocu_ens *e, const double *tol, int max_iter, int *converged);
+/* vcycles and last_l2 of the member's last solve. */
+ocu_status ocu_ens_member_stats(const ocu_ens *e, int member, ocu_mg_stats *stats);
+ocu_status ocu_ens_num_classes(const ocu_ens *e, int *n);
+ocu_status ocu_ens_class_info(const ocu_ens *e, int cls, int *dims, int *members,
+                              ocu_ens_tuning *tuning);
+ocu_status ocu_ens_set_tuning(ocu_ens *e, int cls, const ocu_ens_tuning *tuning);
+/* Per class, times whole solves from a zero guess for several smoothing pairs and colour-sweep
+ * shapes and keeps the fastest that converges every member; leaves every pressure zeroed. */
+ocu_status ocu_ens_autotune(ocu_ens *e, const double *tol, int max_iter);
+
 /* ---- projection (Sol_ProjectDivergence3DDevice<T>, sol_project3d.h:29-129) ------------- */
 ocu_status ocu_project_create(ocu_dtype dtype, ocu_project **out);
 void ocu_project_destroy(ocu_project *p);

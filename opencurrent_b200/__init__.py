@@ -324,6 +324,91 @@ def Sol_MultigridPressure3DDeviceD():
     return Sol_MultigridPressure3DDevice(F64)
 
 
+class PressureEnsemble:
+    """Many independent pressure solves of uneven sizes run together (ocu_ens_* in the C ABI).
+
+    Members with the same dimensions and spacings form a size class; every multigrid step of a
+    class is one launch over all its members and convergence is decided per member on the
+    device.  Each member's pressure is bit-identical to Sol_MultigridPressure3DDevice.solve on
+    that member alone with the same parameters.
+    """
+
+    def __init__(self, dtype, dims, spacings, bc=None, nu1=2, nu2=2, make_symmetric_operator=False,
+                 disable_relax_on_host=False):
+        lib = load()
+        n = len(dims)
+        d = (C.c_int * (3 * n))(*[int(v) for t in dims for v in t])
+        h = (C.c_double * (3 * n))(*[float(v) for t in spacings for v in t])
+        p = MGParams()
+        lib.ocu_mg_params_default(C.byref(p))
+        p.bc = (bc or BoundaryConditionSet(BoundaryCondition(BC_NEUMANN, 0.0))).to_c()
+        p.nu1, p.nu2 = nu1, nu2
+        p.make_symmetric_operator = int(bool(make_symmetric_operator))
+        p.disable_relax_on_host = int(bool(disable_relax_on_host))
+        handle = C.c_void_p()
+        check(lib.ocu_ens_create(dtype, n, d, h, C.byref(p), C.byref(handle)))
+        self._h = handle.value
+        self.dtype = dtype
+        self.count = n
+
+    def rhs(self, m):
+        out = C.c_void_p()
+        check(load().ocu_ens_rhs(self._h, m, C.byref(out)))
+        return Grid3DDevice._borrow(out.value, self)
+
+    def pressure(self, m):
+        out = C.c_void_p()
+        check(load().ocu_ens_pressure(self._h, m, C.byref(out)))
+        return Grid3DDevice._borrow(out.value, self)
+
+    def set_stream(self, stream_handle):
+        check(load().ocu_ens_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    def solve(self, tol, max_iter=20):
+        """tol: absolute L2 tolerance per member.  Returns the number of members converged."""
+        t = (C.c_double * self.count)(*[float(v) for v in tol])
+        conv = C.c_int()
+        check(load().ocu_ens_solve(self._h, t, int(max_iter), C.byref(conv)), allow=(ERR_NOT_CONVERGED,))
+        return conv.value
+
+    def autotune(self, tol, max_iter=20):
+        t = (C.c_double * self.count)(*[float(v) for v in tol])
+        check(load().ocu_ens_autotune(self._h, t, int(max_iter)))
+
+    def member_stats(self, m):
+        st = MGStats()
+        check(load().ocu_ens_member_stats(self._h, m, C.byref(st)))
+        return st
+
+    def classes(self):
+        lib = load()
+        n = C.c_int()
+        check(lib.ocu_ens_num_classes(self._h, C.byref(n)))
+        out = []
+        for c in range(n.value):
+            dims = (C.c_int * 3)()
+            members = C.c_int()
+            t = EnsTuning()
+            check(lib.ocu_ens_class_info(self._h, c, dims, C.byref(members), C.byref(t)))
+            out.append({"dims": tuple(dims), "members": members.value, "nu1": t.nu1, "nu2": t.nu2,
+                        "relax_block": tuple(t.relax_block), "ms": t.ms})
+        return out
+
+    def set_tuning(self, cls, nu1, nu2, relax_block=(32, 4, 2)):
+        t = EnsTuning()
+        t.nu1, t.nu2 = nu1, nu2
+        t.relax_block[:] = list(relax_block)
+        check(load().ocu_ens_set_tuning(self._h, cls, C.byref(t)))
+
+    def __del__(self):
+        try:
+            if self._h:
+                load().ocu_ens_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
 class Sol_MultigridPressureMixed3DDeviceD(_MGBase):
     """FP64-interface mixed solver.  algorithm='ir' (default): FP32 V-cycles inside FP64
     iterative refinement; algorithm='warmstart': the reference algorithm

@@ -61,6 +61,10 @@ class MGStats(C.Structure):
                 ("last_l2", C.c_double), ("last_linf", C.c_double), ("omega", C.c_double)]
 
 
+class EnsTuning(C.Structure):
+    _fields_ = [("nu1", C.c_int), ("nu2", C.c_int), ("relax_block", C.c_int * 3), ("ms", C.c_double)]
+
+
 class NSParams(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double),
@@ -118,6 +122,17 @@ SIGNATURES = {
     "ocu_mg_restrict_residuals": (I, [P, I, I, I, C.POINTER(D), C.POINTER(D)]),
     "ocu_mg_prolong": (I, [P, I, I, I]),
     "ocu_mg_synchronize": (I, [P]),
+    "ocu_ens_create": (I, [I, I, C.POINTER(C.c_int), C.POINTER(D), C.POINTER(MGParams), PP]),
+    "ocu_ens_destroy": (None, [P]),
+    "ocu_ens_set_stream": (I, [P, P]),
+    "ocu_ens_rhs": (I, [P, I, PP]),
+    "ocu_ens_pressure": (I, [P, I, PP]),
+    "ocu_ens_solve": (I, [P, C.POINTER(D), I, C.POINTER(C.c_int)]),
+    "ocu_ens_member_stats": (I, [P, I, C.POINTER(MGStats)]),
+    "ocu_ens_num_classes": (I, [P, C.POINTER(C.c_int)]),
+    "ocu_ens_class_info": (I, [P, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(EnsTuning)]),
+    "ocu_ens_set_tuning": (I, [P, I, C.POINTER(EnsTuning)]),
+    "ocu_ens_autotune": (I, [P, C.POINTER(D), I]),
     "ocu_project_create": (I, [I, PP]),
     "ocu_project_destroy": (None, [P]),
     "ocu_project_set_stream": (I, [P, P]),

@@ -629,6 +629,8 @@ ocu_status launch_relax_color_emit_b(T *u, const T *b, const ocu_layout &L, cons
   dim3 bl(block[0], block[1], block[2]);
   if ((int)bl.x > half) bl.x = half >= 16 ? 16 : (half >= 8 ? 8 : (half >= 4 ? 4 : half));
   const int zb = (L.nx + bl.z - 1) / bl.z;
+  if ((long long)zb * members > 65535)
+    return fail(OCU_ERR_UNSUPPORTED, "[ERROR] ensemble - too many members of size (%d,%d,%d) in one class", L.nx, L.ny, L.nz);
   dim3 grid((half + bl.x - 1) / bl.x, (L.ny + bl.y - 1) / bl.y, (unsigned)(zb * members));
   GhostEmit<T> ge{u, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(p.bc), (T)hx, (T)hy, (T)hz};
   k_relax_color_emit_b<T><<<grid, bl, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c, diag, ge, sel,
@@ -666,6 +668,8 @@ ocu_status launch_prolong_emit_b(const T *uc, const ocu_layout &Lc, T *uf, const
                                  const ocu_bc_set &bc_fine, double hx, double hy, double hz, const BatchSel &sel,
                                  long long cms, long long fms, int members, cudaStream_t s) {
   dim3 block(Lc.nz >= 32 ? 32 : 16, 8);
+  if ((long long)Lc.nx * members > 65535)
+    return fail(OCU_ERR_UNSUPPORTED, "[ERROR] ensemble - too many members of one size in one class");
   dim3 grid((Lc.nz + block.x - 1) / block.x, (Lc.ny + block.y - 1) / block.y, (unsigned)(Lc.nx * members));
   GhostEmit<T> ge{uf, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, to_dev(bc_fine), (T)hx, (T)hy, (T)hz};
   k_prolong_emit_b<T><<<grid, block, 0, s>>>(uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf, Lf.xstride,
@@ -733,6 +737,8 @@ template <typename T>
 ocu_status launch_residual_restrict_b(const T *u, const T *b, const ocu_layout &Lf, T *bc_, const ocu_layout &Lc,
                                       double h, double fx, double fy, double fz, T *rows2, const BatchSel &sel,
                                       long long fms, long long cms, int members, cudaStream_t s) {
+  if ((long long)Lc.nx * members > 65535)
+    return fail(OCU_ERR_UNSUPPORTED, "[ERROR] ensemble - too many members of one size in one class");
   dim3 block(32, 8), grid(1, (Lc.ny + 7) / 8, (unsigned)(Lc.nx * members));
   const ResCoefT<T> c = res_coef<T>(h, fx, fy, fz);
   if (rows2)
@@ -777,6 +783,8 @@ template <typename T>
 ocu_status launch_residual_rows_b(const T *u, const T *b, const ocu_layout &L, double h, double fx, double fy,
                                   double fz, T *rows2, const BatchSel &sel, long long ms, int members,
                                   cudaStream_t s) {
+  if ((long long)L.nx * members > 65535)
+    return fail(OCU_ERR_UNSUPPORTED, "[ERROR] ensemble - too many members of one size in one class");
   dim3 block(32, 8), grid(1, (L.ny + 7) / 8, (unsigned)(L.nx * members));
   k_residual_rows_b<T><<<grid, block, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz,
                                               res_coef<T>(h, fx, fy, fz), rows2, sel, ms);
@@ -840,7 +848,10 @@ __global__ void __launch_bounds__(512) k_bc_fill_b(T *u, long long xs, long long
   const int m = batch_member(sel, blockIdx.x);
   if (m < 0) return;
   level1_fill_block<T>(u + m * ms, xs, ys, nx, ny, nz, bc, hx, hy, hz);
-  if (retire && threadIdx.x == 0) state[m] = 0;
+  if (retire) {
+    __syncthreads();  // every thread has read state[m] before it changes
+    if (threadIdx.x == 0) state[m] = 0;
+  }
 }
 
 template <typename T>

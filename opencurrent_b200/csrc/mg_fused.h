@@ -191,6 +191,35 @@ ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s);
 template <typename T>
 ocu_status launch_coarse_tail_batch(const TailParams<T> &P, const TailBatch &tb, int members, cudaStream_t s);
 
+// Ensemble forms of the level kernels over `members` congruent grids (member m at base + m*ms;
+// ms, fms, cms are member strides in elements).  See kernels_mg_fused.cu.
+template <typename T>
+ocu_status launch_relax_color_emit_b(T *u, const T *b, const ocu_layout &L, const T *diag, int color,
+                                     const RelaxParams &p, double hx, double hy, double hz, const BatchSel &sel,
+                                     long long ms, int members, const int block[3], cudaStream_t s);
+template <typename T>
+ocu_status launch_prolong_emit_b(const T *uc, const ocu_layout &Lc, T *uf, const ocu_layout &Lf,
+                                 const ocu_bc_set &bc_fine, double hx, double hy, double hz, const BatchSel &sel,
+                                 long long cms, long long fms, int members, cudaStream_t s);
+template <typename T>
+ocu_status launch_residual_restrict_b(const T *u, const T *b, const ocu_layout &Lf, T *bc_, const ocu_layout &Lc,
+                                      double h, double fx, double fy, double fz, T *rows2, const BatchSel &sel,
+                                      long long fms, long long cms, int members, cudaStream_t s);
+template <typename T>
+ocu_status launch_residual_rows_b(const T *u, const T *b, const ocu_layout &L, double h, double fx, double fy,
+                                  double fz, T *rows2, const BatchSel &sel, long long ms, int members,
+                                  cudaStream_t s);
+template <typename T>
+ocu_status launch_fold_rows_b(const T *rows, long long nrows, T *partial, long long pstride, double *sums,
+                              const BatchSel &sel, int members, cudaStream_t s);
+template <typename T>
+ocu_status launch_bc_fill_b(T *u, const ocu_layout &L, const ocu_bc_set &bc, double hx, double hy, double hz,
+                            const BatchSel &sel, long long ms, int members, int *state, bool retire,
+                            cudaStream_t s);
+template <typename T>
+ocu_status launch_converge_b(const double *sums, long long ncell, const double *tol, int *state, int *vcycles,
+                             double *last_l2, int *active, int members, bool initial, cudaStream_t s);
+
 // Opaque copy of a CUtensorMap (128 bytes, 64-byte aligned) so host headers need no cuda.h.
 struct alignas(64) SweepTmap {
   unsigned char bytes[128];

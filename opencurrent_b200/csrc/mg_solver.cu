@@ -20,7 +20,6 @@
 
 namespace ocub {
 
-enum { RO_RED_BLACK = 0, RO_BLACK_RED = 1, RO_SYMMETRIC = 2 };
 
 static double min3(double a, double b, double c) { return a < b ? (a < c ? a : c) : (b < c ? b : c); }
 
@@ -85,10 +84,8 @@ static ocu_grid *alloc_grid(ocu_dtype dt, const ocu_layout &L, ocu_status *st) {
 // initialize_base_storage + initialize_storage (sol_mgpressure3d.cpp:401-437,
 // sol_mgpressure3ddev.cu:376-482)
 template <typename T>
-ocu_status MGCore<T>::init(const ocu_bc_set &bc_, bool disable_host, int nx, int ny, int nz, double hx,
-                           double hy, double hz, ocu_grid *rhs, ocu_grid *pressure, cudaStream_t s) {
-  const ocu_dtype dt = sizeof(T) == 8 ? OCU_F64 : OCU_F32;
-  stream = s;
+ocu_status MGCore<T>::set_geometry(const ocu_bc_set &bc_, bool disable_host, int nx, int ny, int nz, double hx,
+                                   double hy, double hz, const ocu_layout &L0) {
   bc = bc_;
   disable_relax_on_host = disable_host;
   num_levels = mg_num_levels(nx, ny, nz);
@@ -108,17 +105,26 @@ ocu_status MGCore<T>::init(const ocu_bc_set &bc_, bool disable_host, int nx, int
   }
   update_bc_between_colors = bc_any_periodic(bc);
   lay.resize(num_levels);
+  lay[0] = L0;
+  for (int l = 1; l < num_levels; l++) layout_compute(dim[l][0], dim[l][1], dim[l][2], 1, 1, 1, 0, 0, 0, &lay[l]);
+  return OCU_OK;
+}
+
+template <typename T>
+ocu_status MGCore<T>::init(const ocu_bc_set &bc_, bool disable_host, int nx, int ny, int nz, double hx,
+                           double hy, double hz, ocu_grid *rhs, ocu_grid *pressure, cudaStream_t s) {
+  const ocu_dtype dt = sizeof(T) == 8 ? OCU_F64 : OCU_F32;
+  stream = s;
+  OCU_TRY(set_geometry(bc_, disable_host, nx, ny, nz, hx, hy, hz, rhs->L));
   grids_u.assign(num_levels, nullptr);
   grids_b.assign(num_levels, nullptr);
   grids_r.assign(num_levels, nullptr);
-  lay[0] = rhs->L;
   grids_b[0] = rhs;
   grids_u[0] = pressure;
   ocu_status st = OCU_OK;
   grids_r[0] = alloc_grid(dt, rhs->L, &st);
   if (!grids_r[0]) return st;
   for (int l = 1; l < num_levels; l++) {
-    layout_compute(dim[l][0], dim[l][1], dim[l][2], 1, 1, 1, 0, 0, 0, &lay[l]);
     grids_u[l] = alloc_grid(dt, lay[l], &st);
     grids_b[l] = alloc_grid(dt, lay[l], &st);
     grids_r[l] = alloc_grid(dt, lay[l], &st);
@@ -360,6 +366,46 @@ int MGCore<T>::tail_start() const {
   return s;
 }
 
+// Tail schedule parameters for levels s..L-1 on the given level origins.
+template <typename T>
+void MGCore<T>::fill_tail_params(TailParams<T> &P, int s, int nu1, int nu2, int coarse_iters, bool symmetric,
+                                 T *const *u_origin, T *const *b_origin) const {
+  const int coarse = num_levels - 1;
+  std::memset(&P, 0, sizeof(P));
+  P.nlev = coarse - s + 1;
+  P.first_level = s;
+  P.nu1 = nu1;
+  P.nu2 = nu2;
+  P.post_order = symmetric ? RO_BLACK_RED : RO_RED_BLACK;
+  P.host_coarse = disable_relax_on_host ? 0 : 1;
+  P.coarse_order = symmetric ? RO_SYMMETRIC : RO_RED_BLACK;
+  int ci = coarse_iters;
+  if (P.host_coarse && P.coarse_order == RO_SYMMETRIC) {
+    if (ci % 2 == 1) ci++;
+    if (ci < 4) ci = 4;
+  }
+  P.coarse_iters = ci;
+  P.cc = make_coarse_coef<T>(relax_params(coarse));
+  for (int l = s; l <= coarse; l++) {
+    TailLevel<T> &v = P.lv[l - s];
+    v.u = u_origin[l];
+    v.b = b_origin[l];
+    v.xs = lay[l].xstride;
+    v.ys = lay[l].ystride;
+    v.nx = dim[l][0]; v.ny = dim[l][1]; v.nz = dim[l][2];
+    v.emit_ok = emit_ok(l) ? 1 : 0;
+    v.periodic = bc_any_periodic(bc) ? 1 : 0;
+    v.bc = to_dev(bc_at_level(l));
+    v.hx = (T)hx(l); v.hy = (T)hy(l); v.hz = (T)hz(l);
+    v.rc = make_relax_coef_d<T>(relax_params(l));
+    const double hh = h[l];
+    v.res.fxh = (T)(fx / (hh * hh));
+    v.res.fyh = (T)(fy / (hh * hh));
+    v.res.fzh = (T)(fz / (hh * hh));
+    v.res.dg = (T)(2 * (fx + fy + fz) / (hh * hh));
+  }
+}
+
 // Levels s..L-1 of a V-cycle: down (relax nu1, clear, residual+restrict), coarsest relax,
 // up (prolong + ghosts, relax nu2 where the absolute level is > 0).
 template <typename T>
@@ -382,39 +428,12 @@ ocu_status MGCore<T>::cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool
       return OCU_OK;
     }
   TailParams<T> P;
-  std::memset(&P, 0, sizeof(P));
-  P.nlev = coarse - s + 1;
-  P.first_level = s;
-  P.nu1 = nu1;
-  P.nu2 = nu2;
-  P.post_order = symmetric ? RO_BLACK_RED : RO_RED_BLACK;
-  P.host_coarse = disable_relax_on_host ? 0 : 1;
-  P.coarse_order = symmetric ? RO_SYMMETRIC : RO_RED_BLACK;
-  int ci = coarse_iters;
-  if (P.host_coarse && P.coarse_order == RO_SYMMETRIC) {
-    if (ci % 2 == 1) ci++;
-    if (ci < 4) ci = 4;
+  std::vector<T *> uo(num_levels), bo(num_levels);
+  for (int l = 0; l < num_levels; l++) {
+    uo[l] = u0(l);
+    bo[l] = b0(l);
   }
-  P.coarse_iters = ci;
-  P.cc = make_coarse_coef<T>(relax_params(coarse));
-  for (int l = s; l <= coarse; l++) {
-    TailLevel<T> &v = P.lv[l - s];
-    v.u = u0(l);
-    v.b = b0(l);
-    v.xs = lay[l].xstride;
-    v.ys = lay[l].ystride;
-    v.nx = dim[l][0]; v.ny = dim[l][1]; v.nz = dim[l][2];
-    v.emit_ok = emit_ok(l) ? 1 : 0;
-    v.periodic = bc_any_periodic(bc) ? 1 : 0;
-    v.bc = to_dev(bc_at_level(l));
-    v.hx = (T)hx(l); v.hy = (T)hy(l); v.hz = (T)hz(l);
-    v.rc = make_relax_coef_d<T>(relax_params(l));
-    const double hh = h[l];
-    v.res.fxh = (T)(fx / (hh * hh));
-    v.res.fyh = (T)(fy / (hh * hh));
-    v.res.fzh = (T)(fz / (hh * hh));
-    v.res.dg = (T)(2 * (fx + fy + fz) / (hh * hh));
-  }
+  fill_tail_params(P, s, nu1, nu2, coarse_iters, symmetric, uo.data(), bo.data());
   return launch_coarse_tail<T>(P, stream);
 }
 

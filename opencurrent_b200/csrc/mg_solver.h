@@ -13,6 +13,9 @@
 
 namespace ocub {
 
+// relax order (sol_mgpressure3d.h: RO_RED_BLACK, RO_BLACK_RED, RO_SYMMETRIC)
+enum { RO_RED_BLACK = 0, RO_BLACK_RED = 1, RO_SYMMETRIC = 2 };
+
 int mg_num_levels(int nx, int ny, int nz);
 
 // One CTA runs the coarse end of a cycle up to 8^3 cells (a 16^3 level already keeps one SM
@@ -83,6 +86,11 @@ struct MGCore : CoreOps {
   ocu_status finish_norms(int fine, double *l2, double *linf) override;
   int tail_start() const override;
   ocu_status cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool symmetric) override;
+  void fill_tail_params(TailParams<T> &P, int s, int nu1, int nu2, int coarse_iters, bool symmetric,
+                        T *const *u_origin, T *const *b_origin) const;
+  // level count, spacings, operator factors, omega and layouts (no allocation)
+  ocu_status set_geometry(const ocu_bc_set &bc, bool disable_host, int nx, int ny, int nz, double hx, double hy,
+                          double hz, const ocu_layout &L0);
   ocu_status init(const ocu_bc_set &bc, bool disable_host, int nx, int ny, int nz, double hx, double hy,
                   double hz, ocu_grid *rhs, ocu_grid *pressure, cudaStream_t s);
   ocu_bc_set bc_at_level(int level) const;

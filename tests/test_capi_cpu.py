@@ -118,3 +118,23 @@ def test_compute_entry_points_fail_loudly_without_gpu():
     with pytest.raises(ocu.OcuError) as e:
         g.init(8, 8, 8)
     assert e.value.status in (_capi.ERR_CUDA, _capi.ERR_ALLOC)
+
+
+def test_ensemble_argument_validation_without_gpu():
+    """ocu_ens_create checks its arguments before touching the device."""
+    lib = ocu.load()
+    h = C.c_void_p()
+    dims = (C.c_int * 6)(32, 32, 32, 16, 16, 16)
+    sp = (C.c_double * 6)(*([1 / 32] * 3 + [1 / 16] * 3))
+    assert lib.ocu_ens_create(_capi.F32, 0, dims, sp, None, C.byref(h)) == _capi.ERR_INVALID_VALUE
+    bad = (C.c_int * 6)(32, 32, 32, 1, 16, 16)
+    assert lib.ocu_ens_create(_capi.F32, 2, bad, sp, None, C.byref(h)) == _capi.ERR_INVALID_VALUE
+    assert b"member 1" in lib.ocu_last_error()
+    badh = (C.c_double * 6)(*([1 / 32] * 3 + [0.0] * 3))
+    assert lib.ocu_ens_create(_capi.F32, 2, dims, badh, None, C.byref(h)) == _capi.ERR_INVALID_VALUE
+    assert lib.ocu_ens_solve(None, None, 4, None) == _capi.ERR_INVALID_VALUE
+    p = _capi.MGParams()
+    lib.ocu_mg_params_default(C.byref(p))
+    p.convergence = _capi.CONVERGENCE_LINF
+    assert lib.ocu_ens_create(_capi.F32, 2, dims, sp, C.byref(p), C.byref(h)) == _capi.ERR_UNSUPPORTED
+    assert not h.value
