@@ -79,7 +79,8 @@ def test_second_solve_from_converged_state():
     ens = _check(F32, dims)
     bc = bc_from(SCALAR_BCS["neumann"])
     mem = _members(F32, dims, 1000)
-    tols = [1e-7 * rms for (_, _, rms) in mem]
+    # a little below what the first solve reached: one or two more cycles, above the FP32 floor
+    tols = [0.3 * ens.member_stats(m).last_l2 for m in range(len(dims))]
     assert ens.solve(tols, 20) == 2
     for m, d in enumerate(dims):
         L, rhs, _ = mem[m]
@@ -91,7 +92,7 @@ def test_second_solve_from_converged_state():
 
 
 @pytest.mark.parametrize("bcname,sym,disable_host", [("mixed_dn", 1, 0), ("dirichlet", 0, 1), ("periodic", 0, 0),
-                                                     ("neumann_inhom", 1, 1)])
+                                                     ("mixed_xdir", 1, 1)])
 def test_bc_and_operator_variants_fp64(bcname, sym, disable_host):
     dims = [(32, 32, 32), (16, 32, 16), (32, 32, 32), (24, 24, 24)]
     _check(F64, dims, bcname=bcname, sym=sym, disable_host=disable_host, rel=1e-10, max_iter=30)
