@@ -212,6 +212,41 @@ ocu_status ocu_mg_prolong(ocu_mg *mg, int core, int coarse, int fine);
 /* Wait for all work the solver enqueued. */
 ocu_status ocu_mg_synchronize(ocu_mg *mg);
 
+/* ---- differentiable advection + projection (periodic MAC grid) ----------------------------
+ * No single counterpart in the reference: the transposes of Sol_SelfAdvection3DDevice /
+ * Sol_PassiveAdvection3DDevice (sol_selfadvection3ddev.cu:135-337,
+ * sol_passiveadvection3ddev.cu:31-78) with the upwind choice frozen, and a chain of `steps`
+ * forward-Euler steps (passive + self advection, then projection) with checkpoints every
+ * `checkpoint_every` steps.  Cotangents use the plain sum inner product over the nx*ny*nz
+ * cells/faces; ghost and padding entries of returned cotangents are zero. */
+/* lam_phi = lam_dphi + c (d dphi/d phi)^T lam_dphi;  lam_{u,v,w} += c (d dphi/d {u,v,w})^T lam_dphi */
+ocu_status ocu_advect_passive_adjoint(const ocu_grid *u, const ocu_grid *v, const ocu_grid *w,
+                                      const ocu_grid *phi, const ocu_grid *lam_dphi, ocu_grid *lam_phi,
+                                      ocu_grid *lam_u, ocu_grid *lam_v, ocu_grid *lam_w, int nx, int ny,
+                                      int nz, double c, double hx, double hy, double hz, int interp,
+                                      ocu_stream s);
+/* lam_{u,v,w} += c (d (du,dv,dw) / d (u,v,w))^T (lam_du, lam_dv, lam_dw) */
+ocu_status ocu_advect_self_adjoint(const ocu_grid *u, const ocu_grid *v, const ocu_grid *w,
+                                   const ocu_grid *lam_du, const ocu_grid *lam_dv,
+                                   const ocu_grid *lam_dw, ocu_grid *lam_u, ocu_grid *lam_v,
+                                   ocu_grid *lam_w, int nx, int ny, int nz, double c, double hx,
+                                   double hy, double hz, int interp, ocu_stream s);
+typedef struct ocu_adj ocu_adj;
+ocu_status ocu_adj_create(ocu_dtype dtype, int nx, int ny, int nz, double hx, double hy, double hz,
+                          int steps, int checkpoint_every, double dt, int interp, double proj_tol,
+                          ocu_adj **out);
+void ocu_adj_destroy(ocu_adj *a);
+ocu_status ocu_adj_set_stream(ocu_adj *a, ocu_stream s);
+/* layouts of the chain's grids: 'u', 'v', 'w' (MAC faces) and 't' (the scalar) */
+ocu_status ocu_adj_layout(const ocu_adj *a, char which, ocu_layout *layout);
+/* runs the chain from (u0, v0, w0, phi0), keeps the checkpoints, writes the final scalar */
+ocu_status ocu_adj_forward(ocu_adj *a, const ocu_grid *u0, const ocu_grid *v0, const ocu_grid *w0,
+                           const ocu_grid *phi0, ocu_grid *phi_out);
+/* given the cotangent of the final scalar, the cotangents of the initial velocity and scalar
+ * of the last forward run (segments recomputed from the checkpoints) */
+ocu_status ocu_adj_backward(ocu_adj *a, const ocu_grid *lam_phi, ocu_grid *lam_u0, ocu_grid *lam_v0,
+                            ocu_grid *lam_w0, ocu_grid *lam_phi0);
+
 /* ---- ensembles of independent pressure solves ---------------------------------------------
  * No single counterpart in the reference: many Sol_MultigridPressure3DDevice<T>::solve calls
  * (sol_mgpressure3d.cpp:332-370) on right-hand sides of uneven sizes, run together.  Members

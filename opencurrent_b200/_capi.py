@@ -122,6 +122,14 @@ SIGNATURES = {
     "ocu_mg_restrict_residuals": (I, [P, I, I, I, C.POINTER(D), C.POINTER(D)]),
     "ocu_mg_prolong": (I, [P, I, I, I]),
     "ocu_mg_synchronize": (I, [P]),
+    "ocu_advect_passive_adjoint": (I, [P] * 9 + [I, I, I, D, D, D, D, I, P]),
+    "ocu_advect_self_adjoint": (I, [P] * 9 + [I, I, I, D, D, D, D, I, P]),
+    "ocu_adj_create": (I, [I, I, I, I, D, D, D, I, I, D, I, D, PP]),
+    "ocu_adj_destroy": (None, [P]),
+    "ocu_adj_set_stream": (I, [P, P]),
+    "ocu_adj_layout": (I, [P, C.c_char, LP]),
+    "ocu_adj_forward": (I, [P, P, P, P, P, P]),
+    "ocu_adj_backward": (I, [P, P, P, P, P, P]),
     "ocu_ens_create": (I, [I, I, C.POINTER(C.c_int), C.POINTER(D), C.POINTER(MGParams), PP]),
     "ocu_ens_destroy": (None, [P]),
     "ocu_ens_set_stream": (I, [P, P]),

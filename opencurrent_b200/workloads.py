@@ -82,3 +82,36 @@ def rayleigh_benard(ocu, nx=128, ny=128, nz=64, dtype=None, seed=0, ra=1e6, pr=0
 def ensemble_sizes(count=512, seed=1, choices=(32, 48, 64, 96)):
     rng = np.random.default_rng(seed)
     return [int(x) for x in rng.choice(np.array(choices), size=count)]
+
+
+def divergence_free_velocity(n, seed=5, kmax=8):
+    """Periodic velocity on the MAC faces of an n^3 grid (h = 1/n): the curl of a vector
+    potential with N(0,1) entries, low-passed to |k| <= kmax, evaluated spectrally at the face
+    positions (u at (i, j+1/2, k+1/2) h, v at (i+1/2, j, k+1/2) h, w at (i+1/2, j+1/2, k) h) and
+    scaled to max |velocity| = 1.  FP64; returns three (n, n, n) arrays."""
+    rng = np.random.default_rng(seed)
+    m = np.fft.fftfreq(n, d=1.0 / n)  # integer wavenumbers
+    mx, my, mz = np.meshgrid(m, m, m, indexing="ij")
+    keep = (mx ** 2 + my ** 2 + mz ** 2) <= kmax ** 2
+    A = [np.fft.fftn(rng.standard_normal((n, n, n))) * keep for _ in range(3)]
+    kx, ky, kz = (2 * np.pi * mx, 2 * np.pi * my, 2 * np.pi * mz)
+    uh = 1j * (ky * A[2] - kz * A[1])
+    vh = 1j * (kz * A[0] - kx * A[2])
+    wh = 1j * (kx * A[1] - ky * A[0])
+
+    def at(fh, sx, sy, sz):
+        phase = np.exp(2j * np.pi * (mx * sx + my * sy + mz * sz) / n)
+        return np.real(np.fft.ifftn(fh * phase))
+
+    u, v, w = at(uh, 0, 0.5, 0.5), at(vh, 0.5, 0, 0.5), at(wh, 0.5, 0.5, 0)
+    s = max(np.abs(u).max(), np.abs(v).max(), np.abs(w).max())
+    return u / s, v / s, w / s
+
+
+def gaussian_blob(n, center, sigma=0.1):
+    """exp(-|x - c|^2 / (2 sigma^2)) at the cell centres of the periodic unit cube (periodic
+    distance), FP64 (n, n, n)."""
+    x = (np.arange(n) + 0.5) / n
+    d = [np.minimum(np.abs(x - c), 1 - np.abs(x - c)) for c in center]
+    dx, dy, dz = np.meshgrid(d[0], d[1], d[2], indexing="ij")
+    return np.exp(-(dx ** 2 + dy ** 2 + dz ** 2) / (2 * sigma ** 2))

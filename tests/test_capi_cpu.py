@@ -138,3 +138,17 @@ def test_ensemble_argument_validation_without_gpu():
     p.convergence = _capi.CONVERGENCE_LINF
     assert lib.ocu_ens_create(_capi.F32, 2, dims, sp, C.byref(p), C.byref(h)) == _capi.ERR_UNSUPPORTED
     assert not h.value
+
+
+def test_adjoint_chain_argument_validation_without_gpu():
+    lib = ocu.load()
+    h = C.c_void_p()
+    args = (_capi.F32, 16, 16, 16, 1 / 16, 1 / 16, 1 / 16)
+    assert lib.ocu_adj_create(*args, 0, 2, 0.01, _capi.IT_FIRST_ORDER_UPWIND, 1e-6, C.byref(h)) == \
+        _capi.ERR_INVALID_VALUE  # no steps
+    assert lib.ocu_adj_create(*args, 4, 2, -0.01, _capi.IT_FIRST_ORDER_UPWIND, 1e-6, C.byref(h)) == \
+        _capi.ERR_INVALID_VALUE  # negative dt
+    assert lib.ocu_adj_create(*args, 4, 2, 0.01, 7, 1e-6, C.byref(h)) == _capi.ERR_INVALID_VALUE
+    assert b"interpolation" in lib.ocu_last_error()
+    assert lib.ocu_adj_forward(None, None, None, None, None, None) == _capi.ERR_INVALID_VALUE
+    assert not h.value
