@@ -426,8 +426,8 @@ struct Ensemble : EnsBase {
   }
 
   // Per class: time the whole class solve (zero initial guess) for every candidate smoothing
-  // pair and colour-sweep block shape, keep the fastest one that converges every member, and
-  // leave the pressures zeroed.
+  // pair and colour-sweep block shape; keep the one that converges the most members, the
+  // fastest among those; leave the pressures zeroed.
   ocu_status autotune(const double *tol, int max_iter) override {
     static const int nus[][2] = {{2, 2}, {1, 1}, {2, 1}, {3, 3}, {1, 2}};
     static const int blocks[][3] = {{32, 4, 2}, {32, 8, 1}, {16, 8, 2}, {32, 2, 4}};
@@ -437,13 +437,16 @@ struct Ensemble : EnsBase {
     ocu_status result = OCU_OK;
     for (size_t ci = 0; ci < cls.size() && result == OCU_OK; ci++) {
       EnsClass<T> &c = *cls[ci];
+      const ocu_ens_tuning original = c.tune;
       ocu_ens_tuning best = c.tune;
       best.ms = 1e300;
+      int best_conv = -1;
       for (const auto &nu : nus) {
         for (const auto &bl : blocks) {
           ocu_ens_tuning t{nu[0], nu[1], {bl[0], bl[1], bl[2]}, 0.0};
           apply_tuning(c, t);
           for (int rep = 0; rep < 2 && result == OCU_OK; rep++) {  // first run records the graphs
+            // (members that cannot reach their tolerance make run() report it; that is data here)
             result = check_cuda(cudaMemsetAsync(c.ubase[0], 0, sizeof(T) * c.ms[0] * c.members, c.stream), "clear");
             if (result != OCU_OK) break;
             result = check_cuda(cudaStreamSynchronize(c.stream), "sync");
@@ -455,14 +458,15 @@ struct Ensemble : EnsBase {
             if (result == OCU_OK) result = check_cuda(cudaEventSynchronize(e1), "cudaEventSynchronize");
             float ms = 0;
             if (result == OCU_OK) result = check_cuda(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-            if (result == OCU_OK && rep == 1 && conv == c.members && ms < best.ms) {
+            if (result == OCU_OK && rep == 1 && (conv > best_conv || (conv == best_conv && ms < best.ms))) {
               best = t;
               best.ms = ms;
+              best_conv = conv;
             }
           }
         }
       }
-      if (best.ms > 1e299) best = c.tune, best.ms = 0;
+      if (best_conv < 0) best = original;
       apply_tuning(c, best);
       if (result == OCU_OK)
         result = check_cuda(cudaMemsetAsync(c.ubase[0], 0, sizeof(T) * c.ms[0] * c.members, c.stream), "clear");

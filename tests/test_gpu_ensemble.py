@@ -76,16 +76,15 @@ def test_uneven_sizes_fp32_match_single_solves():
 def test_second_solve_from_converged_state():
     """A second solve starts from the converged pressures (the reference keeps the initial guess)."""
     dims = [(32, 32, 32), (16, 16, 16)]
-    ens = _check(F32, dims)
+    ens = _check(F32, dims, rel=1e-3)
     bc = bc_from(SCALAR_BCS["neumann"])
     mem = _members(F32, dims, 1000)
-    # a little below what the first solve reached: one or two more cycles, above the FP32 floor
-    tols = [0.3 * ens.member_stats(m).last_l2 for m in range(len(dims))]
+    tols = [1e-6 * rms for (_, _, rms) in mem]
     assert ens.solve(tols, 20) == 2
     for m, d in enumerate(dims):
         L, rhs, _ = mem[m]
         om = O.OracleMG("f", mg_params(bc), *d, 1.0 / d[0], 1.0 / d[1], 1.0 / d[2], rhs, L)
-        om.solve(1e-6 * mem[m][2], 20)
+        om.solve(1e-3 * mem[m][2], 20)
         ok, res = om.solve(tols[m], 20)
         assert ok and ens.member_stats(m).last_l2 == res
         assert_same(ens.pressure(m).copy_to_host(), om.grid("u", 0)[0], f"second solve member {m}")
