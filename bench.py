@@ -575,6 +575,8 @@ def run_kernel_case(args):
         s.prolong(1, 0)
     elif args.kernel_case == "restrict":
         s.restrict_residuals(0, 1, norms=True)
+    elif args.kernel_case == "tail":
+        s.run_vcycles(1)          # one V-cycle: its coarse end is one k_coarse_tail_smem launch
     s.synchronize()
     torch.cuda.synchronize()
     print(json.dumps({"kernel_case": args.kernel_case, "grid": [n] * 3, "ok": True}), flush=True)
@@ -591,7 +593,7 @@ def main():
                     help="levels with at least this many cells use the two-colour TMA pass (0 = off)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-secondary", action="store_true")
-    ap.add_argument("--kernel-case", choices=["relax", "prolong", "restrict"],
+    ap.add_argument("--kernel-case", choices=["relax", "prolong", "restrict", "tail"],
                     help="run a few launches of one kernel on the 256^3 FP32 hierarchy (profiling)")
     args = ap.parse_args()
     if args.kernel_case:

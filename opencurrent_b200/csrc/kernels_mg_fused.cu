@@ -20,25 +20,43 @@
 
 namespace ocub {
 
+// One colour update of cell (i,j,k).  In a block that holds no cell of the outer layer the
+// diagonal is c.ld exactly (every face term is skipped) and there are no ghost writes.  I is the
+// index type: int when the whole allocation fits in 2^31 elements.
+template <typename T, typename I>
+__device__ __forceinline__ void color_cell(T *__restrict__ u, const T *__restrict__ b, I xs, I ys, int i, int j,
+                                           int k, int nx, int ny, int nz, const RelaxCoefD<T> &c,
+                                           const T *__restrict__ diag, bool edge_block, const GhostEmit<T> &ge) {
+  const I id = (I)i * xs + (I)j * ys + k;
+  if (!edge_block) {
+    const T uc = u[id];
+    const T res = relax_res<T>(uc, b[id], u[id - 1], u[id + 1], u[id - ys], u[id + ys], u[id - xs], u[id + xs], c);
+    u[id] = uc + c.omega * res / c.ld;
+    return;
+  }
+  const T nv = relax_value<T>(u[id], b[id], u[id - 1], u[id + 1], u[id - ys], u[id + ys], u[id - xs], u[id + xs], i,
+                              j, k, nx, ny, nz, c, diag);
+  u[id] = nv;
+  ge.emit(i, j, k, nv);
+}
+
+__device__ __forceinline__ bool color_edge_block(int bx, int by, int bz, int nx, int ny, int nz) {
+  return bx == 0 || (bx + 1) * (int)blockDim.x * 2 >= nz || by == 0 || (by + 1) * (int)blockDim.y >= ny || bz == 0 ||
+         (bz + 1) * (int)blockDim.z >= nx;
+}
+
 // Colour sweep + ghost writes: thread (t, j, i), k = 2t + parity.
-template <typename T>
-__global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, const T *__restrict__ b, long long xs,
-                                                          long long ys, int nx, int ny, int nz, int color,
-                                                          RelaxCoefD<T> c, const T *__restrict__ diag,
-                                                          GhostEmit<T> ge) {
+template <typename T, typename I>
+__global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, const T *__restrict__ b, I xs, I ys,
+                                                          int nx, int ny, int nz, int color, RelaxCoefD<T> c,
+                                                          const T *__restrict__ diag,
+                                                          const __grid_constant__ GhostEmit<T> ge) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z * blockDim.z + threadIdx.z;
-  // blocks that hold no cell of the outer layer skip the ghost code entirely
-  const bool edge_block = blockIdx.x == 0 || (blockIdx.x + 1) * blockDim.x * 2 >= (unsigned)nz || blockIdx.y == 0 ||
-                          (blockIdx.y + 1) * blockDim.y >= (unsigned)ny || blockIdx.z == 0 ||
-                          (blockIdx.z + 1) * blockDim.z >= (unsigned)nx;
+  const bool edge_block = color_edge_block(blockIdx.x, blockIdx.y, blockIdx.z, nx, ny, nz);
   if (i >= nx || j >= ny || t >= nz / 2) return;
-  const int k = 2 * t + ((i + j + color) & 1);
-  const long long id = (long long)i * xs + (long long)j * ys + k;
-  const T nv = relax_point<T>(u, b, id, xs, ys, i, j, k, nx, ny, nz, c, diag);
-  u[id] = nv;
-  if (edge_block) ge.emit(i, j, k, nv);
+  color_cell<T, I>(u, b, xs, ys, i, j, 2 * t + ((i + j + color) & 1), nx, ny, nz, c, diag, edge_block, ge);
 }
 
 template <typename T>
@@ -52,7 +70,12 @@ ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const 
   dim3 grid((half + block.x - 1) / block.x, (L.ny + block.y - 1) / block.y, (L.nx + block.z - 1) / block.z);
   GhostEmit<T> ge{nullptr, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(p.bc), (T)hx, (T)hy, (T)hz};
   ge.p = u;
-  k_relax_color_emit<T><<<grid, block, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c, diag, ge);
+  if (L.allocated < (1LL << 31))
+    k_relax_color_emit<T, int><<<grid, block, 0, s>>>(u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c,
+                                                      diag, ge);
+  else
+    k_relax_color_emit<T, long long><<<grid, block, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c,
+                                                            diag, ge);
   return check_launch("k_relax_color_emit");
 }
 
@@ -365,8 +388,11 @@ ocu_status launch_fold_rows(const T *rows, long long nrows, bool is_max, void *s
 // nu2), phases separated by __syncthreads.  Identical operation sequence and arithmetic to the
 // per-level kernels.
 // ------------------------------------------------------------------------------------------
+// The tail's phases are separate (not inlined) functions: the kernel runs each code path only a
+// few times per launch, so one shared copy of every phase keeps its instruction footprint (and
+// the cold instruction fetches that dominated it) small.
 template <typename T>
-__device__ void tail_relax(const TailLevel<T> &lv, int iterations, int order, int nt) {
+__device__ __noinline__ void tail_relax(const TailLevel<T> &lv, int iterations, int order, int nt) {
   GhostEmit<T> ge{lv.u, lv.xs, lv.ys, lv.nx, lv.ny, lv.nz, lv.bc, lv.hx, lv.hy, lv.hz};
   if (order == 2) {
     if (iterations % 2 == 1) iterations++;
@@ -399,66 +425,75 @@ __device__ void tail_relax(const TailLevel<T> &lv, int iterations, int order, in
 
 // The tail schedule on level descriptors lv[0..nlev-1] (lv[0] = level s), held in shared
 // memory.  Works on global memory or on a shared-memory copy; the arithmetic is the same.
+// clear_zero(coarse) + homogeneous ghost fill == zero every cell of the shell and interior;
+// then the residual of f restricted into b of c
+template <typename T>
+__device__ __noinline__ void tail_restrict(const TailLevel<T> &f, const TailLevel<T> &c, int nt) {
+  const int cz = c.nz + 2, cy = c.ny + 2, cx = c.nx + 2;
+  for (int q = threadIdx.x; q < cx * cy * cz; q += nt) {
+    const int i = q / (cy * cz) - 1, j = (q / cz) % cy - 1, k = q % cz - 1;
+    c.u[(long long)i * c.xs + (long long)j * c.ys + k] = (T)0;
+  }
+  for (int q = threadIdx.x; q < c.nx * c.ny * c.nz; q += nt) {
+    const int ic = q / (c.ny * c.nz), jc = (q / c.nz) % c.ny, kc = q % c.nz;
+    const long long ri = (long long)(2 * ic) * f.xs + (long long)(2 * jc) * f.ys + 2 * kc;
+    const T r0 = residual_at<T>(f.u, f.b, ri, f.xs, f.ys, f.res);
+    const T r1 = residual_at<T>(f.u, f.b, ri + 1, f.xs, f.ys, f.res);
+    const T r2 = residual_at<T>(f.u, f.b, ri + f.ys, f.xs, f.ys, f.res);
+    const T r3 = residual_at<T>(f.u, f.b, ri + 1 + f.ys, f.xs, f.ys, f.res);
+    const T r4 = residual_at<T>(f.u, f.b, ri + f.xs, f.xs, f.ys, f.res);
+    const T r5 = residual_at<T>(f.u, f.b, ri + 1 + f.xs, f.xs, f.ys, f.res);
+    const T r6 = residual_at<T>(f.u, f.b, ri + f.ys + f.xs, f.xs, f.ys, f.res);
+    const T r7 = residual_at<T>(f.u, f.b, ri + 1 + f.ys + f.xs, f.xs, f.ys, f.res);
+    c.b[(long long)ic * c.xs + (long long)jc * c.ys + kc] = (T)0.125 * (r0 + r1 + r2 + r3 + r4 + r5 + r6 + r7);
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ __noinline__ void tail_coarsest(const TailLevel<T> &cl, const TailParams<T> &P, int nt) {
+  if (P.host_coarse) {
+    coarse_relax_block<T>(cl.u, cl.b, cl.xs, cl.ys, cl.nx, cl.ny, cl.nz, P.coarse_iters, P.coarse_order, P.cc, cl.bc,
+                          cl.hx, cl.hy, cl.hz);
+  } else {
+    tail_relax<T>(cl, P.coarse_iters, P.coarse_order, nt);
+  }
+  __syncthreads();
+}
+
+// prolongation of c into f with f's ghosts
+template <typename T>
+__device__ __noinline__ void tail_prolong(const TailLevel<T> &f, const TailLevel<T> &c, int nt) {
+  GhostEmit<T> ge{f.u, f.xs, f.ys, f.nx, f.ny, f.nz, f.bc, f.hx, f.hy, f.hz};
+  for (int q = threadIdx.x; q < c.nx * c.ny * c.nz; q += nt) {
+    const int ic = q / (c.ny * c.nz), jc = (q / c.nz) % c.ny, kc = q % c.nz;
+    const long long tc = (long long)ic * c.xs + (long long)jc * c.ys + kc;
+    const long long fi = (long long)(2 * ic + 1) * f.xs + (long long)(2 * jc + 1) * f.ys + (2 * kc + 1);
+    if (f.emit_ok)
+      prolong_cell<T, true>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, &ge);
+    else
+      prolong_cell<T, false>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, nullptr);
+  }
+  __syncthreads();
+  if (!f.emit_ok) {
+    level1_fill_block<T>(f.u, f.xs, f.ys, f.nx, f.ny, f.nz, f.bc, f.hx, f.hy, f.hz);
+    __syncthreads();
+  }
+}
+
+// The tail schedule on level descriptors lv[0..nlev-1] (lv[0] = level s), held in shared
+// memory.  Works on global memory or on a shared-memory copy; the arithmetic is the same.
 template <typename T>
 __device__ void tail_body(const TailLevel<T> *lv, const TailParams<T> &P, int nt) {
   const int L = P.nlev;
   for (int l = 0; l < L - 1; l++) {
-    const TailLevel<T> &f = lv[l];
-    const TailLevel<T> &c = lv[l + 1];
-    tail_relax<T>(f, P.nu1, 0, nt);
-    // clear_zero(coarse) + homogeneous ghost fill == zero every cell of the shell and interior
-    const int cz = c.nz + 2, cy = c.ny + 2, cx = c.nx + 2;
-    for (int q = threadIdx.x; q < cx * cy * cz; q += nt) {
-      const int i = q / (cy * cz) - 1, j = (q / cz) % cy - 1, k = q % cz - 1;
-      c.u[(long long)i * c.xs + (long long)j * c.ys + k] = (T)0;
-    }
-    // residual + restriction into b of the coarse level
-    for (int q = threadIdx.x; q < c.nx * c.ny * c.nz; q += nt) {
-      const int ic = q / (c.ny * c.nz), jc = (q / c.nz) % c.ny, kc = q % c.nz;
-      const long long ri = (long long)(2 * ic) * f.xs + (long long)(2 * jc) * f.ys + 2 * kc;
-      const T r0 = residual_at<T>(f.u, f.b, ri, f.xs, f.ys, f.res);
-      const T r1 = residual_at<T>(f.u, f.b, ri + 1, f.xs, f.ys, f.res);
-      const T r2 = residual_at<T>(f.u, f.b, ri + f.ys, f.xs, f.ys, f.res);
-      const T r3 = residual_at<T>(f.u, f.b, ri + 1 + f.ys, f.xs, f.ys, f.res);
-      const T r4 = residual_at<T>(f.u, f.b, ri + f.xs, f.xs, f.ys, f.res);
-      const T r5 = residual_at<T>(f.u, f.b, ri + 1 + f.xs, f.xs, f.ys, f.res);
-      const T r6 = residual_at<T>(f.u, f.b, ri + f.ys + f.xs, f.xs, f.ys, f.res);
-      const T r7 = residual_at<T>(f.u, f.b, ri + 1 + f.ys + f.xs, f.xs, f.ys, f.res);
-      c.b[(long long)ic * c.xs + (long long)jc * c.ys + kc] = (T)0.125 * (r0 + r1 + r2 + r3 + r4 + r5 + r6 + r7);
-    }
-    __syncthreads();
+    tail_relax<T>(lv[l], P.nu1, 0, nt);
+    tail_restrict<T>(lv[l], lv[l + 1], nt);
   }
-  {  // coarsest level
-    const TailLevel<T> &cl = lv[L - 1];
-    if (P.host_coarse) {
-      coarse_relax_block<T>(cl.u, cl.b, cl.xs, cl.ys, cl.nx, cl.ny, cl.nz, P.coarse_iters, P.coarse_order, P.cc,
-                            cl.bc, cl.hx, cl.hy, cl.hz);
-    } else {
-      tail_relax<T>(cl, P.coarse_iters, P.coarse_order, nt);
-    }
-    __syncthreads();
-  }
+  tail_coarsest<T>(lv[L - 1], P, nt);
   for (int l = L - 2; l >= 0; l--) {
-    const TailLevel<T> &f = lv[l];
-    const TailLevel<T> &c = lv[l + 1];
-    GhostEmit<T> ge{f.u, f.xs, f.ys, f.nx, f.ny, f.nz, f.bc, f.hx, f.hy, f.hz};
-    for (int q = threadIdx.x; q < c.nx * c.ny * c.nz; q += nt) {
-      const int ic = q / (c.ny * c.nz), jc = (q / c.nz) % c.ny, kc = q % c.nz;
-      const long long tc = (long long)ic * c.xs + (long long)jc * c.ys + kc;
-      const long long fi = (long long)(2 * ic + 1) * f.xs + (long long)(2 * jc + 1) * f.ys + (2 * kc + 1);
-      if (f.emit_ok)
-        prolong_cell<T, true>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, &ge);
-      else
-        prolong_cell<T, false>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, nullptr);
-    }
-    __syncthreads();
-    if (!f.emit_ok) {
-      level1_fill_block<T>(f.u, f.xs, f.ys, f.nx, f.ny, f.nz, f.bc, f.hx, f.hy, f.hz);
-      __syncthreads();
-    }
-    if (P.first_level + l > 0) {
-      tail_relax<T>(f, P.nu2, P.post_order, nt);
-    }
+    tail_prolong<T>(lv[l], lv[l + 1], nt);
+    if (P.first_level + l > 0) tail_relax<T>(lv[l], P.nu2, P.post_order, nt);
   }
 }
 
@@ -570,7 +605,9 @@ ocu_status launch_coarse_tail_batch(const TailParams<T> &P, const TailBatch &tb,
                          "cudaFuncSetAttribute(k_coarse_tail_smem)"));
       attr_set.fetch_or(bit);
     }
-    k_coarse_tail_smem<T><<<members, 512, bytes, s>>>(P, tb);
+    // one warp-multiple of threads per ~2 cells of the largest level: small tails take 256
+    const long long top = (long long)P.lv[0].nx * P.lv[0].ny * P.lv[0].nz;
+    k_coarse_tail_smem<T><<<members, top <= 512 ? 256 : 512, bytes, s>>>(P, tb);
     return check_launch("k_coarse_tail_smem");
   }
   k_coarse_tail<T><<<members, 1024, 0, s>>>(P, tb);
@@ -602,21 +639,13 @@ __global__ void __launch_bounds__(256) k_relax_color_emit_b(T *__restrict__ u, c
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = bz * blockDim.z + threadIdx.z;
-  const bool edge_block = blockIdx.x == 0 || (blockIdx.x + 1) * blockDim.x * 2 >= (unsigned)nz || blockIdx.y == 0 ||
-                          (blockIdx.y + 1) * blockDim.y >= (unsigned)ny || bz == 0 ||
-                          (bz + 1) * blockDim.z >= (unsigned)nx;
+  const bool edge_block = color_edge_block(blockIdx.x, blockIdx.y, bz, nx, ny, nz);
   if (i >= nx || j >= ny || t >= nz / 2) return;
   u += m * ms;
   b += m * ms;
-  const int k = 2 * t + ((i + j + color) & 1);
-  const long long id = (long long)i * xs + (long long)j * ys + k;
-  const T nv = relax_point<T>(u, b, id, xs, ys, i, j, k, nx, ny, nz, c, diag);
-  u[id] = nv;
-  if (edge_block) {
-    GhostEmit<T> g = ge;
-    g.p = u;
-    g.emit(i, j, k, nv);
-  }
+  GhostEmit<T> g = ge;
+  g.p = u;
+  color_cell<T, int>(u, b, (int)xs, (int)ys, i, j, 2 * t + ((i + j + color) & 1), nx, ny, nz, c, diag, edge_block, g);
 }
 
 template <typename T>
