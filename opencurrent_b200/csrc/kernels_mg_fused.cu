@@ -81,10 +81,9 @@ ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const 
 
 // Prolongation + correction + ghost writes (devf.cu:94-197 then the level1 fill).
 // EMIT = false compiles the ghost writes out (children that touch no face, or no fusable BCs).
-template <typename T, bool EMIT>
-__device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, long long tc, long long cx, long long cy,
-                                             T *__restrict__ uf, long long f, long long fxs, long long fys, int ic,
-                                             int jc, int kc, const GhostEmit<T> *ge) {
+template <typename T, bool EMIT, typename I = long long>
+__device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, I tc, I cx, I cy, T *__restrict__ uf, I f,
+                                             I fxs, I fys, int ic, int jc, int kc, const GhostEmit<T> *ge) {
   const T w1 = (T)0.421875, w2 = (T)0.140625, w3 = (T)0.046875, w4 = (T)0.015625;
   const int i = 2 * ic + 1, j = 2 * jc + 1, k = 2 * kc + 1;
   // all eight fine values are loaded before the first store: the ghost writes go through
@@ -127,21 +126,21 @@ __device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, long long
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256, 3) k_prolong_emit(const T *__restrict__ uc, long long cx, long long cy, int cnx,
-                                                      int cny, int cnz, T *__restrict__ uf, long long fxs,
-                                                      long long fys, const __grid_constant__ GhostEmit<T> ge) {
+template <typename T, typename I>
+__global__ void __launch_bounds__(256, 3) k_prolong_emit(const T *__restrict__ uc, I cx, I cy, int cnx, int cny,
+                                                         int cnz, T *__restrict__ uf, I fxs, I fys,
+                                                         const __grid_constant__ GhostEmit<T> ge) {
   const int kc = blockIdx.x * blockDim.x + threadIdx.x;
   const int jc = blockIdx.y * blockDim.y + threadIdx.y;
   const int ic = blockIdx.z;
   if (kc >= cnz || jc >= cny || ic >= cnx) return;
-  const long long tc = (long long)ic * cx + (long long)jc * cy + kc;
-  const long long f = (long long)(2 * ic + 1) * fxs + (long long)(2 * jc + 1) * fys + (2 * kc + 1);
+  const I tc = (I)ic * cx + (I)jc * cy + kc;
+  const I f = (I)(2 * ic + 1) * fxs + (I)(2 * jc + 1) * fys + (2 * kc + 1);
   // only children on the fine grid's outer layer are ghost sources
   if (ic == 0 || ic == cnx - 1 || jc == 0 || jc == cny - 1 || kc == 0 || kc == cnz - 1)
-    prolong_cell<T, true>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, &ge);
+    prolong_cell<T, true, I>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, &ge);
   else
-    prolong_cell<T, false>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, nullptr);
+    prolong_cell<T, false, I>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, nullptr);
 }
 
 template <typename T>
@@ -150,8 +149,12 @@ ocu_status launch_prolong_emit(const T *uc, const ocu_layout &Lc, T *uf, const o
   dim3 block(Lc.nz >= 32 ? 32 : 16, 8);
   dim3 grid((Lc.nz + block.x - 1) / block.x, (Lc.ny + block.y - 1) / block.y, Lc.nx);
   GhostEmit<T> ge{uf, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, to_dev(bc_fine), (T)hx, (T)hy, (T)hz};
-  k_prolong_emit<T><<<grid, block, 0, s>>>(uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf, Lf.xstride,
-                                           Lf.ystride, ge);
+  if (Lf.allocated < (1LL << 31) && Lc.allocated < (1LL << 31))
+    k_prolong_emit<T, int><<<grid, block, 0, s>>>(uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
+                                                  (int)Lf.xstride, (int)Lf.ystride, ge);
+  else
+    k_prolong_emit<T, long long><<<grid, block, 0, s>>>(uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
+                                                        Lf.xstride, Lf.ystride, ge);
   return check_launch("k_prolong_emit");
 }
 
@@ -681,14 +684,14 @@ __global__ void __launch_bounds__(256, 3) k_prolong_emit_b(const T *__restrict__
   if (kc >= cnz || jc >= cny) return;
   uc += m * cms;
   uf += m * fms;
-  const long long tc = (long long)ic * cx + (long long)jc * cy + kc;
-  const long long f = (long long)(2 * ic + 1) * fxs + (long long)(2 * jc + 1) * fys + (2 * kc + 1);
+  const int tc = ic * (int)cx + jc * (int)cy + kc;
+  const int f = (2 * ic + 1) * (int)fxs + (2 * jc + 1) * (int)fys + (2 * kc + 1);
   if (ic == 0 || ic == cnx - 1 || jc == 0 || jc == cny - 1 || kc == 0 || kc == cnz - 1) {
     GhostEmit<T> g = ge;
     g.p = uf;
-    prolong_cell<T, true>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, &g);
+    prolong_cell<T, true, int>(uc, tc, (int)cx, (int)cy, uf, f, (int)fxs, (int)fys, ic, jc, kc, &g);
   } else {
-    prolong_cell<T, false>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, nullptr);
+    prolong_cell<T, false, int>(uc, tc, (int)cx, (int)cy, uf, f, (int)fxs, (int)fys, ic, jc, kc, nullptr);
   }
 }
 

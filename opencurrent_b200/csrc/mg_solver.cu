@@ -918,6 +918,8 @@ ocu_status MGSolver::apply_knobs() {
 }
 
 ocu_status MGSolver::set_params(const ocu_mg_params &p) {
+  // unchanged parameters keep the recorded graphs (callers may re-send them before every solve)
+  if (initialized && std::memcmp(&p, &prm, sizeof(p)) == 0) return OCU_OK;
   prm = p;
   cf.bc = p.bc;
   cd.bc = p.bc;
