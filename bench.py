@@ -588,7 +588,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--ir-inner", type=int, default=3)
+    ap.add_argument("--ir-inner", type=int, default=4)
     ap.add_argument("--sweep-cells", type=int, default=0,
                     help="levels with at least this many cells use the two-colour TMA pass (0 = off)")
     ap.add_argument("--skip-cpu", action="store_true")

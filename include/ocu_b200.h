@@ -154,13 +154,13 @@ typedef struct ocu_mg_params {
                                     on the device here; 1 = use the device colour-sweep kernel
                                     instead of the host-order one (see DESIGN) */
   int ir_inner_cycles;           /* OCU_MG_MIXED_IR only: FP32 fine-level cycles per
-                                    correction (0 = default 3) */
+                                    correction (0 = default 4) */
   int store_residual_grids;      /* 1 = keep r_grid(level) filled (read_r); costs N*s */
   int unfused;                   /* 1 = one launch per reference operation (no fused ghost
                                     writes, no fused residual+restriction, no tail kernel);
                                     same results, for A/B timing */
   int tail_cells;                /* levels with at most this many cells run in one single-CTA
-                                    kernel per cycle; 0 = default (512), < 0 = off */
+                                    kernel per cycle; 0 = default (64), < 0 = off */
   int sweep_cells;               /* levels with at least this many cells relax both colours in
                                     one TMA-fed pass (out of place, same results; Dirichlet and
                                     Neumann faces only); <= 0 = off (the default) */

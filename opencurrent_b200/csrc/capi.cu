@@ -280,7 +280,7 @@ void ocu_mg_params_default(ocu_mg_params *p) {
   p->nu1 = 2;
   p->nu2 = 2;
   p->convergence = OCU_CONVERGENCE_L2;
-  p->ir_inner_cycles = 3;
+  p->ir_inner_cycles = 4;
 }
 
 ocu_status ocu_mg_create(ocu_mg_kind kind, const ocu_mg_params *params, ocu_mg **out) {

@@ -59,6 +59,39 @@ __global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, con
   color_cell<T, I>(u, b, xs, ys, i, j, 2 * t + ((i + j + color) & 1), nx, ny, nz, c, diag, edge_block, ge);
 }
 
+// Two cells per thread, 64 columns apart (k = 2t + parity for t and t + 32), for rows of at least
+// 128 cells: both cells' loads are issued before either store (their neighbours are of the other
+// colour, so nothing they read changes in this launch), which doubles the loads in flight.
+template <typename T, typename I>
+__global__ void __launch_bounds__(256) k_relax_color_emit2(T *__restrict__ u, const T *__restrict__ b, I xs, I ys,
+                                                           int nx, int ny, int nz, int color, RelaxCoefD<T> c,
+                                                           const T *__restrict__ diag,
+                                                           const __grid_constant__ GhostEmit<T> ge) {
+  const int t0 = blockIdx.x * 64 + threadIdx.x, t1 = t0 + 32;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z * blockDim.z + threadIdx.z;
+  const int half = nz / 2;
+  const bool edge_block = blockIdx.x == 0 || (int)(blockIdx.x + 1) * 128 >= nz || blockIdx.y == 0 ||
+                          (int)(blockIdx.y + 1) * (int)blockDim.y >= ny || blockIdx.z == 0 ||
+                          (int)(blockIdx.z + 1) * (int)blockDim.z >= nx;
+  if (i >= nx || j >= ny) return;
+  const int par = (i + j + color) & 1;
+  if (edge_block) {
+    if (t0 < half) color_cell<T, I>(u, b, xs, ys, i, j, 2 * t0 + par, nx, ny, nz, c, diag, true, ge);
+    if (t1 < half) color_cell<T, I>(u, b, xs, ys, i, j, 2 * t1 + par, nx, ny, nz, c, diag, true, ge);
+    return;
+  }
+  const I id0 = (I)i * xs + (I)j * ys + (2 * t0 + par), id1 = id0 + 64;
+  const T a0 = u[id0], b0 = b[id0], zm0 = u[id0 - 1], zp0 = u[id0 + 1], ym0 = u[id0 - ys], yp0 = u[id0 + ys];
+  const T xm0 = u[id0 - xs], xp0 = u[id0 + xs];
+  const T a1 = u[id1], b1 = b[id1], zm1 = u[id1 - 1], zp1 = u[id1 + 1], ym1 = u[id1 - ys], yp1 = u[id1 + ys];
+  const T xm1 = u[id1 - xs], xp1 = u[id1 + xs];
+  const T r0 = relax_res<T>(a0, b0, zm0, zp0, ym0, yp0, xm0, xp0, c);
+  const T r1 = relax_res<T>(a1, b1, zm1, zp1, ym1, yp1, xm1, xp1, c);
+  u[id0] = a0 + c.omega * r0 / c.ld;
+  u[id1] = a1 + c.omega * r1 / c.ld;
+}
+
 template <typename T>
 ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const T *diag, int color,
                                    const RelaxParams &p, double hx, double hy, double hz, cudaStream_t s) {
@@ -70,6 +103,12 @@ ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const 
   dim3 grid((half + block.x - 1) / block.x, (L.ny + block.y - 1) / block.y, (L.nx + block.z - 1) / block.z);
   GhostEmit<T> ge{nullptr, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(p.bc), (T)hx, (T)hy, (T)hz};
   ge.p = u;
+  if (half >= 64 && L.allocated < (1LL << 31)) {
+    dim3 b2(32, 4, 2), g2((half + 63) / 64, (L.ny + 3) / 4, (L.nx + 1) / 2);
+    k_relax_color_emit2<T, int><<<g2, b2, 0, s>>>(u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c,
+                                                  diag, ge);
+    return check_launch("k_relax_color_emit2");
+  }
   if (L.allocated < (1LL << 31))
     k_relax_color_emit<T, int><<<grid, block, 0, s>>>(u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c,
                                                       diag, ge);

@@ -767,7 +767,7 @@ ocu_status MGSolver::ir_solve(double tolerance, int max_outer, double *rl2, doub
   *rl2 = l2; *rlinf = linf;
   stats.last_l2 = l2; stats.last_linf = linf;
   if (pick(conv, l2, linf) < tolerance) return OCU_OK;
-  const int inner = prm.ir_inner_cycles > 0 ? prm.ir_inner_cycles : 3;
+  const int inner = prm.ir_inner_cycles > 0 ? prm.ir_inner_cycles : 4;
   ocu_mg_params saved = prm;
   int total_inner = 0;
   (void)L;

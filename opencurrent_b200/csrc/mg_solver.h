@@ -18,9 +18,11 @@ enum { RO_RED_BLACK = 0, RO_BLACK_RED = 1, RO_SYMMETRIC = 2 };
 
 int mg_num_levels(int nx, int ny, int nz);
 
-// One CTA runs the coarse end of a cycle up to 8^3 cells (a 16^3 level already keeps one SM
-// busy longer than its separate launches take).
-constexpr int kDefaultTailCells = 512;
+// The single-CTA coarse tail covers the 4^3 level only by default: measured at 256^3, a V-cycle
+// takes 0.558 ms (FP32) / 0.787 ms (FP64) with the tail at 64 cells against 0.581 / 0.810 ms at
+// 512 cells -- one SM runs a phase of an 8^3 level slower than a separate launch does.
+// (Ensembles run one tail CTA per member and use a larger tail.)
+constexpr int kDefaultTailCells = 64;
 // The two-colour TMA pass is off unless asked for: at 256^3 FP32 it takes 110 us per sweep
 // against 124 us for the two colour launches, but it is instruction-bound, slower in FP64, and a
 // whole solve is not faster with it yet.
