@@ -261,7 +261,7 @@ def run_gpu(args):
     if per_iter == 1:
         kernel_name, alg_bytes = "k_relax_sweep2<float> level 0 (256^3)", 3.0 * ncell * 4
     else:
-        kernel_name, alg_bytes = "k_relax_color_emit<float> level 0 (256^3)", 2.0 * ncell * 4
+        kernel_name, alg_bytes = "k_relax_color_v4 (FP32 colour sweep) level 0 (256^3)", 2.0 * ncell * 4
     sweep_ms = e0.elapsed_time(e1) / (iters * per_iter)
     achieved = alg_bytes / (sweep_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()

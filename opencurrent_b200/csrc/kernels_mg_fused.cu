@@ -59,37 +59,77 @@ __global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, con
   color_cell<T, I>(u, b, xs, ys, i, j, 2 * t + ((i + j + color) & 1), nx, ny, nz, c, diag, edge_block, ge);
 }
 
-// Two cells per thread, 64 columns apart (k = 2t + parity for t and t + 32), for rows of at least
-// 128 cells: both cells' loads are issued before either store (their neighbours are of the other
-// colour, so nothing they read changes in this launch), which doubles the loads in flight.
-template <typename T, typename I>
-__global__ void __launch_bounds__(256) k_relax_color_emit2(T *__restrict__ u, const T *__restrict__ b, I xs, I ys,
-                                                           int nx, int ny, int nz, int color, RelaxCoefD<T> c,
-                                                           const T *__restrict__ diag,
-                                                           const __grid_constant__ GhostEmit<T> ge) {
-  const int t0 = blockIdx.x * 64 + threadIdx.x, t1 = t0 + 32;
+// FP32 colour sweep with 128-bit accesses: a thread owns four consecutive cells of a row (two of
+// each colour) and updates its two cells of the sweep's colour.  Its row neighbours come from
+// the same float4 or, across the float4 boundary, from the adjacent lanes; u of the rows j +- 1
+// and planes i +- 1 and b are float4 loads; the two new values go back with one float4 store
+// (the other two entries rewritten unchanged: nothing else writes them in this launch).  A warp
+// covers 128 consecutive cells of one row (nz a multiple of 128).  Rows on a j or i face take the
+// per-cell path; in the other rows only the z-face cells add their diagonal term (the x and y
+// terms are absent there, so the sum is the reference's sequence) and write their ghosts.
+__device__ __forceinline__ float v4_update(float uc, float bv, float zm, float zp, float ym, float yp, float xm,
+                                           float xp, int k, int nz, const RelaxCoefD<float> &c) {
+  const float res = relax_res<float>(uc, bv, zm, zp, ym, yp, xm, xp, c);
+  float dg = c.ld;
+  if (k == nz - 1) dg += c.zp;
+  if (k == 0) dg += c.zn;
+  return uc + c.omega * res / dg;
+}
+
+__global__ void __launch_bounds__(256, 6) k_relax_color_v4(float *__restrict__ u, const float *__restrict__ b, int xs,
+                                                        int ys, int nx, int ny, int nz, int color,
+                                                        RelaxCoefD<float> c, const __grid_constant__ GhostEmit<float> ge) {
+  const int lane = threadIdx.x;
+  const int k4 = (blockIdx.x * 32 + lane) * 4;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z * blockDim.z + threadIdx.z;
-  const int half = nz / 2;
-  const bool edge_block = blockIdx.x == 0 || (int)(blockIdx.x + 1) * 128 >= nz || blockIdx.y == 0 ||
-                          (int)(blockIdx.y + 1) * (int)blockDim.y >= ny || blockIdx.z == 0 ||
-                          (int)(blockIdx.z + 1) * (int)blockDim.z >= nx;
-  if (i >= nx || j >= ny) return;
+  if (i >= nx || j >= ny) return;  // whole warps (one row each)
   const int par = (i + j + color) & 1;
-  if (edge_block) {
-    if (t0 < half) color_cell<T, I>(u, b, xs, ys, i, j, 2 * t0 + par, nx, ny, nz, c, diag, true, ge);
-    if (t1 < half) color_cell<T, I>(u, b, xs, ys, i, j, 2 * t1 + par, nx, ny, nz, c, diag, true, ge);
+  if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1) {
+    for (int q = 0; q < 2; q++)
+      color_cell<float, int>(u, b, xs, ys, i, j, k4 + par + 2 * q, nx, ny, nz, c, nullptr, true, ge);
     return;
   }
-  const I id0 = (I)i * xs + (I)j * ys + (2 * t0 + par), id1 = id0 + 64;
-  const T a0 = u[id0], b0 = b[id0], zm0 = u[id0 - 1], zp0 = u[id0 + 1], ym0 = u[id0 - ys], yp0 = u[id0 + ys];
-  const T xm0 = u[id0 - xs], xp0 = u[id0 + xs];
-  const T a1 = u[id1], b1 = b[id1], zm1 = u[id1 - 1], zp1 = u[id1 + 1], ym1 = u[id1 - ys], yp1 = u[id1 + ys];
-  const T xm1 = u[id1 - xs], xp1 = u[id1 + xs];
-  const T r0 = relax_res<T>(a0, b0, zm0, zp0, ym0, yp0, xm0, xp0, c);
-  const T r1 = relax_res<T>(a1, b1, zm1, zp1, ym1, yp1, xm1, xp1, c);
-  u[id0] = a0 + c.omega * r0 / c.ld;
-  u[id1] = a1 + c.omega * r1 / c.ld;
+  const int base = i * xs + j * ys + k4;
+  const float4 U = *reinterpret_cast<const float4 *>(u + base);
+  const float4 B = *reinterpret_cast<const float4 *>(b + base);
+  const float4 YM = *reinterpret_cast<const float4 *>(u + base - ys);
+  const float4 YP = *reinterpret_cast<const float4 *>(u + base + ys);
+  const float4 XM = *reinterpret_cast<const float4 *>(u + base - xs);
+  const float4 XP = *reinterpret_cast<const float4 *>(u + base + xs);
+  float left = __shfl_up_sync(0xffffffffu, U.w, 1);
+  float right = __shfl_down_sync(0xffffffffu, U.x, 1);
+  if (lane == 0) left = u[base - 1];    // k4 - 1: a ghost at k = -1 when k4 == 0
+  if (lane == 31) right = u[base + 4];  // k4 + 4: a ghost at k = nz at the row's end
+  float4 out = U;
+  int k0, k1;
+  float v0, v1;
+  if (par == 0) {
+    k0 = k4, k1 = k4 + 2;
+    out.x = v0 = v4_update(U.x, B.x, left, U.y, YM.x, YP.x, XM.x, XP.x, k0, nz, c);
+    out.z = v1 = v4_update(U.z, B.z, U.y, U.w, YM.z, YP.z, XM.z, XP.z, k1, nz, c);
+  } else {
+    k0 = k4 + 1, k1 = k4 + 3;
+    out.y = v0 = v4_update(U.y, B.y, U.x, U.z, YM.y, YP.y, XM.y, XP.y, k0, nz, c);
+    out.w = v1 = v4_update(U.w, B.w, U.z, right, YM.w, YP.w, XM.w, XP.w, k1, nz, c);
+  }
+  *reinterpret_cast<float4 *>(u + base) = out;
+  if (k0 == 0) ge.emit(i, j, k0, v0);
+  if (k1 == nz - 1) ge.emit(i, j, k1, v1);
+}
+
+template <typename T>
+static bool launch_color_v4(T *, const T *, const ocu_layout &, int, const RelaxCoefD<T> &, const GhostEmit<T> &,
+                            cudaStream_t) {
+  return false;
+}
+template <>
+bool launch_color_v4<float>(float *u, const float *b, const ocu_layout &L, int color, const RelaxCoefD<float> &c,
+                            const GhostEmit<float> &ge, cudaStream_t s) {
+  if (L.nz % 128 != 0 || L.allocated >= (1LL << 31) || L.shift % 4 != 0 || L.ystride % 4 != 0) return false;
+  dim3 block(32, 4, 2), grid((L.nz + 127) / 128, (L.ny + 3) / 4, (L.nx + 1) / 2);
+  k_relax_color_v4<<<grid, block, 0, s>>>(u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c, ge);
+  return true;
 }
 
 template <typename T>
@@ -103,12 +143,7 @@ ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const 
   dim3 grid((half + block.x - 1) / block.x, (L.ny + block.y - 1) / block.y, (L.nx + block.z - 1) / block.z);
   GhostEmit<T> ge{nullptr, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(p.bc), (T)hx, (T)hy, (T)hz};
   ge.p = u;
-  if (half >= 64 && L.allocated < (1LL << 31)) {
-    dim3 b2(32, 4, 2), g2((half + 63) / 64, (L.ny + 3) / 4, (L.nx + 1) / 2);
-    k_relax_color_emit2<T, int><<<g2, b2, 0, s>>>(u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c,
-                                                  diag, ge);
-    return check_launch("k_relax_color_emit2");
-  }
+  if (launch_color_v4<T>(u, b, L, color, c, ge, s)) return check_launch("k_relax_color_v4");
   if (L.allocated < (1LL << 31))
     k_relax_color_emit<T, int><<<grid, block, 0, s>>>(u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c,
                                                       diag, ge);
