@@ -120,12 +120,12 @@ __global__ void __launch_bounds__(256, 6) k_relax_color_v4(float *__restrict__ u
 
 template <typename T>
 static bool launch_color_v4(T *, const T *, const ocu_layout &, int, const RelaxCoefD<T> &, const GhostEmit<T> &,
-                            cudaStream_t) {
+                            const T *, cudaStream_t) {
   return false;
 }
 template <>
 bool launch_color_v4<float>(float *u, const float *b, const ocu_layout &L, int color, const RelaxCoefD<float> &c,
-                            const GhostEmit<float> &ge, cudaStream_t s) {
+                            const GhostEmit<float> &ge, const float *, cudaStream_t s) {
   if (L.nz % 128 != 0 || L.allocated >= (1LL << 31) || L.shift % 4 != 0 || L.ystride % 4 != 0) return false;
   dim3 block(32, 4, 2), grid((L.nz + 127) / 128, (L.ny + 3) / 4, (L.nx + 1) / 2);
   k_relax_color_v4<<<grid, block, 0, s>>>(u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c, ge);
@@ -143,7 +143,7 @@ ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const 
   dim3 grid((half + block.x - 1) / block.x, (L.ny + block.y - 1) / block.y, (L.nx + block.z - 1) / block.z);
   GhostEmit<T> ge{nullptr, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(p.bc), (T)hx, (T)hy, (T)hz};
   ge.p = u;
-  if (launch_color_v4<T>(u, b, L, color, c, ge, s)) return check_launch("k_relax_color_v4");
+  if (launch_color_v4<T>(u, b, L, color, c, ge, diag, s)) return check_launch("k_relax_color_v4");
   if (L.allocated < (1LL << 31))
     k_relax_color_emit<T, int><<<grid, block, 0, s>>>(u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c,
                                                       diag, ge);
@@ -201,7 +201,7 @@ __device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, I tc, I c
 }
 
 template <typename T, typename I>
-__global__ void __launch_bounds__(256, 3) k_prolong_emit(const T *__restrict__ uc, I cx, I cy, int cnx, int cny,
+__global__ void __launch_bounds__(256, 4) k_prolong_emit(const T *__restrict__ uc, I cx, I cy, int cnx, int cny,
                                                          int cnz, T *__restrict__ uf, I fxs, I fys,
                                                          const __grid_constant__ GhostEmit<T> ge) {
   const int kc = blockIdx.x * blockDim.x + threadIdx.x;
