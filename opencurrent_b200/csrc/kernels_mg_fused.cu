@@ -217,12 +217,117 @@ __global__ void __launch_bounds__(256, 4) k_prolong_emit(const T *__restrict__ u
     prolong_cell<T, false, I>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, nullptr);
 }
 
+// FP32 prolongation on float4 fine rows: a lane owns two adjacent coarse cells (kc = 2m, 2m+1) of
+// a coarse row and writes their 16 children as four float4 fine-row segments (fine k = 4m..4m+3).
+// The nine coarse rows (ic+-1, jc+-1) are read as float2 at k = 2m, 2m+1, with k = 2m-1 and 2m+2
+// from the adjacent lanes.  Each child uses the same operand order as prolong_cell (including
+// the corner weight of the (-1,0,0) child).  Rows whose children touch a j or i face take
+// prolong_cell; z-face children write their ghosts.  cnz must be a multiple of 64.
+__device__ __forceinline__ float prolong_child(float f, float c000, float X, float Y, float Z, float XY, float XZ,
+                                               float YZ, float XYZ) {
+  const float w1 = 0.421875f, w2 = 0.140625f, w3 = 0.046875f, w4 = 0.015625f;
+  return f + w1 * c000 + w2 * (X + Y + Z) + w3 * (XY + XZ + YZ) + w4 * XYZ;
+}
+
+// Out-of-line paths of k_prolong_v4 (rare: face rows and the z-face ghosts), kept out of the
+// main body so that its register budget holds the coarse window.
+__device__ __noinline__ void prolong_face_pair(const float *__restrict__ uc, int cx, int cy, float *__restrict__ uf,
+                                               int fxs, int fys, int ic, int jc, int kc0, const GhostEmit<float> *ge) {
+  for (int q = 0; q < 2; q++) {
+    const int kc = kc0 + q;
+    const int tc = ic * cx + jc * cy + kc;
+    const int f = (2 * ic + 1) * fxs + (2 * jc + 1) * fys + (2 * kc + 1);
+    prolong_cell<float, true, int>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, ge);
+  }
+}
+
+// ghosts of the four fine cells (2ic+1-dx, 2jc+1-dy, k) just written by this thread
+__device__ __noinline__ void prolong_zghosts(const GhostEmit<float> *ge, const float *uf, int fxs, int fys, int ic,
+                                             int jc, int k) {
+  for (int dx = 0; dx < 2; dx++)
+    for (int dy = 0; dy < 2; dy++) {
+      const int fi = 2 * ic + 1 - dx, fj = 2 * jc + 1 - dy;
+      ge->emit(fi, fj, k, uf[fi * fxs + fj * fys + k]);
+    }
+}
+
+__global__ void __launch_bounds__(256, 4) k_prolong_v4(const float *__restrict__ uc, int cx, int cy, int cnx,
+                                                       int cny, int cnz, float *__restrict__ uf, int fxs, int fys,
+                                                       const __grid_constant__ GhostEmit<float> ge) {
+  const int lane = threadIdx.x;
+  const int m = blockIdx.x * 32 + lane;
+  const int jc = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ic = blockIdx.z * blockDim.z + threadIdx.z;
+  if (ic >= cnx || jc >= cny) return;  // whole warps (one coarse row each)
+  if (ic == 0 || ic == cnx - 1 || jc == 0 || jc == cny - 1) {
+    prolong_face_pair(uc, cx, cy, uf, fxs, fys, ic, jc, 2 * m, &ge);
+    return;
+  }
+  // coarse rows of the plane ic + di as c[dj+1][q], q = 0..3 for coarse k = 2m-1 .. 2m+2
+  auto load_plane = [&](int di, float (&c)[3][4]) {
+#pragma unroll
+    for (int dj = -1; dj <= 1; dj++) {
+      const int base = (ic + di) * cx + (jc + dj) * cy + 2 * m;
+      const float2 v = *reinterpret_cast<const float2 *>(uc + base);
+      float l = __shfl_up_sync(0xffffffffu, v.y, 1), r = __shfl_down_sync(0xffffffffu, v.x, 1);
+      if (lane == 0) l = uc[base - 1];
+      if (lane == 31) r = uc[base + 2];
+      c[dj + 1][0] = l;
+      c[dj + 1][1] = v.x;
+      c[dj + 1][2] = v.y;
+      c[dj + 1][3] = r;
+    }
+  };
+  float c0[3][4], cs[3][4];
+  load_plane(0, c0);
+  float cppp[2];  // corner weight of the (-x, +y, +z) children: coarse (ic+1, jc+1, kc+1)
+#pragma unroll
+  for (int dx = 0; dx < 2; dx++) {  // dx = 0: fine row 2ic+1 (+x side); dx = 1: fine row 2ic (-x side)
+    const int fi = 2 * ic + 1 - dx;
+    float4 F[2];
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+      F[dy] = *reinterpret_cast<const float4 *>(uf + fi * fxs + (2 * jc + 1 - dy) * fys + 4 * m);
+    load_plane(dx ? -1 : 1, cs);
+    if (dx == 0) {
+      cppp[0] = cs[2][2];
+      cppp[1] = cs[2][3];
+    }
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++) {
+      const int sy = dy ? 0 : 2;  // neighbour row in c0/cs on the child's y side
+      float out[4];
+#pragma unroll
+      for (int q = 0; q < 2; q++) {       // coarse cell kc = 2m + q, centre index q + 1
+#pragma unroll
+        for (int dz = 0; dz < 2; dz++) {  // dz = 0: fine k = 2kc+1 (+z side); dz = 1: 2kc (-z side)
+          const int cq = q + 1, sz = dz ? q : q + 2, o = 2 * q + (dz ? 0 : 1);
+          const float XYZ = (dx == 1 && dy == 0 && dz == 0) ? cppp[q] : cs[sy][sz];
+          out[o] = prolong_child((&F[dy].x)[o], c0[1][cq], cs[1][cq], c0[sy][cq], c0[1][sz], cs[sy][cq], cs[1][sz],
+                                 c0[sy][sz], XYZ);
+        }
+      }
+      const int fj = 2 * jc + 1 - dy;
+      *reinterpret_cast<float4 *>(uf + fi * fxs + fj * fys + 4 * m) = make_float4(out[0], out[1], out[2], out[3]);
+    }
+  }
+  if (m == 0 || 4 * m + 3 == 2 * cnz - 1) prolong_zghosts(&ge, uf, fxs, fys, ic, jc, m == 0 ? 0 : 4 * m + 3);
+}
+
 template <typename T>
 ocu_status launch_prolong_emit(const T *uc, const ocu_layout &Lc, T *uf, const ocu_layout &Lf,
                                const ocu_bc_set &bc_fine, double hx, double hy, double hz, cudaStream_t s) {
   dim3 block(Lc.nz >= 32 ? 32 : 16, 8);
   dim3 grid((Lc.nz + block.x - 1) / block.x, (Lc.ny + block.y - 1) / block.y, Lc.nx);
   GhostEmit<T> ge{uf, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, to_dev(bc_fine), (T)hx, (T)hy, (T)hz};
+  if (sizeof(T) == 4 && Lc.nz % 64 == 0 && Lf.allocated < (1LL << 31) && Lc.shift % 2 == 0 && Lf.shift % 4 == 0 &&
+      Lc.ystride % 2 == 0 && Lf.ystride % 4 == 0) {
+    dim3 b4(32, 4, 2), g4(Lc.nz / 64, (Lc.ny + 3) / 4, (Lc.nx + 1) / 2);
+    k_prolong_v4<<<g4, b4, 0, s>>>((const float *)uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz,
+                                   (float *)uf, (int)Lf.xstride, (int)Lf.ystride,
+                                   *reinterpret_cast<const GhostEmit<float> *>(&ge));
+    return check_launch("k_prolong_v4");
+  }
   if (Lf.allocated < (1LL << 31) && Lc.allocated < (1LL << 31))
     k_prolong_emit<T, int><<<grid, block, 0, s>>>(uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
                                                   (int)Lf.xstride, (int)Lf.ystride, ge);

@@ -86,6 +86,51 @@ def test_restrict_and_prolong(dt, knobs):
         assert_same(dm.read_u(lev).copy_to_host(), om.grid("u", lev)[0], f"prolong into {lev}")
 
 
+# Rows of 128 and 256 cells take the FP32 float4 kernels (colour sweep: nz % 128 = 0; prolongation:
+# coarse nz % 64 = 0), including their j/i-face rows, z-face ghosts and lane-edge neighbours.
+LONG_ROWS = [(12, 20, 256), (20, 10, 128)]
+
+
+@pytest.mark.parametrize("dt", [F32, F64])
+@pytest.mark.parametrize("bcname", ["neumann", "periodic", "neumann_inhom", "dirichlet", "mixed_dn", "mixed_all"])
+@pytest.mark.parametrize("shape", LONG_ROWS)
+def test_relax_levels_long_rows(dt, bcname, shape):
+    om, dm, _ = pair(dt, shape, (0.03, 0.02, 0.01), bcname, seed=4)
+    lib = O.lib()
+    for lev in range(om.num_levels):
+        for order in (0, 1, 2):
+            lib.orc_mg_relax(om.h, 0, lev, 2, order)
+            dm.relax(lev, 2, order)
+        dm.synchronize()
+        assert_same(dm.read_u(lev).copy_to_host(), om.grid("u", lev)[0], f"relax level {lev}")
+
+
+@pytest.mark.parametrize("dt", [F32, F64])
+@pytest.mark.parametrize("bcname", ["neumann_inhom", "periodic", "dirichlet", "mixed_all"])
+@pytest.mark.parametrize("shape", LONG_ROWS)
+def test_restrict_and_prolong_long_rows(dt, bcname, shape):
+    import ctypes as C
+    om, dm, _ = pair(dt, shape, (0.03, 0.02, 0.01), bcname, seed=5)
+    lib = O.lib()
+    for lev in range(om.num_levels - 1):
+        l2o, lio = C.c_double(), C.c_double()
+        lib.orc_mg_restrict_residuals(om.h, 0, lev, lev + 1, C.byref(l2o), C.byref(lio))
+        l2d, lid = dm.restrict_residuals(lev, lev + 1, norms=True)
+        assert (l2d, lid) == (l2o.value, lio.value), lev
+        assert_same(dm.read_b(lev + 1).copy_to_host(), om.grid("b", lev + 1)[0], f"restricted b {lev + 1}")
+    rng = np.random.default_rng(6)
+    for lev in range(om.num_levels - 2, -1, -1):
+        # a nonzero coarse correction and fine guess, the same buffers (ghosts included) on both sides
+        for q in (lev + 1, lev):
+            ou, Lq = om.grid("u", q)
+            O.interior(ou, Lq)[:] = rng.uniform(-1, 1, O.interior(ou, Lq).shape).astype(ou.dtype)
+            dm.read_u(q).copy_from_host(ou)
+        lib.orc_mg_prolong(om.h, 0, lev + 1, lev)
+        dm.prolong(lev + 1, lev)
+        dm.synchronize()
+        assert_same(dm.read_u(lev).copy_to_host(), om.grid("u", lev)[0], f"prolong into {lev}")
+
+
 @pytest.mark.parametrize("dt", [F32, F64])
 @pytest.mark.parametrize("knobs", range(len(KNOBS)))
 @pytest.mark.parametrize("case", [((64, 64, 64), "neumann", 0, 0), ((48, 32, 64), "periodic", 1, 0),
