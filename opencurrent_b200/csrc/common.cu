@@ -1,3 +1,4 @@
+#include <cstdlib>
 // Error reporting, layout arithmetic and BoundaryConditionSet helpers shared by the library.
 #include <atomic>
 #include <cmath>
@@ -31,6 +32,14 @@ ocu_status check_cuda(cudaError_t e, const char *what) {
   if (e == cudaSuccess) return OCU_OK;
   set_error("[ERROR] %s - CUDA error \"%s\"", what, cudaGetErrorString(e));
   return OCU_ERR_CUDA;
+}
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char *e = std::getenv("OCU_B200_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
 }
 
 ocu_status check_launch(const char *what) {

@@ -12,6 +12,7 @@ namespace ocub {
 template <typename T>
 __global__ void __launch_bounds__(256) k_bc_level1(Level1Compose<T> c, long long nzreg, long long nyreg,
                                                    long long nxreg) {
+  pdl_entry();
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int nx = c.nx, ny = c.ny, nz = c.nz;
   if (t < nzreg) {  // z faces: side, i in [-1,nx], j in [-1,ny]
@@ -68,7 +69,7 @@ ocu_status launch_bc_level1(T *origin, const ocu_layout &L, const ocu_bc_set &bc
   const long long total = nzreg + nyreg + nxreg;
   const int threads = 256;
   const unsigned blocks = (unsigned)((total + threads - 1) / threads);
-  k_bc_level1<T><<<blocks, threads, 0, s>>>(c, nzreg, nyreg, nxreg);
+  launch_pdl(k_bc_level1<T>, blocks, threads, 0, s, c, nzreg, nyreg, nxreg);
   return check_launch("k_bc_level1");
 }
 
@@ -87,6 +88,7 @@ __device__ __forceinline__ T nocorner_rule(const BCDev &bc, int f, T src, T h, b
 template <typename T>
 __global__ void __launch_bounds__(256) k_bc_nocorners(T *p, long long xs, long long ys, int nx, int ny, int nz,
                                                       BCDev bc, T hx, T hy, T hz) {
+  pdl_entry();
   long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long zreg = 2LL * nx * ny, yreg = 2LL * nx * nz, xreg = 2LL * ny * nz;
   auto at = [&](int i, int j, int k) -> T & { return p[(long long)i * xs + (long long)j * ys + k]; };
@@ -136,7 +138,7 @@ ocu_status launch_bc_nocorners_dev(T *origin, const ocu_layout &L, const ocu_bc_
     return fail(OCU_ERR_LAYOUT, "[ERROR] apply_3d_boundary_conditions_level1_nocorners - must have at least 1 ghost point");
   const long long total = 2LL * L.nx * L.ny + 2LL * L.nx * L.nz + 2LL * L.ny * L.nz;
   const unsigned blocks = (unsigned)((total + 255) / 256);
-  k_bc_nocorners<T><<<blocks, 256, 0, s>>>(origin, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(bc),
+  launch_pdl(k_bc_nocorners<T>, blocks, 256, 0, s, origin, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(bc),
                                            (T)hx, (T)hy, (T)hz);
   return check_launch("k_bc_nocorners");
 }
@@ -148,6 +150,7 @@ ocu_status launch_bc_nocorners_dev(T *origin, const ocu_layout &L, const ocu_bc_
 // ------------------------------------------------------------------------------------------
 template <typename T>
 __global__ void k_mac_bc_x(T *u, T *v, T *w, BCDev bc, long long xs, long long ys, int nx, int ny, int nz) {
+  pdl_entry();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (j >= ny || k >= nz) return;
@@ -179,6 +182,7 @@ __global__ void k_mac_bc_x(T *u, T *v, T *w, BCDev bc, long long xs, long long y
 
 template <typename T>
 __global__ void k_mac_bc_y(T *u, T *v, T *w, BCDev bc, long long xs, long long ys, int nx, int ny, int nz) {
+  pdl_entry();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 1;
   if (i > nx || k >= nz) return;
@@ -210,6 +214,7 @@ __global__ void k_mac_bc_y(T *u, T *v, T *w, BCDev bc, long long xs, long long y
 
 template <typename T>
 __global__ void k_mac_bc_z(T *u, T *v, T *w, BCDev bc, long long xs, long long ys, int nx, int ny, int nz) {
+  pdl_entry();
   const int j = (int)(blockIdx.x * blockDim.x + threadIdx.x) - 1;
   const int i = (int)(blockIdx.y * blockDim.y + threadIdx.y) - 1;
   if (i > nx || j > ny) return;
@@ -248,11 +253,11 @@ ocu_status launch_mac_bc_level1(T *u, T *v, T *w, const ocu_layout &L, int nx, i
     return fail(OCU_ERR_LAYOUT, "[ERROR] apply_3d_mac_boundary_conditions_level1 - must have at least 1 ghost point");
   const BCDev d = to_dev(bc);
   dim3 b(32, 8);
-  k_mac_bc_x<T><<<dim3((nz + 31) / 32, (ny + 7) / 8), b, 0, s>>>(u, v, w, d, L.xstride, L.ystride, nx, ny, nz);
+  launch_pdl(k_mac_bc_x<T>, dim3((nz + 31) / 32, (ny + 7) / 8), b, 0, s, u, v, w, d, L.xstride, L.ystride, nx, ny, nz);
   OCU_TRY(check_launch("k_mac_bc_x"));
-  k_mac_bc_y<T><<<dim3((nz + 31) / 32, (nx + 2 + 7) / 8), b, 0, s>>>(u, v, w, d, L.xstride, L.ystride, nx, ny, nz);
+  launch_pdl(k_mac_bc_y<T>, dim3((nz + 31) / 32, (nx + 2 + 7) / 8), b, 0, s, u, v, w, d, L.xstride, L.ystride, nx, ny, nz);
   OCU_TRY(check_launch("k_mac_bc_y"));
-  k_mac_bc_z<T><<<dim3((ny + 2 + 31) / 32, (nx + 2 + 7) / 8), b, 0, s>>>(u, v, w, d, L.xstride, L.ystride, nx, ny, nz);
+  launch_pdl(k_mac_bc_z<T>, dim3((ny + 2 + 31) / 32, (nx + 2 + 7) / 8), b, 0, s, u, v, w, d, L.xstride, L.ystride, nx, ny, nz);
   return check_launch("k_mac_bc_z");
 }
 
@@ -261,24 +266,28 @@ ocu_status launch_mac_bc_level1(T *u, T *v, T *w, const ocu_layout &L, int nx, i
 // ------------------------------------------------------------------------------------------
 template <typename T>
 __global__ void k_clear(T *buf, long long n, T value) {
+  pdl_entry();
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     buf[i] = value;
 }
 
 template <typename T, typename S>
 __global__ void k_convert(T *dst, const S *src, long long n) {
+  pdl_entry();
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     dst[i] = (T)src[i];
 }
 
 template <typename T>
 __global__ void k_lincomb1(T *res, T a1, const T *g1, long long n) {
+  pdl_entry();
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     res[i] = g1[i] * a1;
 }
 
 template <typename T>
 __global__ void k_lincomb2_1d(T *res, T a1, const T *g1, T a2, const T *g2, long long n) {
+  pdl_entry();
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     res[i] = g1[i] * a1 + g2[i] * a2;
 }
@@ -286,6 +295,7 @@ __global__ void k_lincomb2_1d(T *res, T a1, const T *g1, T a2, const T *g2, long
 template <typename T>
 __global__ void k_lincomb2_3d(T *res, T a1, const T *g1, T a2, const T *g2, long long xs, long long ys,
                               int nx, int ny, int nz) {
+  pdl_entry();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   const int i = blockIdx.z;
@@ -303,19 +313,19 @@ static unsigned grid_for(long long n, int threads) {
 
 template <typename T>
 ocu_status launch_clear(T *buf, long long n, T value, cudaStream_t s) {
-  k_clear<T><<<grid_for(n, 256), 256, 0, s>>>(buf, n, value);
+  launch_pdl(k_clear<T>, grid_for(n, 256), 256, 0, s, buf, n, value);
   return check_launch("k_clear");
 }
 
 template <typename T, typename S>
 ocu_status launch_convert(T *dst, const S *src, long long n, cudaStream_t s) {
-  k_convert<T, S><<<grid_for(n, 256), 256, 0, s>>>(dst, src, n);
+  launch_pdl(k_convert<T, S>, grid_for(n, 256), 256, 0, s, dst, src, n);
   return check_launch("k_convert");
 }
 
 template <typename T>
 ocu_status launch_lincomb1(T *res, T a1, const T *g1, long long n, cudaStream_t s) {
-  k_lincomb1<T><<<grid_for(n, 256), 256, 0, s>>>(res, a1, g1, n);
+  launch_pdl(k_lincomb1<T>, grid_for(n, 256), 256, 0, s, res, a1, g1, n);
   return check_launch("k_lincomb1");
 }
 
@@ -327,11 +337,11 @@ ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, T a2,
   const int waste = (int)(L.allocated - (long long)L.nx * L.ny * L.nz);
   if (waste / (float)L.allocated > .03f) {
     dim3 grid((L.nz + 127) / 128, L.ny, L.nx);
-    k_lincomb2_3d<T><<<grid, 128, 0, s>>>(res + L.shift, a1, g1 + L.shift, a2, g2 + L.shift, L.xstride,
+    launch_pdl(k_lincomb2_3d<T>, grid, 128, 0, s, res + L.shift, a1, g1 + L.shift, a2, g2 + L.shift, L.xstride,
                                           L.ystride, L.nx, L.ny, L.nz);
     return check_launch("k_lincomb2_3d");
   }
-  k_lincomb2_1d<T><<<grid_for(L.allocated, 256), 256, 0, s>>>(res, a1, g1, a2, g2, L.allocated);
+  launch_pdl(k_lincomb2_1d<T>, grid_for(L.allocated, 256), 256, 0, s, res, a1, g1, a2, g2, L.allocated);
   return check_launch("k_lincomb2_1d");
 }
 
@@ -376,6 +386,7 @@ __device__ __forceinline__ void block_tree_256(T *sh, const RedOp<T> &op) {
 template <typename T>
 __global__ void __launch_bounds__(256) k_reduce(const T *origin, long long xs, long long ys, int nx, int ny, int nz,
                                                 RedOp<T> op, T *partial, unsigned *counter, double *result) {
+  pdl_entry();
   __shared__ T sh[256];
   __shared__ bool last;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -447,7 +458,7 @@ ocu_status launch_reduce(const T *origin, const ocu_layout &L, int op, void *d_s
   unsigned *counter = reinterpret_cast<unsigned *>(d_scratch);
   T *partial = reinterpret_cast<T *>(reinterpret_cast<char *>(d_scratch) + 64);
   RedOp<T> r{op};
-  k_reduce<T><<<(unsigned)blocks, 256, 0, s>>>(origin, L.xstride, L.ystride, L.nx, L.ny, L.nz, r, partial,
+  launch_pdl(k_reduce<T>, (unsigned)blocks, 256, 0, s, origin, L.xstride, L.ystride, L.nx, L.ny, L.nz, r, partial,
                                                counter, d_result);
   return check_launch("k_reduce");
 }

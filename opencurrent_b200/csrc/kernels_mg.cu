@@ -39,6 +39,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_relax_color(T *__restrict__ u, const T *__restrict__ b, long long xs,
                                                      long long ys, int nx, int ny, int nz, int color,
                                                      RelaxCoef<T> c, const T *__restrict__ diag) {
+  pdl_entry();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z * blockDim.z + threadIdx.z;
@@ -83,13 +84,14 @@ ocu_status launch_relax_color(T *u, const T *b, const ocu_layout &L, const T *di
   dim3 block(half >= 32 ? 32 : (half >= 16 ? 16 : (half >= 8 ? 8 : 4)), 4, 2);
   block.y = 256 / (block.x * block.z) > 8 ? 8 : 256 / (block.x * block.z);
   dim3 grid((half + block.x - 1) / block.x, (L.ny + block.y - 1) / block.y, (L.nx + block.z - 1) / block.z);
-  k_relax_color<T><<<grid, block, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c, diag);
+  launch_pdl(k_relax_color<T>, grid, block, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c, diag);
   return check_launch("k_relax_color");
 }
 
 // 2D table of the diagonal plus x/y boundary modifiers (sol_mgpressure3ddev.cu:27-43).
 template <typename T>
 __global__ void k_init_diag(T *grid, int nx, int ny, T ld, T xp, T xn, T yp, T yn) {
+  pdl_entry();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   if (i < nx && j < ny) {
@@ -106,7 +108,7 @@ template <typename T>
 ocu_status launch_init_diag(T *diag, int nx, int ny, const RelaxParams &p, cudaStream_t s) {
   const RelaxCoef<T> c = make_relax_coef<T>(p);
   dim3 block(16, 16), grid((nx + 15) / 16, (ny + 15) / 16);
-  k_init_diag<T><<<grid, block, 0, s>>>(diag, nx, ny, c.ld, c.xp, c.xn, c.yp, c.yn);
+  launch_pdl(k_init_diag<T>, grid, block, 0, s, diag, nx, ny, c.ld, c.xp, c.xn, c.yp, c.yn);
   return check_launch("k_init_diag");
 }
 
@@ -120,7 +122,30 @@ template <typename T>
 __global__ void __launch_bounds__(512) k_coarse_relax(T *u, const T *b, long long xs, long long ys, int nx, int ny,
                                                       int nz, int iterations, int order, CoarseCoef<T> c,
                                                       BCDev bc, T hx, T hy, T hz) {
+  pdl_entry();
   coarse_relax_block<T>(u, b, xs, ys, nx, ny, nz, iterations, order, c, bc, hx, hy, hz);
+}
+
+// The same with u and b staged in shared memory (small coarsest levels): the ~4 phases per
+// iteration then wait on shared-memory latency instead of global-memory round trips.
+template <typename T>
+__global__ void __launch_bounds__(512) k_coarse_relax_smem(T *u, const T *b, long long shift, long long n,
+                                                           long long xs, long long ys, int nx, int ny, int nz,
+                                                           int iterations, int order, CoarseCoef<T> c, BCDev bc,
+                                                           T hx, T hy, T hz) {
+  pdl_entry();
+  extern __shared__ __align__(16) unsigned char coarse_smem[];
+  T *su = reinterpret_cast<T *>(coarse_smem);
+  T *sb = su + n;
+  T *ub = u - shift;
+  const T *bb = b - shift;
+  for (long long q = threadIdx.x; q < n; q += blockDim.x) {
+    su[q] = ub[q];
+    sb[q] = bb[q];
+  }
+  __syncthreads();
+  coarse_relax_block<T>(su + shift, sb + shift, xs, ys, nx, ny, nz, iterations, order, c, bc, hx, hy, hz);
+  for (long long q = threadIdx.x; q < n; q += blockDim.x) ub[q] = su[q];
 }
 
 template <typename T>
@@ -135,7 +160,13 @@ ocu_status launch_coarse_relax(T *u, const T *b, const ocu_layout &L, int iterat
     if (iterations % 2 == 1) iterations++;
     if (iterations < 4) iterations = 4;
   }
-  k_coarse_relax<T><<<1, 512, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, iterations, order, c,
+  const size_t bytes = 2 * sizeof(T) * (size_t)L.allocated;
+  if (bytes <= 48 * 1024) {
+    launch_pdl(k_coarse_relax_smem<T>, 1, 512, bytes, s, u, b, L.shift, L.allocated, L.xstride, L.ystride, L.nx,
+               L.ny, L.nz, iterations, order, c, to_dev(p.bc), (T)hx, (T)hy, (T)hz);
+    return check_launch("k_coarse_relax_smem");
+  }
+  launch_pdl(k_coarse_relax<T>, 1, 512, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, iterations, order, c,
                                       to_dev(p.bc), (T)hx, (T)hy, (T)hz);
   return check_launch("k_coarse_relax");
 }
@@ -147,6 +178,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_residual(const T *__restrict__ u, const T *__restrict__ b, T *__restrict__ r,
                                                   long long xs, long long ys, int nx, int ny, int nz, T fxh, T fyh,
                                                   T fzh, T dg) {
+  pdl_entry();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -161,7 +193,7 @@ ocu_status launch_residual(const T *u, const T *b, T *r, const ocu_layout &L, do
                            double fx, double fy, double fz, cudaStream_t s) {
   dim3 block(L.nz >= 64 ? 64 : 32, L.nz >= 64 ? 4 : 8);
   dim3 grid((L.nz + block.x - 1) / block.x, (L.ny + block.y - 1) / block.y, L.nx);
-  k_residual<T><<<grid, block, 0, s>>>(u, b, r, L.xstride, L.ystride, L.nx, L.ny, L.nz, (T)(fx / (h * h)),
+  launch_pdl(k_residual<T>, grid, block, 0, s, u, b, r, L.xstride, L.ystride, L.nx, L.ny, L.nz, (T)(fx / (h * h)),
                                        (T)(fy / (h * h)), (T)(fz / (h * h)), (T)(2 * (fx + fy + fz) / (h * h)));
   return check_launch("k_residual");
 }
@@ -172,6 +204,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_restrict(const T *__restrict__ r, long long rxs, long long rys,
                                                   T *__restrict__ bc_, long long bxs, long long bys, int bnx,
                                                   int bny, int bnz) {
+  pdl_entry();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -187,7 +220,7 @@ ocu_status launch_restrict(const T *r, const ocu_layout &Lf, T *bc_, const ocu_l
                            cudaStream_t s) {
   dim3 block(Lc.nz >= 32 ? 32 : 16, 8);
   dim3 grid((Lc.nz + block.x - 1) / block.x, (Lc.ny + block.y - 1) / block.y, Lc.nx);
-  k_restrict<T><<<grid, block, 0, s>>>(r, Lf.xstride, Lf.ystride, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny,
+  launch_pdl(k_restrict<T>, grid, block, 0, s, r, Lf.xstride, Lf.ystride, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny,
                                        Lc.nz);
   return check_launch("k_restrict");
 }
@@ -199,6 +232,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_prolong(const T *__restrict__ uc, long long cx, long long cy, int cnx,
                                                  int cny, int cnz, T *__restrict__ uf, long long fxs,
                                                  long long fys) {
+  pdl_entry();
   const int kc = blockIdx.x * blockDim.x + threadIdx.x;
   const int jc = blockIdx.y * blockDim.y + threadIdx.y;
   const int ic = blockIdx.z;
@@ -230,7 +264,7 @@ ocu_status launch_prolong(const T *uc, const ocu_layout &Lc, T *uf, const ocu_la
                           cudaStream_t s) {
   dim3 block(Lc.nz >= 32 ? 32 : 16, 8);
   dim3 grid((Lc.nz + block.x - 1) / block.x, (Lc.ny + block.y - 1) / block.y, Lc.nx);
-  k_prolong<T><<<grid, block, 0, s>>>(uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf, Lf.xstride, Lf.ystride);
+  launch_pdl(k_prolong<T>, grid, block, 0, s, uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf, Lf.xstride, Lf.ystride);
   return check_launch("k_prolong");
 }
 
@@ -239,6 +273,7 @@ ocu_status launch_prolong(const T *uc, const ocu_layout &Lc, T *uf, const ocu_la
 // ------------------------------------------------------------------------------------------
 __global__ void k_downcast_interior(const double *__restrict__ r, float *__restrict__ b, long long xs, long long ys,
                                     int nx, int ny, int nz) {
+  pdl_entry();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -249,6 +284,7 @@ __global__ void k_downcast_interior(const double *__restrict__ r, float *__restr
 
 __global__ void k_add_correction(double *__restrict__ x, const float *__restrict__ e, long long xs, long long ys,
                                  int nx, int ny, int nz) {
+  pdl_entry();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -260,14 +296,14 @@ __global__ void k_add_correction(double *__restrict__ x, const float *__restrict
 ocu_status launch_downcast_interior(const double *r, float *b32, const ocu_layout &L,
                                     cudaStream_t s) {
   dim3 block(64, 4), grid((L.nz + 63) / 64, (L.ny + 3) / 4, L.nx);
-  k_downcast_interior<<<grid, block, 0, s>>>(r, b32, L.xstride, L.ystride, L.nx, L.ny, L.nz);
+  launch_pdl(k_downcast_interior, grid, block, 0, s, r, b32, L.xstride, L.ystride, L.nx, L.ny, L.nz);
   return check_launch("k_downcast_interior");
 }
 
 ocu_status launch_add_correction(double *x, const float *e, const ocu_layout &L,
                                  cudaStream_t s) {
   dim3 block(64, 4), grid((L.nz + 63) / 64, (L.ny + 3) / 4, L.nx);
-  k_add_correction<<<grid, block, 0, s>>>(x, e, L.xstride, L.ystride, L.nx, L.ny, L.nz);
+  launch_pdl(k_add_correction, grid, block, 0, s, x, e, L.xstride, L.ystride, L.nx, L.ny, L.nz);
   return check_launch("k_add_correction");
 }
 

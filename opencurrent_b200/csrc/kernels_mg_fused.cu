@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, con
                                                           int nx, int ny, int nz, int color, RelaxCoefD<T> c,
                                                           const T *__restrict__ diag,
                                                           const __grid_constant__ GhostEmit<T> ge) {
+  pdl_entry();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z * blockDim.z + threadIdx.z;
@@ -79,6 +80,7 @@ __device__ __forceinline__ float v4_update(float uc, float bv, float zm, float z
 __global__ void __launch_bounds__(256, 6) k_relax_color_v4(float *__restrict__ u, const float *__restrict__ b, int xs,
                                                         int ys, int nx, int ny, int nz, int color,
                                                         RelaxCoefD<float> c, const __grid_constant__ GhostEmit<float> ge) {
+  pdl_entry();
   const int lane = threadIdx.x;
   const int k4 = (blockIdx.x * 32 + lane) * 4;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -97,10 +99,15 @@ __global__ void __launch_bounds__(256, 6) k_relax_color_v4(float *__restrict__ u
   const float4 YP = *reinterpret_cast<const float4 *>(u + base + ys);
   const float4 XM = *reinterpret_cast<const float4 *>(u + base - xs);
   const float4 XP = *reinterpret_cast<const float4 *>(u + base + xs);
+  // the row neighbours beyond the warp's 128 cells: k4 - 1 for lane 0 (a ghost at k = -1 when
+  // k4 == 0), k4 + 4 for lane 31 (a ghost at k = nz at the row's end).  Every lane loads (the
+  // others a cell of the same lines), so the load issues with the float4 loads and costs no
+  // second round trip.
+  const float E = u[base + (lane == 31 ? 4 : -1)];
   float left = __shfl_up_sync(0xffffffffu, U.w, 1);
   float right = __shfl_down_sync(0xffffffffu, U.x, 1);
-  if (lane == 0) left = u[base - 1];    // k4 - 1: a ghost at k = -1 when k4 == 0
-  if (lane == 31) right = u[base + 4];  // k4 + 4: a ghost at k = nz at the row's end
+  if (lane == 0) left = E;
+  if (lane == 31) right = E;
   float4 out = U;
   int k0, k1;
   float v0, v1;
@@ -128,7 +135,7 @@ bool launch_color_v4<float>(float *u, const float *b, const ocu_layout &L, int c
                             const GhostEmit<float> &ge, const float *, cudaStream_t s) {
   if (L.nz % 128 != 0 || L.allocated >= (1LL << 31) || L.shift % 4 != 0 || L.ystride % 4 != 0) return false;
   dim3 block(32, 4, 2), grid((L.nz + 127) / 128, (L.ny + 3) / 4, (L.nx + 1) / 2);
-  k_relax_color_v4<<<grid, block, 0, s>>>(u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c, ge);
+  launch_pdl(k_relax_color_v4, grid, block, 0, s, u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c, ge);
   return true;
 }
 
@@ -145,10 +152,10 @@ ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const 
   ge.p = u;
   if (launch_color_v4<T>(u, b, L, color, c, ge, diag, s)) return check_launch("k_relax_color_v4");
   if (L.allocated < (1LL << 31))
-    k_relax_color_emit<T, int><<<grid, block, 0, s>>>(u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c,
+    launch_pdl(k_relax_color_emit<T, int>, grid, block, 0, s, u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c,
                                                       diag, ge);
   else
-    k_relax_color_emit<T, long long><<<grid, block, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c,
+    launch_pdl(k_relax_color_emit<T, long long>, grid, block, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c,
                                                             diag, ge);
   return check_launch("k_relax_color_emit");
 }
@@ -204,6 +211,7 @@ template <typename T, typename I>
 __global__ void __launch_bounds__(256, 4) k_prolong_emit(const T *__restrict__ uc, I cx, I cy, int cnx, int cny,
                                                          int cnz, T *__restrict__ uf, I fxs, I fys,
                                                          const __grid_constant__ GhostEmit<T> ge) {
+  pdl_entry();
   const int kc = blockIdx.x * blockDim.x + threadIdx.x;
   const int jc = blockIdx.y * blockDim.y + threadIdx.y;
   const int ic = blockIdx.z;
@@ -254,6 +262,7 @@ __device__ __noinline__ void prolong_zghosts(const GhostEmit<float> *ge, const f
 __global__ void __launch_bounds__(256, 4) k_prolong_v4(const float *__restrict__ uc, int cx, int cy, int cnx,
                                                        int cny, int cnz, float *__restrict__ uf, int fxs, int fys,
                                                        const __grid_constant__ GhostEmit<float> ge) {
+  pdl_entry();
   const int lane = threadIdx.x;
   const int m = blockIdx.x * 32 + lane;
   const int jc = blockIdx.y * blockDim.y + threadIdx.y;
@@ -269,9 +278,10 @@ __global__ void __launch_bounds__(256, 4) k_prolong_v4(const float *__restrict__
     for (int dj = -1; dj <= 1; dj++) {
       const int base = (ic + di) * cx + (jc + dj) * cy + 2 * m;
       const float2 v = *reinterpret_cast<const float2 *>(uc + base);
+      const float E = uc[base + (lane == 31 ? 2 : -1)];  // as in k_relax_color_v4: one load for all lanes
       float l = __shfl_up_sync(0xffffffffu, v.y, 1), r = __shfl_down_sync(0xffffffffu, v.x, 1);
-      if (lane == 0) l = uc[base - 1];
-      if (lane == 31) r = uc[base + 2];
+      if (lane == 0) l = E;
+      if (lane == 31) r = E;
       c[dj + 1][0] = l;
       c[dj + 1][1] = v.x;
       c[dj + 1][2] = v.y;
@@ -323,16 +333,16 @@ ocu_status launch_prolong_emit(const T *uc, const ocu_layout &Lc, T *uf, const o
   if (sizeof(T) == 4 && Lc.nz % 64 == 0 && Lf.allocated < (1LL << 31) && Lc.shift % 2 == 0 && Lf.shift % 4 == 0 &&
       Lc.ystride % 2 == 0 && Lf.ystride % 4 == 0) {
     dim3 b4(32, 4, 2), g4(Lc.nz / 64, (Lc.ny + 3) / 4, (Lc.nx + 1) / 2);
-    k_prolong_v4<<<g4, b4, 0, s>>>((const float *)uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz,
+    launch_pdl(k_prolong_v4, g4, b4, 0, s, (const float *)uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz,
                                    (float *)uf, (int)Lf.xstride, (int)Lf.ystride,
                                    *reinterpret_cast<const GhostEmit<float> *>(&ge));
     return check_launch("k_prolong_v4");
   }
   if (Lf.allocated < (1LL << 31) && Lc.allocated < (1LL << 31))
-    k_prolong_emit<T, int><<<grid, block, 0, s>>>(uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
+    launch_pdl(k_prolong_emit<T, int>, grid, block, 0, s, uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
                                                   (int)Lf.xstride, (int)Lf.ystride, ge);
   else
-    k_prolong_emit<T, long long><<<grid, block, 0, s>>>(uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
+    launch_pdl(k_prolong_emit<T, long long>, grid, block, 0, s, uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
                                                         Lf.xstride, Lf.ystride, ge);
   return check_launch("k_prolong_emit");
 }
@@ -384,6 +394,7 @@ __global__ void __launch_bounds__(256) k_residual_rows(const T *__restrict__ u, 
                                                        T *__restrict__ r, float *__restrict__ r32, long long xs,
                                                        long long ys, int nx, int ny, int nz, ResCoefT<T> c,
                                                        T *__restrict__ rows2, T *__restrict__ rowsinf) {
+  pdl_entry();
   const int lane = threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const int i = blockIdx.z;
@@ -425,6 +436,7 @@ __global__ void __launch_bounds__(256) k_residual_restrict(const T *__restrict__
                                                            ResCoefT<T> c, T *__restrict__ bc_, long long bxs,
                                                            long long bys, int cnx, int cny, int cnz,
                                                            T *__restrict__ rows2, T *__restrict__ rowsinf) {
+  pdl_entry();
   const int lane = threadIdx.x;
   const int jc = blockIdx.y * blockDim.y + threadIdx.y;
   const int ic = blockIdx.z;
@@ -479,6 +491,7 @@ __global__ void __launch_bounds__(256) k_residual_restrict(const T *__restrict__
 template <typename T>
 __global__ void __launch_bounds__(256) k_fold_rows(const T *__restrict__ rows, long long nrows, int is_max,
                                                    T *partial, unsigned *counter, double *result) {
+  pdl_entry();
   __shared__ T sh[256];
   __shared__ bool last;
   const long long idx = (long long)blockIdx.x * 256 + threadIdx.x;
@@ -535,7 +548,7 @@ template <typename T>
 ocu_status launch_residual_rows(const T *u, const T *b, T *r, float *r32, const ocu_layout &L, double h, double fx,
                                 double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s) {
   dim3 block(32, 8), grid(1, (L.ny + 7) / 8, L.nx);
-  k_residual_rows<T><<<grid, block, 0, s>>>(u, b, r, r32, L.xstride, L.ystride, L.nx, L.ny, L.nz,
+  launch_pdl(k_residual_rows<T>, grid, block, 0, s, u, b, r, r32, L.xstride, L.ystride, L.nx, L.ny, L.nz,
                                             res_coef<T>(h, fx, fy, fz), rows2, rowsinf);
   return check_launch("k_residual_rows");
 }
@@ -546,10 +559,10 @@ ocu_status launch_residual_restrict(const T *u, const T *b, const ocu_layout &Lf
   dim3 block(32, 8), grid(1, (Lc.ny + 7) / 8, Lc.nx);
   const ResCoefT<T> c = res_coef<T>(h, fx, fy, fz);
   if (rows2 || rowsinf)
-    k_residual_restrict<T, true><<<grid, block, 0, s>>>(u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
+    launch_pdl(k_residual_restrict<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
                                                         Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf);
   else
-    k_residual_restrict<T, false><<<grid, block, 0, s>>>(u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
+    launch_pdl(k_residual_restrict<T, false>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
                                                          Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr);
   return check_launch("k_residual_restrict");
 }
@@ -560,7 +573,7 @@ ocu_status launch_fold_rows(const T *rows, long long nrows, bool is_max, void *s
   const long long blocks = (nrows + 255) / 256;
   unsigned *counter = reinterpret_cast<unsigned *>(scratch);
   T *partial = reinterpret_cast<T *>(reinterpret_cast<char *>(scratch) + 64);
-  k_fold_rows<T><<<(unsigned)blocks, 256, 0, s>>>(rows, nrows, is_max ? 1 : 0, partial, counter, result);
+  launch_pdl(k_fold_rows<T>, (unsigned)blocks, 256, 0, s, rows, nrows, is_max ? 1 : 0, partial, counter, result);
   return check_launch("k_fold_rows");
 }
 
@@ -688,6 +701,7 @@ __device__ __forceinline__ int batch_member(const BatchSel &sel, int m) {
 template <typename T>
 __global__ void __launch_bounds__(1024) k_coarse_tail(const __grid_constant__ TailParams<T> P,
                                                       const __grid_constant__ TailBatch tb) {
+  pdl_entry();
   __shared__ TailLevel<T> lv[kMaxTailLevels];
   const int m = batch_member(tb.sel, blockIdx.x);
   if (m < 0) return;
@@ -708,6 +722,7 @@ __global__ void __launch_bounds__(1024) k_coarse_tail(const __grid_constant__ Ta
 template <typename T>
 __global__ void __launch_bounds__(512) k_coarse_tail_smem(const __grid_constant__ TailParams<T> P,
                                                            const __grid_constant__ TailBatch tb) {
+  pdl_entry();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ TailLevel<T> lv[kMaxTailLevels];
   __shared__ TailLevel<T> gl[kMaxTailLevels];  // this member's levels in global memory
@@ -789,10 +804,10 @@ ocu_status launch_coarse_tail_batch(const TailParams<T> &P, const TailBatch &tb,
     }
     // one warp-multiple of threads per ~2 cells of the largest level: small tails take 256
     const long long top = (long long)P.lv[0].nx * P.lv[0].ny * P.lv[0].nz;
-    k_coarse_tail_smem<T><<<members, top <= 512 ? 256 : 512, bytes, s>>>(P, tb);
+    launch_pdl(k_coarse_tail_smem<T>, members, top <= 512 ? 256 : 512, bytes, s, P, tb);
     return check_launch("k_coarse_tail_smem");
   }
-  k_coarse_tail<T><<<members, 1024, 0, s>>>(P, tb);
+  launch_pdl(k_coarse_tail<T>, members, 1024, 0, s, P, tb);
   return check_launch("k_coarse_tail");
 }
 
@@ -815,6 +830,7 @@ __global__ void __launch_bounds__(256) k_relax_color_emit_b(T *__restrict__ u, c
                                                             RelaxCoefD<T> c, const T *__restrict__ diag,
                                                             const __grid_constant__ GhostEmit<T> ge, BatchSel sel,
                                                             long long ms, int zb) {
+  pdl_entry();
   const int m = batch_member(sel, blockIdx.z / zb);
   if (m < 0) return;
   const int bz = blockIdx.z % zb;
@@ -844,7 +860,7 @@ ocu_status launch_relax_color_emit_b(T *u, const T *b, const ocu_layout &L, cons
     return fail(OCU_ERR_UNSUPPORTED, "[ERROR] ensemble - too many members of size (%d,%d,%d) in one class", L.nx, L.ny, L.nz);
   dim3 grid((half + bl.x - 1) / bl.x, (L.ny + bl.y - 1) / bl.y, (unsigned)(zb * members));
   GhostEmit<T> ge{u, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(p.bc), (T)hx, (T)hy, (T)hz};
-  k_relax_color_emit_b<T><<<grid, bl, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c, diag, ge, sel,
+  launch_pdl(k_relax_color_emit_b<T>, grid, bl, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c, diag, ge, sel,
                                               ms, zb);
   return check_launch("k_relax_color_emit_b");
 }
@@ -855,6 +871,7 @@ __global__ void __launch_bounds__(256, 3) k_prolong_emit_b(const T *__restrict__
                                                            long long fxs, long long fys,
                                                            const __grid_constant__ GhostEmit<T> ge, BatchSel sel,
                                                            long long cms, long long fms) {
+  pdl_entry();
   const int m = batch_member(sel, blockIdx.z / cnx);
   if (m < 0) return;
   const int ic = blockIdx.z % cnx;
@@ -883,7 +900,7 @@ ocu_status launch_prolong_emit_b(const T *uc, const ocu_layout &Lc, T *uf, const
     return fail(OCU_ERR_UNSUPPORTED, "[ERROR] ensemble - too many members of one size in one class");
   dim3 grid((Lc.nz + block.x - 1) / block.x, (Lc.ny + block.y - 1) / block.y, (unsigned)(Lc.nx * members));
   GhostEmit<T> ge{uf, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, to_dev(bc_fine), (T)hx, (T)hy, (T)hz};
-  k_prolong_emit_b<T><<<grid, block, 0, s>>>(uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf, Lf.xstride,
+  launch_pdl(k_prolong_emit_b<T>, grid, block, 0, s, uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf, Lf.xstride,
                                              Lf.ystride, ge, sel, cms, fms);
   return check_launch("k_prolong_emit_b");
 }
@@ -897,6 +914,7 @@ __global__ void __launch_bounds__(256) k_residual_restrict_b(const T *__restrict
                                                              long long bys, int cnx, int cny, int cnz,
                                                              T *__restrict__ rows2, BatchSel sel, long long fms,
                                                              long long cms) {
+  pdl_entry();
   const int m = batch_member(sel, blockIdx.z / cnx);
   if (m < 0) return;
   const int ic = blockIdx.z % cnx;
@@ -953,11 +971,11 @@ ocu_status launch_residual_restrict_b(const T *u, const T *b, const ocu_layout &
   dim3 block(32, 8), grid(1, (Lc.ny + 7) / 8, (unsigned)(Lc.nx * members));
   const ResCoefT<T> c = res_coef<T>(h, fx, fy, fz);
   if (rows2)
-    k_residual_restrict_b<T, true><<<grid, block, 0, s>>>(u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
+    launch_pdl(k_residual_restrict_b<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
                                                           Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, sel,
                                                           fms, cms);
   else
-    k_residual_restrict_b<T, false><<<grid, block, 0, s>>>(u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c,
+    launch_pdl(k_residual_restrict_b<T, false>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c,
                                                            bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr,
                                                            sel, fms, cms);
   return check_launch("k_residual_restrict_b");
@@ -969,6 +987,7 @@ __global__ void __launch_bounds__(256) k_residual_rows_b(const T *__restrict__ u
                                                          long long xs, long long ys, int nx, int ny, int nz,
                                                          ResCoefT<T> c, T *__restrict__ rows2, BatchSel sel,
                                                          long long ms) {
+  pdl_entry();
   const int m = batch_member(sel, blockIdx.z / nx);
   if (m < 0) return;
   const int i = blockIdx.z % nx;
@@ -997,7 +1016,7 @@ ocu_status launch_residual_rows_b(const T *u, const T *b, const ocu_layout &L, d
   if ((long long)L.nx * members > 65535)
     return fail(OCU_ERR_UNSUPPORTED, "[ERROR] ensemble - too many members of one size in one class");
   dim3 block(32, 8), grid(1, (L.ny + 7) / 8, (unsigned)(L.nx * members));
-  k_residual_rows_b<T><<<grid, block, 0, s>>>(u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz,
+  launch_pdl(k_residual_rows_b<T>, grid, block, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz,
                                               res_coef<T>(h, fx, fy, fz), rows2, sel, ms);
   return check_launch("k_residual_rows_b");
 }
@@ -1007,6 +1026,7 @@ ocu_status launch_residual_rows_b(const T *u, const T *b, const ocu_layout &L, d
 template <typename T>
 __global__ void __launch_bounds__(256) k_fold_rows_b(const T *__restrict__ rows, long long nrows, T *partial,
                                                      long long pstride, double *sums, BatchSel sel) {
+  pdl_entry();
   __shared__ T sh[256];
   const int m = batch_member(sel, blockIdx.x);
   if (m < 0) return;
@@ -1046,7 +1066,7 @@ __global__ void __launch_bounds__(256) k_fold_rows_b(const T *__restrict__ rows,
 template <typename T>
 ocu_status launch_fold_rows_b(const T *rows, long long nrows, T *partial, long long pstride, double *sums,
                               const BatchSel &sel, int members, cudaStream_t s) {
-  k_fold_rows_b<T><<<members, 256, 0, s>>>(rows, nrows, partial, pstride, sums, sel);
+  launch_pdl(k_fold_rows_b<T>, members, 256, 0, s, rows, nrows, partial, pstride, sums, sel);
   return check_launch("k_fold_rows_b");
 }
 
@@ -1056,6 +1076,7 @@ template <typename T>
 __global__ void __launch_bounds__(512) k_bc_fill_b(T *u, long long xs, long long ys, int nx, int ny, int nz,
                                                    const __grid_constant__ BCDev bc, T hx, T hy, T hz, BatchSel sel,
                                                    long long ms, int *state, int retire) {
+  pdl_entry();
   const int m = batch_member(sel, blockIdx.x);
   if (m < 0) return;
   level1_fill_block<T>(u + m * ms, xs, ys, nx, ny, nz, bc, hx, hy, hz);
@@ -1069,7 +1090,7 @@ template <typename T>
 ocu_status launch_bc_fill_b(T *u, const ocu_layout &L, const ocu_bc_set &bc, double hx, double hy, double hz,
                             const BatchSel &sel, long long ms, int members, int *state, bool retire,
                             cudaStream_t s) {
-  k_bc_fill_b<T><<<members, 512, 0, s>>>(u, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(bc), (T)hx, (T)hy,
+  launch_pdl(k_bc_fill_b<T>, members, 512, 0, s, u, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(bc), (T)hx, (T)hy,
                                          (T)hz, sel, ms, state, retire ? 1 : 0);
   return check_launch("k_bc_fill_b");
 }
@@ -1082,6 +1103,7 @@ template <typename T>
 __global__ void __launch_bounds__(1024) k_converge_b(const double *sums, long long ncell, const double *tol,
                                                      int *state, int *vcycles, double *last_l2, int *active,
                                                      int members, int initial) {
+  pdl_entry();
   __shared__ int cnt;
   if (threadIdx.x == 0) cnt = 0;
   __syncthreads();
@@ -1107,7 +1129,7 @@ __global__ void __launch_bounds__(1024) k_converge_b(const double *sums, long lo
 template <typename T>
 ocu_status launch_converge_b(const double *sums, long long ncell, const double *tol, int *state, int *vcycles,
                              double *last_l2, int *active, int members, bool initial, cudaStream_t s) {
-  k_converge_b<T><<<1, 1024, 0, s>>>(sums, ncell, tol, state, vcycles, last_l2, active, members, initial ? 1 : 0);
+  launch_pdl(k_converge_b<T>, 1, 1024, 0, s, sums, ncell, tol, state, vcycles, last_l2, active, members, initial ? 1 : 0);
   return check_launch("k_converge_b");
 }
 

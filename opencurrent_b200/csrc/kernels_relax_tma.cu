@@ -120,6 +120,7 @@ __global__ void __launch_bounds__(SweepTile<T>::THREADS, 3) k_relax_sweep2(
     const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_b, T *__restrict__ u_out,
     long long xs, long long ys, SweepArgs a, RelaxCoefD<T> c, const T *__restrict__ diag, GhostEmit<T> ge,
     int *__restrict__ err) {
+  pdl_entry();
   using S = SweepTile<T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // TMA destinations must be 128-byte aligned: align the base explicitly
@@ -368,7 +369,7 @@ ocu_status launch_relax_sweep2(const SweepTmap &tm_u_in, const SweepTmap &tm_b, 
   CUtensorMap tu, tb;
   std::memcpy(&tu, tm_u_in.bytes, sizeof(tu));
   std::memcpy(&tb, tm_b.bytes, sizeof(tb));
-  k_relax_sweep2<T><<<(unsigned)grid, S::THREADS, S::SMEM, s>>>(tu, tb, u_out, L.xstride, L.ystride, a, c, diag, ge,
+  launch_pdl(k_relax_sweep2<T>, (unsigned)grid, S::THREADS, S::SMEM, s, tu, tb, u_out, L.xstride, L.ystride, a, c, diag, ge,
                                                                err);
   return check_launch("k_relax_sweep2");
 }

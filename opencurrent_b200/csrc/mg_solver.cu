@@ -197,7 +197,9 @@ ocu_status MGCore<T>::apply_bc(int level) {
 
 template <typename T>
 ocu_status MGCore<T>::clear_zero(int level) {
-  return check_cuda(cudaMemsetAsync(grids_u[level]->buf, 0, sizeof(T) * lay[level].allocated, stream), "clear_zero");
+  // a kernel rather than a memset node, so that the launches around it keep their programmatic
+  // (overlapped) dependencies
+  return launch_clear<T>(static_cast<T *>(grids_u[level]->buf), lay[level].allocated, (T)0, stream);
 }
 
 // clear_zero(level) followed by apply_boundary_conditions(level).  Below level 0 the boundary

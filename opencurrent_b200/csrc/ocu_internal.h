@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 
 #include "../../include/ocu_b200.h"
 
@@ -27,6 +28,39 @@ unsigned long long launch_count();
 void set_capturing(bool on);
 unsigned long long launch_count_captured();
 const char *last_error_text();
+
+// ---- programmatic dependent launch ---------------------------------------------------------
+// The multigrid, grid and boundary kernels are launched with
+// cudaLaunchAttributeProgrammaticStreamSerialization: the next kernel of a stream may be
+// scheduled while its predecessor is still running.  Every kernel launched this way starts with
+// pdl_entry(): griddepcontrol.wait returns once the predecessor grid has completed and its
+// memory operations are visible, so nothing is read or written before that; the
+// launch_dependents that follows lets the successor's blocks be scheduled early.  A kernel
+// launched without the attribute passes the wait at once.  OCU_B200_PDL=0 turns the attribute off.
+bool pdl_enabled();
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args &&...args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_entry() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+#endif
 
 inline size_t dtype_size(ocu_dtype d) { return d == OCU_F64 ? 8 : 4; }
 
