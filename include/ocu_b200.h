@@ -164,6 +164,11 @@ typedef struct ocu_mg_params {
   int sweep_cells;               /* levels with at least this many cells relax both colours in
                                     one TMA-fed pass (out of place, same results; Dirichlet and
                                     Neumann faces only); <= 0 = off (the default) */
+  int leg_cells;                 /* levels below 0 with at most this many cells run the down-leg
+                                    (nu1 iterations + residual restriction) and the up-leg
+                                    (prolongation + nu2 iterations) of a V-cycle as one launch
+                                    each (same results; nu1, nu2 <= 2); <= 0 = off (the
+                                    default) */
 } ocu_mg_params;
 
 typedef struct ocu_mg_stats {

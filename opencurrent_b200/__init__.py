@@ -213,6 +213,7 @@ class _MGBase:
         self.unfused = False
         self.tail_cells = 0
         self.sweep_cells = 0
+        self.leg_cells = 0
         self._h = None
         self._rhs = None
 
@@ -227,6 +228,7 @@ class _MGBase:
         p.unfused = int(bool(self.unfused))
         p.tail_cells = int(self.tail_cells)
         p.sweep_cells = int(self.sweep_cells)
+        p.leg_cells = int(self.leg_cells)
         return p
 
     def initialize_storage(self, nx, ny, nz, hx, hy, hz, rhs):

@@ -350,13 +350,6 @@ ocu_status launch_prolong_emit(const T *uc, const ocu_layout &Lc, T *uf, const o
 // ------------------------------------------------------------------------------------------
 // Residual helpers
 // ------------------------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ T residual_at(const T *__restrict__ u, const T *__restrict__ b, long long id, long long xs,
-                                         long long ys, const ResCoefT<T> &c) {
-  return b[id] - (c.fzh * (u[id - 1] + u[id + 1]) + c.fyh * (u[id - ys] + u[id + ys]) +
-                  c.fxh * (u[id - xs] + u[id + xs]) - c.dg * u[id]);
-}
-
 // Fold one 64-wide chunk of a fine row into the lane accumulators in reference order:
 // this lane holds r at k = base + 2*lane (+1); virtual lane t needs k = base + t and
 // base + 32 + t, held by lanes t/2 and 16 + t/2.

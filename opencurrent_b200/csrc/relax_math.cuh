@@ -65,4 +65,13 @@ __device__ __forceinline__ T relax_point(const T *__restrict__ u, const T *__res
                         nx, ny, nz, c, diag);
 }
 
+// Residual b - L u of one cell (devf.cu:68-90, devd.cu:94-114), the operand order of every
+// residual kernel.
+template <typename T>
+__device__ __forceinline__ T residual_at(const T *__restrict__ u, const T *__restrict__ b, long long id, long long xs,
+                                         long long ys, const ResCoefT<T> &c) {
+  return b[id] - (c.fzh * (u[id - 1] + u[id + 1]) + c.fyh * (u[id - ys] + u[id + ys]) +
+                  c.fxh * (u[id - xs] + u[id + xs]) - c.dg * u[id]);
+}
+
 }  // namespace ocub
