@@ -437,7 +437,9 @@ __global__ void __launch_bounds__(256) k_residual_restrict(const T *__restrict__
   const bool want2 = NORM && rows2 != nullptr, wantinf = NORM && rowsinf != nullptr;
   T acc2[4] = {0, 0, 0, 0}, accinf[4] = {0, 0, 0, 0};
   const long long frow = (long long)(2 * ic) * xs + (long long)(2 * jc) * ys;
-  for (int cbase = 0; cbase < cnz; cbase += 32) {
+  // with norms a warp walks its whole row (the fold runs along k); without, one 32-cell chunk
+  const int cfirst = NORM ? 0 : blockIdx.x * 32, cend = NORM ? cnz : min(cfirst + 32, cnz);
+  for (int cbase = cfirst; cbase < cend; cbase += 32) {
     const int kc = cbase + lane;
     T r[8];
     if (kc < cnz) {
@@ -458,6 +460,95 @@ __global__ void __launch_bounds__(256) k_residual_restrict(const T *__restrict__
     }
     if (NORM && (want2 || wantinf)) {
       // fine rows: (di,dj) = (0,0): r0,r1 ; (0,1): r2,r3 ; (1,0): r4,r5 ; (1,1): r6,r7
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        fold_chunk<T>(r[2 * q], r[2 * q + 1], 2 * cbase, nz, lane, acc2[q], accinf[q], want2, wantinf);
+    }
+  }
+  if (NORM) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * ic + (q >> 1), j = 2 * jc + (q & 1);
+      if (want2) {
+        const T v = warp_tree<T>(acc2[q], false);
+        if (lane == 0) rows2[(long long)i * ny + j] = v;
+      }
+      if (wantinf) {
+        const T v = warp_tree<T>(accinf[q], true);
+        if (lane == 0) rowsinf[(long long)i * ny + j] = v;
+      }
+    }
+  }
+}
+
+// The same with 2-wide vector loads: a lane's two children of a fine row are one float2/double2,
+// and so are their neighbours in the rows j-1 / j+2 and planes i-1 / i+2; the row neighbours
+// k-1 and k+2 are scalar loads of the same lines.  24 load instructions per coarse cell instead
+// of 64; each residual is residual_at's expression on the same operands.
+template <typename T> struct Vec2T;
+template <> struct Vec2T<float> { using type = float2; };
+template <> struct Vec2T<double> { using type = double2; };
+
+template <typename T>
+__device__ __forceinline__ T residual_pt(T bv, T uc, T zm, T zp, T ym, T yp, T xm, T xp, const ResCoefT<T> &c) {
+  return bv - (c.fzh * (zm + zp) + c.fyh * (ym + yp) + c.fxh * (xm + xp) - c.dg * uc);
+}
+
+template <typename T, bool NORM>
+__global__ void __launch_bounds__(256) k_residual_restrict_v2(const T *__restrict__ u, const T *__restrict__ b,
+                                                              long long xs, long long ys, int nx, int ny, int nz,
+                                                              ResCoefT<T> c, T *__restrict__ bc_, long long bxs,
+                                                              long long bys, int cnx, int cny, int cnz,
+                                                              T *__restrict__ rows2, T *__restrict__ rowsinf) {
+  using V = typename Vec2T<T>::type;
+  pdl_entry();
+  const int lane = threadIdx.x;
+  const int jc = blockIdx.y * blockDim.y + threadIdx.y;
+  const int ic = blockIdx.z;
+  if (jc >= cny) return;
+  const bool want2 = NORM && rows2 != nullptr, wantinf = NORM && rowsinf != nullptr;
+  T acc2[4] = {0, 0, 0, 0}, accinf[4] = {0, 0, 0, 0};
+  const long long f00 = (long long)(2 * ic) * xs + (long long)(2 * jc) * ys;
+  // with norms a warp walks its whole row (the fold runs along k); without, one 32-cell chunk
+  const int cfirst = NORM ? 0 : blockIdx.x * 32, cend = NORM ? cnz : min(cfirst + 32, cnz);
+  for (int cbase = cfirst; cbase < cend; cbase += 32) {
+    const int kc = cbase + lane;
+    const bool act = kc < cnz;
+    const long long kk = 2 * (act ? kc : cnz - 1);  // lanes past the row end read the last pair
+    V U[2][2], B[2][2], Yo[2][2], Xo[2][2];
+    T Lz[2][2], Rz[2][2];
+#pragma unroll
+    for (int di = 0; di < 2; di++)
+#pragma unroll
+      for (int dj = 0; dj < 2; dj++) {
+        const long long row = f00 + di * xs + dj * ys + kk;
+        U[di][dj] = *reinterpret_cast<const V *>(u + row);
+        B[di][dj] = *reinterpret_cast<const V *>(b + row);
+        Yo[di][dj] = *reinterpret_cast<const V *>(u + row + (dj ? ys : -ys));  // rows 2jc-1 / 2jc+2
+        Xo[di][dj] = *reinterpret_cast<const V *>(u + row + (di ? xs : -xs));  // planes 2ic-1 / 2ic+2
+        Lz[di][dj] = u[row - 1];
+        Rz[di][dj] = u[row + 2];
+      }
+    T r[8];
+#pragma unroll
+    for (int di = 0; di < 2; di++)
+#pragma unroll
+      for (int dj = 0; dj < 2; dj++)
+#pragma unroll
+        for (int dk = 0; dk < 2; dk++) {
+          const V &uc = U[di][dj];
+          const T ucv = dk ? uc.y : uc.x, bv = dk ? B[di][dj].y : B[di][dj].x;
+          const T zm = dk ? uc.x : Lz[di][dj], zp = dk ? Rz[di][dj] : uc.y;
+          const V &ymv = dj ? U[di][0] : Yo[di][0], &ypv = dj ? Yo[di][1] : U[di][1];
+          const V &xmv = di ? U[0][dj] : Xo[0][dj], &xpv = di ? Xo[1][dj] : U[1][dj];
+          const T ym = dk ? ymv.y : ymv.x, yp = dk ? ypv.y : ypv.x;
+          const T xm = dk ? xmv.y : xmv.x, xp = dk ? xpv.y : xpv.x;
+          r[4 * di + 2 * dj + dk] = act ? residual_pt<T>(bv, ucv, zm, zp, ym, yp, xm, xp, c) : (T)0;
+        }
+    if (act)
+      bc_[(long long)ic * bxs + (long long)jc * bys + kc] =
+          (T)0.125 * (r[0] + r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7]);
+    if (NORM && (want2 || wantinf)) {
 #pragma unroll
       for (int q = 0; q < 4; q++)
         fold_chunk<T>(r[2 * q], r[2 * q + 1], 2 * cbase, nz, lane, acc2[q], accinf[q], want2, wantinf);
@@ -551,12 +642,25 @@ ocu_status launch_residual_restrict(const T *u, const T *b, const ocu_layout &Lf
                                     double h, double fx, double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s) {
   dim3 block(32, 8), grid(1, (Lc.ny + 7) / 8, Lc.nx);
   const ResCoefT<T> c = res_coef<T>(h, fx, fy, fz);
-  if (rows2 || rowsinf)
-    launch_pdl(k_residual_restrict<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
-                                                        Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf);
-  else
-    launch_pdl(k_residual_restrict<T, false>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
-                                                         Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr);
+  if (sizeof(T) == 4 && Lf.shift % 2 == 0 && Lf.xstride % 2 == 0 && Lf.ystride % 2 == 0 && Lf.nz == 2 * Lc.nz) {
+    if (rows2 || rowsinf) {
+      launch_pdl(k_residual_restrict_v2<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny,
+                 Lf.nz, c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf);
+    } else {
+      dim3 gridc((Lc.nz + 31) / 32, (Lc.ny + 7) / 8, Lc.nx);
+      launch_pdl(k_residual_restrict_v2<T, false>, gridc, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny,
+                 Lf.nz, c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr);
+    }
+    return check_launch("k_residual_restrict_v2");
+  }
+  if (rows2 || rowsinf) {
+    launch_pdl(k_residual_restrict<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz,
+               c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf);
+  } else {
+    dim3 gridc((Lc.nz + 31) / 32, (Lc.ny + 7) / 8, Lc.nx);
+    launch_pdl(k_residual_restrict<T, false>, gridc, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz,
+               c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr);
+  }
   return check_launch("k_residual_restrict");
 }
 
