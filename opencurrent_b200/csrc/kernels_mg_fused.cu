@@ -63,15 +63,25 @@ __global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, con
 // FP32 colour sweep with 128-bit accesses: a thread owns four consecutive cells of a row (two of
 // each colour) and updates its two cells of the sweep's colour.  Its row neighbours come from
 // the same float4 or, across the float4 boundary, from the adjacent lanes; u of the rows j +- 1
-// and planes i +- 1 and b are float4 loads; the two new values go back with one float4 store
-// (the other two entries rewritten unchanged: nothing else writes them in this launch).  A warp
-// covers 128 consecutive cells of one row (nz a multiple of 128).  Rows on a j or i face take the
-// per-cell path; in the other rows only the z-face cells add their diagonal term (the x and y
-// terms are absent there, so the sum is the reference's sequence) and write their ghosts.
+// and planes i +- 1 and b are float4 loads (ghost rows and planes included); the two new values
+// go back with one float4 store (the other two entries rewritten unchanged: nothing else writes
+// them in this launch).  A warp covers 128 consecutive cells of one row (nz a multiple of 128).
+// The diagonal adds the face terms of relax_dg in its order (x, y only on face rows).  Rows on a
+// j or i face write every ghost of their cells (GhostEmit); in the other rows only the z-face
+// ghosts exist, and they are stored directly with the z rule (for a cell whose i and j are
+// interior, GhostEmit writes exactly that one ghost).  The planes i = 0 and nx - 1 hold the
+// slowest rows, so their blocks are scheduled first.
 __device__ __forceinline__ float v4_update(float uc, float bv, float zm, float zp, float ym, float yp, float xm,
-                                           float xp, int k, int nz, const RelaxCoefD<float> &c) {
+                                           float xp, int i, int j, int k, int nx, int ny, int nz, bool face_row,
+                                           const RelaxCoefD<float> &c) {
   const float res = relax_res<float>(uc, bv, zm, zp, ym, yp, xm, xp, c);
   float dg = c.ld;
+  if (face_row) {
+    if (i == nx - 1) dg += c.xp;
+    if (i == 0) dg += c.xn;
+    if (j == ny - 1) dg += c.yp;
+    if (j == 0) dg += c.yn;
+  }
   if (k == nz - 1) dg += c.zp;
   if (k == 0) dg += c.zn;
   return uc + c.omega * res / dg;
@@ -84,14 +94,12 @@ __global__ void __launch_bounds__(256, 6) k_relax_color_v4(float *__restrict__ u
   const int lane = threadIdx.x;
   const int k4 = (blockIdx.x * 32 + lane) * 4;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z * blockDim.z + threadIdx.z;
+  // block row 0 takes the last plane pair, the others shift by one: both face planes run first
+  const int bz = blockIdx.z == 0 ? gridDim.z - 1 : blockIdx.z - 1;
+  const int i = bz * blockDim.z + threadIdx.z;
   if (i >= nx || j >= ny) return;  // whole warps (one row each)
   const int par = (i + j + color) & 1;
-  if (i == 0 || i == nx - 1 || j == 0 || j == ny - 1) {
-    for (int q = 0; q < 2; q++)
-      color_cell<float, int>(u, b, xs, ys, i, j, k4 + par + 2 * q, nx, ny, nz, c, nullptr, true, ge);
-    return;
-  }
+  const bool face_row = i == 0 || i == nx - 1 || j == 0 || j == ny - 1;
   const int base = i * xs + j * ys + k4;
   const float4 U = *reinterpret_cast<const float4 *>(u + base);
   const float4 B = *reinterpret_cast<const float4 *>(b + base);
@@ -113,16 +121,31 @@ __global__ void __launch_bounds__(256, 6) k_relax_color_v4(float *__restrict__ u
   float v0, v1;
   if (par == 0) {
     k0 = k4, k1 = k4 + 2;
-    out.x = v0 = v4_update(U.x, B.x, left, U.y, YM.x, YP.x, XM.x, XP.x, k0, nz, c);
-    out.z = v1 = v4_update(U.z, B.z, U.y, U.w, YM.z, YP.z, XM.z, XP.z, k1, nz, c);
+    out.x = v0 = v4_update(U.x, B.x, left, U.y, YM.x, YP.x, XM.x, XP.x, i, j, k0, nx, ny, nz, face_row, c);
+    out.z = v1 = v4_update(U.z, B.z, U.y, U.w, YM.z, YP.z, XM.z, XP.z, i, j, k1, nx, ny, nz, face_row, c);
   } else {
     k0 = k4 + 1, k1 = k4 + 3;
-    out.y = v0 = v4_update(U.y, B.y, U.x, U.z, YM.y, YP.y, XM.y, XP.y, k0, nz, c);
-    out.w = v1 = v4_update(U.w, B.w, U.z, right, YM.w, YP.w, XM.w, XP.w, k1, nz, c);
+    out.y = v0 = v4_update(U.y, B.y, U.x, U.z, YM.y, YP.y, XM.y, XP.y, i, j, k0, nx, ny, nz, face_row, c);
+    out.w = v1 = v4_update(U.w, B.w, U.z, right, YM.w, YP.w, XM.w, XP.w, i, j, k1, nx, ny, nz, face_row, c);
   }
   *reinterpret_cast<float4 *>(u + base) = out;
-  if (k0 == 0) ge.emit(i, j, k0, v0);
-  if (k1 == nz - 1) ge.emit(i, j, k1, v1);
+  if (face_row) {
+    ge.emit(i, j, k0, v0);
+    ge.emit(i, j, k1, v1);
+    return;
+  }
+  // z-face ghosts of an interior row: a Dirichlet/Neumann ghost's source is the adjacent cell, a
+  // periodic ghost's the cell on the opposite face
+  const int row = base - k4;
+  const int tn = ge.bc.type[FZ_NEG], tp = ge.bc.type[FZ_POS];
+  if (k0 == 0) {
+    if (tn == OCU_BC_DIRICHELET || tn == OCU_BC_NEUMANN) u[row - 1] = ge.template rule<FZ_NEG>(v0, ge.hz);
+    if (tp == OCU_BC_PERIODIC) u[row + nz] = ge.template rule<FZ_POS>(v0, ge.hz);
+  }
+  if (k1 == nz - 1) {
+    if (tp == OCU_BC_DIRICHELET || tp == OCU_BC_NEUMANN) u[row + nz] = ge.template rule<FZ_POS>(v1, ge.hz);
+    if (tn == OCU_BC_PERIODIC) u[row - 1] = ge.template rule<FZ_NEG>(v1, ge.hz);
+  }
 }
 
 template <typename T>
