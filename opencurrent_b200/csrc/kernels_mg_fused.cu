@@ -54,8 +54,11 @@ __global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, con
   pdl_entry();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int i = blockIdx.z * blockDim.z + threadIdx.z;
-  const bool edge_block = color_edge_block(blockIdx.x, blockIdx.y, blockIdx.z, nx, ny, nz);
+  // block row 0 takes the last plane block: the blocks of both face planes (all edge blocks,
+  // the slowest) run first
+  const int bz = blockIdx.z == 0 ? gridDim.z - 1 : blockIdx.z - 1;
+  const int i = bz * blockDim.z + threadIdx.z;
+  const bool edge_block = color_edge_block(blockIdx.x, blockIdx.y, bz, nx, ny, nz);
   if (i >= nx || j >= ny || t >= nz / 2) return;
   color_cell<T, I>(u, b, xs, ys, i, j, 2 * t + ((i + j + color) & 1), nx, ny, nz, c, diag, edge_block, ge);
 }
@@ -252,33 +255,23 @@ __global__ void __launch_bounds__(256, 4) k_prolong_emit(const T *__restrict__ u
 // a coarse row and writes their 16 children as four float4 fine-row segments (fine k = 4m..4m+3).
 // The nine coarse rows (ic+-1, jc+-1) are read as float2 at k = 2m, 2m+1, with k = 2m-1 and 2m+2
 // from the adjacent lanes.  Each child uses the same operand order as prolong_cell (including
-// the corner weight of the (-1,0,0) child).  Rows whose children touch a j or i face take
-// prolong_cell; z-face children write their ghosts.  cnz must be a multiple of 64.
+// the corner weight of the (-1,0,0) child).  Coarse rows whose children touch a j or i face
+// write every ghost of their children (GhostEmit); the others only have z-face ghosts, stored
+// with the z rule.  cnz must be a multiple of 64.
 __device__ __forceinline__ float prolong_child(float f, float c000, float X, float Y, float Z, float XY, float XZ,
                                                float YZ, float XYZ) {
   const float w1 = 0.421875f, w2 = 0.140625f, w3 = 0.046875f, w4 = 0.015625f;
   return f + w1 * c000 + w2 * (X + Y + Z) + w3 * (XY + XZ + YZ) + w4 * XYZ;
 }
 
-// Out-of-line paths of k_prolong_v4 (rare: face rows and the z-face ghosts), kept out of the
-// main body so that its register budget holds the coarse window.
-__device__ __noinline__ void prolong_face_pair(const float *__restrict__ uc, int cx, int cy, float *__restrict__ uf,
-                                               int fxs, int fys, int ic, int jc, int kc0, const GhostEmit<float> *ge) {
-  for (int q = 0; q < 2; q++) {
-    const int kc = kc0 + q;
-    const int tc = ic * cx + jc * cy + kc;
-    const int f = (2 * ic + 1) * fxs + (2 * jc + 1) * fys + (2 * kc + 1);
-    prolong_cell<float, true, int>(uc, tc, cx, cy, uf, f, fxs, fys, ic, jc, kc, ge);
-  }
-}
-
-// ghosts of the four fine cells (2ic+1-dx, 2jc+1-dy, k) just written by this thread
-__device__ __noinline__ void prolong_zghosts(const GhostEmit<float> *ge, const float *uf, int fxs, int fys, int ic,
-                                             int jc, int k) {
+// Ghosts of the 16 fine cells a thread of a face row wrote (re-read from u): every ghost rule,
+// out of line so that the main body keeps its register budget.
+__device__ __noinline__ void prolong_row_ghosts(const GhostEmit<float> *ge, const float *uf, int fxs, int fys, int ic,
+                                                int jc, int k0) {
   for (int dx = 0; dx < 2; dx++)
     for (int dy = 0; dy < 2; dy++) {
       const int fi = 2 * ic + 1 - dx, fj = 2 * jc + 1 - dy;
-      ge->emit(fi, fj, k, uf[fi * fxs + fj * fys + k]);
+      for (int q = 0; q < 4; q++) ge->emit(fi, fj, k0 + q, uf[fi * fxs + fj * fys + k0 + q]);
     }
 }
 
@@ -289,13 +282,13 @@ __global__ void __launch_bounds__(256, 4) k_prolong_v4(const float *__restrict__
   const int lane = threadIdx.x;
   const int m = blockIdx.x * 32 + lane;
   const int jc = blockIdx.y * blockDim.y + threadIdx.y;
-  const int ic = blockIdx.z * blockDim.z + threadIdx.z;
+  // block row 0 takes the last coarse plane pair: both face planes (the slowest rows) run first
+  const int bz = blockIdx.z == 0 ? gridDim.z - 1 : blockIdx.z - 1;
+  const int ic = bz * blockDim.z + threadIdx.z;
   if (ic >= cnx || jc >= cny) return;  // whole warps (one coarse row each)
-  if (ic == 0 || ic == cnx - 1 || jc == 0 || jc == cny - 1) {
-    prolong_face_pair(uc, cx, cy, uf, fxs, fys, ic, jc, 2 * m, &ge);
-    return;
-  }
-  // coarse rows of the plane ic + di as c[dj+1][q], q = 0..3 for coarse k = 2m-1 .. 2m+2
+  const bool face = ic == 0 || ic == cnx - 1 || jc == 0 || jc == cny - 1;
+  // coarse rows of the plane ic + di as c[dj+1][q], q = 0..3 for coarse k = 2m-1 .. 2m+2 (ghost
+  // rows and planes included)
   auto load_plane = [&](int di, float (&c)[3][4]) {
 #pragma unroll
     for (int dj = -1; dj <= 1; dj++) {
@@ -314,6 +307,7 @@ __global__ void __launch_bounds__(256, 4) k_prolong_v4(const float *__restrict__
   float c0[3][4], cs[3][4];
   load_plane(0, c0);
   float cppp[2];  // corner weight of the (-x, +y, +z) children: coarse (ic+1, jc+1, kc+1)
+  const int tn = ge.bc.type[FZ_NEG], tp = ge.bc.type[FZ_POS], fnz = 2 * cnz;
 #pragma unroll
   for (int dx = 0; dx < 2; dx++) {  // dx = 0: fine row 2ic+1 (+x side); dx = 1: fine row 2ic (-x side)
     const int fi = 2 * ic + 1 - dx;
@@ -340,11 +334,21 @@ __global__ void __launch_bounds__(256, 4) k_prolong_v4(const float *__restrict__
                                  c0[sy][sz], XYZ);
         }
       }
-      const int fj = 2 * jc + 1 - dy;
-      *reinterpret_cast<float4 *>(uf + fi * fxs + fj * fys + 4 * m) = make_float4(out[0], out[1], out[2], out[3]);
+      const int fr = fi * fxs + (2 * jc + 1 - dy) * fys;  // fine row, k = 0
+      *reinterpret_cast<float4 *>(uf + fr + 4 * m) = make_float4(out[0], out[1], out[2], out[3]);
+      if (!face) {  // z-face ghosts of an interior fine row (GhostEmit writes exactly these there)
+        if (m == 0) {
+          if (tn == OCU_BC_DIRICHELET || tn == OCU_BC_NEUMANN) uf[fr - 1] = ge.template rule<FZ_NEG>(out[0], ge.hz);
+          if (tp == OCU_BC_PERIODIC) uf[fr + fnz] = ge.template rule<FZ_POS>(out[0], ge.hz);
+        }
+        if (4 * m + 3 == fnz - 1) {
+          if (tp == OCU_BC_DIRICHELET || tp == OCU_BC_NEUMANN) uf[fr + fnz] = ge.template rule<FZ_POS>(out[3], ge.hz);
+          if (tn == OCU_BC_PERIODIC) uf[fr - 1] = ge.template rule<FZ_NEG>(out[3], ge.hz);
+        }
+      }
     }
   }
-  if (m == 0 || 4 * m + 3 == 2 * cnz - 1) prolong_zghosts(&ge, uf, fxs, fys, ic, jc, m == 0 ? 0 : 4 * m + 3);
+  if (face) prolong_row_ghosts(&ge, uf, fxs, fys, ic, jc, 4 * m);
 }
 
 template <typename T>
