@@ -42,6 +42,10 @@ bool pdl_enabled() {
   return on;
 }
 
+static thread_local bool g_pdl_suppressed = false;
+bool pdl_suppressed() { return g_pdl_suppressed; }
+void set_pdl_suppressed(bool on) { g_pdl_suppressed = on; }
+
 ocu_status check_launch(const char *what) {
   count_launch();
   return check_cuda(cudaGetLastError(), what);

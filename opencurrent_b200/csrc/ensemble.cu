@@ -297,7 +297,11 @@ struct Ensemble : EnsBase {
     OCU_TRY(check_cuda(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture"));
     set_capturing(true);
     const unsigned long long n0 = launch_count_captured();
-    ocu_status st = enqueue();
+    ocu_status st;
+    {
+      PdlSuppress no_pdl;  // the classes run concurrently on their own streams
+      st = enqueue();
+    }
     *kernels = (int)(launch_count_captured() - n0);
     set_capturing(false);
     cudaGraph_t g = nullptr;

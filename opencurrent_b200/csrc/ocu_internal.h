@@ -38,6 +38,15 @@ const char *last_error_text();
 // launch_dependents that follows lets the successor's blocks be scheduled early.  A kernel
 // launched without the attribute passes the wait at once.  OCU_B200_PDL=0 turns the attribute off.
 bool pdl_enabled();
+// Launches on several concurrent streams (ensemble classes) go without the attribute: a
+// successor's early-scheduled blocks would hold SM slots the other streams' kernels could use.
+bool pdl_suppressed();
+void set_pdl_suppressed(bool on);
+struct PdlSuppress {
+  bool prev;
+  PdlSuppress() : prev(pdl_suppressed()) { set_pdl_suppressed(true); }
+  ~PdlSuppress() { set_pdl_suppressed(prev); }
+};
 
 template <typename... KArgs, typename... Args>
 inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
@@ -51,7 +60,7 @@ inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t s
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   attr[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = attr;
-  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  cfg.numAttrs = (pdl_enabled() && !pdl_suppressed()) ? 1 : 0;
   cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
