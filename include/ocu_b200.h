@@ -169,6 +169,9 @@ typedef struct ocu_mg_params {
                                     (prolongation + nu2 iterations) of a V-cycle as one launch
                                     each (same results; nu1, nu2 <= 2); <= 0 = off (the
                                     default) */
+  int tail_ctas;                 /* CTAs (2..8) of the thread-block cluster that runs the tail
+                                    kernel, its phases spread over them; 0 or 1 = one CTA
+                                    (the default) */
 } ocu_mg_params;
 
 typedef struct ocu_mg_stats {

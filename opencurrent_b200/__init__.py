@@ -214,6 +214,7 @@ class _MGBase:
         self.tail_cells = 0
         self.sweep_cells = 0
         self.leg_cells = 0
+        self.tail_ctas = 0
         self._h = None
         self._rhs = None
 
@@ -229,6 +230,7 @@ class _MGBase:
         p.tail_cells = int(self.tail_cells)
         p.sweep_cells = int(self.sweep_cells)
         p.leg_cells = int(self.leg_cells)
+        p.tail_ctas = int(self.tail_ctas)
         return p
 
     def initialize_storage(self, nx, ny, nz, hx, hy, hz, rhs):

@@ -220,6 +220,9 @@ ocu_status launch_fold_rows(const T *rows, long long nrows, bool is_max, void *s
 template <typename T>
 ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s);
 // The same schedule for `members` grids at once, one CTA per member.
+// The tail over the CTAs of one cluster (2..8 CTAs; every tail level with fused ghost writes).
+template <typename T>
+ocu_status launch_coarse_tail_cluster(const TailParams<T> &P, int ctas, cudaStream_t s);
 template <typename T>
 ocu_status launch_coarse_tail_batch(const TailParams<T> &P, const TailBatch &tb, int members, cudaStream_t s);
 

@@ -520,6 +520,11 @@ ocu_status MGCore<T>::cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool
     bo[l] = b0(l);
   }
   fill_tail_params(P, s, nu1, nu2, coarse_iters, symmetric, uo.data(), bo.data());
+  if (tail_ctas >= 2) {  // the cluster form needs fused ghost writes on every tail level
+    bool all_emit = true;
+    for (int l = s; l <= coarse; l++) all_emit = all_emit && emit_ok(l);
+    if (all_emit) return launch_coarse_tail_cluster<T>(P, tail_ctas, stream);
+  }
   return launch_coarse_tail<T>(P, stream);
 }
 
@@ -1017,6 +1022,7 @@ ocu_status MGSolver::apply_knobs() {
   if (cf.sweep_cells > 0 && cf.num_levels > 0) OCU_TRY(cf.ensure_sweep_buffers());
   if (cd.sweep_cells > 0 && cd.num_levels > 0) OCU_TRY(cd.ensure_sweep_buffers());
   cf.leg_cells = cd.leg_cells = prm.leg_cells <= 0 ? kDefaultLegCells : prm.leg_cells;
+  cf.tail_ctas = cd.tail_ctas = prm.tail_ctas <= 0 ? kDefaultTailCtas : (prm.tail_ctas > 8 ? 8 : prm.tail_ctas);
   if (cf.leg_cells > 0 && cf.num_levels > 0) OCU_TRY(cf.ensure_leg_buffers());
   if (cd.leg_cells > 0 && cd.num_levels > 0) OCU_TRY(cd.ensure_leg_buffers());
   return OCU_OK;

@@ -34,6 +34,12 @@ constexpr int kDefaultSweepCells = 0;
 // launches (98 / 108 against 96 / 113 us from 32^3): the redundant halo work (about 7 updates
 // per cell) costs what the saved launches do.
 constexpr long long kDefaultLegCells = 0;
+// CTAs of the thread-block cluster that runs the tail kernel (1 = a single CTA).  One by
+// default: with the tail phases spread over a cluster (global memory, cluster barriers) a
+// 256^3 FP32 V-cycle takes 488 / 517 us with the tail at 4096 / 32768 cells against 476 us with
+// the per-operation launches down to the 4^3 level (FP64: 796 / 828 against 775 us) -- a phase
+// costs about what a launch with programmatic dependencies does.
+constexpr int kDefaultTailCtas = 1;
 double mg_optimal_omega(double fx, double fy, double fz);
 
 // The virtual level operations of Sol_MultigridPressure3DBase (sol_mgpressure3d.h:76-80).
@@ -87,6 +93,7 @@ struct MGCore : CoreOps {
   int sweep_cells = kDefaultSweepCells;  // levels with at least this many cells use the two-colour pass
   long long leg_cells = kDefaultLegCells;  // levels below 0 with at most this many cells run one-launch legs
   std::vector<ocu_grid *> grids_uleg;      // their second u buffer
+  int tail_ctas = kDefaultTailCtas;        // CTAs of the cluster that runs the tail kernel
   // two-colour pass: per level a second u buffer (ping-pong) and the TMA maps of u, u2 and b
   std::vector<ocu_grid *> grids_u2;
   std::vector<SweepTmap> tm_u, tm_u2, tm_b;
