@@ -405,7 +405,11 @@ def run_differentiable(torch, ocu, n=96, steps=32, every=8, directions=8):
         ch.interior(lam, "t").copy_(d)
         return loss, ch.backward(lam)
 
-    ch32, in32, t32 = setup(ocu.F32, 1e-5)
+    # projection tolerance (L-infinity of the pressure residual): 3e-5 is the tightest this FP32
+    # flow reaches; at 1e-5 every projection stops at max_iter and retries from zero (2 x 16
+    # cycles, 4.4x the chain's time) for the same gradient (9.1e-8 against 9.6e-8 relative to FP64)
+    proj_tol32 = 3e-5
+    ch32, in32, t32 = setup(ocu.F32, proj_tol32)
     loss_grad(ch32, in32, t32)  # warm-up (records the graphs)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -433,7 +437,7 @@ def run_differentiable(torch, ocu, n=96, steps=32, every=8, directions=8):
         fd = (lp - lm) / (2 * eps)
         ad = sum(float((g * d).sum()) for g, d in zip(g64, dirs))
         worst = max(worst, abs(fd - ad) / max(abs(fd), 1e-300))
-    return {"adjoint_96cube_32steps_fp32_ms": round(ms, 2),
+    return {"adjoint_96cube_32steps_fp32_ms": round(ms, 2), "adjoint_proj_tol_fp32": proj_tol32,
             "adjoint_fd_max_rel_err_fp64": float(f"{worst:.3e}"),
             "adjoint_fp32_vs_fp64_grad_rel_l2": float(f"{(num / den) ** 0.5:.3e}")}
 
