@@ -75,11 +75,11 @@ __global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, con
 // ghosts exist, and they are stored directly with the z rule (for a cell whose i and j are
 // interior, GhostEmit writes exactly that one ghost).  The planes i = 0 and nx - 1 hold the
 // slowest rows, so their blocks are scheduled first.
-__device__ __forceinline__ float v4_update(float uc, float bv, float zm, float zp, float ym, float yp, float xm,
-                                           float xp, int i, int j, int k, int nx, int ny, int nz, bool face_row,
-                                           const RelaxCoefD<float> &c) {
-  const float res = relax_res<float>(uc, bv, zm, zp, ym, yp, xm, xp, c);
-  float dg = c.ld;
+template <typename T>
+__device__ __forceinline__ T v4_update(T uc, T bv, T zm, T zp, T ym, T yp, T xm, T xp, int i, int j, int k, int nx,
+                                       int ny, int nz, bool face_row, const RelaxCoefD<T> &c) {
+  const T res = relax_res<T>(uc, bv, zm, zp, ym, yp, xm, xp, c);
+  T dg = c.ld;
   if (face_row) {
     if (i == nx - 1) dg += c.xp;
     if (i == 0) dg += c.xn;
@@ -125,12 +125,12 @@ __global__ void __launch_bounds__(256, 6) k_relax_color_v4(float *__restrict__ u
   float v0, v1;
   if (par == 0) {
     k0 = k4, k1 = k4 + 2;
-    out.x = v0 = v4_update(U.x, B.x, left, U.y, YM.x, YP.x, XM.x, XP.x, i, j, k0, nx, ny, nz, face_row, c);
-    out.z = v1 = v4_update(U.z, B.z, U.y, U.w, YM.z, YP.z, XM.z, XP.z, i, j, k1, nx, ny, nz, face_row, c);
+    out.x = v0 = v4_update<float>(U.x, B.x, left, U.y, YM.x, YP.x, XM.x, XP.x, i, j, k0, nx, ny, nz, face_row, c);
+    out.z = v1 = v4_update<float>(U.z, B.z, U.y, U.w, YM.z, YP.z, XM.z, XP.z, i, j, k1, nx, ny, nz, face_row, c);
   } else {
     k0 = k4 + 1, k1 = k4 + 3;
-    out.y = v0 = v4_update(U.y, B.y, U.x, U.z, YM.y, YP.y, XM.y, XP.y, i, j, k0, nx, ny, nz, face_row, c);
-    out.w = v1 = v4_update(U.w, B.w, U.z, right, YM.w, YP.w, XM.w, XP.w, i, j, k1, nx, ny, nz, face_row, c);
+    out.y = v0 = v4_update<float>(U.y, B.y, U.x, U.z, YM.y, YP.y, XM.y, XP.y, i, j, k0, nx, ny, nz, face_row, c);
+    out.w = v1 = v4_update<float>(U.w, B.w, U.z, right, YM.w, YP.w, XM.w, XP.w, i, j, k1, nx, ny, nz, face_row, c);
   }
   *reinterpret_cast<float4 *>(u + base) = out;
   if (face_row) {
@@ -259,20 +259,21 @@ __global__ void __launch_bounds__(256, 4) k_prolong_emit(const T *__restrict__ u
 // the corner weight of the (-1,0,0) child).  Coarse rows whose children touch a j or i face
 // write every ghost of their children (GhostEmit); the others only have z-face ghosts, stored
 // with the z rule.  cnz must be a multiple of 64.
-__device__ __forceinline__ float prolong_child(float f, float c000, float X, float Y, float Z, float XY, float XZ,
-                                               float YZ, float XYZ) {
-  const float w1 = 0.421875f, w2 = 0.140625f, w3 = 0.046875f, w4 = 0.015625f;
+template <typename T>
+__device__ __forceinline__ T prolong_child(T f, T c000, T X, T Y, T Z, T XY, T XZ, T YZ, T XYZ) {
+  const T w1 = (T)0.421875, w2 = (T)0.140625, w3 = (T)0.046875, w4 = (T)0.015625;
   return f + w1 * c000 + w2 * (X + Y + Z) + w3 * (XY + XZ + YZ) + w4 * XYZ;
 }
 
 // Ghosts of the 16 fine cells a thread of a face row wrote (re-read from u): every ghost rule,
 // out of line so that the main body keeps its register budget.
-__device__ __noinline__ void prolong_row_ghosts(const GhostEmit<float> *ge, const float *uf, int fxs, int fys, int ic,
-                                                int jc, int k0) {
+template <typename T, int KN>
+__device__ __noinline__ void prolong_row_ghosts(const GhostEmit<T> *ge, const T *uf, int fxs, int fys, int ic, int jc,
+                                                int k0) {
   for (int dx = 0; dx < 2; dx++)
     for (int dy = 0; dy < 2; dy++) {
       const int fi = 2 * ic + 1 - dx, fj = 2 * jc + 1 - dy;
-      for (int q = 0; q < 4; q++) ge->emit(fi, fj, k0 + q, uf[fi * fxs + fj * fys + k0 + q]);
+      for (int q = 0; q < KN; q++) ge->emit(fi, fj, k0 + q, uf[fi * fxs + fj * fys + k0 + q]);
     }
 }
 
@@ -331,7 +332,7 @@ __global__ void __launch_bounds__(256, 4) k_prolong_v4(const float *__restrict__
         for (int dz = 0; dz < 2; dz++) {  // dz = 0: fine k = 2kc+1 (+z side); dz = 1: 2kc (-z side)
           const int cq = q + 1, sz = dz ? q : q + 2, o = 2 * q + (dz ? 0 : 1);
           const float XYZ = (dx == 1 && dy == 0 && dz == 0) ? cppp[q] : cs[sy][sz];
-          out[o] = prolong_child((&F[dy].x)[o], c0[1][cq], cs[1][cq], c0[sy][cq], c0[1][sz], cs[sy][cq], cs[1][sz],
+          out[o] = prolong_child<float>((&F[dy].x)[o], c0[1][cq], cs[1][cq], c0[sy][cq], c0[1][sz], cs[sy][cq], cs[1][sz],
                                  c0[sy][sz], XYZ);
         }
       }
@@ -349,7 +350,78 @@ __global__ void __launch_bounds__(256, 4) k_prolong_v4(const float *__restrict__
       }
     }
   }
-  if (face) prolong_row_ghosts(&ge, uf, fxs, fys, ic, jc, 4 * m);
+  if (face) prolong_row_ghosts<float, 4>(&ge, uf, fxs, fys, ic, jc, 4 * m);
+}
+
+// FP64 prolongation on double2 fine rows: a lane owns one coarse cell of a row (its 8 children
+// are four double2 segments, fine k = 2kc, 2kc+1); coarse rows around it are scalar loads with
+// the row neighbours from the adjacent lanes; same child sums, ghost writes and block order as
+// k_prolong_v4.  cnz must be a multiple of 32.
+__global__ void __launch_bounds__(256, 4) k_prolong_v2d(const double *__restrict__ uc, int cx, int cy, int cnx,
+                                                        int cny, int cnz, double *__restrict__ uf, int fxs, int fys,
+                                                        const __grid_constant__ GhostEmit<double> ge) {
+  pdl_entry();
+  const int lane = threadIdx.x;
+  const int kc = blockIdx.x * 32 + lane;
+  const int jc = blockIdx.y * blockDim.y + threadIdx.y;
+  const int bz = blockIdx.z == 0 ? gridDim.z - 1 : blockIdx.z - 1;  // face planes first
+  const int ic = bz * blockDim.z + threadIdx.z;
+  if (ic >= cnx || jc >= cny) return;  // whole warps (one coarse row each)
+  const bool face = ic == 0 || ic == cnx - 1 || jc == 0 || jc == cny - 1;
+  // coarse rows of the plane ic + di as c[dj+1][q], q = 0..2 for coarse k = kc-1 .. kc+1
+  auto load_plane = [&](int di, double (&c)[3][3]) {
+#pragma unroll
+    for (int dj = -1; dj <= 1; dj++) {
+      const int base = (ic + di) * cx + (jc + dj) * cy + kc;
+      const double v = uc[base];
+      const double E = uc[base + (lane == 31 ? 1 : -1)];
+      double l = __shfl_up_sync(0xffffffffu, v, 1), r = __shfl_down_sync(0xffffffffu, v, 1);
+      if (lane == 0) l = E;
+      if (lane == 31) r = E;
+      c[dj + 1][0] = l;
+      c[dj + 1][1] = v;
+      c[dj + 1][2] = r;
+    }
+  };
+  double c0[3][3], cs[3][3];
+  load_plane(0, c0);
+  double cppp = 0;  // corner weight of the (-x, +y, +z) child: coarse (ic+1, jc+1, kc+1)
+  const int tn = ge.bc.type[FZ_NEG], tp = ge.bc.type[FZ_POS], fnz = 2 * cnz;
+#pragma unroll
+  for (int dx = 0; dx < 2; dx++) {  // dx = 0: fine row 2ic+1 (+x side); dx = 1: fine row 2ic (-x side)
+    const int fi = 2 * ic + 1 - dx;
+    double2 F[2];
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+      F[dy] = *reinterpret_cast<const double2 *>(uf + fi * fxs + (2 * jc + 1 - dy) * fys + 2 * kc);
+    load_plane(dx ? -1 : 1, cs);
+    if (dx == 0) cppp = cs[2][2];
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++) {
+      const int sy = dy ? 0 : 2;
+      double out[2];
+#pragma unroll
+      for (int dz = 0; dz < 2; dz++) {  // dz = 0: fine k = 2kc+1 (+z side, .y); dz = 1: 2kc (-z side, .x)
+        const int sz = dz ? 0 : 2, o = dz ? 0 : 1;
+        const double XYZ = (dx == 1 && dy == 0 && dz == 0) ? cppp : cs[sy][sz];
+        out[o] = prolong_child<double>(o ? F[dy].y : F[dy].x, c0[1][1], cs[1][1], c0[sy][1], c0[1][sz], cs[sy][1],
+                                       cs[1][sz], c0[sy][sz], XYZ);
+      }
+      const int fr = fi * fxs + (2 * jc + 1 - dy) * fys;  // fine row, k = 0
+      *reinterpret_cast<double2 *>(uf + fr + 2 * kc) = make_double2(out[0], out[1]);
+      if (!face) {  // z-face ghosts of an interior fine row
+        if (kc == 0) {
+          if (tn == OCU_BC_DIRICHELET || tn == OCU_BC_NEUMANN) uf[fr - 1] = ge.template rule<FZ_NEG>(out[0], ge.hz);
+          if (tp == OCU_BC_PERIODIC) uf[fr + fnz] = ge.template rule<FZ_POS>(out[0], ge.hz);
+        }
+        if (2 * kc + 1 == fnz - 1) {
+          if (tp == OCU_BC_DIRICHELET || tp == OCU_BC_NEUMANN) uf[fr + fnz] = ge.template rule<FZ_POS>(out[1], ge.hz);
+          if (tn == OCU_BC_PERIODIC) uf[fr - 1] = ge.template rule<FZ_NEG>(out[1], ge.hz);
+        }
+      }
+    }
+  }
+  if (face) prolong_row_ghosts<double, 2>(&ge, uf, fxs, fys, ic, jc, 2 * kc);
 }
 
 template <typename T>
@@ -365,6 +437,13 @@ ocu_status launch_prolong_emit(const T *uc, const ocu_layout &Lc, T *uf, const o
                                    (float *)uf, (int)Lf.xstride, (int)Lf.ystride,
                                    *reinterpret_cast<const GhostEmit<float> *>(&ge));
     return check_launch("k_prolong_v4");
+  }
+  if (sizeof(T) == 8 && Lc.nz % 32 == 0 && Lf.allocated < (1LL << 31) && Lf.shift % 2 == 0 &&
+      Lf.ystride % 2 == 0) {
+    dim3 b2(32, 4, 2), g2(Lc.nz / 32, (Lc.ny + 3) / 4, (Lc.nx + 1) / 2);
+    launch_pdl(k_prolong_v2d, g2, b2, 0, s, (const double *)uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny,
+               Lc.nz, (double *)uf, (int)Lf.xstride, (int)Lf.ystride, *reinterpret_cast<const GhostEmit<double> *>(&ge));
+    return check_launch("k_prolong_v2d");
   }
   if (Lf.allocated < (1LL << 31) && Lc.allocated < (1LL << 31))
     launch_pdl(k_prolong_emit<T, int>, grid, block, 0, s, uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
