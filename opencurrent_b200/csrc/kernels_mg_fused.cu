@@ -487,9 +487,18 @@ __device__ __forceinline__ T warp_tree(T v, bool is_max) {
   return v;
 }
 
+template <typename T> struct Vec2T;
+template <> struct Vec2T<float> { using type = float2; };
+template <> struct Vec2T<double> { using type = double2; };
+
+template <typename T>
+__device__ __forceinline__ T residual_pt(T bv, T uc, T zm, T zp, T ym, T yp, T xm, T xp, const ResCoefT<T> &c) {
+  return bv - (c.fzh * (zm + zp) + c.fyh * (ym + yp) + c.fxh * (xm + xp) - c.dg * uc);
+}
+
 // Residual over one fine row per warp (chunks of 64 along k): optional outputs r (T), r as
 // float (the refinement solver's FP32 right-hand side), and per-row norm partials.
-template <typename T>
+template <typename T, bool VEC>
 __global__ void __launch_bounds__(256) k_residual_rows(const T *__restrict__ u, const T *__restrict__ b,
                                                        T *__restrict__ r, float *__restrict__ r32, long long xs,
                                                        long long ys, int nx, int ny, int nz, ResCoefT<T> c,
@@ -502,6 +511,30 @@ __global__ void __launch_bounds__(256) k_residual_rows(const T *__restrict__ u, 
   const bool want2 = rows2 != nullptr, wantinf = rowsinf != nullptr;
   T acc2 = 0, accinf = 0;
   const long long row = (long long)i * xs + (long long)j * ys;
+  if (VEC) {  // nz even, rows 16-byte aligned: a lane's two cells and their neighbours as 2-wide loads
+    using V = typename Vec2T<T>::type;
+    for (int base = 0; base < nz; base += 64) {
+      const int k0 = base + 2 * lane;
+      T e0 = 0, e1 = 0;
+      if (k0 < nz) {
+        const long long id = row + k0;
+        const V U = *reinterpret_cast<const V *>(u + id), B = *reinterpret_cast<const V *>(b + id);
+        const V YM = *reinterpret_cast<const V *>(u + id - ys), YP = *reinterpret_cast<const V *>(u + id + ys);
+        const V XM = *reinterpret_cast<const V *>(u + id - xs), XP = *reinterpret_cast<const V *>(u + id + xs);
+        const T L = u[id - 1], R = u[id + 2];
+        e0 = residual_pt<T>(B.x, U.x, L, U.y, YM.x, YP.x, XM.x, XP.x, c);
+        e1 = residual_pt<T>(B.y, U.y, U.x, R, YM.y, YP.y, XM.y, XP.y, c);
+        if (r) {
+          V o;
+          o.x = e0;
+          o.y = e1;
+          *reinterpret_cast<V *>(r + id) = o;
+        }
+        if (r32) *reinterpret_cast<float2 *>(r32 + id) = make_float2((float)e0, (float)e1);
+      }
+      if (want2 || wantinf) fold_chunk<T>(e0, e1, base, nz, lane, acc2, accinf, want2, wantinf);
+    }
+  } else {
   for (int base = 0; base < nz; base += 64) {
     const int k0 = base + 2 * lane;
     T e0 = 0, e1 = 0;
@@ -516,6 +549,7 @@ __global__ void __launch_bounds__(256) k_residual_rows(const T *__restrict__ u, 
       if (r32) r32[row + k0 + 1] = (float)e1;
     }
     if (want2 || wantinf) fold_chunk<T>(e0, e1, base, nz, lane, acc2, accinf, want2, wantinf);
+  }
   }
   if (want2) {
     const T v = warp_tree<T>(acc2, false);
@@ -592,15 +626,6 @@ __global__ void __launch_bounds__(256) k_residual_restrict(const T *__restrict__
 // and so are their neighbours in the rows j-1 / j+2 and planes i-1 / i+2; the row neighbours
 // k-1 and k+2 are scalar loads of the same lines.  24 load instructions per coarse cell instead
 // of 64; each residual is residual_at's expression on the same operands.
-template <typename T> struct Vec2T;
-template <> struct Vec2T<float> { using type = float2; };
-template <> struct Vec2T<double> { using type = double2; };
-
-template <typename T>
-__device__ __forceinline__ T residual_pt(T bv, T uc, T zm, T zp, T ym, T yp, T xm, T xp, const ResCoefT<T> &c) {
-  return bv - (c.fzh * (zm + zp) + c.fyh * (ym + yp) + c.fxh * (xm + xp) - c.dg * uc);
-}
-
 template <typename T, bool NORM>
 __global__ void __launch_bounds__(256) k_residual_restrict_v2(const T *__restrict__ u, const T *__restrict__ b,
                                                               long long xs, long long ys, int nx, int ny, int nz,
@@ -739,8 +764,13 @@ template <typename T>
 ocu_status launch_residual_rows(const T *u, const T *b, T *r, float *r32, const ocu_layout &L, double h, double fx,
                                 double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s) {
   dim3 block(32, 8), grid(1, (L.ny + 7) / 8, L.nx);
-  launch_pdl(k_residual_rows<T>, grid, block, 0, s, u, b, r, r32, L.xstride, L.ystride, L.nx, L.ny, L.nz,
-                                            res_coef<T>(h, fx, fy, fz), rows2, rowsinf);
+  // the 2-wide path needs even rows starting on 2-element boundaries (r32 shares the layout)
+  if (L.nz % 2 == 0 && L.shift % 2 == 0 && L.xstride % 2 == 0 && L.ystride % 2 == 0)
+    launch_pdl(k_residual_rows<T, true>, grid, block, 0, s, u, b, r, r32, L.xstride, L.ystride, L.nx, L.ny, L.nz,
+               res_coef<T>(h, fx, fy, fz), rows2, rowsinf);
+  else
+    launch_pdl(k_residual_rows<T, false>, grid, block, 0, s, u, b, r, r32, L.xstride, L.ystride, L.nx, L.ny, L.nz,
+               res_coef<T>(h, fx, fy, fz), rows2, rowsinf);
   return check_launch("k_residual_rows");
 }
 
