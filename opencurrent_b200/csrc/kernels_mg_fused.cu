@@ -307,16 +307,20 @@ __global__ void __launch_bounds__(256, 4) k_prolong_v4(const float *__restrict__
     }
   };
   float c0[3][4], cs[3][4];
+  // all 16 fine values first: loads placed after a store to uf could not be issued before it
+  float4 FF[2][2];
+#pragma unroll
+  for (int dx = 0; dx < 2; dx++)
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+      FF[dx][dy] = *reinterpret_cast<const float4 *>(uf + (2 * ic + 1 - dx) * fxs + (2 * jc + 1 - dy) * fys + 4 * m);
   load_plane(0, c0);
   float cppp[2];  // corner weight of the (-x, +y, +z) children: coarse (ic+1, jc+1, kc+1)
   const int tn = ge.bc.type[FZ_NEG], tp = ge.bc.type[FZ_POS], fnz = 2 * cnz;
 #pragma unroll
   for (int dx = 0; dx < 2; dx++) {  // dx = 0: fine row 2ic+1 (+x side); dx = 1: fine row 2ic (-x side)
     const int fi = 2 * ic + 1 - dx;
-    float4 F[2];
-#pragma unroll
-    for (int dy = 0; dy < 2; dy++)
-      F[dy] = *reinterpret_cast<const float4 *>(uf + fi * fxs + (2 * jc + 1 - dy) * fys + 4 * m);
+    const float4 *F = FF[dx];
     load_plane(dx ? -1 : 1, cs);
     if (dx == 0) {
       cppp[0] = cs[2][2];
@@ -384,16 +388,19 @@ __global__ void __launch_bounds__(256, 4) k_prolong_v2d(const double *__restrict
     }
   };
   double c0[3][3], cs[3][3];
+  double2 FF[2][2];  // all 8 fine values before the first store
+#pragma unroll
+  for (int dx = 0; dx < 2; dx++)
+#pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+      FF[dx][dy] = *reinterpret_cast<const double2 *>(uf + (2 * ic + 1 - dx) * fxs + (2 * jc + 1 - dy) * fys + 2 * kc);
   load_plane(0, c0);
   double cppp = 0;  // corner weight of the (-x, +y, +z) child: coarse (ic+1, jc+1, kc+1)
   const int tn = ge.bc.type[FZ_NEG], tp = ge.bc.type[FZ_POS], fnz = 2 * cnz;
 #pragma unroll
   for (int dx = 0; dx < 2; dx++) {  // dx = 0: fine row 2ic+1 (+x side); dx = 1: fine row 2ic (-x side)
     const int fi = 2 * ic + 1 - dx;
-    double2 F[2];
-#pragma unroll
-    for (int dy = 0; dy < 2; dy++)
-      F[dy] = *reinterpret_cast<const double2 *>(uf + fi * fxs + (2 * jc + 1 - dy) * fys + 2 * kc);
+    const double2 *F = FF[dx];
     load_plane(dx ? -1 : 1, cs);
     if (dx == 0) cppp = cs[2][2];
 #pragma unroll
@@ -569,8 +576,15 @@ __global__ void __launch_bounds__(256) k_residual_restrict(const T *__restrict__
                                                            long long xs, long long ys, int nx, int ny, int nz,
                                                            ResCoefT<T> c, T *__restrict__ bc_, long long bxs,
                                                            long long bys, int cnx, int cny, int cnz,
-                                                           T *__restrict__ rows2, T *__restrict__ rowsinf) {
+                                                           T *__restrict__ rows2, T *__restrict__ rowsinf, T *__restrict__ zero_u,
+    long long zero_n) {
   pdl_entry();
+  if (zero_u) {  // the coarser level's clear (its whole buffer, as a memset), nothing here reads it
+    const long long nthreads = (long long)gridDim.x * gridDim.y * gridDim.z * blockDim.x * blockDim.y;
+    const long long tid = ((long long)(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) *
+                              (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
+    for (long long q = tid; q < zero_n; q += nthreads) zero_u[q] = (T)0;
+  }
   const int lane = threadIdx.x;
   const int jc = blockIdx.y * blockDim.y + threadIdx.y;
   const int ic = blockIdx.z;
@@ -631,9 +645,16 @@ __global__ void __launch_bounds__(256) k_residual_restrict_v2(const T *__restric
                                                               long long xs, long long ys, int nx, int ny, int nz,
                                                               ResCoefT<T> c, T *__restrict__ bc_, long long bxs,
                                                               long long bys, int cnx, int cny, int cnz,
-                                                              T *__restrict__ rows2, T *__restrict__ rowsinf) {
+                                                              T *__restrict__ rows2, T *__restrict__ rowsinf, T *__restrict__ zero_u,
+    long long zero_n) {
   using V = typename Vec2T<T>::type;
   pdl_entry();
+  if (zero_u) {  // the coarser level's clear (its whole buffer, as a memset), nothing here reads it
+    const long long nthreads = (long long)gridDim.x * gridDim.y * gridDim.z * blockDim.x * blockDim.y;
+    const long long tid = ((long long)(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) *
+                              (blockDim.x * blockDim.y) + threadIdx.y * blockDim.x + threadIdx.x;
+    for (long long q = tid; q < zero_n; q += nthreads) zero_u[q] = (T)0;
+  }
   const int lane = threadIdx.x;
   const int jc = blockIdx.y * blockDim.y + threadIdx.y;
   const int ic = blockIdx.z;
@@ -776,27 +797,28 @@ ocu_status launch_residual_rows(const T *u, const T *b, T *r, float *r32, const 
 
 template <typename T>
 ocu_status launch_residual_restrict(const T *u, const T *b, const ocu_layout &Lf, T *bc_, const ocu_layout &Lc,
-                                    double h, double fx, double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s) {
+                                    double h, double fx, double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s,
+                                    T *zero_u, long long zero_n) {
   dim3 block(32, 8), grid(1, (Lc.ny + 7) / 8, Lc.nx);
   const ResCoefT<T> c = res_coef<T>(h, fx, fy, fz);
   if (sizeof(T) == 4 && Lf.shift % 2 == 0 && Lf.xstride % 2 == 0 && Lf.ystride % 2 == 0 && Lf.nz == 2 * Lc.nz) {
     if (rows2 || rowsinf) {
       launch_pdl(k_residual_restrict_v2<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny,
-                 Lf.nz, c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf);
+                 Lf.nz, c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf, zero_u, zero_n);
     } else {
       dim3 gridc((Lc.nz + 31) / 32, (Lc.ny + 7) / 8, Lc.nx);
       launch_pdl(k_residual_restrict_v2<T, false>, gridc, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny,
-                 Lf.nz, c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr);
+                 Lf.nz, c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr, zero_u, zero_n);
     }
     return check_launch("k_residual_restrict_v2");
   }
   if (rows2 || rowsinf) {
     launch_pdl(k_residual_restrict<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz,
-               c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf);
+               c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf, zero_u, zero_n);
   } else {
     dim3 gridc((Lc.nz + 31) / 32, (Lc.ny + 7) / 8, Lc.nx);
     launch_pdl(k_residual_restrict<T, false>, gridc, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz,
-               c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr);
+               c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr, zero_u, zero_n);
   }
   return check_launch("k_residual_restrict");
 }
@@ -1456,7 +1478,7 @@ INST_B(double)
                                               double, double, double, T *, T *, cudaStream_t);                 \
   template ocu_status launch_residual_restrict<T>(const T *, const T *, const ocu_layout &, T *,                \
                                                   const ocu_layout &, double, double, double, double, T *, T *, \
-                                                  cudaStream_t);                                               \
+                                                  cudaStream_t, T *, long long);                               \
   template ocu_status launch_fold_rows<T>(const T *, long long, bool, void *, double *, cudaStream_t);          \
   template ocu_status launch_coarse_tail<T>(const TailParams<T> &, cudaStream_t);                               \
   template ocu_status launch_coarse_tail_cluster<T>(const TailParams<T> &, int, cudaStream_t);                   \

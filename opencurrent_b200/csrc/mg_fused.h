@@ -213,7 +213,8 @@ ocu_status launch_residual_rows(const T *u, const T *b, T *r, float *r32, const 
                                 double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s);
 template <typename T>
 ocu_status launch_residual_restrict(const T *u, const T *b, const ocu_layout &Lf, T *bc_, const ocu_layout &Lc,
-                                    double h, double fx, double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s);
+                                    double h, double fx, double fy, double fz, T *rows2, T *rowsinf, cudaStream_t s,
+                                    T *zero_u = nullptr, long long zero_n = 0);
 template <typename T>
 ocu_status launch_fold_rows(const T *rows, long long nrows, bool is_max, void *scratch, double *result,
                             cudaStream_t s);

@@ -403,6 +403,31 @@ ocu_status MGCore<T>::enqueue_restrict_residuals(int fine, int coarse, bool want
   return OCU_OK;
 }
 
+// clear_level(fine + 1) then the restriction into it.  On the fused path the clear (the whole
+// buffer of the coarser level, the memset it stands for) rides in the restriction kernel: one
+// launch less per level and cycle.
+template <typename T>
+ocu_status MGCore<T>::clear_and_restrict(int fine, bool want_l2, bool want_linf) {
+  const int coarse = fine + 1;
+  if (!fused || store_residuals) {
+    OCU_TRY(clear_level(coarse));
+    return enqueue_restrict_residuals(fine, coarse, want_l2, want_linf);
+  }
+  const bool norms = want_l2 || want_linf;
+  T *rows2 = want_l2 ? (T *)rows : nullptr;
+  T *rowsinf = want_linf ? (T *)rows + rows_stride : nullptr;
+  OCU_TRY(launch_residual_restrict<T>(u0(fine), b0(fine), lay[fine], b0(coarse), lay[coarse], h[fine], fx, fy, fz,
+                                      rows2, rowsinf, stream, static_cast<T *>(grids_u[coarse]->buf),
+                                      lay[coarse].allocated));
+  const long long nrows = (long long)dim[fine][0] * dim[fine][1];
+  if (want_l2) OCU_TRY(launch_fold_rows<T>(rows2, nrows, false, red_scratch, d_norms, stream));
+  if (want_linf) OCU_TRY(launch_fold_rows<T>(rowsinf, nrows, true, red_scratch, d_norms + 1, stream));
+  if (norms)
+    OCU_TRY(check_cuda(cudaMemcpyAsync(h_norms, d_norms, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                       "norm readback"));
+  return OCU_OK;
+}
+
 // The squared-residual sum is folded in T, divided by the cell count in T and square-rooted in
 // T (sol_mgpressure3ddev.cu:263-268).
 template <typename T>
@@ -616,8 +641,7 @@ ocu_status MGSolver::enq_down(CoreOps *c, int a, int b) {
       continue;
     }
     OCU_TRY(c->relax(level, prm.nu1, RO_RED_BLACK));
-    OCU_TRY(c->clear_level(level + 1));
-    OCU_TRY(c->enqueue_restrict_residuals(level, level + 1, false, false));
+    OCU_TRY(c->clear_and_restrict(level, false, false));
   }
   return OCU_OK;
 }
@@ -658,8 +682,7 @@ ocu_status MGSolver::do_fmg_graph(double tolerance, int max_iter, double *rl2, d
   }
   OCU_TRY(run_segment(c, SEG_RAMP, [&]() -> ocu_status {
     for (int level = 0; level < num_levels - 1; level++) {
-      OCU_TRY(c->clear_level(level + 1));
-      OCU_TRY(c->enqueue_restrict_residuals(level, level + 1, false, false));
+      OCU_TRY(c->clear_and_restrict(level, false, false));
     }
     for (int f = num_levels - 1; f >= 1; f--) {
       const int s = ts > f ? ts : f;
@@ -674,8 +697,7 @@ ocu_status MGSolver::do_fmg_graph(double tolerance, int max_iter, double *rl2, d
     num_vcyc++;
     OCU_TRY(run_segment(c, SEG_PRE0 + nv, [&]() -> ocu_status {
       OCU_TRY(c->relax(0, prm.nu1, RO_RED_BLACK));
-      OCU_TRY(c->clear_level(1));
-      return c->enqueue_restrict_residuals(0, 1, wl2, wlinf);
+      return c->clear_and_restrict(0, wl2, wlinf);
     }));
     if (wl2 || wlinf) {
       OCU_TRY(c->finish_norms(0, wl2 ? rl2 : nullptr, wlinf ? rlinf : nullptr));
@@ -716,8 +738,7 @@ ocu_status MGSolver::do_vcycle_graph(double tolerance, int max_iter, double *rl2
   for (int i_cyc = 0; i_cyc < max_iter; i_cyc++) {
     OCU_TRY(run_segment(c, SEG_PRE0 + nv, [&]() -> ocu_status {
       OCU_TRY(c->relax(0, prm.nu1, RO_RED_BLACK));
-      OCU_TRY(c->clear_level(1));
-      return c->enqueue_restrict_residuals(0, 1, wl2, wlinf);
+      return c->clear_and_restrict(0, wl2, wlinf);
     }));
     if (wl2 || wlinf) OCU_TRY(c->finish_norms(0, wl2 ? rl2 : nullptr, wlinf ? rlinf : nullptr));
     if (pick(conv, *rl2, *rlinf) < tolerance) {
@@ -750,8 +771,7 @@ ocu_status MGSolver::do_fmg(double tolerance, int max_iter, double *rl2, double 
     return OCU_OK;
   }
   for (int level = 0; level < num_levels - 1; level++) {
-    OCU_TRY(c->clear_level(level + 1));
-    OCU_TRY(c->enqueue_restrict_residuals(level, level + 1, false, false));
+    OCU_TRY(c->clear_and_restrict(level, false, false));
   }
   for (int fine_level = num_levels - 1; fine_level >= 0; fine_level--) {
     const int level_ncyc = (fine_level == 0) ? max_iter + 1 : 1;
@@ -787,11 +807,10 @@ ocu_status MGSolver::cycle(CoreOps *c, int fine_level, double tolerance, double 
       continue;
     }
     OCU_TRY(c->relax(level, prm.nu1, RO_RED_BLACK));
-    OCU_TRY(c->clear_level(level + 1));
     if (level == 0) {
       double *l2 = (conv & OCU_CONVERGENCE_CALC_L2) ? rl2 : nullptr;
       double *linf = (conv & OCU_CONVERGENCE_CALC_LINF) ? rlinf : nullptr;
-      OCU_TRY(c->enqueue_restrict_residuals(0, 1, l2 != nullptr, linf != nullptr));
+      OCU_TRY(c->clear_and_restrict(0, l2 != nullptr, linf != nullptr));
       if (l2 || linf) OCU_TRY(c->finish_norms(0, l2, linf));
       stats.last_l2 = *rl2;
       stats.last_linf = *rlinf;
@@ -801,7 +820,7 @@ ocu_status MGSolver::cycle(CoreOps *c, int fine_level, double tolerance, double 
         return OCU_OK;
       }
     } else {
-      OCU_TRY(c->enqueue_restrict_residuals(level, level + 1, false, false));
+      OCU_TRY(c->clear_and_restrict(level, false, false));
     }
   }
   OCU_TRY(c->cycle_tail(s, prm.nu1, prm.nu2, coarse_iters(), sym));

@@ -57,6 +57,7 @@ struct CoreOps {
   virtual ocu_status clear_level(int level) = 0;
   // restrict_residuals split at the host wait: enqueue, then finish_norms for the numbers
   virtual ocu_status enqueue_restrict_residuals(int fine, int coarse, bool want_l2, bool want_linf) = 0;
+  virtual ocu_status clear_and_restrict(int fine, bool want_l2, bool want_linf) = 0;
   virtual ocu_status finish_norms(int fine, double *l2, double *linf) = 0;
   // levels tail_start()..L-1 of a V-cycle in one launch
   virtual int tail_start() const = 0;
@@ -111,6 +112,7 @@ struct MGCore : CoreOps {
   ocu_status leg_up(int level, int nu2, int order) override;
   LegLevel<T> leg_level(int level, const T *u_in, T *u_out) const;
   ocu_status enqueue_restrict_residuals(int fine, int coarse, bool want_l2, bool want_linf) override;
+  ocu_status clear_and_restrict(int fine, bool want_l2, bool want_linf) override;
   ocu_status finish_norms(int fine, double *l2, double *linf) override;
   int tail_start() const override;
   ocu_status cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool symmetric) override;
