@@ -138,8 +138,8 @@ ocu_status launch_bc_nocorners_dev(T *origin, const ocu_layout &L, const ocu_bc_
     return fail(OCU_ERR_LAYOUT, "[ERROR] apply_3d_boundary_conditions_level1_nocorners - must have at least 1 ghost point");
   const long long total = 2LL * L.nx * L.ny + 2LL * L.nx * L.nz + 2LL * L.ny * L.nz;
   const unsigned blocks = (unsigned)((total + 255) / 256);
-  launch_pdl(k_bc_nocorners<T>, blocks, 256, 0, s, origin, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(bc),
-                                           (T)hx, (T)hy, (T)hz);
+  launch_pdl(k_bc_nocorners<T>, blocks, 256, 0, s, origin, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(bc), (T)hx,
+             (T)hy, (T)hz);
   return check_launch("k_bc_nocorners");
 }
 
@@ -338,7 +338,7 @@ ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, T a2,
   if (waste / (float)L.allocated > .03f) {
     dim3 grid((L.nz + 127) / 128, L.ny, L.nx);
     launch_pdl(k_lincomb2_3d<T>, grid, 128, 0, s, res + L.shift, a1, g1 + L.shift, a2, g2 + L.shift, L.xstride,
-                                          L.ystride, L.nx, L.ny, L.nz);
+               L.ystride, L.nx, L.ny, L.nz);
     return check_launch("k_lincomb2_3d");
   }
   launch_pdl(k_lincomb2_1d<T>, grid_for(L.allocated, 256), 256, 0, s, res, a1, g1, a2, g2, L.allocated);
@@ -459,7 +459,7 @@ ocu_status launch_reduce(const T *origin, const ocu_layout &L, int op, void *d_s
   T *partial = reinterpret_cast<T *>(reinterpret_cast<char *>(d_scratch) + 64);
   RedOp<T> r{op};
   launch_pdl(k_reduce<T>, (unsigned)blocks, 256, 0, s, origin, L.xstride, L.ystride, L.nx, L.ny, L.nz, r, partial,
-                                               counter, d_result);
+             counter, d_result);
   return check_launch("k_reduce");
 }
 

@@ -162,12 +162,12 @@ ocu_status launch_coarse_relax(T *u, const T *b, const ocu_layout &L, int iterat
   }
   const size_t bytes = 2 * sizeof(T) * (size_t)L.allocated;
   if (bytes <= 48 * 1024) {
-    launch_pdl(k_coarse_relax_smem<T>, 1, 512, bytes, s, u, b, L.shift, L.allocated, L.xstride, L.ystride, L.nx,
-               L.ny, L.nz, iterations, order, c, to_dev(p.bc), (T)hx, (T)hy, (T)hz);
+    launch_pdl(k_coarse_relax_smem<T>, 1, 512, bytes, s, u, b, L.shift, L.allocated, L.xstride, L.ystride, L.nx, L.ny,
+               L.nz, iterations, order, c, to_dev(p.bc), (T)hx, (T)hy, (T)hz);
     return check_launch("k_coarse_relax_smem");
   }
   launch_pdl(k_coarse_relax<T>, 1, 512, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, iterations, order, c,
-                                      to_dev(p.bc), (T)hx, (T)hy, (T)hz);
+             to_dev(p.bc), (T)hx, (T)hy, (T)hz);
   return check_launch("k_coarse_relax");
 }
 
@@ -194,7 +194,7 @@ ocu_status launch_residual(const T *u, const T *b, T *r, const ocu_layout &L, do
   dim3 block(L.nz >= 64 ? 64 : 32, L.nz >= 64 ? 4 : 8);
   dim3 grid((L.nz + block.x - 1) / block.x, (L.ny + block.y - 1) / block.y, L.nx);
   launch_pdl(k_residual<T>, grid, block, 0, s, u, b, r, L.xstride, L.ystride, L.nx, L.ny, L.nz, (T)(fx / (h * h)),
-                                       (T)(fy / (h * h)), (T)(fz / (h * h)), (T)(2 * (fx + fy + fz) / (h * h)));
+             (T)(fy / (h * h)), (T)(fz / (h * h)), (T)(2 * (fx + fy + fz) / (h * h)));
   return check_launch("k_residual");
 }
 
@@ -221,7 +221,7 @@ ocu_status launch_restrict(const T *r, const ocu_layout &Lf, T *bc_, const ocu_l
   dim3 block(Lc.nz >= 32 ? 32 : 16, 8);
   dim3 grid((Lc.nz + block.x - 1) / block.x, (Lc.ny + block.y - 1) / block.y, Lc.nx);
   launch_pdl(k_restrict<T>, grid, block, 0, s, r, Lf.xstride, Lf.ystride, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny,
-                                       Lc.nz);
+             Lc.nz);
   return check_launch("k_restrict");
 }
 

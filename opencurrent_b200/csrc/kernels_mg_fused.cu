@@ -179,11 +179,11 @@ ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const 
   ge.p = u;
   if (launch_color_v4<T>(u, b, L, color, c, ge, diag, s)) return check_launch("k_relax_color_v4");
   if (L.allocated < (1LL << 31))
-    launch_pdl(k_relax_color_emit<T, int>, grid, block, 0, s, u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz, color, c,
-                                                      diag, ge);
+    launch_pdl(k_relax_color_emit<T, int>, grid, block, 0, s, u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz,
+               color, c, diag, ge);
   else
-    launch_pdl(k_relax_color_emit<T, long long>, grid, block, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c,
-                                                            diag, ge);
+    launch_pdl(k_relax_color_emit<T, long long>, grid, block, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color,
+               c, diag, ge);
   return check_launch("k_relax_color_emit");
 }
 
@@ -196,15 +196,18 @@ __device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, I tc, I c
   const int i = 2 * ic + 1, j = 2 * jc + 1, k = 2 * kc + 1;
   // all eight fine values are loaded before the first store: the ghost writes go through
   // another pointer, so loads placed after a store could not be issued until it completed
-  const T f000 = gld<CG>(uf + f), f100 = gld<CG>(uf + f - fxs), f010 = gld<CG>(uf + f - fys), f001 = gld<CG>(uf + f - 1);
-  const T f110 = gld<CG>(uf + f - fxs - fys), f101 = gld<CG>(uf + f - fxs - 1), f011 = gld<CG>(uf + f - fys - 1), f111 = gld<CG>(uf + f - fxs - fys - 1);
+  const T f000 = gld<CG>(uf + f), f100 = gld<CG>(uf + f - fxs), f010 = gld<CG>(uf + f - fys);
+  const T f001 = gld<CG>(uf + f - 1);
+  const T f110 = gld<CG>(uf + f - fxs - fys), f101 = gld<CG>(uf + f - fxs - 1), f011 = gld<CG>(uf + f - fys - 1);
+  const T f111 = gld<CG>(uf + f - fxs - fys - 1);
   const T c000 = gld<CG>(uc + tc);
   const T c0p0 = gld<CG>(uc + tc + cy), c00p = gld<CG>(uc + tc + 1), c0pp = gld<CG>(uc + tc + cy + 1);
   const T c0m0 = gld<CG>(uc + tc - cy), c00m = gld<CG>(uc + tc - 1), c0mm = gld<CG>(uc + tc - cy - 1);
   const T c0mp = gld<CG>(uc + tc - cy + 1), c0pm = gld<CG>(uc + tc + cy - 1);
   T v;
   {  // children on the +x side of the coarse centre (coarse plane x+1)
-    const T cp00 = gld<CG>(uc + tc + cx), cpp0 = gld<CG>(uc + tc + cx + cy), cp0p = gld<CG>(uc + tc + cx + 1), cppp = gld<CG>(uc + tc + cx + cy + 1);
+    const T cp00 = gld<CG>(uc + tc + cx), cpp0 = gld<CG>(uc + tc + cx + cy), cp0p = gld<CG>(uc + tc + cx + 1);
+    const T cppp = gld<CG>(uc + tc + cx + cy + 1);
     const T cpm0 = gld<CG>(uc + tc + cx - cy), cp0m = gld<CG>(uc + tc + cx - 1), cpmm = gld<CG>(uc + tc + cx - cy - 1);
     const T cppm = gld<CG>(uc + tc + cx + cy - 1), cpmp = gld<CG>(uc + tc + cx - cy + 1);
     v = f000 + w1 * c000 + w2 * (cp00 + c0p0 + c00p) + w3 * (cpp0 + cp0p + c0pp) + w4 * cppp;
@@ -222,8 +225,10 @@ __device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, I tc, I c
     uf[f - fxs] = v; if (EMIT) ge->emit(i - 1, j, k, v);
   }
   {  // remaining children on the -x side (coarse plane x-1)
-    const T cm00 = gld<CG>(uc + tc - cx), cmm0 = gld<CG>(uc + tc - cx - cy), cm0p = gld<CG>(uc + tc - cx + 1), cm0m = gld<CG>(uc + tc - cx - 1);
-    const T cmmm = gld<CG>(uc + tc - cx - cy - 1), cmp0 = gld<CG>(uc + tc - cx + cy), cmpm = gld<CG>(uc + tc - cx + cy - 1);
+    const T cm00 = gld<CG>(uc + tc - cx), cmm0 = gld<CG>(uc + tc - cx - cy), cm0p = gld<CG>(uc + tc - cx + 1);
+    const T cm0m = gld<CG>(uc + tc - cx - 1);
+    const T cmmm = gld<CG>(uc + tc - cx - cy - 1), cmp0 = gld<CG>(uc + tc - cx + cy);
+    const T cmpm = gld<CG>(uc + tc - cx + cy - 1);
     const T cmmp = gld<CG>(uc + tc - cx - cy + 1);
     v = f110 + w1 * c000 + w2 * (cm00 + c0m0 + c00p) + w3 * (cmm0 + cm0p + c0mp) + w4 * cmmp;
     uf[f - fxs - fys] = v; if (EMIT) ge->emit(i - 1, j - 1, k, v);
@@ -441,23 +446,22 @@ ocu_status launch_prolong_emit(const T *uc, const ocu_layout &Lc, T *uf, const o
       Lc.ystride % 2 == 0 && Lf.ystride % 4 == 0) {
     dim3 b4(32, 4, 2), g4(Lc.nz / 64, (Lc.ny + 3) / 4, (Lc.nx + 1) / 2);
     launch_pdl(k_prolong_v4, g4, b4, 0, s, (const float *)uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz,
-                                   (float *)uf, (int)Lf.xstride, (int)Lf.ystride,
-                                   *reinterpret_cast<const GhostEmit<float> *>(&ge));
+               (float *)uf, (int)Lf.xstride, (int)Lf.ystride, *reinterpret_cast<const GhostEmit<float> *>(&ge));
     return check_launch("k_prolong_v4");
   }
   if (sizeof(T) == 8 && Lc.nz % 32 == 0 && Lf.allocated < (1LL << 31) && Lf.shift % 2 == 0 &&
       Lf.ystride % 2 == 0) {
     dim3 b2(32, 4, 2), g2(Lc.nz / 32, (Lc.ny + 3) / 4, (Lc.nx + 1) / 2);
-    launch_pdl(k_prolong_v2d, g2, b2, 0, s, (const double *)uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny,
-               Lc.nz, (double *)uf, (int)Lf.xstride, (int)Lf.ystride, *reinterpret_cast<const GhostEmit<double> *>(&ge));
+    launch_pdl(k_prolong_v2d, g2, b2, 0, s, (const double *)uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz,
+               (double *)uf, (int)Lf.xstride, (int)Lf.ystride, *reinterpret_cast<const GhostEmit<double> *>(&ge));
     return check_launch("k_prolong_v2d");
   }
   if (Lf.allocated < (1LL << 31) && Lc.allocated < (1LL << 31))
     launch_pdl(k_prolong_emit<T, int>, grid, block, 0, s, uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
-                                                  (int)Lf.xstride, (int)Lf.ystride, ge);
+               (int)Lf.xstride, (int)Lf.ystride, ge);
   else
     launch_pdl(k_prolong_emit<T, long long>, grid, block, 0, s, uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
-                                                        Lf.xstride, Lf.ystride, ge);
+               Lf.xstride, Lf.ystride, ge);
   return check_launch("k_prolong_emit");
 }
 
@@ -803,8 +807,8 @@ ocu_status launch_residual_restrict(const T *u, const T *b, const ocu_layout &Lf
   const ResCoefT<T> c = res_coef<T>(h, fx, fy, fz);
   if (sizeof(T) == 4 && Lf.shift % 2 == 0 && Lf.xstride % 2 == 0 && Lf.ystride % 2 == 0 && Lf.nz == 2 * Lc.nz) {
     if (rows2 || rowsinf) {
-      launch_pdl(k_residual_restrict_v2<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny,
-                 Lf.nz, c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf, zero_u, zero_n);
+      launch_pdl(k_residual_restrict_v2<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz,
+                 c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf, zero_u, zero_n);
     } else {
       dim3 gridc((Lc.nz + 31) / 32, (Lc.ny + 7) / 8, Lc.nx);
       launch_pdl(k_residual_restrict_v2<T, false>, gridc, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny,
@@ -813,12 +817,12 @@ ocu_status launch_residual_restrict(const T *u, const T *b, const ocu_layout &Lf
     return check_launch("k_residual_restrict_v2");
   }
   if (rows2 || rowsinf) {
-    launch_pdl(k_residual_restrict<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz,
-               c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf, zero_u, zero_n);
+    launch_pdl(k_residual_restrict<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c,
+               bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, rowsinf, zero_u, zero_n);
   } else {
     dim3 gridc((Lc.nz + 31) / 32, (Lc.ny + 7) / 8, Lc.nx);
-    launch_pdl(k_residual_restrict<T, false>, gridc, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz,
-               c, bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr, zero_u, zero_n);
+    launch_pdl(k_residual_restrict<T, false>, gridc, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c,
+               bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, nullptr, zero_u, zero_n);
   }
   return check_launch("k_residual_restrict");
 }
@@ -1172,8 +1176,8 @@ ocu_status launch_relax_color_emit_b(T *u, const T *b, const ocu_layout &L, cons
     return fail(OCU_ERR_UNSUPPORTED, "[ERROR] ensemble - too many members of size (%d,%d,%d) in one class", L.nx, L.ny, L.nz);
   dim3 grid((half + bl.x - 1) / bl.x, (L.ny + bl.y - 1) / bl.y, (unsigned)(zb * members));
   GhostEmit<T> ge{u, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(p.bc), (T)hx, (T)hy, (T)hz};
-  launch_pdl(k_relax_color_emit_b<T>, grid, bl, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c, diag, ge, sel,
-                                              ms, zb);
+  launch_pdl(k_relax_color_emit_b<T>, grid, bl, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color, c, diag, ge,
+             sel, ms, zb);
   return check_launch("k_relax_color_emit_b");
 }
 
@@ -1213,7 +1217,7 @@ ocu_status launch_prolong_emit_b(const T *uc, const ocu_layout &Lc, T *uf, const
   dim3 grid((Lc.nz + block.x - 1) / block.x, (Lc.ny + block.y - 1) / block.y, (unsigned)(Lc.nx * members));
   GhostEmit<T> ge{uf, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, to_dev(bc_fine), (T)hx, (T)hy, (T)hz};
   launch_pdl(k_prolong_emit_b<T>, grid, block, 0, s, uc, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf, Lf.xstride,
-                                             Lf.ystride, ge, sel, cms, fms);
+             Lf.ystride, ge, sel, cms, fms);
   return check_launch("k_prolong_emit_b");
 }
 
@@ -1283,13 +1287,11 @@ ocu_status launch_residual_restrict_b(const T *u, const T *b, const ocu_layout &
   dim3 block(32, 8), grid(1, (Lc.ny + 7) / 8, (unsigned)(Lc.nx * members));
   const ResCoefT<T> c = res_coef<T>(h, fx, fy, fz);
   if (rows2)
-    launch_pdl(k_residual_restrict_b<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c, bc_,
-                                                          Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, sel,
-                                                          fms, cms);
+    launch_pdl(k_residual_restrict_b<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c,
+               bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, rows2, sel, fms, cms);
   else
     launch_pdl(k_residual_restrict_b<T, false>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz, c,
-                                                           bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr,
-                                                           sel, fms, cms);
+               bc_, Lc.xstride, Lc.ystride, Lc.nx, Lc.ny, Lc.nz, nullptr, sel, fms, cms);
   return check_launch("k_residual_restrict_b");
 }
 
@@ -1329,7 +1331,7 @@ ocu_status launch_residual_rows_b(const T *u, const T *b, const ocu_layout &L, d
     return fail(OCU_ERR_UNSUPPORTED, "[ERROR] ensemble - too many members of one size in one class");
   dim3 block(32, 8), grid(1, (L.ny + 7) / 8, (unsigned)(L.nx * members));
   launch_pdl(k_residual_rows_b<T>, grid, block, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz,
-                                              res_coef<T>(h, fx, fy, fz), rows2, sel, ms);
+             res_coef<T>(h, fx, fy, fz), rows2, sel, ms);
   return check_launch("k_residual_rows_b");
 }
 
@@ -1403,7 +1405,7 @@ ocu_status launch_bc_fill_b(T *u, const ocu_layout &L, const ocu_bc_set &bc, dou
                             const BatchSel &sel, long long ms, int members, int *state, bool retire,
                             cudaStream_t s) {
   launch_pdl(k_bc_fill_b<T>, members, 512, 0, s, u, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(bc), (T)hx, (T)hy,
-                                         (T)hz, sel, ms, state, retire ? 1 : 0);
+             (T)hz, sel, ms, state, retire ? 1 : 0);
   return check_launch("k_bc_fill_b");
 }
 

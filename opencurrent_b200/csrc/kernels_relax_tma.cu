@@ -369,8 +369,8 @@ ocu_status launch_relax_sweep2(const SweepTmap &tm_u_in, const SweepTmap &tm_b, 
   CUtensorMap tu, tb;
   std::memcpy(&tu, tm_u_in.bytes, sizeof(tu));
   std::memcpy(&tb, tm_b.bytes, sizeof(tb));
-  launch_pdl(k_relax_sweep2<T>, (unsigned)grid, S::THREADS, S::SMEM, s, tu, tb, u_out, L.xstride, L.ystride, a, c, diag, ge,
-                                                               err);
+  launch_pdl(k_relax_sweep2<T>, (unsigned)grid, S::THREADS, S::SMEM, s, tu, tb, u_out, L.xstride, L.ystride, a, c, diag,
+             ge, err);
   return check_launch("k_relax_sweep2");
 }
 
