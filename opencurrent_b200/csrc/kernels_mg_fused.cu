@@ -436,6 +436,37 @@ __global__ void __launch_bounds__(256, 4) k_prolong_v2d(const double *__restrict
   if (face) prolong_row_ghosts<double, 2>(&ge, uf, fxs, fys, ic, jc, 2 * kc);
 }
 
+// coarse levels up to this many cells prolong with one thread per fine cell
+constexpr long long kProlongFineCells = 32768;
+
+// Prolongation with one thread per FINE cell: the child's coarse octant (eight values), the
+// same sum and corner rule as prolong_cell, then its ghosts.  For the small levels, whose
+// launches are latency-bound: a thread's chain is one child instead of eight children and
+// their ghost writes.
+template <typename T>
+__global__ void __launch_bounds__(256) k_prolong_fine(const T *__restrict__ uc, int cx, int cy, int cnx, int cny,
+                                                      int cnz, T *__restrict__ uf, int fxs, int fys,
+                                                      const __grid_constant__ GhostEmit<T> ge) {
+  pdl_entry();
+  const int fk = blockIdx.x * blockDim.x + threadIdx.x;
+  const int fj = blockIdx.y * blockDim.y + threadIdx.y;
+  const int bz = blockIdx.z == 0 ? gridDim.z - 1 : blockIdx.z - 1;  // face planes first
+  const int fi = bz * blockDim.z + threadIdx.z;
+  if (fk >= 2 * cnz || fj >= 2 * cny || fi >= 2 * cnx) return;
+  const int dx = 1 - (fi & 1), dy = 1 - (fj & 1), dz = 1 - (fk & 1);  // 1: the child on the parent's - side
+  const int sx = dx ? -cx : cx, sy = dy ? -cy : cy, sz = dz ? -1 : 1;
+  const int tc = (fi >> 1) * cx + (fj >> 1) * cy + (fk >> 1);
+  const int f = fi * fxs + fj * fys + fk;
+  const T fv = uf[f];
+  const T c000 = uc[tc], X = uc[tc + sx], Y = uc[tc + sy], Z = uc[tc + sz];
+  const T XY = uc[tc + sx + sy], XZ = uc[tc + sx + sz], YZ = uc[tc + sy + sz];
+  // the (-x, +y, +z) child takes its corner weight from (+1, +1, +1), as prolong_cell does
+  const T XYZ = (dx == 1 && dy == 0 && dz == 0) ? uc[tc + cx + cy + 1] : uc[tc + sx + sy + sz];
+  const T v = prolong_child<T>(fv, c000, X, Y, Z, XY, XZ, YZ, XYZ);
+  uf[f] = v;
+  ge.emit(fi, fj, fk, v);
+}
+
 template <typename T>
 ocu_status launch_prolong_emit(const T *uc, const ocu_layout &Lc, T *uf, const ocu_layout &Lf,
                                const ocu_bc_set &bc_fine, double hx, double hy, double hz, cudaStream_t s) {
@@ -455,6 +486,15 @@ ocu_status launch_prolong_emit(const T *uc, const ocu_layout &Lc, T *uf, const o
     launch_pdl(k_prolong_v2d, g2, b2, 0, s, (const double *)uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz,
                (double *)uf, (int)Lf.xstride, (int)Lf.ystride, *reinterpret_cast<const GhostEmit<double> *>(&ge));
     return check_launch("k_prolong_v2d");
+  }
+  if (Lf.allocated < (1LL << 31) && (long long)Lc.nx * Lc.ny * Lc.nz <= kProlongFineCells) {
+    const int fz = 2 * Lc.nz;
+    dim3 bf(fz >= 32 ? 32 : (fz >= 16 ? 16 : (fz >= 8 ? 8 : 4)), 4, 2);
+    bf.y = 256 / (bf.x * bf.z) > 8 ? 8 : 256 / (bf.x * bf.z);
+    dim3 gf((fz + bf.x - 1) / bf.x, (2 * Lc.ny + bf.y - 1) / bf.y, (2 * Lc.nx + bf.z - 1) / bf.z);
+    launch_pdl(k_prolong_fine<T>, gf, bf, 0, s, uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,
+               (int)Lf.xstride, (int)Lf.ystride, ge);
+    return check_launch("k_prolong_fine");
   }
   if (Lf.allocated < (1LL << 31) && Lc.allocated < (1LL << 31))
     launch_pdl(k_prolong_emit<T, int>, grid, block, 0, s, uc, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz, uf,

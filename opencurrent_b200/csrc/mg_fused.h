@@ -69,6 +69,76 @@ __device__ void coarse_relax_block(T *u, const T *b, long long xs, long long ys,
   const int nt = blockDim.x;
   const int ncell = nx * ny * nz;
   auto at = [&](int i, int j, int k) -> T & { return u[(long long)i * xs + (long long)j * ys + k]; };
+  const int nzf = nx * ny, nyf = nx * nz, nxf = ny * nz, nghost = 2 * (nzf + nyf + nxf);
+  if (ncell <= nt && nghost <= nt) {
+    // every thread owns at most one cell and one face ghost: their indices, diagonal and ghost
+    // rule are worked out once, and each of the 4 phases of an iteration is a short chain
+    const int q = threadIdx.x;
+    const bool own = q < ncell;
+    int i = 0, j = 0, k = 0;
+    long long id = 0;
+    T dg = c.ld;
+    if (own) {
+      i = q / (ny * nz), j = (q / nz) % ny, k = q % nz;
+      id = (long long)i * xs + (long long)j * ys + k;
+      const T x_mod = (i == 0) ? c.xn : (i == nx - 1) ? c.xp : (T)0;
+      const T y_mod = (j == 0) ? c.yn : (j == ny - 1) ? c.yp : (T)0;
+      const T z_mod = (k == 0) ? c.zn : (k == nz - 1) ? c.zp : (T)0;
+      dg = c.ld + x_mod + y_mod + z_mod;
+    }
+    // ghost item: dst <- src (periodic copy) or host_face(src) (Dirichlet / Neumann)
+    int gkind = 0, gf = 0;  // 0 none, 1 copy, 2 rule
+    long long gdst = 0, gsrc = 0;
+    T gh = 0;
+    bool gneg = false;
+    if (q < nghost) {
+      int r = q, gi, gj, gk, si, sj, sk;
+      if (r < 2 * nzf) {
+        const int side = r / nzf;
+        gi = si = (r % nzf) / ny, gj = sj = (r % nzf) % ny;
+        gf = side ? FZ_POS : FZ_NEG, gh = hz, gneg = !side;
+        gk = side ? nz : -1;
+        sk = bc.ty(gf) == OCU_BC_PERIODIC ? (side ? 0 : nz - 1) : (side ? nz - 1 : 0);
+      } else if ((r -= 2 * nzf) < 2 * nyf) {
+        const int side = r / nyf;
+        gi = si = (r % nyf) / nz, gk = sk = (r % nyf) % nz;
+        gf = side ? FY_POS : FY_NEG, gh = hy, gneg = !side;
+        gj = side ? ny : -1;
+        sj = bc.ty(gf) == OCU_BC_PERIODIC ? (side ? 0 : ny - 1) : (side ? ny - 1 : 0);
+      } else {
+        r -= 2 * nyf;
+        const int side = r / nxf;
+        gj = sj = (r % nxf) / nz, gk = sk = (r % nxf) % nz;
+        gf = side ? FX_POS : FX_NEG, gh = hx, gneg = !side;
+        gi = side ? nx : -1;
+        si = bc.ty(gf) == OCU_BC_PERIODIC ? (side ? 0 : nx - 1) : (side ? nx - 1 : 0);
+      }
+      const int t = bc.ty(gf);
+      gkind = t == OCU_BC_PERIODIC ? 1 : (t == OCU_BC_DIRICHELET || t == OCU_BC_NEUMANN) ? 2 : 0;
+      gdst = (long long)gi * xs + (long long)gj * ys + gk;
+      gsrc = (long long)si * xs + (long long)sj * ys + sk;
+    }
+    for (int it = 0; it < iterations; it++) {
+      for (int rb = 0; rb < 2; rb++) {
+        int color = rb;
+        if (order == 1 || (order == 2 && it >= iterations / 2)) color = !rb;
+        if (own && ((i + j + color) & 1) == (k & 1)) {
+          T residual = (-c.h * c.h * b[id] - c.ld * u[id]);
+          residual = (T)((double)residual + c.fz * (double)(u[id - 1] + u[id + 1]));
+          residual = (T)((double)residual + c.fy * (double)(u[id + ys] + u[id - ys]));
+          residual = (T)((double)residual + c.fx * (double)(u[id + xs] + u[id - xs]));
+          u[id] = u[id] + c.omega * residual / dg;
+        }
+        __syncthreads();
+        if (gkind == 1) u[gdst] = u[gsrc];
+        else if (gkind == 2) u[gdst] = host_face<T>(bc, gf, u[gsrc], gh, gneg);
+        __syncthreads();
+      }
+    }
+    level1_fill_block<T>(u, xs, ys, nx, ny, nz, bc, hx, hy, hz);
+    __syncthreads();
+    return;
+  }
   for (int it = 0; it < iterations; it++) {
     for (int rb = 0; rb < 2; rb++) {
       int color = rb;
@@ -87,8 +157,7 @@ __device__ void coarse_relax_block(T *u, const T *b, long long xs, long long ys,
         u[id] = u[id] + c.omega * residual / (c.ld + x_mod + y_mod + z_mod);
       }
       __syncthreads();
-      const int nzf = nx * ny, nyf = nx * nz, nxf = ny * nz;
-      for (int q = threadIdx.x; q < 2 * (nzf + nyf + nxf); q += nt) {
+      for (int q = threadIdx.x; q < nghost; q += nt) {
         int r = q;
         if (r < 2 * nzf) {
           const int side = r / nzf, i = (r % nzf) / ny, j = (r % nzf) % ny;
