@@ -767,6 +767,41 @@ __global__ void __launch_bounds__(256) k_residual_restrict_v2(const T *__restric
   }
 }
 
+// coarse levels up to this many cells restrict with one thread per fine cell
+constexpr long long kRestrictFineCells = 32768;
+
+// Residual + restriction for the small levels, without norms: eight lanes per coarse cell, one
+// child each; the group's first lane gathers the eight residuals by shuffles and sums them in
+// the per-operation kernels' order.  Short per-thread chains for latency-bound launches.
+template <typename T>
+__global__ void __launch_bounds__(256) k_residual_restrict_fine(const T *__restrict__ u, const T *__restrict__ b,
+                                                                int xs, int ys, ResCoefT<T> c, T *__restrict__ bc_,
+                                                                int bxs, int bys, int cnx, int cny, int cnz,
+                                                                T *__restrict__ zero_u, long long zero_n) {
+  pdl_entry();
+  if (zero_u) {  // the coarser level's clear (its whole buffer, as a memset), nothing here reads it
+    const long long nthreads = (long long)gridDim.x * gridDim.y * gridDim.z * blockDim.x;
+    const long long tid = ((long long)(blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * blockDim.x +
+                          threadIdx.x;
+    for (long long q = tid; q < zero_n; q += nthreads) zero_u[q] = (T)0;
+  }
+  const int child = threadIdx.x & 7;
+  const int kc = blockIdx.x * (blockDim.x >> 3) + (threadIdx.x >> 3);
+  const int jc = blockIdx.y, ic = blockIdx.z;
+  const bool act = kc < cnz;
+  const int di = child >> 2, dj = (child >> 1) & 1, dk = child & 1;
+  const long long id = (long long)(2 * ic + di) * xs + (long long)(2 * jc + dj) * ys + 2 * (act ? kc : 0) + dk;
+  const T r = residual_at<T>(u, b, id, xs, ys, c);
+  // gather the group's residuals in child order r0..r7 = (0,0,0), (0,0,1), (0,1,0), ... (1,1,1)
+  const int g = threadIdx.x & 31 & ~7;
+  T rr[8];
+#pragma unroll
+  for (int n = 0; n < 8; n++) rr[n] = __shfl_sync(0xffffffffu, r, g + n);
+  if (act && child == 0)
+    bc_[(long long)ic * bxs + (long long)jc * bys + kc] =
+        (T)0.125 * (rr[0] + rr[1] + rr[2] + rr[3] + rr[4] + rr[5] + rr[6] + rr[7]);
+}
+
 // 256-wide fold of row values (grid1dops.cu:33-115), one launch: block b folds rows
 // [256b, 256b+256), the last block folds the block partials.  Writes the T result as double.
 template <typename T>
@@ -845,6 +880,14 @@ ocu_status launch_residual_restrict(const T *u, const T *b, const ocu_layout &Lf
                                     T *zero_u, long long zero_n) {
   dim3 block(32, 8), grid(1, (Lc.ny + 7) / 8, Lc.nx);
   const ResCoefT<T> c = res_coef<T>(h, fx, fy, fz);
+  if (!rows2 && !rowsinf && (long long)Lc.nx * Lc.ny * Lc.nz <= kRestrictFineCells && Lf.allocated < (1LL << 31) &&
+      Lc.allocated < (1LL << 31)) {
+    const int per_block = Lc.nz >= 32 ? 32 : (Lc.nz >= 16 ? 16 : (Lc.nz >= 8 ? 8 : 4));  // coarse cells
+    dim3 gf((Lc.nz + per_block - 1) / per_block, Lc.ny, Lc.nx);
+    launch_pdl(k_residual_restrict_fine<T>, gf, dim3(8 * per_block), 0, s, u, b, (int)Lf.xstride, (int)Lf.ystride, c,
+               bc_, (int)Lc.xstride, (int)Lc.ystride, Lc.nx, Lc.ny, Lc.nz, zero_u, zero_n);
+    return check_launch("k_residual_restrict_fine");
+  }
   if (sizeof(T) == 4 && Lf.shift % 2 == 0 && Lf.xstride % 2 == 0 && Lf.ystride % 2 == 0 && Lf.nz == 2 * Lc.nz) {
     if (rows2 || rowsinf) {
       launch_pdl(k_residual_restrict_v2<T, true>, grid, block, 0, s, u, b, Lf.xstride, Lf.ystride, Lf.nx, Lf.ny, Lf.nz,
