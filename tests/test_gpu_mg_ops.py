@@ -109,7 +109,7 @@ def test_relax_levels_long_rows(dt, bcname, shape):
 
 @pytest.mark.parametrize("dt", [F32, F64])
 @pytest.mark.parametrize("bcname", ["neumann_inhom", "periodic", "dirichlet", "mixed_all"])
-@pytest.mark.parametrize("shape", LONG_ROWS)
+@pytest.mark.parametrize("shape", LONG_ROWS + [(80, 220, 128)])  # the last: float4 prolongation (coarse > 64^3 cells)
 def test_restrict_and_prolong_long_rows(dt, bcname, shape):
     import ctypes as C
     om, dm, _ = pair(dt, shape, (0.03, 0.02, 0.01), bcname, seed=5)
