@@ -98,6 +98,21 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- helpers ----
+def solve_alg_bytes(n, s, vcycles, outer):
+    """Compulsory HBM bytes of a multigrid solve: 12.57 N s per level-0 V-cycle (nu1 = nu2 = 2,
+    no post-smooth on level 0: 10.25 N s on level 0, 16.25 N_l s on each coarser level), one FMG
+    ramp (the cycles from the coarser levels, 12.57/7 N s) per FMG, and for the refinement solver
+    per outer step the FP64 residual + FP32 right-hand side (2N*8 + N*4) and the update
+    (2N*8 + N*4), plus the initial residual."""
+    N = float(n) ** 3
+    cycle = 12.57 * N * s
+    ramps = max(outer, 1)
+    b = vcycles * cycle + ramps * cycle / 7.0
+    if outer:
+        b += (outer + 1) * (2 * N * 8 + N * 4) + outer * (2 * N * 8 + N * 4)
+    return b
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -295,8 +310,11 @@ def run_gpu(args):
         "fp64_mg_ms": round(ms_fp64, 4),
         "speedup_mixed_vs_fp64": round(ms_fp64 / ms_mixed, 3),
         "mixed": {"outer_iterations": st_mixed.outer_iterations, "fp32_vcycles": st_mixed.vcycles,
-                  "rel_residual": res_holder["mixed"] / rms_b, "max_rel_err_vs_fp64_mg": err_vs_fp64},
-        "fp64": {"vcycles": st_fp64.vcycles, "rel_residual": res_holder["fp64"] / rms_b},
+                  "rel_residual": res_holder["mixed"] / rms_b, "max_rel_err_vs_fp64_mg": err_vs_fp64,
+                  "alg_gbs": round(solve_alg_bytes(n, 4, st_mixed.vcycles, st_mixed.outer_iterations)
+                                   / (ms_mixed * 1e-3) / 1e9, 1)},
+        "fp64": {"vcycles": st_fp64.vcycles, "rel_residual": res_holder["fp64"] / rms_b,
+                 "alg_gbs": round(solve_alg_bytes(n, 8, st_fp64.vcycles, 0) / (ms_fp64 * 1e-3) / 1e9, 1)},
         "roofline": {"bound": "hbm", "kernel": kernel_name,
                      "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
