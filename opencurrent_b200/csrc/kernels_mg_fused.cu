@@ -24,7 +24,11 @@ namespace ocub {
 // One colour update of cell (i,j,k).  In a block that holds no cell of the outer layer the
 // diagonal is c.ld exactly (every face term is skipped) and there are no ghost writes.  I is the
 // index type: int when the whole allocation fits in 2^31 elements.
-template <typename T, typename I>
+// ZFAST: rows off the x and y faces in an edge block (an edge block only through z) take a short
+// path -- relax_dg's sequence reduces to the z terms (the FP64 table holds ld there) and the
+// cell's only ghosts are its z ghosts.  Used where it measured faster: the large FP64 levels and
+// the ensemble sweeps (on the small levels the longer kernel was slower).
+template <typename T, typename I, bool ZFAST = false>
 __device__ __forceinline__ void color_cell(T *__restrict__ u, const T *__restrict__ b, I xs, I ys, int i, int j,
                                            int k, int nx, int ny, int nz, const RelaxCoefD<T> &c,
                                            const T *__restrict__ diag, bool edge_block, const GhostEmit<T> &ge) {
@@ -33,6 +37,25 @@ __device__ __forceinline__ void color_cell(T *__restrict__ u, const T *__restric
     const T uc = u[id];
     const T res = relax_res<T>(uc, b[id], u[id - 1], u[id + 1], u[id - ys], u[id + ys], u[id - xs], u[id + xs], c);
     u[id] = uc + c.omega * res / c.ld;
+    return;
+  }
+  if (ZFAST && i > 0 && i < nx - 1 && j > 0 && j < ny - 1) {
+    const T uc = u[id];
+    const T res = relax_res<T>(uc, b[id], u[id - 1], u[id + 1], u[id - ys], u[id + ys], u[id - xs], u[id + xs], c);
+    T dg = c.ld;
+    if (k == nz - 1) dg += c.zp;
+    if (k == 0) dg += c.zn;
+    const T nv = uc + c.omega * res / dg;
+    u[id] = nv;
+    const int tn = ge.bc.type[FZ_NEG], tp = ge.bc.type[FZ_POS];
+    if (k == 0) {
+      if (tn == OCU_BC_DIRICHELET || tn == OCU_BC_NEUMANN) u[id - 1] = ge.template rule<FZ_NEG>(nv, ge.hz);
+      if (tp == OCU_BC_PERIODIC) u[id + nz] = ge.template rule<FZ_POS>(nv, ge.hz);
+    }
+    if (k == nz - 1) {
+      if (tp == OCU_BC_DIRICHELET || tp == OCU_BC_NEUMANN) u[id + 1] = ge.template rule<FZ_POS>(nv, ge.hz);
+      if (tn == OCU_BC_PERIODIC) u[id - nz] = ge.template rule<FZ_NEG>(nv, ge.hz);
+    }
     return;
   }
   const T nv = relax_value<T>(u[id], b[id], u[id - 1], u[id + 1], u[id - ys], u[id + ys], u[id - xs], u[id + xs], i,
@@ -47,8 +70,9 @@ __device__ __forceinline__ bool color_edge_block(int bx, int by, int bz, int nx,
 }
 
 // Colour sweep + ghost writes: thread (t, j, i), k = 2t + parity.
-template <typename T, typename I>
-__global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, const T *__restrict__ b, I xs, I ys,
+template <typename T, typename I, bool ZFAST>
+__global__ void __launch_bounds__(256, 6) k_relax_color_emit(T *__restrict__ u, const T *__restrict__ b,
+                                                                         I xs, I ys,
                                                           int nx, int ny, int nz, int color, RelaxCoefD<T> c,
                                                           const T *__restrict__ diag,
                                                           const __grid_constant__ GhostEmit<T> ge) {
@@ -61,7 +85,7 @@ __global__ void __launch_bounds__(256) k_relax_color_emit(T *__restrict__ u, con
   const int i = bz * blockDim.z + threadIdx.z;
   const bool edge_block = color_edge_block(blockIdx.x, blockIdx.y, bz, nx, ny, nz);
   if (i >= nx || j >= ny || t >= nz / 2) return;
-  color_cell<T, I>(u, b, xs, ys, i, j, 2 * t + ((i + j + color) & 1), nx, ny, nz, c, diag, edge_block, ge);
+  color_cell<T, I, ZFAST>(u, b, xs, ys, i, j, 2 * t + ((i + j + color) & 1), nx, ny, nz, c, diag, edge_block, ge);
 }
 
 // FP32 colour sweep with 128-bit accesses: a thread owns four consecutive cells of a row (two of
@@ -178,12 +202,18 @@ ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const 
   GhostEmit<T> ge{nullptr, L.xstride, L.ystride, L.nx, L.ny, L.nz, to_dev(p.bc), (T)hx, (T)hy, (T)hz};
   ge.p = u;
   if (launch_color_v4<T>(u, b, L, color, c, ge, diag, s)) return check_launch("k_relax_color_v4");
-  if (L.allocated < (1LL << 31))
-    launch_pdl(k_relax_color_emit<T, int>, grid, block, 0, s, u, b, (int)L.xstride, (int)L.ystride, L.nx, L.ny, L.nz,
-               color, c, diag, ge);
-  else
-    launch_pdl(k_relax_color_emit<T, long long>, grid, block, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny, L.nz, color,
-               c, diag, ge);
+  const bool zfast = sizeof(T) == 8 && (long long)L.nx * L.ny * L.nz >= (1LL << 21);  // FP64, 128^3 and up
+  if (L.allocated < (1LL << 31)) {
+    if (zfast)
+      launch_pdl(k_relax_color_emit<T, int, true>, grid, block, 0, s, u, b, (int)L.xstride, (int)L.ystride, L.nx,
+                 L.ny, L.nz, color, c, diag, ge);
+    else
+      launch_pdl(k_relax_color_emit<T, int, false>, grid, block, 0, s, u, b, (int)L.xstride, (int)L.ystride, L.nx,
+                 L.ny, L.nz, color, c, diag, ge);
+  } else {
+    launch_pdl(k_relax_color_emit<T, long long, false>, grid, block, 0, s, u, b, L.xstride, L.ystride, L.nx, L.ny,
+               L.nz, color, c, diag, ge);
+  }
   return check_launch("k_relax_color_emit");
 }
 
@@ -1231,7 +1261,7 @@ ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s) {
 // bit-identical to the single-grid kernel applied to that member alone.
 // ------------------------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_relax_color_emit_b(T *__restrict__ u, const T *__restrict__ b, long long xs,
+__global__ void __launch_bounds__(256, 6) k_relax_color_emit_b(T *__restrict__ u, const T *__restrict__ b, long long xs,
                                                             long long ys, int nx, int ny, int nz, int color,
                                                             RelaxCoefD<T> c, const T *__restrict__ diag,
                                                             const __grid_constant__ GhostEmit<T> ge, BatchSel sel,
@@ -1249,7 +1279,8 @@ __global__ void __launch_bounds__(256) k_relax_color_emit_b(T *__restrict__ u, c
   b += m * ms;
   GhostEmit<T> g = ge;
   g.p = u;
-  color_cell<T, int>(u, b, (int)xs, (int)ys, i, j, 2 * t + ((i + j + color) & 1), nx, ny, nz, c, diag, edge_block, g);
+  color_cell<T, int, true>(u, b, (int)xs, (int)ys, i, j, 2 * t + ((i + j + color) & 1), nx, ny, nz, c, diag, edge_block,
+                           g);
 }
 
 template <typename T>
