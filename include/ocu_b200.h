@@ -151,8 +151,9 @@ typedef struct ocu_mg_params {
   int convergence;               /* ocu_convergence */
   int make_symmetric_operator;
   int disable_relax_on_host;     /* kept for API parity: the coarsest level is always relaxed
-                                    on the device here; 1 = use the device colour-sweep kernel
-                                    instead of the host-order one (see DESIGN) */
+                                    on the device here; 0 = one CTA runs the reference host
+                                    routine's arithmetic and ghost fills, 1 = the device
+                                    colour-sweep kernels relax it */
   int ir_inner_cycles;           /* OCU_MG_MIXED_IR only: FP32 fine-level cycles per
                                     correction (0 = default 4) */
   int store_residual_grids;      /* 1 = keep r_grid(level) filled (read_r); costs N*s */
