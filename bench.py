@@ -581,6 +581,17 @@ def run_kernel_case(args):
     import torch
     import opencurrent_b200 as ocu
 
+    if args.kernel_case == "flow":
+        # two steps of the Rayleigh-Benard flow on a 256x256x128 FP32 grid (each field 33.5 MB,
+        # a kernel reads 3-7 of them: more than L2 holds)
+        eq = ocu.Eqn_IncompressibleNS3D(ocu.F32)
+        eq.set_parameters(rayleigh_benard(ocu, 256, 256, 128))
+        for _ in range(2):
+            eq.advance_one_step(eq.get_max_stable_timestep())
+        torch.cuda.synchronize()
+        print(json.dumps({"kernel_case": "flow", "grid": [256, 256, 128], "ok": True}), flush=True)
+        return
+
     n = N_CFG3
     h = 1.0 / n
     L = ocu.layout(n, n, n)
@@ -615,8 +626,9 @@ def main():
                     help="levels with at least this many cells use the two-colour TMA pass (0 = off)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-secondary", action="store_true")
-    ap.add_argument("--kernel-case", choices=["relax", "prolong", "restrict", "tail"],
-                    help="run a few launches of one kernel on the 256^3 FP32 hierarchy (profiling)")
+    ap.add_argument("--kernel-case", choices=["relax", "prolong", "restrict", "tail", "flow"],
+                    help="run a few launches of one kernel on the 256^3 FP32 hierarchy, or two "
+                         "256x256x128 flow steps (profiling)")
     args = ap.parse_args()
     if args.kernel_case:
         run_kernel_case(args)

@@ -3,6 +3,7 @@
 // All arithmetic reproduces the reference expression order; the library is compiled with
 // --fmad=false so every product and sum is rounded exactly as written.
 #include <cfloat>
+#include <cstdint>
 
 #include "bc_device.cuh"
 #include "ocu_internal.h"
@@ -304,6 +305,38 @@ __global__ void k_lincomb2_3d(T *res, T a1, const T *g1, T a2, const T *g2, long
   res[id] = g1[id] * a1 + g2[id] * a2;
 }
 
+// The same sum over 16-byte groups of a row: k = 0 of every row is 16-byte aligned (checked by
+// the launcher), a row's last group may be partial.  Per element the arithmetic is unchanged.
+template <typename T>
+__global__ void k_lincomb2_3dv(T *res, T a1, const T *g1, T a2, const T *g2, long long xs, long long ys, int ny,
+                               int nz, int cpr, long long nchunks) {
+  pdl_entry();
+  constexpr int V = 16 / (int)sizeof(T);
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < nchunks;
+       c += (long long)gridDim.x * blockDim.x) {
+    const long long row = c / cpr;
+    const int k0 = (int)(c - row * cpr) * V;
+    const int i = (int)(row / ny), j = (int)(row - (long long)i * ny);
+    const long long id = (long long)i * xs + (long long)j * ys + k0;
+    if (k0 + V <= nz) {
+      if constexpr (sizeof(T) == 4) {
+        const float4 x = *reinterpret_cast<const float4 *>(g1 + id), y = *reinterpret_cast<const float4 *>(g2 + id);
+        float4 r;
+        r.x = x.x * a1 + y.x * a2; r.y = x.y * a1 + y.y * a2;
+        r.z = x.z * a1 + y.z * a2; r.w = x.w * a1 + y.w * a2;
+        *reinterpret_cast<float4 *>(res + id) = r;
+      } else {
+        const double2 x = *reinterpret_cast<const double2 *>(g1 + id), y = *reinterpret_cast<const double2 *>(g2 + id);
+        double2 r;
+        r.x = x.x * a1 + y.x * a2; r.y = x.y * a1 + y.y * a2;
+        *reinterpret_cast<double2 *>(res + id) = r;
+      }
+    } else {
+      for (int e = 0; k0 + e < nz; e++) res[id + e] = g1[id + e] * a1 + g2[id + e] * a2;
+    }
+  }
+}
+
 static unsigned grid_for(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
   if (b > 148LL * 32) b = 148LL * 32;
@@ -336,6 +369,16 @@ ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, T a2,
                            cudaStream_t s) {
   const int waste = (int)(L.allocated - (long long)L.nx * L.ny * L.nz);
   if (waste / (float)L.allocated > .03f) {
+    const auto a16 = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    if (a16(res + L.shift) && a16(g1 + L.shift) && a16(g2 + L.shift) && (L.ystride * sizeof(T)) % 16 == 0 &&
+        (L.xstride * sizeof(T)) % 16 == 0 && L.nx > 0 && L.ny > 0 && L.nz > 0) {
+      constexpr int V = 16 / (int)sizeof(T);
+      const int cpr = (L.nz + V - 1) / V;
+      const long long nchunks = (long long)L.nx * L.ny * cpr;
+      launch_pdl(k_lincomb2_3dv<T>, grid_for(nchunks, 256), 256, 0, s, res + L.shift, a1, g1 + L.shift, a2,
+                 g2 + L.shift, L.xstride, L.ystride, L.ny, L.nz, cpr, nchunks);
+      return check_launch("k_lincomb2_3dv");
+    }
     dim3 grid((L.nz + 127) / 128, L.ny, L.nx);
     launch_pdl(k_lincomb2_3d<T>, grid, 128, 0, s, res + L.shift, a1, g1 + L.shift, a2, g2 + L.shift, L.xstride,
                L.ystride, L.nx, L.ny, L.nz);
@@ -383,8 +426,10 @@ __device__ __forceinline__ void block_tree_256(T *sh, const RedOp<T> &op) {
   }
 }
 
+constexpr int kReduceThreads = 512;  // 16 warps, 16 of a block's 256 rows each; two blocks per SM
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_reduce(const T *origin, long long xs, long long ys, int nx, int ny, int nz,
+__global__ void __launch_bounds__(kReduceThreads, 2) k_reduce(const T *origin, long long xs, long long ys, int nx, int ny, int nz,
                                                 RedOp<T> op, T *partial, unsigned *counter, double *result) {
   pdl_entry();
   __shared__ T sh[256];
@@ -392,22 +437,48 @@ __global__ void __launch_bounds__(256) k_reduce(const T *origin, long long xs, l
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const long long nrows = (long long)nx * ny;
   const long long row0 = (long long)blockIdx.x * 256;
-  for (int rr = 0; rr < 32; rr++) {
-    const int slot = warp * 32 + rr;
-    const long long q = row0 + slot;
-    T acc = op.identity();
-    if (q < nrows) {
-      const int i = (int)(q / ny), j = (int)(q % ny);
-      const T *base = origin + (long long)i * xs + (long long)j * ys;
-      int k = lane;
-      if (k < nz) acc = op.process(base[k]);
-      for (k += 32; k < nz; k += 32) acc = op.reduce(op.process(base[k]), acc);
-      for (int o = 16; o > 0; o >>= 1) {
-        T other = __shfl_down_sync(0xffffffffu, acc, o);
-        acc = op.reduce(acc, other);
+  // A warp folds its RB rows together: each row in its own order (lane-strided over k, then
+  // the shuffle tree), the loads of the RB rows interleaved so that they are in flight
+  // together.  Rows beyond nrows carry the identity, as in reduce_per_cta.
+  constexpr int RW = 256 / (kReduceThreads / 32);  // rows of a warp
+  constexpr int RB = 8;
+  static_assert(RW % RB == 0, "rows of a warp in whole groups");
+  for (int r0 = 0; r0 < RW; r0 += RB) {
+    T acc[RB];
+    const T *base[RB];
+    bool ok[RB];
+    // consecutive rows: one division for the first, then step j (wrapping into i)
+    const long long qb = row0 + warp * RW + r0;
+    int i = (int)(qb / ny), j = (int)(qb - (long long)i * ny);
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+      ok[r] = qb + r < nrows;
+      acc[r] = op.identity();
+      base[r] = ok[r] ? origin + (long long)i * xs + (long long)j * ys : origin;
+      if (++j == ny) {
+        j = 0;
+        ++i;
       }
     }
-    if (lane == 0) sh[slot] = acc;  // rows beyond nrows carry the identity, as in reduce_per_cta
+    // per step of k the loads of all RB rows first (a row beyond nrows reads row 0, which
+    // exists, and is ignored), then the folds, each row in its own order
+    for (int k = lane; k < nz; k += 32) {
+      T v[RB];
+#pragma unroll
+      for (int r = 0; r < RB; r++) v[r] = base[r][k];
+#pragma unroll
+      for (int r = 0; r < RB; r++)
+        if (ok[r]) acc[r] = k == lane ? op.process(v[r]) : op.reduce(op.process(v[r]), acc[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < RB; r++) {
+      T a = acc[r];
+      for (int o = 16; o > 0; o >>= 1) {
+        T other = __shfl_down_sync(0xffffffffu, a, o);
+        a = op.reduce(a, other);
+      }
+      if (lane == 0) sh[warp * RW + r0 + r] = a;
+    }
   }
   __syncthreads();
   block_tree_256(sh, op);
@@ -427,7 +498,7 @@ __global__ void __launch_bounds__(256) k_reduce(const T *origin, long long xs, l
     const long long nb = (count + 255) / 256;
     for (long long b = 0; b < nb; b++) {
       const long long idx = b * 256 + threadIdx.x;
-      sh[threadIdx.x] = idx < count ? vp[idx] : op.identity();
+      if (threadIdx.x < 256) sh[threadIdx.x] = idx < count ? vp[idx] : op.identity();
       __syncthreads();
       block_tree_256(sh, op);
       if (threadIdx.x == 0) vp[b] = sh[0];
@@ -458,7 +529,7 @@ ocu_status launch_reduce(const T *origin, const ocu_layout &L, int op, void *d_s
   unsigned *counter = reinterpret_cast<unsigned *>(d_scratch);
   T *partial = reinterpret_cast<T *>(reinterpret_cast<char *>(d_scratch) + 64);
   RedOp<T> r{op};
-  launch_pdl(k_reduce<T>, (unsigned)blocks, 256, 0, s, origin, L.xstride, L.ystride, L.nx, L.ny, L.nz, r, partial,
+  launch_pdl(k_reduce<T>, (unsigned)blocks, kReduceThreads, 0, s, origin, L.xstride, L.ystride, L.nx, L.ny, L.nz, r, partial,
              counter, d_result);
   return check_launch("k_reduce");
 }
