@@ -8,48 +8,60 @@
 
 namespace ocub {
 
-static inline void shape(int nx, int ny, int nz, dim3 *grid, dim3 *block) {
+// A thread visits CI cells along i (the same k, j): their loads are independent, so they are in
+// flight together, and a plane's values serve the neighbouring cells as well.  The light
+// stencils take kCellsI; self-advection, which is bound by instruction issue, takes one.
+constexpr int kCellsI = 4;
+
+static inline void shape(int nx, int ny, int nz, dim3 *grid, dim3 *block, int ci = kCellsI) {
   *block = nz >= 64 ? dim3(64, 4) : dim3(32, 8);
-  *grid = dim3((nz + block->x - 1) / block->x, (ny + block->y - 1) / block->y, nx);
+  *grid = dim3((nz + block->x - 1) / block->x, (ny + block->y - 1) / block->y, (nx + ci - 1) / ci);
 }
 
-#define CELL_INDEX                                              \
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;          \
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;          \
-  const int i = blockIdx.z;                                     \
-  if (k >= nz || j >= ny || i >= nx) return;                    \
-  const long long id = (long long)i * xs + (long long)j * ys + k;
+#define CELL_LOOP_BEGIN_CI(CI)                                    \
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;            \
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;            \
+  if (k >= nz || j >= ny) return;                                 \
+  _Pragma("unroll") for (int ci = 0; ci < (CI); ci++) {           \
+    const int i = blockIdx.z * (CI) + ci;                         \
+    if (i >= nx) break;                                           \
+    const long long id = (long long)i * xs + (long long)j * ys + k;
+#define CELL_LOOP_BEGIN CELL_LOOP_BEGIN_CI(kCellsI)
+#define CELL_LOOP_END }
 
 // Sol_Divergence3DDevice_calculate_divergence (sol_divergence3ddev.cu:23-45)
 template <typename T>
 __global__ void k_divergence(const T *__restrict__ u, const T *__restrict__ v, const T *__restrict__ w,
                              T *__restrict__ div, T ihx, T ihy, T ihz, long long xs, long long ys, int nx, int ny,
                              int nz) {
-  CELL_INDEX
+  CELL_LOOP_BEGIN
   div[id] = ihx * (u[id + xs] - u[id]) + ihy * (v[id + ys] - v[id]) + ihz * (w[id + 1] - w[id]);
+  CELL_LOOP_END
 }
 
 // Sol_Gradient3DDevice_subtract_grad (sol_gradient3ddev.cu:24-47)
 template <typename T>
 __global__ void k_gradient(T *__restrict__ u, T *__restrict__ v, T *__restrict__ w, const T *__restrict__ phi,
                            T c, T ihx, T ihy, T ihz, long long xs, long long ys, int nx, int ny, int nz) {
-  CELL_INDEX
+  CELL_LOOP_BEGIN
   const T p = phi[id];
   u[id] += c * ihx * (p - phi[id - xs]);
   v[id] += c * ihy * (p - phi[id - ys]);
   w[id] += c * ihz * (p - phi[id - 1]);
+  CELL_LOOP_END
 }
 
 // Sol_LaplacianCentered3DDevice_stencil (sol_laplaciancent3ddev.cu:28-60)
 template <typename T>
 __global__ void k_laplacian(const T *__restrict__ phi, T *__restrict__ dphidt, T ihx2, T ihy2, T ihz2, T c,
                             long long xs, long long ys, int nx, int ny, int nz) {
-  CELL_INDEX
+  CELL_LOOP_BEGIN
   const T p = phi[id];
   const T d = dphidt[id];
   const T lap = ihz2 * (phi[id + 1] + phi[id - 1] - ((T)2) * p) + ihy2 * (phi[id + ys] + phi[id - ys] - ((T)2) * p) +
                 ihx2 * (phi[id + xs] + phi[id - xs] - ((T)2) * p);
   dphidt[id] = d + c * lap;
+  CELL_LOOP_END
 }
 
 // InterpolatorFirstOrderUpwind / InterpolatorSecondOrderCentered (interpolation.h:35-48)
@@ -65,7 +77,7 @@ __global__ void __launch_bounds__(256) k_advect_self(const T *__restrict__ u, co
                                                      const T *__restrict__ w, T *__restrict__ dudt,
                                                      T *__restrict__ dvdt, T *__restrict__ dwdt, T ihx, T ihy,
                                                      T ihz, long long xs, long long ys, int nx, int ny, int nz) {
-  CELL_INDEX
+  CELL_LOOP_BEGIN_CI(1)
   const T half = (T)0.5;
   const long long pi = id + xs, pj = id + ys, pk = id + 1, mi = id - xs, mj = id - ys, mk = id - 1;
   const T ui = u[id], vi = v[id], wi = w[id];
@@ -102,6 +114,7 @@ __global__ void __launch_bounds__(256) k_advect_self(const T *__restrict__ u, co
   b = half * (wi + w[mk]);
   d3 = (a * interp<T, IT>(a, wi, w[pk])) - (b * interp<T, IT>(b, w[mk], wi));
   dwdt[id] = -d1 * ihx - d2 * ihy - d3 * ihz;
+  CELL_LOOP_END
 }
 
 // Sol_PassiveAdvection3D_apply_interp (sol_passiveadvection3ddev.cu:31-78)
@@ -110,7 +123,7 @@ __global__ void __launch_bounds__(256) k_advect_passive(const T *__restrict__ u,
                                                         const T *__restrict__ w, const T *__restrict__ phi,
                                                         T *__restrict__ dphidt, T ihx, T ihy, T ihz, long long xs,
                                                         long long ys, int nx, int ny, int nz) {
-  CELL_INDEX
+  CELL_LOOP_BEGIN
   const T p = phi[id];
   const T upi = u[id + xs], uij = u[id];
   const T du = upi * interp<T, IT>(upi, p, phi[id + xs]) - uij * interp<T, IT>(uij, phi[id - xs], p);
@@ -119,14 +132,16 @@ __global__ void __launch_bounds__(256) k_advect_passive(const T *__restrict__ u,
   const T wpk = w[id + 1], wij = w[id];
   const T dw = wpk * interp<T, IT>(wpk, p, phi[id + 1]) - wij * interp<T, IT>(wij, phi[id - 1], p);
   dphidt[id] = (-du * ihx) - (dv * ihy) - (dw * ihz);
+  CELL_LOOP_END
 }
 
 // Eqn_IncompressibleNS3D_add_thermal_force (eqn_incompressns3d.cu:25-44)
 template <typename T>
 __global__ void k_thermal_force(T *__restrict__ dvdt, T c, const T *__restrict__ temp, long long nbr, long long xs,
                                 long long ys, int nx, int ny, int nz) {
-  CELL_INDEX
+  CELL_LOOP_BEGIN
   dvdt[id] += ((T)0.5) * c * (temp[id] + temp[id - nbr]);
+  CELL_LOOP_END
 }
 
 template <typename T>
@@ -167,7 +182,7 @@ ocu_status launch_advect_self(const T *u, const T *v, const T *w, T *du, T *dv, 
                               const ocu_layout &L, int nx, int ny, int nz, double hx, double hy,
                               double hz, int it, cudaStream_t s) {
   dim3 g, b;
-  shape(nx, ny, nz, &g, &b);
+  shape(nx, ny, nz, &g, &b, 1);
   const T ihx = (T)(1 / hx), ihy = (T)(1 / hy), ihz = (T)(1 / hz);
   if (it == OCU_IT_FIRST_ORDER_UPWIND)
     k_advect_self<T, OCU_IT_FIRST_ORDER_UPWIND><<<g, b, 0, s>>>(u, v, w, du, dv, dw, ihx, ihy, ihz, L.xstride,
