@@ -111,10 +111,12 @@ def test_reductions(dt, shape):
 
 
 @pytest.mark.parametrize("dt", DTYPES)
-@pytest.mark.parametrize("pad", [(0, 0, 0), (1, 1, 14)])
-def test_linear_combination(dt, pad):
+@pytest.mark.parametrize("nz,pad", [(30, (0, 0, 0)), (31, (0, 0, 0)), (32, (1, 1, 14))])
+def test_linear_combination(dt, nz, pad):
+    """The interior-only sweep (these layouts are more than 3 % padding): rows that end in a
+    partial 16-byte group (nz = 30 in FP32, 31 in both precisions) and whole groups."""
     rng = np.random.default_rng(14)
-    L = O.layout(20, 18, 30 if pad[2] == 0 else 32, 1, 1, 1, *pad)
+    L = O.layout(20, 18, nz, 1, 1, 1, *pad)
     a, b = rand_buffer(L, dt, rng), rand_buffer(L, dt, rng)
     ga, gb, gr = dev_grid(a, dt, L), dev_grid(b, dt, L), dev_grid(np.zeros_like(a), dt, L)
     gr.linear_combination(0.7, ga, -1.3, gb)
