@@ -98,6 +98,23 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- helpers ----
+def ir_alg_bytes(n, cycles, outer, ramp_iters=4):
+    """Compulsory HBM bytes of the refinement solve with the split-layout FP32 inner solver
+    (s = 4): per refinement step `cycles` level-0 V-cycles (12.57 N s each, as in
+    solve_alg_bytes), the right-hand side restricted down ((2 + 1/8) N_l s per level) and the
+    nested-iteration ramp (prolongation (2 + 1/8) N_l s + ramp_iters red-black iterations of
+    3 N_l s on each level >= 1, and the prolongation into level 0); plus the FP64 residual + FP32
+    right-hand side per step and the initial residual (2N*8 + N*4 each) and the update per step
+    (2N*8 + N*4)."""
+    N = float(n) ** 3
+    s = 4
+    coarse = N / 7.0  # sum over levels >= 1
+    ramp = 2.125 * N * s + 2.125 * coarse * s + (2.125 + 3 * ramp_iters) * coarse * s + 2.125 * N * s
+    b = outer * (cycles * 12.57 * N * s + ramp)
+    b += (outer + 1) * (2 * N * 8 + N * 4) + outer * (2 * N * 8 + N * 4)
+    return b
+
+
 def solve_alg_bytes(n, s, vcycles, outer):
     """Compulsory HBM bytes of a multigrid solve: 12.57 N s per level-0 V-cycle (nu1 = nu2 = 2,
     no post-smooth on level 0: 10.25 N s on level 0, 16.25 N_l s on each coarser level), one FMG
@@ -240,13 +257,23 @@ def run_gpu(args):
     ms_fp64, _ = timed(lambda: res_holder.__setitem__("fp64", one_solve(fp64)), args.steps, args.warmup)
     st_fp64 = fp64.stats
 
-    # error of the mixed result against the plain FP64 solution (both mean-removed)
+    # errors against an FP64 multigrid solution driven past the tolerance (the FP64 solver here,
+    # bit-identical to the oracle's restatement and within 1e-15 of the reference's own device
+    # solver in the GPU tests), all mean-removed: max relative and relative L2
     x_mixed = mixed.pressure().copy_to_host()
     x_fp64 = fp64.pressure().copy_to_host()
-    xm, xd = interior(x_mixed, L).copy(), interior(x_fp64, L).copy()
-    xm -= xm.mean()
-    xd -= xd.mean()
-    err_vs_fp64 = float(np.abs(xm - xd).max() / np.abs(xd).max())
+    _capi.check(lib.ocu_grid_clear(fp64.pressure().handle, 0.0, sh))
+    ok_ref, res_ref = fp64.solve(1e-12 * rms_b, 40)
+    x_ref = interior(fp64.pressure().copy_to_host(), L).copy()
+    x_ref -= x_ref.mean()
+
+    def errs(x):
+        d = interior(x, L).copy()
+        d -= d.mean()
+        return (float(np.abs(d - x_ref).max() / np.abs(x_ref).max()),
+                float(np.linalg.norm(d - x_ref) / np.linalg.norm(x_ref)))
+
+    err_mixed, err_fp64 = errs(x_mixed), errs(x_fp64)
 
     # end to end through the public API with host buffers: H2D rhs, solve, D2H pressure
     def e2e_step():
@@ -258,29 +285,25 @@ def run_gpu(args):
     ms_e2e, _ = timed(e2e_step, max(1, args.steps // 2), 1)
     bytes_grid = int(L.allocated) * 8
 
-    # dominant kernel: the level-0 FP32 relaxation of the refinement solver's inner hierarchy, as
-    # the V-cycles issue it -- one two-colour TMA pass per iteration when the level qualifies
-    # (reads u and b, writes u: 3N values), else two colour launches (each 2N values: all of u,
-    # half of b, half of u written)
+    # dominant kernel: the level-0 colour sweep of the refinement solver's split FP32 hierarchy
+    # (k_chq_relax), launched as the V-cycles launch it: one colour reads the other colour's
+    # array and its own u and b and writes its own u -- 2N*4 bytes, N = 256^3
     iters = 20
-    mixed.relax(0, 2, 0, core=1)
+    mixed.relax(0, 2, 0, core=2)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     c0 = ocu.kernel_launch_count()
     e0.record(stream)
-    mixed.relax(0, iters, 0, core=1)
+    mixed.relax(0, iters, 0, core=2)
     e1.record(stream)
     torch.cuda.synchronize()
     per_iter = (ocu.kernel_launch_count() - c0) // iters
     ncell = n ** 3
-    if per_iter == 1:
-        kernel_name, alg_bytes = "k_relax_sweep2<float> level 0 (256^3)", 3.0 * ncell * 4
-    else:
-        kernel_name, alg_bytes = "k_relax_color_v4 (FP32 colour sweep) level 0 (256^3)", 2.0 * ncell * 4
+    kernel_name, alg_bytes = "k_chq_relax (FP32 split-layout colour sweep) level 0 (256^3)", 2.0 * ncell * 4
     sweep_ms = e0.elapsed_time(e1) / (iters * per_iter)
     achieved = alg_bytes / (sweep_ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profile_traffic("relax_sweep2_f32_256cube.md" if per_iter == 1 else "relax_color_f32_256cube.md")
+    traffic = profile_traffic("chq_relax_f32_256cube.md")
 
     secondary = {}
     if rank == 0 and not args.skip_secondary:
@@ -310,11 +333,15 @@ def run_gpu(args):
         "fp64_mg_ms": round(ms_fp64, 4),
         "speedup_mixed_vs_fp64": round(ms_fp64 / ms_mixed, 3),
         "mixed": {"outer_iterations": st_mixed.outer_iterations, "fp32_vcycles": st_mixed.vcycles,
-                  "rel_residual": res_holder["mixed"] / rms_b, "max_rel_err_vs_fp64_mg": err_vs_fp64,
-                  "alg_gbs": round(solve_alg_bytes(n, 4, st_mixed.vcycles, st_mixed.outer_iterations)
+                  "rel_residual": res_holder["mixed"] / rms_b,
+                  "max_rel_err_vs_fp64_reference": err_mixed[0], "rel_l2_err_vs_fp64_reference": err_mixed[1],
+                  "alg_gbs": round(ir_alg_bytes(n, args.ir_inner, st_mixed.outer_iterations)
                                    / (ms_mixed * 1e-3) / 1e9, 1)},
         "fp64": {"vcycles": st_fp64.vcycles, "rel_residual": res_holder["fp64"] / rms_b,
+                 "max_rel_err_vs_fp64_reference": err_fp64[0], "rel_l2_err_vs_fp64_reference": err_fp64[1],
                  "alg_gbs": round(solve_alg_bytes(n, 8, st_fp64.vcycles, 0) / (ms_fp64 * 1e-3) / 1e9, 1)},
+        "fp64_reference": {"solver": "FP64 multigrid of this library driven to 1e-12 relative",
+                           "rel_residual": res_ref / rms_b, "converged": bool(ok_ref)},
         "roofline": {"bound": "hbm", "kernel": kernel_name,
                      "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -581,6 +608,25 @@ def run_kernel_case(args):
     import torch
     import opencurrent_b200 as ocu
 
+    if args.kernel_case == "chequer":
+        # the refinement solver's split FP32 hierarchy at 256^3: colour sweeps of level 0, the
+        # residual + restriction into level 1, the prolongation back
+        n = N_CFG3
+        L = ocu.layout(n, n, n)
+        rhs = ocu.Grid3DDevice(ocu.F64)
+        rhs.init(n, n, n)
+        rhs.copy_from_host(padded(fourier_rhs(n), L, np.float64))
+        s = ocu.Sol_MultigridPressureMixed3DDeviceD("ir")
+        s.bc = ocu.BoundaryConditionSet(ocu.BoundaryCondition(ocu.BC_NEUMANN, 0.0))
+        s.initialize_storage(n, n, n, 1.0 / n, 1.0 / n, 1.0 / n, rhs)
+        s.relax(0, 2, 0, core=2)
+        s.restrict_residuals(0, 1, core=2)
+        s.prolong(1, 0, core=2)
+        s.synchronize()
+        torch.cuda.synchronize()
+        print(json.dumps({"kernel_case": "chequer", "grid": [n] * 3, "ok": True}), flush=True)
+        return
+
     if args.kernel_case == "flow":
         # two steps of the Rayleigh-Benard flow on a 256x256x128 FP32 grid (each field 33.5 MB,
         # a kernel reads 3-7 of them: more than L2 holds)
@@ -626,7 +672,7 @@ def main():
                     help="levels with at least this many cells use the two-colour TMA pass (0 = off)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-secondary", action="store_true")
-    ap.add_argument("--kernel-case", choices=["relax", "prolong", "restrict", "tail", "flow"],
+    ap.add_argument("--kernel-case", choices=["relax", "prolong", "restrict", "tail", "flow", "chequer"],
                     help="run a few launches of one kernel on the 256^3 FP32 hierarchy, or two "
                          "256x256x128 flow steps (profiling)")
     args = ap.parse_args()

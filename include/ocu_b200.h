@@ -173,6 +173,14 @@ typedef struct ocu_mg_params {
   int tail_ctas;                 /* CTAs (2..8) of the thread-block cluster that runs the tail
                                     kernel, its phases spread over them; 0 or 1 = one CTA
                                     (the default) */
+  int ir_inner_exact;            /* OCU_MG_MIXED_IR only: 0 (default) = the FP32 correction
+                                    solves run on red/black split colour arrays with fused
+                                    multiply-adds (this library's own inner solver, checked
+                                    against FP64 multigrid at the tolerance); 1 = they run on
+                                    the reference-layout kernels, bit-identical to the CPU
+                                    oracle's restatement.  Hierarchies the split solver does not
+                                    take (one level, an odd periodic axis, a coarsest level
+                                    larger than 48 KB of shared memory) always use the latter. */
 } ocu_mg_params;
 
 typedef struct ocu_mg_stats {
@@ -206,7 +214,9 @@ ocu_grid *ocu_mg_level_grid(ocu_mg *mg, char which, int level);
 ocu_status ocu_mg_get_stats(const ocu_mg *mg, ocu_mg_stats *stats);
 /* The level operations the cycle is built from (protected in the reference,
  * sol_mgpressure3d.h:76-80), exposed for testing and kernel timing.  core = 0 acts on the
- * interface precision, core = 1 on the FP32 hierarchy of a mixed solver.  They enqueue work and
+ * interface precision, core = 1 on the FP32 hierarchy of a mixed solver, core = 2 on the
+ * red/black split FP32 hierarchy of an OCU_MG_MIXED_IR solver (relax order 0 or 1; restriction
+ * into the next level without norms).  They enqueue work and
  * return without waiting, except restrict_residuals when a norm is requested. */
 /* relax(level, iterations, order): order 0 red-black, 1 black-red, 2 symmetric
  * (sol_mgpressure3ddev.cu:190-248). */

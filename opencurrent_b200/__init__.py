@@ -215,6 +215,7 @@ class _MGBase:
         self.sweep_cells = 0
         self.leg_cells = 0
         self.tail_ctas = 0
+        self.ir_inner_exact = False
         self._h = None
         self._rhs = None
 
@@ -231,6 +232,7 @@ class _MGBase:
         p.sweep_cells = int(self.sweep_cells)
         p.leg_cells = int(self.leg_cells)
         p.tail_ctas = int(self.tail_ctas)
+        p.ir_inner_exact = int(bool(self.ir_inner_exact))
         return p
 
     def initialize_storage(self, nx, ny, nz, hx, hy, hz, rhs):

@@ -357,7 +357,23 @@ static ocu_status pick_core(ocu_mg *mg, int core, int level, CoreOps **out) {
   return OCU_OK;
 }
 
+// core 2: the red/black split FP32 hierarchy of a refinement solver (ir_chequer.cu)
+static ocu_status pick_chequer(ocu_mg *mg, int level, ChequerMG **out) {
+  OCU_NOT_NULL(mg, "solver");
+  if (!mg->s.initialized) return fail(OCU_ERR_NOT_INITIALIZED, "[ERROR] level operation - not initialized");
+  if (!mg->s.chq) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] level operation - solver has no split FP32 hierarchy");
+  if (level < 0 || level >= mg->s.chq->levels()) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] level operation - bad level %d", level);
+  *out = mg->s.chq.get();
+  return OCU_OK;
+}
+
 ocu_status ocu_mg_relax(ocu_mg *mg, int core, int level, int iterations, int order) {
+  if (core == 2) {
+    ChequerMG *q;
+    OCU_TRY(pick_chequer(mg, level, &q));
+    if (iterations < 0 || order < 0 || order > 1) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] relax - bad arguments");
+    return q->relax_level(level, iterations, order == 1, mg->s.stream);
+  }
   CoreOps *c;
   OCU_TRY(pick_core(mg, core, level, &c));
   if (iterations < 0 || order < 0 || order > 2) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] relax - bad arguments");
@@ -365,12 +381,24 @@ ocu_status ocu_mg_relax(ocu_mg *mg, int core, int level, int iterations, int ord
 }
 
 ocu_status ocu_mg_relax_sweep(ocu_mg *mg, int core, int level, int color) {
+  if (core == 2) {
+    ChequerMG *q;
+    OCU_TRY(pick_chequer(mg, level, &q));
+    return q->sweep_level(level, color, mg->s.stream);
+  }
   CoreOps *c;
   OCU_TRY(pick_core(mg, core, level, &c));
   return c->relax_sweep(level, color & 1);
 }
 
 ocu_status ocu_mg_restrict_residuals(ocu_mg *mg, int core, int fine, int coarse, double *l2, double *linf) {
+  if (core == 2) {
+    ChequerMG *q;
+    OCU_TRY(pick_chequer(mg, fine, &q));
+    if (coarse != fine + 1 || coarse >= q->levels() || l2 || linf)
+      return fail(OCU_ERR_INVALID_VALUE, "[ERROR] restrict_residuals - the split hierarchy restricts into the next level, without norms");
+    return q->restrict_level(fine, mg->s.stream);
+  }
   CoreOps *c;
   OCU_TRY(pick_core(mg, core, fine, &c));
   if (coarse != fine && coarse != fine + 1) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] restrict_residuals - bad levels");
@@ -379,6 +407,12 @@ ocu_status ocu_mg_restrict_residuals(ocu_mg *mg, int core, int fine, int coarse,
 }
 
 ocu_status ocu_mg_prolong(ocu_mg *mg, int core, int coarse, int fine) {
+  if (core == 2) {
+    ChequerMG *q;
+    OCU_TRY(pick_chequer(mg, fine, &q));
+    if (coarse != fine + 1 || coarse >= q->levels()) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] prolong - bad levels");
+    return q->prolong_level(coarse, mg->s.stream);
+  }
   CoreOps *c;
   OCU_TRY(pick_core(mg, core, fine, &c));
   if (coarse != fine + 1 || coarse >= c->levels()) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] prolong - bad levels");

@@ -882,6 +882,7 @@ ocu_status MGSolver::mixed_warmstart_fmg(double tolerance, int max_iter, double 
 // a fixed FP32 FMG schedule (ir_inner_cycles fine-level cycles, homogeneous boundary values)
 // and update x += (double) e.  max_outer bounds the refinement steps.
 ocu_status MGSolver::ir_solve(double tolerance, int max_outer, double *rl2, double *rlinf) {
+  if (chq && prm.ir_inner_exact == 0) return ir_solve_chequer(tolerance, max_outer, rl2, rlinf);
   const int conv = prm.convergence;
   const ocu_layout &L = cd.lay[0];
   double l2 = 0, linf = 0;
@@ -912,6 +913,57 @@ ocu_status MGSolver::ir_solve(double tolerance, int max_outer, double *rl2, doub
     OCU_TRY(ir_residual(&l2, &linf));
     stats.outer_iterations = outer;
     stats.vcycles = total_inner;
+    *rl2 = l2; *rlinf = linf;
+    stats.last_l2 = l2; stats.last_linf = linf;
+    if (pick(conv, l2, linf) < tolerance) return OCU_OK;
+  }
+  return OCU_ERR_NOT_CONVERGED;
+}
+
+// The same refinement with the split-layout FP32 correction solver (ir_chequer.cu).  One
+// captured graph per refinement step: clear the correction, FMG ramp + ir_inner_cycles fine-level
+// V-cycles, x += e, the level-0 ghost refresh with the caller's boundary values, the FP64
+// residual (written as float into the correction's right-hand side) and its norms.  The host
+// waits once per step, for the norms.
+enum { SEG_CHQ_FIRST = 0, SEG_CHQ_STEP = 1 };
+
+ocu_status MGSolver::ir_chequer_residual_tail() {
+  const ocu_layout &L = cd.lay[0];
+  double *rows2 = (double *)cd.rows, *rowsinf = (double *)cd.rows + cd.rows_stride;
+  const long long nrows = (long long)L.nx * L.ny;
+  OCU_TRY(chq->enqueue_residual(cd.u0(0), cd.b0(0), L, cd.h[0], cd.fx, cd.fy, cd.fz, rows2, rowsinf, stream));
+  OCU_TRY(launch_fold_rows<double>(rows2, nrows, false, cd.red_scratch, cd.d_norms, stream));
+  OCU_TRY(launch_fold_rows<double>(rowsinf, nrows, true, cd.red_scratch, cd.d_norms + 1, stream));
+  return check_cuda(cudaMemcpyAsync(cd.h_norms, cd.d_norms, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream),
+                    "norm readback");
+}
+
+ocu_status MGSolver::ir_solve_chequer(double tolerance, int max_outer, double *rl2, double *rlinf) {
+  const int conv = prm.convergence;
+  double l2 = 0, linf = 0;
+  stats.outer_iterations = 0;
+  stats.vcycles = 0;
+  double_mode = true;
+  OCU_TRY(run_segment(chq.get(), SEG_CHQ_FIRST, [&]() -> ocu_status {
+    OCU_TRY(cd.apply_bc(0));
+    return ir_chequer_residual_tail();
+  }));
+  OCU_TRY(cd.finish_norms(0, &l2, &linf));
+  *rl2 = l2; *rlinf = linf;
+  stats.last_l2 = l2; stats.last_linf = linf;
+  if (pick(conv, l2, linf) < tolerance) return OCU_OK;
+  const int inner = prm.ir_inner_cycles > 0 ? prm.ir_inner_cycles : 4;
+  const int citers = coarse_iters();
+  for (int outer = 1; outer <= max_outer; outer++) {
+    OCU_TRY(run_segment(chq.get(), SEG_CHQ_STEP, [&]() -> ocu_status {
+      OCU_TRY(chq->enqueue_fmg(prm.nu1, prm.nu2, inner, citers, prm.nu1 + prm.nu2, stream));
+      OCU_TRY(chq->enqueue_add_correction(cd.u0(0), cd.lay[0], stream));
+      OCU_TRY(cd.apply_bc(0));
+      return ir_chequer_residual_tail();
+    }));
+    OCU_TRY(cd.finish_norms(0, &l2, &linf));
+    stats.outer_iterations = outer;
+    stats.vcycles = outer * inner;
     *rl2 = l2; *rlinf = linf;
     stats.last_l2 = l2; stats.last_linf = linf;
     if (pick(conv, l2, linf) < tolerance) return OCU_OK;
@@ -1024,6 +1076,10 @@ ocu_status MGSolver::initialize_storage(int nx, int ny, int nz, double hx, doubl
       if (kind == OCU_MG_MIXED_IR) bc_make_homogeneous(&fbc);
       OCU_TRY(cf.init(fbc, dis, nx, ny, nz, hx, hy, hz, rhs_f, pf, stream));
       cf.d_err = cd.d_err;  // one timeout word, read back with the FP64 norms
+      if (kind == OCU_MG_MIXED_IR && ChequerMG::suits(cd.dim, fbc)) {
+        chq.reset(new ChequerMG());
+        OCU_TRY(chq->init(cd.dim, cd.h, cd.fx, cd.fy, cd.fz, cd.omega, fbc));
+      }
     }
   }
   stats.num_levels = num_levels;

@@ -8,6 +8,7 @@
 #include <memory>
 #include <vector>
 
+#include "ir_chequer.h"
 #include "mg_fused.h"
 #include "ocu_internal.h"
 
@@ -163,6 +164,7 @@ struct MGSolver {
     }
   };
   std::unique_ptr<ocu_grid, GridDeleter> pressure_f;  // FP32 u0 of the mixed solvers
+  std::unique_ptr<ChequerMG> chq;  // split-layout FP32 correction solver (OCU_MG_MIXED_IR)
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;  // used when the caller's stream is the legacy NULL stream
   ocu_mg_stats stats{};
@@ -198,6 +200,8 @@ struct MGSolver {
   ocu_status ir_residual(double *l2, double *linf);
   ocu_status mixed_warmstart_fmg(double tol, int max_iter, double *l2, double *linf);
   ocu_status ir_solve(double tol, int max_outer, double *l2, double *linf);
+  ocu_status ir_solve_chequer(double tol, int max_outer, double *l2, double *linf);
+  ocu_status ir_chequer_residual_tail();
   ocu_status fmg_dispatch(double tol, int max_iter, double *l2, double *linf);
   ocu_status solve(double *residual, double tol, int max_iter);
   ocu_status run_vcycles(int count);
