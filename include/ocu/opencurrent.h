@@ -354,6 +354,40 @@ class Sol_ProjectDivergence3DDevice : public ErrorHandler {
 typedef Sol_ProjectDivergence3DDevice<float> Sol_ProjectDivergence3DDeviceF;
 typedef Sol_ProjectDivergence3DDevice<double> Sol_ProjectDivergence3DDeviceD;
 
+// Sol_ProjectDivergenceMixed3DDeviceD (sol_projectmixed3d.h:28-45): FP64 fields, mixed-precision
+// pressure solver.  As for Sol_MultigridPressureMixed3DDeviceD, the default pressure algorithm is
+// FP32 V-cycles inside FP64 iterative refinement; use_reference_algorithm() (before
+// initialize_storage) selects the reference's FP32 warm start + FP64 FMG.
+class Sol_ProjectDivergenceMixed3DDeviceD : public ErrorHandler {
+  ocu_project *_p = nullptr;
+  ocu_mg_kind _kind = OCU_MG_MIXED_IR;
+  Grid3DDevice<double> _div;
+ public:
+  BoundaryConditionSet bc;
+  Grid3DDevice<double> *u = nullptr, *v = nullptr, *w = nullptr;
+  ~Sol_ProjectDivergenceMixed3DDeviceD() { ocu_project_destroy(_p); }
+  void use_reference_algorithm(bool on = true) { _kind = on ? OCU_MG_MIXED_WARMSTART : OCU_MG_MIXED_IR; }
+  bool initialize_storage(int nx, int ny, int nz, double hx, double hy, double hz, Grid3DDevice<double> *u_,
+                          Grid3DDevice<double> *v_, Grid3DDevice<double> *w_) {
+    u = u_; v = v_; w = w_;
+    if (!_p && !check_ok(ocu_project_create_with(_kind, &_p))) return false;
+    ocu_bc_set s = bc.c();
+    ocu_project_set_stream(_p, detail::stream());
+    if (!check_ok(ocu_project_initialize_storage(_p, nx, ny, nz, hx, hy, hz, u->handle(), v->handle(), w->handle(), &s)))
+      return false;
+    _div.attach(ocu_project_divergence(_p));
+    return true;
+  }
+  bool solve(double tolerance = 1e-5) {
+    clear_error();
+    ocu_status st = ocu_project_solve(_p, tolerance);
+    if (st == OCU_ERR_NOT_CONVERGED) { add_error(); return false; }
+    return check_ok(st);
+  }
+  bool solve_divergence_only() { clear_error(); return check_ok(ocu_project_solve_divergence_only(_p)); }
+  Grid3DDevice<double> &divergence() { return _div; }
+};
+
 template <typename T>
 class Sol_SelfAdvection3DDevice : public ErrorHandler {
   int _nx = 0, _ny = 0, _nz = 0;

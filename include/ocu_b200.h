@@ -181,6 +181,13 @@ typedef struct ocu_mg_params {
                                     oracle's restatement.  Hierarchies the split solver does not
                                     take (one level, an odd periodic axis, a coarsest level
                                     larger than 48 KB of shared memory) always use the latter. */
+  int wait_limit;                /* polls of a bounded device wait (the two-colour TMA pass
+                                    waiting for its loads) before it gives up; the solve then
+                                    returns OCU_ERR_TIMEOUT and the next one starts clean.
+                                    0 = the default (about a second).  Negative: a test of that
+                                    path -- each launch of the pass first waits -wait_limit polls
+                                    on a barrier nothing completes, gives up before issuing any
+                                    load, and the solve reports OCU_ERR_TIMEOUT */
 } ocu_mg_params;
 
 typedef struct ocu_mg_stats {
@@ -307,6 +314,12 @@ ocu_status ocu_ens_autotune(ocu_ens *e, const double *tol, int max_iter);
 
 /* ---- projection (Sol_ProjectDivergence3DDevice<T>, sol_project3d.h:29-129) ------------- */
 ocu_status ocu_project_create(ocu_dtype dtype, ocu_project **out);
+/* The same with the pressure solver's kind chosen: OCU_MG_F32 / OCU_MG_F64 are
+ * Sol_ProjectDivergence3DDevice<float/double> (ocu_project_create); OCU_MG_MIXED_WARMSTART is
+ * Sol_ProjectDivergenceMixed3DDeviceD (sol_projectmixed3d.h:28-45, sol_projectmixed3d.cu:24-94:
+ * FP64 fields, the reference mixed pressure solver); OCU_MG_MIXED_IR is that class with this
+ * library's FP32-in-FP64 refinement solver instead.  The mixed kinds take FP64 grids. */
+ocu_status ocu_project_create_with(ocu_mg_kind pressure_kind, ocu_project **out);
 void ocu_project_destroy(ocu_project *p);
 ocu_status ocu_project_set_stream(ocu_project *p, ocu_stream s);
 /* initialize_storage (sol_project3ddev.cu:100-135): u,v,w borrowed MAC grids of one layout. */

@@ -216,6 +216,7 @@ class _MGBase:
         self.leg_cells = 0
         self.tail_ctas = 0
         self.ir_inner_exact = False
+        self.wait_limit = 0
         self._h = None
         self._rhs = None
 
@@ -233,6 +234,7 @@ class _MGBase:
         p.leg_cells = int(self.leg_cells)
         p.tail_ctas = int(self.tail_ctas)
         p.ir_inner_exact = int(bool(self.ir_inner_exact))
+        p.wait_limit = int(self.wait_limit)
         return p
 
     def initialize_storage(self, nx, ny, nz, hx, hy, hz, rhs):
@@ -428,11 +430,14 @@ class Sol_MultigridPressureMixed3DDeviceD(_MGBase):
 class Sol_ProjectDivergence3DDevice:
     """Sol_ProjectDivergence3DDevice<T> (ocuequation/sol_project3d.h:74-93)."""
 
-    def __init__(self, dtype=F32):
+    def __init__(self, dtype=F32, _kind=None):
         self.dtype = dtype
         self.bc = BoundaryConditionSet()
         h = C.c_void_p()
-        check(load().ocu_project_create(dtype, C.byref(h)))
+        if _kind is None:
+            check(load().ocu_project_create(dtype, C.byref(h)))
+        else:
+            check(load().ocu_project_create_with(_kind, C.byref(h)))
         self._h = h.value
         self._keep = None
 
@@ -469,6 +474,17 @@ class Sol_ProjectDivergence3DDevice:
                 self._h = None
         except Exception:
             pass
+
+
+class Sol_ProjectDivergenceMixed3DDeviceD(Sol_ProjectDivergence3DDevice):
+    """Sol_ProjectDivergenceMixed3DDeviceD (ocuequation/sol_projectmixed3d.h:28-45): FP64 fields,
+    mixed-precision pressure solver.  algorithm "warmstart" is the reference's mixed solver (FP32
+    FMG warm start + FP64 FMG); "ir" this library's FP32-in-FP64 refinement (the default, as for
+    Sol_MultigridPressureMixed3DDeviceD)."""
+
+    def __init__(self, algorithm="ir"):
+        kind = MG_MIXED_IR if algorithm == "ir" else MG_MIXED_WARMSTART
+        super().__init__(F64, _kind=kind)
 
 
 class _BorrowedMG(_MGBase):

@@ -55,7 +55,7 @@ class MGParams(C.Structure):
                 ("ir_inner_cycles", C.c_int), ("store_residual_grids", C.c_int),
                 ("unfused", C.c_int), ("tail_cells", C.c_int), ("sweep_cells", C.c_int),
                 ("leg_cells", C.c_int), ("tail_ctas", C.c_int),
-                ("ir_inner_exact", C.c_int)]
+                ("ir_inner_exact", C.c_int), ("wait_limit", C.c_int)]
 
 
 class MGStats(C.Structure):
@@ -144,6 +144,7 @@ SIGNATURES = {
     "ocu_ens_set_tuning": (I, [P, I, C.POINTER(EnsTuning)]),
     "ocu_ens_autotune": (I, [P, C.POINTER(D), I]),
     "ocu_project_create": (I, [I, PP]),
+    "ocu_project_create_with": (I, [I, PP]),
     "ocu_project_destroy": (None, [P]),
     "ocu_project_set_stream": (I, [P, P]),
     "ocu_project_initialize_storage": (I, [P, I, I, I, D, D, D, P, P, P, BP]),

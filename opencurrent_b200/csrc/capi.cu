@@ -431,12 +431,21 @@ ocu_status ocu_mg_get_stats(const ocu_mg *mg, ocu_mg_stats *stats) {
 }
 
 // ---- projection -----------------------------------------------------------------------------
-ocu_status ocu_project_create(ocu_dtype dtype, ocu_project **out) {
+ocu_status ocu_project_create_with(ocu_mg_kind kind, ocu_project **out) {
   OCU_NOT_NULL(out, "out");
+  *out = nullptr;
+  if (kind < OCU_MG_F32 || kind > OCU_MG_MIXED_WARMSTART)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] ocu_project_create_with - bad pressure solver kind");
   *out = new (std::nothrow) ocu_project();
   if (!*out) return fail(OCU_ERR_ALLOC, "[ERROR] ocu_project_create - out of host memory");
-  (*out)->s.dtype = dtype;
+  (*out)->s.dtype = kind == OCU_MG_F32 ? OCU_F32 : OCU_F64;
+  (*out)->s.mg_kind = kind;
   return OCU_OK;
+}
+
+ocu_status ocu_project_create(ocu_dtype dtype, ocu_project **out) {
+  if (dtype != OCU_F32 && dtype != OCU_F64) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] ocu_project_create - bad dtype");
+  return ocu_project_create_with(dtype == OCU_F64 ? OCU_MG_F64 : OCU_MG_F32, out);
 }
 
 void ocu_project_destroy(ocu_project *p) { delete p; }

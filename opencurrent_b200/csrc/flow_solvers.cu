@@ -31,7 +31,8 @@ ProjectSolver::~ProjectSolver() {
   if (divergence) { cudaFree(divergence->buf); delete divergence; }
 }
 
-// initialize_storage (sol_project3ddev.cu:100-135, initialize_device_storage :28-53)
+// initialize_storage (sol_project3ddev.cu:100-135, initialize_device_storage :28-53; the mixed
+// class, sol_projectmixed3d.cu:48-91, differs only in its pressure solver)
 ocu_status ProjectSolver::initialize_storage(int nx_, int ny_, int nz_, double hx_, double hy_, double hz_,
                                              ocu_grid *u_, ocu_grid *v_, ocu_grid *w_, const ocu_bc_set &bc_) {
   if (!u_ || !v_ || !w_) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_ProjectDivergence3DDevice::initialize_storage - null grid");
@@ -59,7 +60,7 @@ ocu_status ProjectSolver::initialize_storage(int nx_, int ny_, int nz_, double h
   divergence = new ocu_grid{dtype, Ld, nullptr, true};
   OCU_TRY(check_cuda(cudaMalloc(&divergence->buf, dtype_size(dtype) * Ld.allocated), "cudaMalloc(divergence)"));
   OCU_TRY(check_cuda(cudaMemset(divergence->buf, 0, dtype_size(dtype) * Ld.allocated), "cudaMemset(divergence)"));
-  mg = new ocu_mg(dtype == OCU_F64 ? OCU_MG_F64 : OCU_MG_F32, p);
+  mg = new ocu_mg(mg_kind >= 0 ? (ocu_mg_kind)mg_kind : (dtype == OCU_F64 ? OCU_MG_F64 : OCU_MG_F32), p);
   mg->s.set_stream(stream);
   OCU_TRY(mg->s.initialize_storage(nx, ny, nz, hx, hy, hz, divergence));
   if (!layout_match(u->L, mg->s.pressure->L))

@@ -7,6 +7,7 @@ namespace ocub {
 
 struct ProjectSolver {
   ocu_dtype dtype = OCU_F32;
+  int mg_kind = -1;  // pressure solver kind (ocu_mg_kind; -1: plain, of the fields' precision)
   ocu_bc_set bc{};
   int nx = 0, ny = 0, nz = 0;
   double hx = 0, hy = 0, hz = 0;

@@ -84,7 +84,21 @@ __device__ __forceinline__ void split_index(int t, int div, int sh, int &quot, i
 // colour row (one float4); the z neighbours are the other colour's entries m - 1 + p .. m + p
 // of the same row (p = row parity of this colour), the x and y neighbours its entries m of the
 // four neighbouring rows.
-__global__ void __launch_bounds__(256) k_chq_relax(ChqG g, ChqK k, ChqBC bc, int color) {
+// Launch shapes, measured at 256^3 with CUDA events on back-to-back launches: the colour sweep
+// in blocks of 128 (one iteration 49.9 us against 51.4 with 256 and 62.1 with 512 threads), the
+// restriction and the prolongation capped at 64 registers for four blocks of 256 per SM
+// (restriction 45.1 us against 49.0 at three blocks and 61.6 at two; prolongation 36.7 us
+// against 42.6 uncapped).
+#ifndef CHQ_RELAX_THREADS
+#define CHQ_RELAX_THREADS 128
+#endif
+#ifndef CHQ_RESTRICT_MINB
+#define CHQ_RESTRICT_MINB 4
+#endif
+#ifndef CHQ_PROLONG_MINB
+#define CHQ_PROLONG_MINB 4
+#endif
+__global__ void __launch_bounds__(CHQ_RELAX_THREADS) k_chq_relax(ChqG g, ChqK k, ChqBC bc, int color) {
   pdl_entry();
   const int qpr = g.rz >> 2;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -176,7 +190,7 @@ __device__ __forceinline__ void load4(const FRow &r, int m2, float v[4]) {
 // row (I, J)), restricted (the mean of each cell's eight) into the coarse right-hand side; the
 // coarse pair's u is zeroed (the next V-cycle leg starts from zero).  All lanes of a warp share
 // (I, J), so every row and boundary decision is uniform across the warp.
-__global__ void __launch_bounds__(256, 3) k_chq_restrict(ChqG f, ChqG c, ChqK k, ChqBC bc, int cm, int cmsh) {
+__global__ void __launch_bounds__(256, CHQ_RESTRICT_MINB) k_chq_restrict(ChqG f, ChqG c, ChqK k, ChqBC bc, int cm, int cmsh) {
   pdl_entry();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)c.nx * c.ny * cm) return;
@@ -260,7 +274,7 @@ __global__ void __launch_bounds__(256, 3) k_chq_restrict(ChqG f, ChqG c, ChqK k,
 // row (I, J)) into its sixteen children, added to the fine u.  Coarse values outside the domain
 // follow the homogeneous rules axis by axis (a corner is the product of the face signs times the
 // cell).  Rows are warp-uniform; the eight fine float2 pairs are loaded before the first store.
-__global__ void __launch_bounds__(256) k_chq_prolong(ChqG c, ChqG f, ChqBC bc, int cm, int cmsh) {
+__global__ void __launch_bounds__(256, CHQ_PROLONG_MINB) k_chq_prolong(ChqG c, ChqG f, ChqBC bc, int cm, int cmsh) {
   pdl_entry();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)c.nx * c.ny * cm) return;
@@ -368,14 +382,14 @@ struct ChqTail {
 };
 
 struct SG {
-  float *u[2], *b[2];
+  float *u0, *u1, *b0, *b1;
   int nx, ny, nz, rz, M, mlog, ylog, nzlog;
 };
 
 __device__ __forceinline__ SG sg_of(const SLv &l, float *sm) {
   const int n = l.nx * l.ny * l.rz;
   SG g;
-  g.u[0] = sm + l.off; g.u[1] = g.u[0] + n; g.b[0] = g.u[0] + 2 * n; g.b[1] = g.u[0] + 3 * n;
+  g.u0 = sm + l.off; g.u1 = g.u0 + n; g.b0 = g.u0 + 2 * n; g.b1 = g.u0 + 3 * n;
   g.nx = l.nx; g.ny = l.ny; g.nz = l.nz; g.rz = l.rz; g.M = (l.nz + 1) >> 1;
   g.mlog = l.mlog; g.ylog = l.ylog; g.nzlog = l.nzlog;
   return g;
@@ -388,40 +402,27 @@ __device__ __forceinline__ void dec(int q, int d, int lg, int &hi, int &lo) {
 
 // entry of cell (i, j, k) (inside the domain)
 __device__ __forceinline__ int s_id(const SG &g, int i, int j, int k) { return (i * g.ny + j) * g.rz + (k >> 1); }
-__device__ __forceinline__ float s_u(const SG &g, int i, int j, int k) { return g.u[(i + j + k) & 1][s_id(g, i, j, k)]; }
+// colour arrays by a run-time colour (selects: indexing a small array member with a run-time
+// value would put the struct in local memory)
+__device__ __forceinline__ float *s_ucol(const SG &g, int c) { return c ? g.u1 : g.u0; }
+__device__ __forceinline__ float *s_bcol(const SG &g, int c) { return c ? g.b1 : g.b0; }
 
-// value of cell (i, j, k), homogeneous rules applied axis by axis outside the domain (the
-// cell at (i0, j0, k0) is the one the ghost belongs to)
-__device__ __forceinline__ float s_at(const SG &g, const ChqBC &bc, int i, int j, int k, int i0, int j0, int k0) {
-  float sg = 1.f;
-  if (i < 0) { if (bc.px) i = g.nx - 1; else { i = i0; sg = bc.sxn; } }
-  else if (i >= g.nx) { if (bc.px) i = 0; else { i = i0; sg = bc.sxp; } }
-  if (j < 0) { if (bc.py) j = g.ny - 1; else { j = j0; sg *= bc.syn; } }
-  else if (j >= g.ny) { if (bc.py) j = 0; else { j = j0; sg *= bc.syp; } }
-  if (k < 0) { if (bc.pz) k = g.nz - 1; else { k = k0; sg *= bc.szn; } }
-  else if (k >= g.nz) { if (bc.pz) k = 0; else { k = k0; sg *= bc.szp; } }
-  return sg * s_u(g, i, j, k);
-}
 
-__device__ __forceinline__ bool s_inside(const SG &g, int i, int j, int k) {
-  return i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
-}
-
-__device__ __forceinline__ void s_sums(const SG &g, const ChqBC &bc, int i, int j, int k, float &sx, float &sy,
-                                       float &sz) {
-  if (s_inside(g, i, j, k)) {
-    const int xs = g.ny * g.rz, id = s_id(g, i, j, k);
-    const float *o = g.u[(i + j + k + 1) & 1];
-    const int p = (i + j + k) & 1 ? 1 : 0;  // cell k = 2m + p' of its colour; neighbours k -/+ 1
-    (void)p;
-    sx = o[id - xs] + o[id + xs];
-    sy = o[id - g.rz] + o[id + g.rz];
-    sz = o[((k - 1) >> 1) + (id - (k >> 1))] + o[((k + 1) >> 1) + (id - (k >> 1))];
-  } else {
-    sx = s_at(g, bc, i - 1, j, k, i, j, k) + s_at(g, bc, i + 1, j, k, i, j, k);
-    sy = s_at(g, bc, i, j - 1, k, i, j, k) + s_at(g, bc, i, j + 1, k, i, j, k);
-    sz = s_at(g, bc, i, j, k - 1, i, j, k) + s_at(g, bc, i, j, k + 1, i, j, k);
-  }
+// Neighbour sums of cell (i, j, k), whose entry in its colour array is id (the same entry of the
+// other colour's array o holds its x and y neighbours in the neighbouring rows); uv is its value.
+// Faces apply the homogeneous rules with selects (the same as the level kernels).
+__device__ __forceinline__ void s_sums(const SG &g, const ChqBC &bc, int i, int j, int k, int id, const float *o,
+                                       float uv, float &sx, float &sy, float &sz) {
+  const int xs = g.ny * g.rz, rs = id - (k >> 1);
+  const float xm = i > 0 ? o[id - xs] : (bc.px ? o[id + (g.nx - 1) * xs] : bc.sxn * uv);
+  const float xp = i < g.nx - 1 ? o[id + xs] : (bc.px ? o[id - (g.nx - 1) * xs] : bc.sxp * uv);
+  const float ym = j > 0 ? o[id - g.rz] : (bc.py ? o[id + (g.ny - 1) * g.rz] : bc.syn * uv);
+  const float yp = j < g.ny - 1 ? o[id + g.rz] : (bc.py ? o[id - (g.ny - 1) * g.rz] : bc.syp * uv);
+  const float zm = k > 0 ? o[rs + ((k - 1) >> 1)] : (bc.pz ? o[rs + ((g.nz - 1) >> 1)] : bc.szn * uv);
+  const float zp = k < g.nz - 1 ? o[rs + ((k + 1) >> 1)] : (bc.pz ? o[rs] : bc.szp * uv);
+  sx = xm + xp;
+  sy = ym + yp;
+  sz = zm + zp;
 }
 
 __device__ __forceinline__ float s_mod(const SG &g, const ChqBC &bc, int i, int j, int k) {
@@ -437,18 +438,19 @@ __device__ __forceinline__ float s_mod(const SG &g, const ChqBC &bc, int i, int 
 
 __device__ void s_relax(const SG &g, const ChqK &kk, const ChqBC &bc, int color) {
   const int cells = g.nx * g.ny * g.M;
-  float *u = g.u[color];
-  const float *b = g.b[color];
+  float *u = s_ucol(g, color);
+  const float *b = s_bcol(g, color), *o = s_ucol(g, color ^ 1);
   for (int q = threadIdx.x; q < cells; q += blockDim.x) {
     int row, m, i, j;
     dec(q, g.M, g.mlog, row, m);
     dec(row, g.ny, g.ylog, i, j);
     const int k = 2 * m + ((i + j + color) & 1);
     if (k >= g.nz) continue;
-    float sx, sy, sz;
-    s_sums(g, bc, i, j, k, sx, sy, sz);
     const int id = row * g.rz + m;
-    u[id] = relax_cell(u[id], b[id], sx, sy, sz, kk, s_mod(g, bc, i, j, k));
+    const float uv = u[id];
+    float sx, sy, sz;
+    s_sums(g, bc, i, j, k, id, o, uv, sx, sy, sz);
+    u[id] = relax_cell(uv, b[id], sx, sy, sz, kk, s_mod(g, bc, i, j, k));
   }
 }
 
@@ -459,10 +461,11 @@ __device__ void s_residual(const SG &g, const ChqK &kk, const ChqBC &bc, float *
     int row, k, i, j;
     dec(q, g.nz, g.nzlog, row, k);
     dec(row, g.ny, g.ylog, i, j);
-    float sx, sy, sz;
-    s_sums(g, bc, i, j, k, sx, sy, sz);
     const int col = (i + j + k) & 1, id = row * g.rz + (k >> 1);
-    (col ? r1 : r0)[id] = residual_cell(g.u[col][id], g.b[col][id], sx, sy, sz, kk);
+    const float uv = s_ucol(g, col)[id];
+    float sx, sy, sz;
+    s_sums(g, bc, i, j, k, id, s_ucol(g, col ^ 1), uv, sx, sy, sz);
+    (col ? r1 : r0)[id] = residual_cell(uv, s_bcol(g, col)[id], sx, sy, sz, kk);
   }
 }
 
@@ -483,9 +486,17 @@ __device__ void s_restrict_sum(const SG &f, const SG &c, const float *r0, const 
         sum += r0[id] + r1[id];
       }
     const int col = (I + J + K) & 1, cid = row * c.rz + (K >> 1);
-    c.b[col][cid] = 0.125f * sum;
-    c.u[col][cid] = 0.f;
+    s_bcol(c, col)[cid] = 0.125f * sum;
+    s_ucol(c, col)[cid] = 0.f;
   }
+}
+
+// the coarse neighbour index along one axis of a fine cell's parent, with the face rule's sign
+__device__ __forceinline__ int s_nbr(int I, int d, int n, bool per, float sneg, float spos, float &sg) {
+  const int I2 = I + d;
+  if (I2 < 0) { if (per) return n - 1; sg = sneg; return I; }
+  if (I2 >= n) { if (per) return 0; sg = spos; return I; }
+  return I2;
 }
 
 // trilinear prolongation into every fine cell
@@ -496,22 +507,17 @@ __device__ void s_prolong(const SG &c, const SG &f, const ChqBC &bc) {
     dec(q, f.nz, f.nzlog, row, k);
     dec(row, f.ny, f.ylog, i, j);
     const int I = i >> 1, J = j >> 1, K = k >> 1;
-    const int si = (i & 1) ? 1 : -1, sj = (j & 1) ? 1 : -1, sk = (k & 1) ? 1 : -1;
-    float c000, s1, s2, s3;
-    if (I + si >= 0 && I + si < c.nx && J + sj >= 0 && J + sj < c.ny && K + sk >= 0 && K + sk < c.nz) {
-      c000 = s_u(c, I, J, K);
-      s1 = s_u(c, I + si, J, K) + s_u(c, I, J + sj, K) + s_u(c, I, J, K + sk);
-      s2 = s_u(c, I + si, J + sj, K) + s_u(c, I + si, J, K + sk) + s_u(c, I, J + sj, K + sk);
-      s3 = s_u(c, I + si, J + sj, K + sk);
-    } else {
-      c000 = s_at(c, bc, I, J, K, I, J, K);
-      s1 = s_at(c, bc, I + si, J, K, I, J, K) + s_at(c, bc, I, J + sj, K, I, J, K) + s_at(c, bc, I, J, K + sk, I, J, K);
-      s2 = s_at(c, bc, I + si, J + sj, K, I, J, K) + s_at(c, bc, I + si, J, K + sk, I, J, K) +
-           s_at(c, bc, I, J + sj, K + sk, I, J, K);
-      s3 = s_at(c, bc, I + si, J + sj, K + sk, I, J, K);
-    }
+    float gx = 1.f, gy = 1.f, gz = 1.f;
+    const int I2 = s_nbr(I, (i & 1) ? 1 : -1, c.nx, bc.px, bc.sxn, bc.sxp, gx);
+    const int J2 = s_nbr(J, (j & 1) ? 1 : -1, c.ny, bc.py, bc.syn, bc.syp, gy);
+    const int K2 = s_nbr(K, (k & 1) ? 1 : -1, c.nz, bc.pz, bc.szn, bc.szp, gz);
+    auto cv = [&](int x, int y, int z) { return s_ucol(c, (x + y + z) & 1)[(x * c.ny + y) * c.rz + (z >> 1)]; };
+    const float c000 = cv(I, J, K);
+    const float s1 = gx * cv(I2, J, K) + gy * cv(I, J2, K) + gz * cv(I, J, K2);
+    const float s2 = gx * gy * cv(I2, J2, K) + gx * gz * cv(I2, J, K2) + gy * gz * cv(I, J2, K2);
+    const float s3 = gx * gy * gz * cv(I2, J2, K2);
     const float v = __fmaf_rn(27.f, c000, __fmaf_rn(9.f, s1, __fmaf_rn(3.f, s2, s3)));
-    float *u = f.u[(i + j + k) & 1];
+    float *u = s_ucol(f, (i + j + k) & 1);
     const int id = row * f.rz + (k >> 1);
     u[id] = __fmaf_rn(v, 0.015625f, u[id]);
   }
@@ -525,34 +531,44 @@ __device__ void s_relax_iters(const SG &g, const ChqK &kk, const ChqBC &bc, int 
     }
 }
 
-__device__ void s_restrict(const ChqTail &T, float *sm, int l) {
-  const SG f = sg_of(T.lv[l], sm), c = sg_of(T.lv[l + 1], sm);
+// The phases read the level table from shared memory (a copy of the launch parameters made
+// with constant indices: indexing the parameter array with a run-time level would give every
+// thread a local-memory copy of it).
+__device__ void s_restrict(const ChqTail &T, const SLv *lv, float *sm, int l) {
+  const SG f = sg_of(lv[l], sm), c = sg_of(lv[l + 1], sm);
   float *r0 = sm + T.scratch, *r1 = r0 + f.nx * f.ny * f.rz;
-  s_residual(f, T.lv[l].k, T.bc, r0, r1);
+  s_residual(f, lv[l].k, T.bc, r0, r1);
   __syncthreads();
   s_restrict_sum(f, c, r0, r1);
   __syncthreads();
 }
 
 // one V-cycle from tail level a (0-based within the tail)
-__device__ void s_vcycle(const ChqTail &T, float *sm, int a) {
+__device__ void s_vcycle(const ChqTail &T, const SLv *lv, float *sm, int a) {
   const int last = T.nlev - 1;
   for (int l = a; l < last; l++) {
-    s_relax_iters(sg_of(T.lv[l], sm), T.lv[l].k, T.bc, T.nu1);
-    s_restrict(T, sm, l);
+    s_relax_iters(sg_of(lv[l], sm), lv[l].k, T.bc, T.nu1);
+    s_restrict(T, lv, sm, l);
   }
-  s_relax_iters(sg_of(T.lv[last], sm), T.lv[last].k, T.bc, T.citers);
+  s_relax_iters(sg_of(lv[last], sm), lv[last].k, T.bc, T.citers);
   for (int l = last - 1; l >= a; l--) {
-    s_prolong(sg_of(T.lv[l + 1], sm), sg_of(T.lv[l], sm), T.bc);
+    s_prolong(sg_of(lv[l + 1], sm), sg_of(lv[l], sm), T.bc);
     __syncthreads();
-    if (!(l == 0 && T.level0)) s_relax_iters(sg_of(T.lv[l], sm), T.lv[l].k, T.bc, T.nu2);
+    if (!(l == 0 && T.level0)) s_relax_iters(sg_of(lv[l], sm), lv[l].k, T.bc, T.nu2);
   }
 }
 
 __global__ void __launch_bounds__(1024) k_chq_tail(ChqTail T) {
   pdl_entry();
   extern __shared__ float sm[];
-  const SLv &L0 = T.lv[0];
+  __shared__ SLv lv[kChqMaxTail];
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int l = 0; l < kChqMaxTail; l++)
+      if (l < T.nlev) lv[l] = T.lv[l];
+  }
+  __syncthreads();
+  const SLv &L0 = lv[0];
   const int n0 = L0.nx * L0.ny * L0.rz;
   float *g0 = sm + L0.off;
   for (int q = threadIdx.x; q < n0; q += blockDim.x) {
@@ -563,21 +579,21 @@ __global__ void __launch_bounds__(1024) k_chq_tail(ChqTail T) {
   }
   // the coarser levels (their padding entries stay zero)
   for (int l = 1; l < T.nlev; l++) {
-    const int n = 4 * T.lv[l].nx * T.lv[l].ny * T.lv[l].rz;
-    for (int q = threadIdx.x; q < n; q += blockDim.x) sm[T.lv[l].off + q] = 0.f;
+    const int n = 4 * lv[l].nx * lv[l].ny * lv[l].rz;
+    for (int q = threadIdx.x; q < n; q += blockDim.x) sm[lv[l].off + q] = 0.f;
   }
   __syncthreads();
   if (T.fmg) {
-    for (int l = 0; l < T.nlev - 1; l++) s_restrict(T, sm, l);
+    for (int l = 0; l < T.nlev - 1; l++) s_restrict(T, lv, sm, l);
     const int last = T.nlev - 1;
-    s_relax_iters(sg_of(T.lv[last], sm), T.lv[last].k, T.bc, T.citers);
+    s_relax_iters(sg_of(lv[last], sm), lv[last].k, T.bc, T.citers);
     for (int f = last - 1; f >= 0; f--) {
-      s_prolong(sg_of(T.lv[f + 1], sm), sg_of(T.lv[f], sm), T.bc);
+      s_prolong(sg_of(lv[f + 1], sm), sg_of(lv[f], sm), T.bc);
       __syncthreads();
-      s_vcycle(T, sm, f);
+      s_vcycle(T, lv, sm, f);
     }
   } else {
-    s_vcycle(T, sm, 0);
+    s_vcycle(T, lv, sm, 0);
   }
   for (int q = threadIdx.x; q < n0; q += blockDim.x) {
     L0.gu0[q] = g0[q];
@@ -701,10 +717,10 @@ static size_t scratch_smem(const std::array<int, 3> &d) { return level_smem(d) /
 // Largest shared-memory footprint of the tail kernel (opt-in above 48 KB).
 constexpr size_t kTailSmemCap = 200 * 1024;
 // Levels with at most this many cells join the single-CTA tail (OCU_B200_CHQ_TAIL overrides;
-// the coarsest level always runs there).  Only the coarsest by default: measured at 256^3, a
-// refinement solve takes 4.54 ms with the 4^3 level alone in the tail, 4.81 ms with 8^3 and
-// 5.02 ms with 16^3 -- a shared-memory phase over those levels costs more than a launch.
-constexpr long long kChqTailCells = 0;
+// the coarsest level always runs there).  Measured at 256^3 (refinement solve, one box): 3.82 ms
+// with only the coarsest level (4^3) in the tail, 3.75 ms with 8^3 too, 3.78 ms with 16^3 too --
+// a tail phase over a 16^3 level costs about what a launch with programmatic dependencies does.
+constexpr long long kChqTailCells = 512;
 
 static long long tail_cells_setting() {
   const char *e = std::getenv("OCU_B200_CHQ_TAIL");
@@ -799,10 +815,10 @@ ocu_status ChequerMG::relax(int l, int iterations, bool reverse, cudaStream_t s)
   const ChqK k = make_k(L.h, fx, fy, fz, omega);
   const ChqBC b = make_bc(bc, fx, fy, fz);
   const long long threads = (long long)L.nx * L.ny * (L.rz / 4);
-  const int blocks = (int)((threads + 255) / 256);
+  const int blocks = (int)((threads + CHQ_RELAX_THREADS - 1) / CHQ_RELAX_THREADS);
   for (int it = 0; it < iterations; it++)
     for (int h = 0; h < 2; h++) {
-      launch_pdl(k_chq_relax, dim3(blocks), dim3(256), 0, s, g, k, b, reverse ? 1 - h : h);
+      launch_pdl(k_chq_relax, dim3(blocks), dim3(CHQ_RELAX_THREADS), 0, s, g, k, b, reverse ? 1 - h : h);
       OCU_TRY(check_launch("k_chq_relax"));
     }
   return OCU_OK;

@@ -50,7 +50,8 @@ struct SweepTile {
   static constexpr int NU = 4 + D;                     // u plane buffers (s-1 .. s+2, + D)
   static constexpr int NB = 2 + D;                     // b plane buffers (s, s+1, + D)
   static constexpr int THREADS = 256;
-  // plane buffers, then NU mbarriers and the abort word; +128 to align the base by hand
+  // plane buffers, then NU mbarriers, the abort word (8 bytes) and the barrier of the
+  // timeout test (8 bytes); +128 to align the base by hand
   static constexpr size_t SMEM = (size_t)(NU + NB) * PLANE * sizeof(T) + NU * sizeof(unsigned long long) + 16 + 128;
   static_assert((PLANE * sizeof(T)) % 128 == 0, "TMA destinations stay 128-byte aligned");
 };
@@ -100,6 +101,8 @@ struct SweepArgs {
   int first_color;    // colour updated first (0 = red)
   int ntk;            // tiles along k
   long long steps;    // tiles * nx (plane steps of the whole level)
+  int wait_limit;     // polls of a load wait before the launch gives up (kWaitLimit by default)
+  int stall_test;     // testing the timeout path: first wait on a barrier nothing completes
 };
 
 // One relax update from shared memory at offset o of the current plane buffer.  `inner`: the
@@ -128,6 +131,7 @@ __global__ void __launch_bounds__(SweepTile<T>::THREADS, 3) k_relax_sweep2(
   T *bs = us + S::NU * S::PLANE;
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(bs + S::NB * S::PLANE);
   int &abort_flag = *reinterpret_cast<int *>(bar + S::NU);
+  unsigned long long *stall_bar = bar + S::NU + 1;  // never arrived at: only the timeout test waits on it
 
   const int cA = a.first_color, cB = !a.first_color;
   const unsigned bytes = (unsigned)(S::PLANE * sizeof(T));
@@ -136,11 +140,22 @@ __global__ void __launch_bounds__(SweepTile<T>::THREADS, 3) k_relax_sweep2(
   if (threadIdx.x == 0) {
     abort_flag = 0;
     for (int q = 0; q < S::NU; q++) mbar_init(&bar[q], 1);
+    mbar_init(stall_bar, 1);
     mbar_init_fence();
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&tm_u)) : "memory");
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<unsigned long long>(&tm_b)) : "memory");
   }
   __syncthreads();
+  if (a.stall_test) {
+    // the timeout path without a fault: a wait that nothing completes runs out of polls before
+    // any load is issued, so the CTA has nothing in flight when it returns
+    if (threadIdx.x == 0 && !mbar_wait_bounded(stall_bar, 0u, a.wait_limit)) {
+      atomicOr(err, 1);
+      abort_flag = 1;
+    }
+    __syncthreads();
+    if (abort_flag) return;
+  }
 
   int gbase = 0;   // loads are numbered across this CTA's runs: slot = g % NU (u), g % NB (b)
   int issued = 0;  // (thread 0) loads issued in the current run
@@ -178,11 +193,12 @@ __global__ void __launch_bounds__(SweepTile<T>::THREADS, 3) k_relax_sweep2(
         // loads 0..n+2 must have landed (step 0 also needs loads 0 and 1)
         for (int m = (n == 0 ? 0 : n + 2); m <= n + 2; m++) {
           const int g = gbase + m;
-          if (!mbar_wait_bounded(&bar[g % S::NU], (unsigned)((g / S::NU) & 1), kWaitLimit)) {
+          if (!mbar_wait_bounded(&bar[g % S::NU], (unsigned)((g / S::NU) & 1), a.wait_limit)) {
             atomicOr(err, 1);
             abort_flag = 1;
-            // let the copies already issued land before the CTA's shared memory goes away
-            for (int q = m + 1; q < issued; q++)
+            // let the copies already issued -- the one waited for included -- land before the
+            // CTA's shared memory goes away (each wait again bounded, by the default limit)
+            for (int q = m; q < issued; q++)
               mbar_wait_bounded(&bar[(gbase + q) % S::NU], (unsigned)(((gbase + q) / S::NU) & 1), kWaitLimit);
             break;
           }
@@ -349,7 +365,7 @@ static ocu_status sweep_slots(int *slots) {
 template <typename T>
 ocu_status launch_relax_sweep2(const SweepTmap &tm_u_in, const SweepTmap &tm_b, T *u_out, const ocu_layout &L,
                                const T *diag, int first_color, const RelaxParams &p, double hx, double hy, double hz,
-                               int *err, cudaStream_t s) {
+                               int *err, cudaStream_t s, int wait_limit) {
   using S = SweepTile<T>;
   int slots = 0;
   OCU_TRY(sweep_slots<T>(&slots));
@@ -360,6 +376,8 @@ ocu_status launch_relax_sweep2(const SweepTmap &tm_u_in, const SweepTmap &tm_b, 
   a.ntk = (L.nz + S::TK - 1) / S::TK;
   const int ntj = (L.ny + S::TJ - 1) / S::TJ;
   a.steps = (long long)a.ntk * ntj * L.nx;
+  a.stall_test = wait_limit < 0;
+  a.wait_limit = wait_limit < 0 ? -wait_limit : (wait_limit > 0 ? wait_limit : kWaitLimit);
   // one wave of resident CTAs, at least 8 plane steps each
   long long grid = a.steps / 8;
   if (grid > slots) grid = slots;
@@ -378,9 +396,9 @@ template ocu_status make_sweep_tmap<float>(const void *, const ocu_layout &, Swe
 template ocu_status make_sweep_tmap<double>(const void *, const ocu_layout &, SweepTmap *);
 template ocu_status launch_relax_sweep2<float>(const SweepTmap &, const SweepTmap &, float *, const ocu_layout &,
                                                const float *, int, const RelaxParams &, double, double, double, int *,
-                                               cudaStream_t);
+                                               cudaStream_t, int);
 template ocu_status launch_relax_sweep2<double>(const SweepTmap &, const SweepTmap &, double *, const ocu_layout &,
                                                 const double *, int, const RelaxParams &, double, double, double,
-                                                int *, cudaStream_t);
+                                                int *, cudaStream_t, int);
 
 }  // namespace ocub

@@ -331,13 +331,14 @@ struct alignas(64) SweepTmap {
 };
 // Two-colour sweep (kernels_relax_tma.cu): supported layouts/BCs, the tensor map of one grid
 // buffer, and the launch u_in (through its map) -> u_out.  err: device word set to 1 when a
-// bounded wait inside the kernel gives up.
+// bounded wait inside the kernel gives up; wait_limit: polls before a wait gives up (0 = the
+// default, about a second; negative = the timeout test, see ocu_mg_params.wait_limit).
 bool sweep2_supported(const ocu_layout &L, const ocu_bc_set &bc);
 template <typename T>
 ocu_status make_sweep_tmap(const void *buf, const ocu_layout &L, SweepTmap *out);
 template <typename T>
 ocu_status launch_relax_sweep2(const SweepTmap &tm_u_in, const SweepTmap &tm_b, T *u_out, const ocu_layout &L,
                                const T *diag, int first_color, const RelaxParams &p, double hx, double hy, double hz,
-                               int *err, cudaStream_t s);
+                               int *err, cudaStream_t s, int wait_limit = 0);
 
 }  // namespace ocub

@@ -359,9 +359,9 @@ ocu_status MGCore<T>::relax_pairs(int level, int iterations, int order) {
   int it = 0;
   for (; it + 1 < iterations; it += 2) {
     OCU_TRY(launch_relax_sweep2<T>(tm_u[level], tm_b[level], origin<T>(grids_u2[level]), lay[level], dg, first(it), p,
-                                   hx(level), hy(level), hz(level), d_err, stream));
+                                   hx(level), hy(level), hz(level), d_err, stream, wait_limit));
     OCU_TRY(launch_relax_sweep2<T>(tm_u2[level], tm_b[level], u0(level), lay[level], dg, first(it + 1), p, hx(level),
-                                   hy(level), hz(level), d_err, stream));
+                                   hy(level), hz(level), d_err, stream, wait_limit));
   }
   for (; it < iterations; it++)
     for (int rb = 0; rb < 2; rb++)
@@ -1098,6 +1098,7 @@ ocu_status MGSolver::apply_knobs() {
   if (cd.sweep_cells > 0 && cd.num_levels > 0) OCU_TRY(cd.ensure_sweep_buffers());
   cf.leg_cells = cd.leg_cells = prm.leg_cells <= 0 ? kDefaultLegCells : prm.leg_cells;
   cf.tail_ctas = cd.tail_ctas = prm.tail_ctas <= 0 ? kDefaultTailCtas : (prm.tail_ctas > 8 ? 8 : prm.tail_ctas);
+  cf.wait_limit = cd.wait_limit = prm.wait_limit;
   if (cf.leg_cells > 0 && cf.num_levels > 0) OCU_TRY(cf.ensure_leg_buffers());
   if (cd.leg_cells > 0 && cd.num_levels > 0) OCU_TRY(cd.ensure_leg_buffers());
   return OCU_OK;

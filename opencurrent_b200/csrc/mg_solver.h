@@ -100,6 +100,7 @@ struct MGCore : CoreOps {
   std::vector<ocu_grid *> grids_u2;
   std::vector<SweepTmap> tm_u, tm_u2, tm_b;
   int *d_err = nullptr;           // set by kernels whose bounded waits gave up (inside d_norms)
+  int wait_limit = 0;             // polls of such a wait before it gives up (0 = the default)
 
   ~MGCore();
   ocu_status clear_level(int level) override;

@@ -532,12 +532,16 @@ static ocu_bc orc_convert_bc(const ocu_bc *b)
   return r;
 }
 
-orc_project *orc_project_create(int dtype, const ocu_bc_set *bc, int nx, int ny, int nz,
-                                double hx, double hy, double hz, void *u, void *v, void *w,
-                                const ocu_layout *Lm)
+/* kind: 0 = Sol_ProjectDivergence3DDevice<float>, 1 = <double>, 2 =
+ * Sol_ProjectDivergenceMixed3DDeviceD (the reference mixed pressure solver,
+ * sol_projectmixed3d.cu:48-91), 3 = the same with the FP32-in-FP64 refinement solver. */
+orc_project *orc_project_create_kind(int kind, const ocu_bc_set *bc, int nx, int ny, int nz,
+                                     double hx, double hy, double hz, void *u, void *v, void *w,
+                                     const ocu_layout *Lm, int inner_cycles)
 {
   orc_project *p = (orc_project *)calloc(1, sizeof(orc_project));
   orc_mg_params prm;
+  const int dtype = kind == 0 ? OCU_F32 : OCU_F64;
   size_t es = dtype == OCU_F64 ? 8 : 4;
   p->dtype = dtype; p->bc = *bc;
   p->nx = nx; p->ny = ny; p->nz = nz; p->hx = hx; p->hy = hy; p->hz = hz;
@@ -550,8 +554,20 @@ orc_project *orc_project_create(int dtype, const ocu_bc_set *bc, int nx, int ny,
   prm.bc.zneg = orc_convert_bc(&bc->zneg); prm.bc.zpos = orc_convert_bc(&bc->zpos);
   prm.nu1 = 2; prm.nu2 = 2;
   prm.convergence = OCU_CONVERGENCE_LINF;
-  p->mg = orc_mg_create(dtype, &prm, nx, ny, nz, hx, hy, hz, p->div, &p->Ldiv);
+  if (kind == 2)
+    p->mg = orc_mgmixed_create(&prm, nx, ny, nz, hx, hy, hz, (double *)p->div, &p->Ldiv);
+  else if (kind == 3)
+    p->mg = orc_mgir_create(&prm, nx, ny, nz, hx, hy, hz, (double *)p->div, &p->Ldiv, inner_cycles);
+  else
+    p->mg = orc_mg_create(dtype, &prm, nx, ny, nz, hx, hy, hz, p->div, &p->Ldiv);
   return p;
+}
+
+orc_project *orc_project_create(int dtype, const ocu_bc_set *bc, int nx, int ny, int nz,
+                                double hx, double hy, double hz, void *u, void *v, void *w,
+                                const ocu_layout *Lm)
+{
+  return orc_project_create_kind(dtype == OCU_F64 ? 1 : 0, bc, nx, ny, nz, hx, hy, hz, u, v, w, Lm, 4);
 }
 
 void orc_project_destroy(orc_project *p)

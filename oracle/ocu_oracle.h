@@ -120,6 +120,12 @@ typedef struct orc_project orc_project;
 orc_project *orc_project_create(int dtype, const ocu_bc_set *bc, int nx, int ny, int nz,
                                 double hx, double hy, double hz, void *u, void *v, void *w,
                                 const ocu_layout *mac_layout);
+/* kind 0/1: FP32/FP64; 2: Sol_ProjectDivergenceMixed3DDeviceD (reference mixed pressure
+ * solver, sol_projectmixed3d.cu:48-91); 3: the same class with the FP32-in-FP64 refinement
+ * solver (inner_cycles per correction).  Kinds 2 and 3 take double grids. */
+orc_project *orc_project_create_kind(int kind, const ocu_bc_set *bc, int nx, int ny, int nz,
+                                     double hx, double hy, double hz, void *u, void *v, void *w,
+                                     const ocu_layout *mac_layout, int inner_cycles);
 void orc_project_destroy(orc_project *p);
 int orc_project_solve(orc_project *p, double tolerance);
 int orc_project_solve_divergence_only(orc_project *p);

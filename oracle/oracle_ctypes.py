@@ -113,6 +113,8 @@ def _setup(L):
     L.orc_mg_omega.restype = d
     L.orc_project_create.argtypes = [i, BP, i, i, i, d, d, d, P, P, P, LP]
     L.orc_project_create.restype = P
+    L.orc_project_create_kind.argtypes = [i, BP, i, i, i, d, d, d, P, P, P, LP, i]
+    L.orc_project_create_kind.restype = P
     L.orc_project_destroy.argtypes = [P]
     L.orc_project_solve.argtypes = [P, d]
     L.orc_project_solve_divergence_only.argtypes = [P]

@@ -125,6 +125,85 @@ static void projection() {
   CHECK(max_div <= 2e-4f);
 }
 
+// projectdoubletest.cpp-style check of the mixed class: max |div| <= 1e-10 after an FP64
+// projection with the mixed pressure solver, both algorithms
+static void projection_mixed(bool reference_algorithm) {
+  const int nx = 32, ny = 32, nz = 32;
+  const double hx = 1.0 / nx, hy = 1.0 / ny, hz = 1.0 / nz;
+  Grid3DDeviceD u, v, w;
+  REQUIRE(u.init(nx + 1, ny, nz, 1, 1, 1, 0, 1, 1));
+  REQUIRE(v.init(nx, ny + 1, nz, 1, 1, 1, 1, 0, 1));
+  REQUIRE(w.init(nx, ny, nz + 1, 1, 1, 1, 1, 1, 0));
+  Grid3DHostD hu, hv, hw;
+  hu.init_congruent(u);
+  hv.init_congruent(v);
+  hw.init_congruent(w);
+  for (int i = 0; i < nx; i++)
+    for (int j = 0; j < ny; j++)
+      for (int k = 0; k < nz; k++) {
+        hu.at(i, j, k) = std::sin(((double)k) / nz * 4 * M_PI) + std::cos(((double)j) / ny * 2 * M_PI);
+        hv.at(i, j, k) = std::sin(((double)i) / nx * 6 * M_PI);
+        hw.at(i, j, k) = std::cos(((double)j) / ny * 8 * M_PI) * std::sin(((double)i) / nx * 2 * M_PI);
+      }
+  CHECK(u.copy_all_data(hu));
+  CHECK(v.copy_all_data(hv));
+  CHECK(w.copy_all_data(hw));
+  Sol_ProjectDivergenceMixed3DDeviceD project;
+  if (reference_algorithm) project.use_reference_algorithm();
+  BoundaryCondition closed;
+  closed.type = BC_FORCED_INFLOW_VARIABLE_SLIP;
+  project.bc = BoundaryConditionSet(closed);
+  CHECK(project.initialize_storage(nx, ny, nz, hx, hy, hz, &u, &v, &w));
+  CHECK(project.solve(1e-10));
+  CHECK(project.solve_divergence_only());
+  double max_div = 1;
+  CHECK(project.divergence().reduce_maxabs(max_div));
+  CHECK(max_div <= 1e-10);
+}
+
+// failure paths through the facade: max_iter exhausted (false, the reference's sticky error
+// stays clear on the solver, as Sol_MultigridPressure3DBase::solve sets none), a projection whose
+// pressure solve fails (false, any_error() set), both usable afterwards
+static void failure_paths() {
+  const int n = 32;
+  Grid3DDeviceF rhs;
+  REQUIRE(rhs.init(n, n, n, 1, 1, 1));
+  Grid3DHostF h;
+  h.init_congruent(rhs);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+      for (int k = 0; k < n; k++) h.at(i, j, k) = std::cos(M_PI * (i + .5) / n) * std::cos(2 * M_PI * (k + .5) / n);
+  CHECK(rhs.copy_all_data(h));
+  Sol_MultigridPressure3DDeviceF solver;
+  BoundaryCondition neumann;
+  neumann.type = BC_NEUMANN;
+  solver.bc = BoundaryConditionSet(neumann);
+  REQUIRE(solver.initialize_storage(n, n, n, 1.0 / n, 1.0 / n, 1.0 / n, &rhs));
+  double residual = 0;
+  CHECK(!solver.solve(residual, 1e-30, 2));
+  CHECK(std::isfinite(residual) && residual > 0);
+  CHECK(!solver.any_error());
+  CHECK(solver.solve(residual, 1e-4, 20));
+
+  const int nx = 16, ny = 16, nz = 16;
+  Grid3DDeviceF u, v, w;
+  REQUIRE(u.init(nx + 1, ny, nz, 1, 1, 1, 0, 1, 1));
+  REQUIRE(v.init(nx, ny + 1, nz, 1, 1, 1, 1, 0, 1));
+  REQUIRE(w.init(nx, ny, nz + 1, 1, 1, 1, 1, 1, 0));
+  u.clear(1.0f);
+  v.clear(-0.5f);
+  w.clear(0.25f);
+  Sol_ProjectDivergence3DDeviceF project;
+  BoundaryCondition closed;
+  closed.type = BC_FORCED_INFLOW_VARIABLE_SLIP;
+  project.bc = BoundaryConditionSet(closed);
+  CHECK(project.initialize_storage(nx, ny, nz, 1.0 / nx, 1.0 / ny, 1.0 / nz, &u, &v, &w));
+  CHECK(!project.solve(1e-30));
+  CHECK(project.any_error());
+  CHECK(project.solve(1e-3));
+  CHECK(!project.any_error());
+}
+
 static void ns_smoke() {
   Eqn_IncompressibleNS3DParamsD params;
   params.init_grids(32, 32, 16);
@@ -166,6 +245,9 @@ int main() {
   all_dirichlet(0.5);
   neumann_fp32();
   projection();
+  projection_mixed(false);
+  projection_mixed(true);
+  failure_paths();
   ns_smoke();
   if (failures) {
     std::printf("FACADE FAILED (%d)\n", failures);
