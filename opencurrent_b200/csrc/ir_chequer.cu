@@ -607,6 +607,7 @@ struct OuterCoef {
   double fxh, fyh, fzh, dg;
 };
 
+template <bool VEC>
 __global__ void __launch_bounds__(256) k_chq_outer_residual(const double *__restrict__ x, const double *__restrict__ b,
                                                             long long xs, long long ys, int nx, int ny, int nz,
                                                             OuterCoef c, float *__restrict__ B0,
@@ -625,6 +626,20 @@ __global__ void __launch_bounds__(256) k_chq_outer_residual(const double *__rest
   float *__restrict__ Bo = s ? B0 : B1;
   double acc2 = 0, accinf = 0;
   for (int m = lane; 2 * m < nz; m += 32) {
+    if (VEC) {  // nz even, rows on 16-byte boundaries: the pair and its neighbours as double2
+      const long long id = row + 2 * m;
+      const double2 X = *reinterpret_cast<const double2 *>(x + id), B = *reinterpret_cast<const double2 *>(b + id);
+      const double2 YM = *reinterpret_cast<const double2 *>(x + id - ys), YP = *reinterpret_cast<const double2 *>(x + id + ys);
+      const double2 XM = *reinterpret_cast<const double2 *>(x + id - xs), XP = *reinterpret_cast<const double2 *>(x + id + xs);
+      const double zl = x[id - 1], zr = x[id + 2];
+      const double r0 = B.x - (c.fzh * (zl + X.y) + c.fyh * (YM.x + YP.x) + c.fxh * (XM.x + XP.x) - c.dg * X.x);
+      const double r1 = B.y - (c.fzh * (X.x + zr) + c.fyh * (YM.y + YP.y) + c.fxh * (XM.y + XP.y) - c.dg * X.y);
+      Bs[crow + m] = (float)r0;
+      Bo[crow + m] = (float)r1;
+      acc2 += r0 * r0 + r1 * r1;
+      accinf = fmax(accinf, fmax(fabs(r0), fabs(r1)));
+      continue;
+    }
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       const int k = 2 * m + h;
@@ -649,6 +664,7 @@ __global__ void __launch_bounds__(256) k_chq_outer_residual(const double *__rest
 }
 
 // x += (double) e on the interior, e on the level-0 colour arrays.
+template <bool VEC>
 __global__ void __launch_bounds__(256) k_chq_add_correction(double *__restrict__ x, long long xs, long long ys,
                                                             int nx, int ny, int nz, const float *__restrict__ E0,
                                                             const float *__restrict__ E1, int rz) {
@@ -660,8 +676,16 @@ __global__ void __launch_bounds__(256) k_chq_add_correction(double *__restrict__
   const long long id = (long long)i * xs + (long long)j * ys + 2 * m;
   const long long cid = ((long long)i * ny + j) * rz + m;
   const bool s = (i + j) & 1;
-  x[id] = x[id] + (double)(s ? E1 : E0)[cid];
-  if (2 * m + 1 < nz) x[id + 1] = x[id + 1] + (double)(s ? E0 : E1)[cid];
+  const float e0 = (s ? E1 : E0)[cid], e1 = (s ? E0 : E1)[cid];
+  if (VEC) {
+    double2 X = *reinterpret_cast<double2 *>(x + id);
+    X.x = X.x + (double)e0;
+    X.y = X.y + (double)e1;
+    *reinterpret_cast<double2 *>(x + id) = X;
+    return;
+  }
+  x[id] = x[id] + (double)e0;
+  if (2 * m + 1 < nz) x[id + 1] = x[id + 1] + (double)e1;
 }
 
 }  // namespace
@@ -915,6 +939,11 @@ ocu_status ChequerMG::enqueue_fmg(int nu1, int nu2, int cycles, int coarse_iters
   return OCU_OK;
 }
 
+// the FP64 grid's pairs (k, k+1), k even, are 16-byte aligned double2
+static bool vec_ok(const ocu_layout &L) {
+  return L.nz % 2 == 0 && L.shift % 2 == 0 && L.xstride % 2 == 0 && L.ystride % 2 == 0;
+}
+
 ocu_status ChequerMG::enqueue_residual(const double *x, const double *b, const ocu_layout &L, double h, double fx_,
                                        double fy_, double fz_, double *rows2, double *rowsinf, cudaStream_t s) {
   const ChqLevel &C0 = lv[0];
@@ -924,8 +953,12 @@ ocu_status ChequerMG::enqueue_residual(const double *x, const double *b, const o
   c.fzh = fz_ / (h * h);
   c.dg = 2 * (fx_ + fy_ + fz_) / (h * h);
   dim3 block(32, 8), grid(1, (L.ny + 7) / 8, L.nx);
-  launch_pdl(k_chq_outer_residual, grid, block, 0, s, x, b, (long long)L.xstride, (long long)L.ystride, L.nx, L.ny,
-             L.nz, c, C0.b[0], C0.b[1], C0.rz, rows2, rowsinf);
+  if (vec_ok(L))
+    launch_pdl(k_chq_outer_residual<true>, grid, block, 0, s, x, b, (long long)L.xstride, (long long)L.ystride, L.nx,
+               L.ny, L.nz, c, C0.b[0], C0.b[1], C0.rz, rows2, rowsinf);
+  else
+    launch_pdl(k_chq_outer_residual<false>, grid, block, 0, s, x, b, (long long)L.xstride, (long long)L.ystride, L.nx,
+               L.ny, L.nz, c, C0.b[0], C0.b[1], C0.rz, rows2, rowsinf);
   return check_launch("k_chq_outer_residual");
 }
 
@@ -933,8 +966,12 @@ ocu_status ChequerMG::enqueue_add_correction(double *x, const ocu_layout &L, cud
   const ChqLevel &C0 = lv[0];
   const int mz = (L.nz + 1) / 2;
   dim3 block(64, 4), grid((mz + 63) / 64, (L.ny + 3) / 4, L.nx);
-  launch_pdl(k_chq_add_correction, grid, block, 0, s, x, (long long)L.xstride, (long long)L.ystride, L.nx, L.ny,
-             L.nz, C0.u[0], C0.u[1], C0.rz);
+  if (vec_ok(L))
+    launch_pdl(k_chq_add_correction<true>, grid, block, 0, s, x, (long long)L.xstride, (long long)L.ystride, L.nx,
+               L.ny, L.nz, C0.u[0], C0.u[1], C0.rz);
+  else
+    launch_pdl(k_chq_add_correction<false>, grid, block, 0, s, x, (long long)L.xstride, (long long)L.ystride, L.nx,
+               L.ny, L.nz, C0.u[0], C0.u[1], C0.rz);
   return check_launch("k_chq_add_correction");
 }
 
