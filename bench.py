@@ -542,8 +542,9 @@ def cpu_threads():
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
 
 
-def cpu_solve_once(kind="mixed"):
-    """One 256^3 solve by the oracle's restatement of the reference algorithm."""
+def cpu_solve_once(kind="mixed", threads=None):
+    """One 256^3 solve by the oracle's restatement of the reference algorithm (OpenMP over
+    `threads` host threads, all of them by default)."""
     from oracle import oracle_ctypes as O
     n = N_CFG3
     L = O.layout(n, n, n)
@@ -554,7 +555,7 @@ def cpu_solve_once(kind="mixed"):
     prm.bc = O.bcset_all(4, 0.0)
     prm.nu1 = prm.nu2 = 2
     prm.convergence = 0x05
-    O.lib().orc_ns_set_omp_threads(cpu_threads())
+    O.lib().orc_ns_set_omp_threads(threads or cpu_threads())
     m = O.OracleMG(kind, prm, n, n, n, 1 / n, 1 / n, 1 / n, rhs, L)
     t0 = time.perf_counter()
     ok, res = m.solve(TOL_REL * rms, 30)
@@ -563,10 +564,13 @@ def cpu_solve_once(kind="mixed"):
 
 
 def cpu_baseline_sample(args):
+    """All host cores, and one core -- the reference's host code is single-threaded."""
     ms, ok, rel = cpu_solve_once("mixed")
+    ms1, ok1, _ = cpu_solve_once("mixed", threads=1)
     return {"value": round(ms, 1), "unit": "ms", "cores": cpu_threads(), "kind": "port",
             "sample": f"one full 256^3 solve to 1e-10 by the oracle's restatement of the reference mixed "
-                      f"solver (FP32 FMG warm start + FP64 FMG), OpenMP, converged={bool(ok)}, rel={rel:.2e}"}
+                      f"solver (FP32 FMG warm start + FP64 FMG), OpenMP, converged={bool(ok)}, rel={rel:.2e}",
+            "one_core": {"value": round(ms1, 1), "unit": "ms", "cores": 1, "converged": bool(ok1)}}
 
 
 def run_reference(args):

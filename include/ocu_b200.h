@@ -95,8 +95,10 @@ ocu_status ocu_grid_reduce(const ocu_grid *g, ocu_reduce_op op, double *result, 
  * All calls on a device share that array and it keeps the previous call's contents (each call
  * clears what must start at zero), so calls that overlap on the GPU -- other streams or host
  * threads without ordering between them -- race and must be serialised by the caller.  The
- * first call on a device looks up the array's device address while that device is current;
- * make that first call before any stream capture.  Blocks the host until the result is back. */
+ * first call on a device looks up the array's device address while that device is current and
+ * keeps it for the life of the process, so the device must not be reset (cudaDeviceReset)
+ * after that first call.  Every call blocks the host until the result is back, so the
+ * function cannot be called on a stream that is being captured into a graph. */
 ocu_status ocu_grid_reduce_noalloc(const ocu_grid *g, ocu_reduce_op op, double *result, ocu_stream s);
 
 /* ---- ghost cells (ocustorage/grid3dboundary.h:26-70) --------------------------------- */

@@ -367,8 +367,8 @@ ocu_status launch_lincomb1(T *res, T a1, const T *g1, long long n, cudaStream_t 
 template <typename T>
 ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, T a2, const T *g2,
                            cudaStream_t s) {
-  const int waste = (int)(L.allocated - (long long)L.nx * L.ny * L.nz);
-  if (waste / (float)L.allocated > .03f) {
+  const long long waste = L.allocated - (long long)L.nx * L.ny * L.nz;
+  if ((double)waste > 0.03 * (double)L.allocated) {
     const auto a16 = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
     if (a16(res + L.shift) && a16(g1 + L.shift) && a16(g2 + L.shift) && (L.ystride * sizeof(T)) % 16 == 0 &&
         (L.xstride * sizeof(T)) % 16 == 0 && L.nx > 0 && L.ny > 0 && L.nz > 0) {

@@ -49,6 +49,24 @@ def test_noalloc_matches_allocating_reduce_twice(dtype, shape):
         assert first == ref and second == ref, (op, ref, first, second)
 
 
+def test_noalloc_allocates_nothing():
+    """After the first call (which only looks up the static array's address), calls leave the
+    device's free memory unchanged; an allocation of any size would take at least one 2 MB
+    page from it."""
+    import torch
+
+    lib = ocu.load()
+    g = _grid(ocu.F64, (128, 96, 40), seed=4)
+    _reduce(lib.ocu_grid_reduce_noalloc, g, _capi.REDUCE_SQRSUM)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for op in OPS:
+        _reduce(lib.ocu_grid_reduce_noalloc, g, op)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+
+
 def test_noalloc_back_to_back_different_grids():
     """Consecutive calls on different grids: the shared scratch carries no state across calls."""
     lib = ocu.load()
