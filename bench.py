@@ -390,25 +390,35 @@ def run_secondary(torch, ocu, _capi, lib, stream, sh):
     out["fp32_64cube_solve_ms"] = round(e0.elapsed_time(e1) / reps, 4)
     out["fp32_64cube_vcycles"] = s.stats.vcycles
 
-    # 100 steps of the 128x128x64 FP32 Boussinesq flow
-    pp = rayleigh_benard(ocu, 128, 128, 64)
-    eq = ocu.Eqn_IncompressibleNS3D(ocu.F32)
-    eq.set_parameters(pp)
-    _capi.check(lib.ocu_ns_set_stream(eq._h, sh))
-    for _ in range(3):
-        eq.advance_one_step(eq.get_max_stable_timestep())
-    torch.cuda.synchronize()
-    e0.record(stream)
-    steps = 100
-    unconverged = 0
-    for _ in range(steps):
-        unconverged += 0 if eq.advance_one_step(eq.get_max_stable_timestep()) else 1
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
+    # 100 steps of the 128x128x64 FP32 Boussinesq flow: the reference's projection (FP32
+    # multigrid, which cannot reach the 1e-5 divergence target at Ra = 1e6 and retries from zero
+    # every step), and the library option solving the pressure by FP32 V-cycles in FP64
+    # refinement (every projection converged)
+    def ns_run(mixed):
+        pp = rayleigh_benard(ocu, 128, 128, 64)
+        pp.mixed_pressure = mixed
+        eq = ocu.Eqn_IncompressibleNS3D(ocu.F32)
+        eq.set_parameters(pp)
+        _capi.check(lib.ocu_ns_set_stream(eq._h, sh))
+        for _ in range(3):
+            eq.advance_one_step(eq.get_max_stable_timestep())
+        torch.cuda.synchronize()
+        e0.record(stream)
+        steps = 100
+        unconverged = 0
+        for _ in range(steps):
+            unconverged += 0 if eq.advance_one_step(eq.get_max_stable_timestep()) else 1
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return steps, e0.elapsed_time(e1), unconverged
+
+    steps, ms, unconverged = ns_run(False)
     out["ns_128x128x64_fp32_steps_per_s"] = round(steps / (ms * 1e-3), 2)
     out["ns_ms_per_step"] = round(ms / steps, 4)
     out["ns_steps_projection_above_tol"] = unconverged
+    steps, ms, unconverged = ns_run(True)
+    out["ns_128x128x64_fp32_fp64_pressure_steps_per_s"] = round(steps / (ms * 1e-3), 2)
+    out["ns_fp64_pressure_steps_projection_above_tol"] = unconverged
     out.update(run_ensemble(torch, ocu, stream, sh))
     out.update(run_differentiable(torch, ocu))
     return out

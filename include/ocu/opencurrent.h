@@ -460,6 +460,8 @@ class Eqn_IncompressibleNS3DParams {
   InterpolationType advection_scheme = IT_FIRST_ORDER_UPWIND;
   TimeStepType time_step = TS_FORWARD_EULER;
   double cfl_factor = 1;
+  // not a reference field: the projection's pressure solved by FP32 V-cycles in FP64 refinement
+  bool mixed_pressure = false;
   void init_grids(int nx_, int ny_, int nz_, bool pinned = true) {
     nx = nx_; ny = ny_; nz = nz_;
     init_u.init(nx + 1, ny, nz, 1, 1, 1, pinned, 0, 1, 1);
@@ -489,6 +491,7 @@ class Eqn_IncompressibleNS3D : public ErrorHandler {
     c.gravity = (double)p.gravity; c.bouyancy = (double)p.bouyancy;
     c.thermal_diffusion = (double)p.thermal_diffusion; c.viscosity = (double)p.viscosity;
     c.advection_scheme = p.advection_scheme; c.time_step = p.time_step; c.cfl_factor = p.cfl_factor;
+    c.mixed_pressure = p.mixed_pressure ? 1 : 0;
     ocu_ns_set_stream(_ns, detail::stream());
     return check_ok(ocu_ns_set_parameters(_ns, &c, p.init_u.buffer(), p.init_v.buffer(), p.init_w.buffer(), p.init_temp.buffer()));
   }

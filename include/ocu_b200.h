@@ -322,6 +322,10 @@ ocu_status ocu_project_create(ocu_dtype dtype, ocu_project **out);
  * FP64 fields, the reference mixed pressure solver); OCU_MG_MIXED_IR is that class with this
  * library's FP32-in-FP64 refinement solver instead.  The mixed kinds take FP64 grids. */
 ocu_status ocu_project_create_with(ocu_mg_kind pressure_kind, ocu_project **out);
+/* Field precision and pressure solver chosen separately; besides the combinations above, FP32
+ * fields with OCU_MG_MIXED_IR (an FP64 pressure solved by FP32 V-cycles in FP64 refinement,
+ * applied to the FP32 velocity in double).  Not a reference class. */
+ocu_status ocu_project_create_fields(ocu_dtype fields, ocu_mg_kind pressure_kind, ocu_project **out);
 void ocu_project_destroy(ocu_project *p);
 ocu_status ocu_project_set_stream(ocu_project *p, ocu_stream s);
 /* initialize_storage (sol_project3ddev.cu:100-135): u,v,w borrowed MAC grids of one layout. */
@@ -349,6 +353,10 @@ typedef struct ocu_ns_params {
   int advection_scheme;          /* ocu_interpolation */
   int time_step;                 /* ocu_timestep */
   double cfl_factor;
+  int mixed_pressure;            /* not a reference field (0 = the reference's projection): 1 = the
+                                    projection's pressure is solved by FP32 V-cycles inside FP64
+                                    refinement (FP64 pressure, the fields keep their precision),
+                                    which reaches tolerances an FP32 multigrid cannot */
 } ocu_ns_params;
 
 /* Eqn_IncompressibleNS3DParams() defaults (eqn_incompressns3d.h:62-73). */

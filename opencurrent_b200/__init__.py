@@ -582,6 +582,8 @@ class Eqn_IncompressibleNS3DParams:
         self.advection_scheme = p.advection_scheme
         self.time_step = p.time_step
         self.cfl_factor = p.cfl_factor
+        # library option, not a reference field: FP64 pressure by FP32 V-cycles in FP64 refinement
+        self.mixed_pressure = False
         self.init_u = self.init_v = self.init_w = self.init_temp = None
         self.layouts = {}
 
@@ -608,6 +610,7 @@ class Eqn_IncompressibleNS3DParams:
         p.gravity, p.bouyancy = self.gravity, self.bouyancy
         p.thermal_diffusion, p.viscosity = self.thermal_diffusion, self.viscosity
         p.advection_scheme, p.time_step, p.cfl_factor = self.advection_scheme, self.time_step, self.cfl_factor
+        p.mixed_pressure = int(bool(self.mixed_pressure))
         return p
 
 

@@ -74,7 +74,7 @@ class NSParams(C.Structure):
                 ("vertical_direction", C.c_int), ("gravity", C.c_double),
                 ("bouyancy", C.c_double), ("thermal_diffusion", C.c_double),
                 ("viscosity", C.c_double), ("advection_scheme", C.c_int),
-                ("time_step", C.c_int), ("cfl_factor", C.c_double)]
+                ("time_step", C.c_int), ("cfl_factor", C.c_double), ("mixed_pressure", C.c_int)]
 
 
 # symbol -> (restype, argtypes); the exported-symbol test checks this table against the header
@@ -145,6 +145,7 @@ SIGNATURES = {
     "ocu_ens_autotune": (I, [P, C.POINTER(D), I]),
     "ocu_project_create": (I, [I, PP]),
     "ocu_project_create_with": (I, [I, PP]),
+    "ocu_project_create_fields": (I, [I, I, PP]),
     "ocu_project_destroy": (None, [P]),
     "ocu_project_set_stream": (I, [P, P]),
     "ocu_project_initialize_storage": (I, [P, I, I, I, D, D, D, P, P, P, BP]),

@@ -443,6 +443,21 @@ ocu_status ocu_project_create_with(ocu_mg_kind kind, ocu_project **out) {
   return OCU_OK;
 }
 
+ocu_status ocu_project_create_fields(ocu_dtype fields, ocu_mg_kind kind, ocu_project **out) {
+  OCU_NOT_NULL(out, "out");
+  *out = nullptr;
+  if (fields == OCU_F32 && kind == OCU_MG_MIXED_IR) {
+    *out = new (std::nothrow) ocu_project();
+    if (!*out) return fail(OCU_ERR_ALLOC, "[ERROR] ocu_project_create - out of host memory");
+    (*out)->s.dtype = OCU_F32;
+    (*out)->s.mg_kind = kind;
+    return OCU_OK;
+  }
+  if ((fields == OCU_F32) != (kind == OCU_MG_F32))
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] ocu_project_create_fields - unsupported field / pressure combination");
+  return ocu_project_create_with(kind, out);
+}
+
 ocu_status ocu_project_create(ocu_dtype dtype, ocu_project **out) {
   if (dtype != OCU_F32 && dtype != OCU_F64) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] ocu_project_create - bad dtype");
   return ocu_project_create_with(dtype == OCU_F64 ? OCU_MG_F64 : OCU_MG_F32, out);

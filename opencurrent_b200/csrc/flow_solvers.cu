@@ -29,6 +29,7 @@ static bool convert_bc(const ocu_bc &b, ocu_bc *out) {
 ProjectSolver::~ProjectSolver() {
   delete mg;
   if (divergence) { cudaFree(divergence->buf); delete divergence; }
+  if (divergence64) { cudaFree(divergence64->buf); delete divergence64; }
 }
 
 // initialize_storage (sol_project3ddev.cu:100-135, initialize_device_storage :28-53; the mixed
@@ -62,11 +63,19 @@ ocu_status ProjectSolver::initialize_storage(int nx_, int ny_, int nz_, double h
   OCU_TRY(check_cuda(cudaMemset(divergence->buf, 0, dtype_size(dtype) * Ld.allocated), "cudaMemset(divergence)"));
   mg = new ocu_mg(mg_kind >= 0 ? (ocu_mg_kind)mg_kind : (dtype == OCU_F64 ? OCU_MG_F64 : OCU_MG_F32), p);
   mg->s.set_stream(stream);
-  OCU_TRY(mg->s.initialize_storage(nx, ny, nz, hx, hy, hz, divergence));
+  ocu_grid *rhs = divergence;
+  if (p64()) {  // FP32 fields, FP64 pressure: the pressure solve reads an FP64 copy of the divergence
+    divergence64 = new ocu_grid{OCU_F64, Ld, nullptr, true};
+    OCU_TRY(check_cuda(cudaMalloc(&divergence64->buf, 8 * Ld.allocated), "cudaMalloc(divergence64)"));
+    OCU_TRY(check_cuda(cudaMemset(divergence64->buf, 0, 8 * Ld.allocated), "cudaMemset(divergence64)"));
+    rhs = divergence64;
+  }
+  OCU_TRY(mg->s.initialize_storage(nx, ny, nz, hx, hy, hz, rhs));
   if (!layout_match(u->L, mg->s.pressure->L))
     return fail(OCU_ERR_LAYOUT, "[ERROR] Sol_ProjectDivergence3DDevice::initialize_storage - pressure layout mismatch");
   // pressure().clear_zero(); convergence = CONVERGENCE_LINF (sol_project3ddev.cu:131-132)
-  OCU_TRY(check_cuda(cudaMemsetAsync(mg->s.pressure->buf, 0, dtype_size(dtype) * Ld.allocated, stream), "clear_zero"));
+  OCU_TRY(check_cuda(cudaMemsetAsync(mg->s.pressure->buf, 0, dtype_size(mg->s.pressure->dtype) * Ld.allocated, stream),
+                     "clear_zero"));
   p.convergence = OCU_CONVERGENCE_LINF;
   mg->s.set_params(p);
   initialized = true;
@@ -97,7 +106,25 @@ ocu_status ProjectSolver::solve_t(double tolerance) {
 // report OCU_ERR_NOT_CONVERGED, as the reference returns false.
 ocu_status ProjectSolver::solve(double tolerance) {
   if (!initialized) return fail(OCU_ERR_NOT_INITIALIZED, "[ERROR] Sol_ProjectDivergence3DDevice::solve - not initialized");
+  if (p64()) return solve_f32_p64(tolerance);
   return dtype == OCU_F64 ? solve_t<double>(tolerance) : solve_t<float>(tolerance);
+}
+
+// FP32 fields with the pressure solved by FP32 V-cycles inside FP64 refinement (a library
+// option, no reference counterpart): the same steps as solve_t<float>, with the FP32
+// divergence widened to double for the pressure solve and the FP64 pressure gradient applied to
+// the FP32 velocity in double.
+ocu_status ProjectSolver::solve_f32_p64(double tolerance) {
+  OCU_TRY(divergence_only_t<float>());
+  OCU_TRY(launch_convert<double, float>((double *)divergence64->buf, (const float *)divergence->buf,
+                                        divergence->L.allocated, stream));
+  double residual = 0;
+  ocu_status st = mg->s.solve(&residual, tolerance, 15);
+  if (st != OCU_OK && st != OCU_ERR_NOT_CONVERGED) return st;
+  OCU_TRY(launch_gradient_p64(origin<float>(u), origin<float>(v), origin<float>(w), origin<double>(mg->s.pressure),
+                              u->L, nx, ny, nz, hx, hy, hz, -1.0, stream));
+  OCU_TRY(launch_mac_bc_level1<float>(origin<float>(u), origin<float>(v), origin<float>(w), u->L, nx, ny, nz, bc, stream));
+  return st;
 }
 
 ocu_status ProjectSolver::solve_divergence_only() {
@@ -191,6 +218,7 @@ ocu_status NSSolver::set_parameters(const ocu_ns_params &p, const void *iu, cons
   OCU_TRY(check_cuda(cudaMemcpy(w->buf, iw, es * Lw.allocated, cudaMemcpyHostToDevice), "copy init_w"));
   OCU_TRY(check_cuda(cudaMemcpy(t->buf, it, es * Lt.allocated, cudaMemcpyHostToDevice), "copy init_temp"));
   proj.dtype = dtype;
+  proj.mg_kind = p.mixed_pressure ? OCU_MG_MIXED_IR : -1;
   proj.set_stream(stream);
   OCU_TRY(proj.initialize_storage(p.nx, p.ny, p.nz, p.hx, p.hy, p.hz, u, v, w, p.flow_bc));
   if (dtype == OCU_F64) {
@@ -282,11 +310,16 @@ ocu_status NSSolver::step_t(double dtv) {
     }
   }
   if (prm.time_step == OCU_TS_ADAMS_BASHFORD2) {
+    // this step's derivatives become the previous ones by exchanging the buffers, where the
+    // reference copies them (eqn_incompressns3d.cu:390-396).  The derivative kernels overwrite
+    // every cell the update reads, except the u/v/w face layers i = nx / j = ny / k = nz, which
+    // only the viscous term adds to; those faces of the velocity are set by the boundary
+    // conditions after the update, so the velocity and temperature are the reference's.
     lastdt = dtv;
-    const size_t es = sizeof(T);
-    OCU_TRY(check_cuda(cudaMemcpyAsync(ldt->buf, dt->buf, es * dt->L.allocated, cudaMemcpyDeviceToDevice, stream), "AB2 copy"));
-    for (int c = 0; c < 3; c++)
-      OCU_TRY(check_cuda(cudaMemcpyAsync(ls[c]->buf, ds[c]->buf, es * ds[c]->L.allocated, cudaMemcpyDeviceToDevice, stream), "AB2 copy"));
+    std::swap(dt, ldt);
+    std::swap(du, ldu);
+    std::swap(dv, ldv);
+    std::swap(dw, ldw);
   }
   return proj.solve(prm.max_divergence);
 }

@@ -8,6 +8,7 @@ namespace ocub {
 struct ProjectSolver {
   ocu_dtype dtype = OCU_F32;
   int mg_kind = -1;  // pressure solver kind (ocu_mg_kind; -1: plain, of the fields' precision)
+  ocu_grid *divergence64 = nullptr;  // FP32 fields with a refinement-solved FP64 pressure: its rhs
   ocu_bc_set bc{};
   int nx = 0, ny = 0, nz = 0;
   double hx = 0, hy = 0, hz = 0;
@@ -24,6 +25,8 @@ struct ProjectSolver {
   ocu_status solve_divergence_only();
   void set_stream(cudaStream_t s);
   template <typename T> ocu_status solve_t(double tolerance);
+  ocu_status solve_f32_p64(double tolerance);
+  bool p64() const { return dtype == OCU_F32 && mg_kind >= 0 && mg_kind != OCU_MG_F32; }
   template <typename T> ocu_status divergence_only_t();
 };
 

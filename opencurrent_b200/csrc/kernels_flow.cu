@@ -51,6 +51,20 @@ __global__ void k_gradient(T *__restrict__ u, T *__restrict__ v, T *__restrict__
   CELL_LOOP_END
 }
 
+// The same update with the pressure in double and the velocity in T: the difference and the
+// update in double, rounded to T once (the projection with a refinement-solved FP64 pressure).
+template <typename T>
+__global__ void k_gradient_p64(T *__restrict__ u, T *__restrict__ v, T *__restrict__ w, const double *__restrict__ phi,
+                               double c, double ihx, double ihy, double ihz, long long xs, long long ys, int nx, int ny,
+                               int nz) {
+  CELL_LOOP_BEGIN
+  const double p = phi[id];
+  u[id] = (T)((double)u[id] + c * ihx * (p - phi[id - xs]));
+  v[id] = (T)((double)v[id] + c * ihy * (p - phi[id - ys]));
+  w[id] = (T)((double)w[id] + c * ihz * (p - phi[id - 1]));
+  CELL_LOOP_END
+}
+
 // Sol_LaplacianCentered3DDevice_stencil (sol_laplaciancent3ddev.cu:28-60)
 template <typename T>
 __global__ void k_laplacian(const T *__restrict__ phi, T *__restrict__ dphidt, T ihx2, T ihy2, T ihz2, T c,
@@ -164,6 +178,15 @@ ocu_status launch_gradient(T *u, T *v, T *w, const T *phi, const ocu_layout &L, 
   k_gradient<T><<<g, b, 0, s>>>(u, v, w, phi, coefficient, (T)(1 / hx), (T)(1 / hy), (T)(1 / hz), L.xstride,
                                 L.ystride, nx, ny, nz);
   return check_launch("k_gradient");
+}
+
+ocu_status launch_gradient_p64(float *u, float *v, float *w, const double *phi, const ocu_layout &L, int nx, int ny,
+                              int nz, double hx, double hy, double hz, double coefficient, cudaStream_t s) {
+  dim3 g, b;
+  shape(nx, ny, nz, &g, &b);
+  k_gradient_p64<float><<<g, b, 0, s>>>(u, v, w, phi, coefficient, 1 / hx, 1 / hy, 1 / hz, L.xstride, L.ystride, nx,
+                                        ny, nz);
+  return check_launch("k_gradient_p64");
 }
 
 template <typename T>

@@ -178,6 +178,9 @@ template <typename T>
 ocu_status launch_gradient(T *u, T *v, T *w, const T *phi, const ocu_layout &L, int nx, int ny,
                            int nz, double hx, double hy, double hz, T coefficient,
                            cudaStream_t s);
+// u, v, w (float) -= c grad(phi) with phi in double
+ocu_status launch_gradient_p64(float *u, float *v, float *w, const double *phi, const ocu_layout &L, int nx, int ny,
+                              int nz, double hx, double hy, double hz, double coefficient, cudaStream_t s);
 template <typename T>
 ocu_status launch_laplacian(const T *phi, T *dphidt, const ocu_layout &L, int nx, int ny,
                             int nz, double hx, double hy, double hz, T coefficient,
