@@ -167,14 +167,6 @@ typedef struct ocu_mg_params {
   int sweep_cells;               /* levels with at least this many cells relax both colours in
                                     one TMA-fed pass (out of place, same results; Dirichlet and
                                     Neumann faces only); <= 0 = off (the default) */
-  int leg_cells;                 /* levels below 0 with at most this many cells run the down-leg
-                                    (nu1 iterations + residual restriction) and the up-leg
-                                    (prolongation + nu2 iterations) of a V-cycle as one launch
-                                    each (same results; nu1, nu2 <= 2); <= 0 = off (the
-                                    default) */
-  int tail_ctas;                 /* CTAs (2..8) of the thread-block cluster that runs the tail
-                                    kernel, its phases spread over them; 0 or 1 = one CTA
-                                    (the default) */
   int ir_inner_exact;            /* OCU_MG_MIXED_IR only: 0 (default) = the FP32 correction
                                     solves run on red/black split colour arrays with fused
                                     multiply-adds (this library's own inner solver, checked

@@ -213,8 +213,6 @@ class _MGBase:
         self.unfused = False
         self.tail_cells = 0
         self.sweep_cells = 0
-        self.leg_cells = 0
-        self.tail_ctas = 0
         self.ir_inner_exact = False
         self.wait_limit = 0
         self._h = None
@@ -231,8 +229,6 @@ class _MGBase:
         p.unfused = int(bool(self.unfused))
         p.tail_cells = int(self.tail_cells)
         p.sweep_cells = int(self.sweep_cells)
-        p.leg_cells = int(self.leg_cells)
-        p.tail_ctas = int(self.tail_ctas)
         p.ir_inner_exact = int(bool(self.ir_inner_exact))
         p.wait_limit = int(self.wait_limit)
         return p

@@ -54,7 +54,6 @@ class MGParams(C.Structure):
                 ("make_symmetric_operator", C.c_int), ("disable_relax_on_host", C.c_int),
                 ("ir_inner_cycles", C.c_int), ("store_residual_grids", C.c_int),
                 ("unfused", C.c_int), ("tail_cells", C.c_int), ("sweep_cells", C.c_int),
-                ("leg_cells", C.c_int), ("tail_ctas", C.c_int),
                 ("ir_inner_exact", C.c_int), ("wait_limit", C.c_int)]
 
 

@@ -10,7 +10,6 @@
 // (i,j) row, lane t folds k = t, t+32, ... and the 32 lanes fold 16/8/4/2/1; rows are folded by
 // 256-wide trees (grid1dops.cu:33-115) in k_fold_rows.
 #include <atomic>
-#include <cooperative_groups.h>
 #include <cstring>
 
 #include "bc_device.cuh"
@@ -219,27 +218,27 @@ ocu_status launch_relax_color_emit(T *u, const T *b, const ocu_layout &L, const 
 
 // Prolongation + correction + ghost writes (devf.cu:94-197 then the level1 fill).
 // EMIT = false compiles the ghost writes out (children that touch no face, or no fusable BCs).
-template <typename T, bool EMIT, typename I = long long, bool CG = false>
+template <typename T, bool EMIT, typename I = long long>
 __device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, I tc, I cx, I cy, T *__restrict__ uf, I f,
                                              I fxs, I fys, int ic, int jc, int kc, const GhostEmit<T> *ge) {
   const T w1 = (T)0.421875, w2 = (T)0.140625, w3 = (T)0.046875, w4 = (T)0.015625;
   const int i = 2 * ic + 1, j = 2 * jc + 1, k = 2 * kc + 1;
   // all eight fine values are loaded before the first store: the ghost writes go through
   // another pointer, so loads placed after a store could not be issued until it completed
-  const T f000 = gld<CG>(uf + f), f100 = gld<CG>(uf + f - fxs), f010 = gld<CG>(uf + f - fys);
-  const T f001 = gld<CG>(uf + f - 1);
-  const T f110 = gld<CG>(uf + f - fxs - fys), f101 = gld<CG>(uf + f - fxs - 1), f011 = gld<CG>(uf + f - fys - 1);
-  const T f111 = gld<CG>(uf + f - fxs - fys - 1);
-  const T c000 = gld<CG>(uc + tc);
-  const T c0p0 = gld<CG>(uc + tc + cy), c00p = gld<CG>(uc + tc + 1), c0pp = gld<CG>(uc + tc + cy + 1);
-  const T c0m0 = gld<CG>(uc + tc - cy), c00m = gld<CG>(uc + tc - 1), c0mm = gld<CG>(uc + tc - cy - 1);
-  const T c0mp = gld<CG>(uc + tc - cy + 1), c0pm = gld<CG>(uc + tc + cy - 1);
+  const T f000 = uf[f], f100 = uf[f - fxs], f010 = uf[f - fys];
+  const T f001 = uf[f - 1];
+  const T f110 = uf[f - fxs - fys], f101 = uf[f - fxs - 1], f011 = uf[f - fys - 1];
+  const T f111 = uf[f - fxs - fys - 1];
+  const T c000 = uc[tc];
+  const T c0p0 = uc[tc + cy], c00p = uc[tc + 1], c0pp = uc[tc + cy + 1];
+  const T c0m0 = uc[tc - cy], c00m = uc[tc - 1], c0mm = uc[tc - cy - 1];
+  const T c0mp = uc[tc - cy + 1], c0pm = uc[tc + cy - 1];
   T v;
   {  // children on the +x side of the coarse centre (coarse plane x+1)
-    const T cp00 = gld<CG>(uc + tc + cx), cpp0 = gld<CG>(uc + tc + cx + cy), cp0p = gld<CG>(uc + tc + cx + 1);
-    const T cppp = gld<CG>(uc + tc + cx + cy + 1);
-    const T cpm0 = gld<CG>(uc + tc + cx - cy), cp0m = gld<CG>(uc + tc + cx - 1), cpmm = gld<CG>(uc + tc + cx - cy - 1);
-    const T cppm = gld<CG>(uc + tc + cx + cy - 1), cpmp = gld<CG>(uc + tc + cx - cy + 1);
+    const T cp00 = uc[tc + cx], cpp0 = uc[tc + cx + cy], cp0p = uc[tc + cx + 1];
+    const T cppp = uc[tc + cx + cy + 1];
+    const T cpm0 = uc[tc + cx - cy], cp0m = uc[tc + cx - 1], cpmm = uc[tc + cx - cy - 1];
+    const T cppm = uc[tc + cx + cy - 1], cpmp = uc[tc + cx - cy + 1];
     v = f000 + w1 * c000 + w2 * (cp00 + c0p0 + c00p) + w3 * (cpp0 + cp0p + c0pp) + w4 * cppp;
     uf[f] = v; if (EMIT) ge->emit(i, j, k, v);
     v = f010 + w1 * c000 + w2 * (cp00 + c0m0 + c00p) + w3 * (cpm0 + cp0p + c0mp) + w4 * cpmp;
@@ -250,16 +249,16 @@ __device__ __forceinline__ void prolong_cell(const T *__restrict__ uc, I tc, I c
     uf[f - fys - 1] = v; if (EMIT) ge->emit(i, j - 1, k - 1, v);
     // the -x child with (0,0) y/z offsets takes its corner weight from cppp, as the reference
     // kernel does (devf.cu:94-197)
-    const T cm00 = gld<CG>(uc + tc - cx), cmp0 = gld<CG>(uc + tc - cx + cy), cm0p = gld<CG>(uc + tc - cx + 1);
+    const T cm00 = uc[tc - cx], cmp0 = uc[tc - cx + cy], cm0p = uc[tc - cx + 1];
     v = f100 + w1 * c000 + w2 * (cm00 + c0p0 + c00p) + w3 * (cmp0 + cm0p + c0pp) + w4 * cppp;
     uf[f - fxs] = v; if (EMIT) ge->emit(i - 1, j, k, v);
   }
   {  // remaining children on the -x side (coarse plane x-1)
-    const T cm00 = gld<CG>(uc + tc - cx), cmm0 = gld<CG>(uc + tc - cx - cy), cm0p = gld<CG>(uc + tc - cx + 1);
-    const T cm0m = gld<CG>(uc + tc - cx - 1);
-    const T cmmm = gld<CG>(uc + tc - cx - cy - 1), cmp0 = gld<CG>(uc + tc - cx + cy);
-    const T cmpm = gld<CG>(uc + tc - cx + cy - 1);
-    const T cmmp = gld<CG>(uc + tc - cx - cy + 1);
+    const T cm00 = uc[tc - cx], cmm0 = uc[tc - cx - cy], cm0p = uc[tc - cx + 1];
+    const T cm0m = uc[tc - cx - 1];
+    const T cmmm = uc[tc - cx - cy - 1], cmp0 = uc[tc - cx + cy];
+    const T cmpm = uc[tc - cx + cy - 1];
+    const T cmmp = uc[tc - cx - cy + 1];
     v = f110 + w1 * c000 + w2 * (cm00 + c0m0 + c00p) + w3 * (cmm0 + cm0p + c0mp) + w4 * cmmp;
     uf[f - fxs - fys] = v; if (EMIT) ge->emit(i - 1, j - 1, k, v);
     v = f101 + w1 * c000 + w2 * (cm00 + c0p0 + c00m) + w3 * (cmp0 + cm0m + c0pm) + w4 * cmpm;
@@ -968,19 +967,8 @@ ocu_status launch_fold_rows(const T *rows, long long nrows, bool is_max, void *s
 // The tail's phases are separate (not inlined) functions: the kernel runs each code path only a
 // few times per launch, so one shared copy of every phase keeps its instruction footprint (and
 // the cold instruction fetches that dominated it) small.
-// Phase barrier of the tail: the CTA, or (CLU) every CTA of the cluster.  The cluster barrier's
-// arrive has release and its wait acquire semantics, so a phase sees every global store of the
-// phases before it; the loads of data other CTAs wrote go through L2 (relax_point_cg,
-// residual_at_cg, prolong_cell<..., CG>).
-template <bool CLU>
-__device__ __forceinline__ void tail_sync() {
-  if constexpr (CLU) cooperative_groups::this_cluster().sync();
-  else __syncthreads();
-}
-
-// Phases take their cells from t0 in steps of nt: threadIdx.x / blockDim.x for one CTA, the
-// thread's rank in the cluster / the cluster's threads for CLU.
-template <typename T, bool CLU>
+// Phases take their cells from t0 in steps of nt (threadIdx.x / blockDim.x).
+template <typename T>
 __device__ __noinline__ void tail_relax(const TailLevel<T> &lv, int iterations, int order, int t0, int nt) {
   GhostEmit<T> ge{lv.u, lv.xs, lv.ys, lv.nx, lv.ny, lv.nz, lv.bc, lv.hx, lv.hy, lv.hz};
   if (order == 2) {
@@ -997,22 +985,16 @@ __device__ __noinline__ void tail_relax(const TailLevel<T> &lv, int iterations, 
         const int i = q / (lv.ny * half), rem = q % (lv.ny * half), j = rem / half, t = rem % half;
         const int k = 2 * t + ((i + j + color) & 1);
         const long long id = (long long)i * lv.xs + (long long)j * lv.ys + k;
-        T nv;
-        if constexpr (CLU)
-          nv = relax_point_cg<T>(lv.u, lv.b, id, lv.xs, lv.ys, i, j, k, lv.nx, lv.ny, lv.nz, lv.rc);
-        else
-          nv = relax_point<T>(lv.u, lv.b, id, lv.xs, lv.ys, i, j, k, lv.nx, lv.ny, lv.nz, lv.rc, nullptr);
+        const T nv = relax_point<T>(lv.u, lv.b, id, lv.xs, lv.ys, i, j, k, lv.nx, lv.ny, lv.nz, lv.rc, nullptr);
         lv.u[id] = nv;
         if (lv.emit_ok) ge.emit(i, j, k, nv);
       }
-      tail_sync<CLU>();
-      // without fused ghost writes (one CTA only): refresh between colours when periodic, else
-      // after both (sol_mgpressure3ddev.cu:235-241)
-      if constexpr (!CLU) {
-        if (!lv.emit_ok && (lv.periodic || rb == 1)) {
-          level1_fill_block<T>(lv.u, lv.xs, lv.ys, lv.nx, lv.ny, lv.nz, lv.bc, lv.hx, lv.hy, lv.hz);
-          __syncthreads();
-        }
+      __syncthreads();
+      // without fused ghost writes: refresh between colours when periodic, else after both
+      // (sol_mgpressure3ddev.cu:235-241)
+      if (!lv.emit_ok && (lv.periodic || rb == 1)) {
+        level1_fill_block<T>(lv.u, lv.xs, lv.ys, lv.nx, lv.ny, lv.nz, lv.bc, lv.hx, lv.hy, lv.hz);
+        __syncthreads();
       }
     }
   }
@@ -1020,7 +1002,7 @@ __device__ __noinline__ void tail_relax(const TailLevel<T> &lv, int iterations, 
 
 // clear_zero(coarse) + homogeneous ghost fill == zero every cell of the shell and interior;
 // then the residual of f restricted into b of c
-template <typename T, bool CLU>
+template <typename T>
 __device__ __noinline__ void tail_restrict(const TailLevel<T> &f, const TailLevel<T> &c, int t0, int nt) {
   const int cz = c.nz + 2, cy = c.ny + 2, cx = c.nx + 2;
   for (int q = t0; q < cx * cy * cz; q += nt) {
@@ -1033,32 +1015,28 @@ __device__ __noinline__ void tail_restrict(const TailLevel<T> &f, const TailLeve
     T r[8];
     const long long off[8] = {0, 1, f.ys, 1 + f.ys, f.xs, 1 + f.xs, f.ys + f.xs, 1 + f.ys + f.xs};
 #pragma unroll
-    for (int n = 0; n < 8; n++) {
-      if constexpr (CLU) r[n] = residual_at_cg<T>(f.u, f.b, ri + off[n], f.xs, f.ys, f.res);
-      else r[n] = residual_at<T>(f.u, f.b, ri + off[n], f.xs, f.ys, f.res);
-    }
+    for (int n = 0; n < 8; n++) r[n] = residual_at<T>(f.u, f.b, ri + off[n], f.xs, f.ys, f.res);
     c.b[(long long)ic * c.xs + (long long)jc * c.ys + kc] =
         (T)0.125 * (r[0] + r[1] + r[2] + r[3] + r[4] + r[5] + r[6] + r[7]);
   }
-  tail_sync<CLU>();
+  __syncthreads();
 }
 
-// The coarsest level: the host routine's arithmetic in one CTA (rank 0 of a cluster; every
-// other CTA waits at the barrier), or the device colour sweeps.
-template <typename T, bool CLU>
-__device__ __noinline__ void tail_coarsest(const TailLevel<T> &cl, const TailParams<T> &P, int t0, int nt, int rank) {
+// The coarsest level: the host routine's arithmetic by the CTA (block-wide), or the device
+// colour sweeps.
+template <typename T>
+__device__ __noinline__ void tail_coarsest(const TailLevel<T> &cl, const TailParams<T> &P, int t0, int nt) {
   if (P.host_coarse) {
-    if (rank == 0)
-      coarse_relax_block<T>(cl.u, cl.b, cl.xs, cl.ys, cl.nx, cl.ny, cl.nz, P.coarse_iters, P.coarse_order, P.cc,
-                            cl.bc, cl.hx, cl.hy, cl.hz);
+    coarse_relax_block<T>(cl.u, cl.b, cl.xs, cl.ys, cl.nx, cl.ny, cl.nz, P.coarse_iters, P.coarse_order, P.cc,
+                          cl.bc, cl.hx, cl.hy, cl.hz);
   } else {
-    tail_relax<T, CLU>(cl, P.coarse_iters, P.coarse_order, t0, nt);
+    tail_relax<T>(cl, P.coarse_iters, P.coarse_order, t0, nt);
   }
-  tail_sync<CLU>();
+  __syncthreads();
 }
 
 // prolongation of c into f with f's ghosts
-template <typename T, bool CLU>
+template <typename T>
 __device__ __noinline__ void tail_prolong(const TailLevel<T> &f, const TailLevel<T> &c, int t0, int nt) {
   GhostEmit<T> ge{f.u, f.xs, f.ys, f.nx, f.ny, f.nz, f.bc, f.hx, f.hy, f.hz};
   for (int q = t0; q < c.nx * c.ny * c.nz; q += nt) {
@@ -1066,32 +1044,30 @@ __device__ __noinline__ void tail_prolong(const TailLevel<T> &f, const TailLevel
     const long long tc = (long long)ic * c.xs + (long long)jc * c.ys + kc;
     const long long fi = (long long)(2 * ic + 1) * f.xs + (long long)(2 * jc + 1) * f.ys + (2 * kc + 1);
     if (f.emit_ok)
-      prolong_cell<T, true, long long, CLU>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, &ge);
+      prolong_cell<T, true, long long>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, &ge);
     else
-      prolong_cell<T, false, long long, CLU>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, nullptr);
+      prolong_cell<T, false, long long>(c.u, tc, c.xs, c.ys, f.u, fi, f.xs, f.ys, ic, jc, kc, nullptr);
   }
-  tail_sync<CLU>();
-  if constexpr (!CLU) {
-    if (!f.emit_ok) {
-      level1_fill_block<T>(f.u, f.xs, f.ys, f.nx, f.ny, f.nz, f.bc, f.hx, f.hy, f.hz);
-      __syncthreads();
-    }
+  __syncthreads();
+  if (!f.emit_ok) {
+    level1_fill_block<T>(f.u, f.xs, f.ys, f.nx, f.ny, f.nz, f.bc, f.hx, f.hy, f.hz);
+    __syncthreads();
   }
 }
 
 // The tail schedule on level descriptors lv[0..nlev-1] (lv[0] = level s), held in shared
 // memory.  Works on global memory or on a shared-memory copy; the arithmetic is the same.
-template <typename T, bool CLU>
-__device__ void tail_body(const TailLevel<T> *lv, const TailParams<T> &P, int t0, int nt, int rank) {
+template <typename T>
+__device__ void tail_body(const TailLevel<T> *lv, const TailParams<T> &P, int t0, int nt) {
   const int L = P.nlev;
   for (int l = 0; l < L - 1; l++) {
-    tail_relax<T, CLU>(lv[l], P.nu1, 0, t0, nt);
-    tail_restrict<T, CLU>(lv[l], lv[l + 1], t0, nt);
+    tail_relax<T>(lv[l], P.nu1, 0, t0, nt);
+    tail_restrict<T>(lv[l], lv[l + 1], t0, nt);
   }
-  tail_coarsest<T, CLU>(lv[L - 1], P, t0, nt, rank);
+  tail_coarsest<T>(lv[L - 1], P, t0, nt);
   for (int l = L - 2; l >= 0; l--) {
-    tail_prolong<T, CLU>(lv[l], lv[l + 1], t0, nt);
-    if (P.first_level + l > 0) tail_relax<T, CLU>(lv[l], P.nu2, P.post_order, t0, nt);
+    tail_prolong<T>(lv[l], lv[l + 1], t0, nt);
+    if (P.first_level + l > 0) tail_relax<T>(lv[l], P.nu2, P.post_order, t0, nt);
   }
 }
 
@@ -1115,7 +1091,7 @@ __global__ void __launch_bounds__(1024) k_coarse_tail(const __grid_constant__ Ta
     lv[threadIdx.x] = d;
   }
   __syncthreads();
-  tail_body<T, false>(lv, P, threadIdx.x, blockDim.x, 0);
+  tail_body<T>(lv, P, threadIdx.x, blockDim.x);
 }
 
 // Shared-memory variant: every tail level's u and b (interior + ghost shell, compact strides)
@@ -1167,7 +1143,7 @@ __global__ void __launch_bounds__(512) k_coarse_tail_smem(const __grid_constant_
     }
   }
   __syncthreads();
-  tail_body<T, false>(lv, P, threadIdx.x, nt, 0);
+  tail_body<T>(lv, P, threadIdx.x, nt);
   __syncthreads();
   for (int l = 0; l < L; l++) {  // write back: u with its ghost shell, b interior below level s
     const TailLevel<T> &g = gl[l];
@@ -1181,41 +1157,6 @@ __global__ void __launch_bounds__(512) k_coarse_tail_smem(const __grid_constant_
       if (l > 0 && i >= 0 && i < g.nx && j >= 0 && j < g.ny && k >= 0 && k < g.nz) g.b[gi] = sh.b[si];
     }
   }
-}
-
-// Cluster variant: the tail's phases spread over the CTAs of one thread-block cluster, separated
-// by cluster barriers (hardware, no spin) instead of one CTA's __syncthreads; data in global
-// memory (the tail levels are L2-resident).  Requires fused ghost writes on every tail level.
-template <typename T>
-__global__ void __launch_bounds__(512) k_coarse_tail_cluster(const __grid_constant__ TailParams<T> P) {
-  pdl_entry();
-  __shared__ TailLevel<T> lv[kMaxTailLevels];
-  if (threadIdx.x < P.nlev) lv[threadIdx.x] = P.lv[threadIdx.x];
-  __syncthreads();
-  const cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
-  const int rank = (int)cl.block_rank(), nb = (int)cl.num_blocks();
-  tail_body<T, true>(lv, P, rank * blockDim.x + threadIdx.x, nb * blockDim.x, rank);
-}
-
-template <typename T>
-ocu_status launch_coarse_tail_cluster(const TailParams<T> &P, int ctas, cudaStream_t s) {
-  if (ctas < 2 || ctas > 8)
-    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] launch_coarse_tail_cluster - cluster of %d CTAs", ctas);
-  cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3(ctas);
-  cfg.blockDim = dim3(512);
-  cfg.stream = s;
-  cudaLaunchAttribute attr[2];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = ctas;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[1].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = (pdl_enabled() && !pdl_suppressed()) ? 2 : 1;
-  cudaLaunchKernelEx(&cfg, k_coarse_tail_cluster<T>, P);
-  return check_launch("k_coarse_tail_cluster");
 }
 
 template <typename T>
@@ -1606,7 +1547,6 @@ INST_B(double)
                                                   cudaStream_t, T *, long long);                               \
   template ocu_status launch_fold_rows<T>(const T *, long long, bool, void *, double *, cudaStream_t);          \
   template ocu_status launch_coarse_tail<T>(const TailParams<T> &, cudaStream_t);                               \
-  template ocu_status launch_coarse_tail_cluster<T>(const TailParams<T> &, int, cudaStream_t);                   \
   template ocu_status launch_coarse_tail_batch<T>(const TailParams<T> &, const TailBatch &, int, cudaStream_t);
 INST(float)
 INST(double)

@@ -227,38 +227,6 @@ struct TailParams {
   CoarseCoef<T> cc;
 };
 
-// One V-cycle leg of a small level as a single launch (kernels_mg_legs.cu): the down-leg relaxes
-// nu1 iterations, clears the coarser level and restricts the residual into its b; the up-leg
-// prolongs the coarser level's u into this one and relaxes nu2 iterations.  u_in -> u_out is out
-// of place (the level's two u buffers alternate).
-constexpr int kLegMaxNu = 2;
-constexpr int kLegMaxHalo = 2 * kLegMaxNu + 1;
-
-template <typename T>
-struct LegLevel {
-  const T *u_in;      // origin of the level's current u
-  T *u_out;           // origin of the other u buffer (written: interior + ghost shell)
-  const T *b;         // origin of b
-  long long xs, ys;
-  int n[3];           // nx, ny, nz
-  int per[3];         // axis periodic on both faces
-  BCDev bc;
-  T h[3];             // spacings of the ghost rules
-  RelaxCoefD<T> rc;
-  ResCoefT<T> res;
-  int passes;         // colour passes: 2 * nu
-  int order;          // RO_RED_BLACK or RO_BLACK_RED (up-leg)
-  T *cu;              // coarser level: origin of u (prolongation source)
-  T *cb;              // coarser level: origin of b (restriction target)
-  long long cxs, cys;
-  int cn[3];
-  T *cu_base;         // coarser level: start of the u buffer, c_alloc elements (cleared)
-  long long c_alloc;
-};
-
-template <typename T>
-ocu_status launch_leg(const LegLevel<T> &P, bool up, cudaStream_t s);
-
 // Member selection of the ensemble (batched) launches: member m of a level lives at
 // base + m * stride; a launch processes the members whose state equals `want`.  state ==
 // nullptr: a single grid (member 0 only).
@@ -291,8 +259,6 @@ template <typename T>
 ocu_status launch_coarse_tail(const TailParams<T> &P, cudaStream_t s);
 // The same schedule for `members` grids at once, one CTA per member.
 // The tail over the CTAs of one cluster (2..8 CTAs; every tail level with fused ghost writes).
-template <typename T>
-ocu_status launch_coarse_tail_cluster(const TailParams<T> &P, int ctas, cudaStream_t s);
 template <typename T>
 ocu_status launch_coarse_tail_batch(const TailParams<T> &P, const TailBatch &tb, int members, cudaStream_t s);
 

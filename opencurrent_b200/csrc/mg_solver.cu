@@ -57,8 +57,6 @@ MGCore<T>::~MGCore() {
   }
   for (auto g : grids_u2)
     if (g) { cudaFree(g->buf); delete g; }
-  for (auto g : grids_uleg)
-    if (g) { cudaFree(g->buf); delete g; }
   for (auto p : diag) cudaFree(p);
   if (red_scratch) cudaFree(red_scratch);
   if (rows) cudaFree(rows);
@@ -151,7 +149,6 @@ ocu_status MGCore<T>::init(const ocu_bc_set &bc_, bool disable_host, int nx, int
   std::memset(h_norms, 0, 4 * sizeof(double));
   d_err = reinterpret_cast<int *>(d_norms + 2);
   grids_u2.assign(num_levels, nullptr);
-  grids_uleg.assign(num_levels, nullptr);
   tm_u.resize(num_levels);
   tm_u2.resize(num_levels);
   tm_b.resize(num_levels);
@@ -174,87 +171,6 @@ ocu_status MGCore<T>::ensure_sweep_buffers() {
     OCU_TRY(make_sweep_tmap<T>(grids_b[l]->buf, lay[l], &tm_b[l]));
   }
   return OCU_OK;
-}
-
-template <typename T>
-ocu_status MGCore<T>::ensure_leg_buffers() {
-  const ocu_dtype dt = sizeof(T) == 8 ? OCU_F64 : OCU_F32;
-  ocu_status st = OCU_OK;
-  for (int l = 1; l + 1 < num_levels; l++) {
-    if (grids_uleg[l] || (long long)dim[l][0] * dim[l][1] * dim[l][2] > leg_cells) continue;
-    grids_uleg[l] = alloc_grid(dt, lay[l], &st);
-    if (!grids_uleg[l]) return st;
-  }
-  return OCU_OK;
-}
-
-template <typename T>
-bool MGCore<T>::leg_ok(int level, int nu) const {
-  if (!fused || store_residuals || leg_cells <= 0 || nu < 1 || nu > kLegMaxNu) return false;
-  if (level < 1 || level >= tail_start() || level + 1 >= num_levels) return false;
-  if (level >= (int)grids_uleg.size() || !grids_uleg[level]) return false;
-  if ((long long)dim[level][0] * dim[level][1] * dim[level][2] > leg_cells || !emit_ok(level)) return false;
-  const ocu_bc_set b = bc_at_level(level);
-  const ocu_bc *f[6] = {&b.xneg, &b.xpos, &b.yneg, &b.ypos, &b.zneg, &b.zpos};
-  for (int a = 0; a < 3; a++) {
-    if (dim[level][a] & 1) return false;
-    if ((f[2 * a]->type == OCU_BC_PERIODIC) != (f[2 * a + 1]->type == OCU_BC_PERIODIC)) return false;
-  }
-  return true;
-}
-
-template <typename T>
-LegLevel<T> MGCore<T>::leg_level(int level, const T *u_in, T *u_out) const {
-  LegLevel<T> P;
-  std::memset(&P, 0, sizeof(P));
-  const ocu_bc_set b = bc_at_level(level);
-  P.u_in = u_in;
-  P.u_out = u_out;
-  P.b = origin<T>(grids_b[level]);
-  P.xs = lay[level].xstride;
-  P.ys = lay[level].ystride;
-  const int per[3] = {b.xneg.type == OCU_BC_PERIODIC, b.yneg.type == OCU_BC_PERIODIC, b.zneg.type == OCU_BC_PERIODIC};
-  for (int a = 0; a < 3; a++) {
-    P.n[a] = dim[level][a];
-    P.per[a] = per[a];
-    P.cn[a] = dim[level + 1][a];
-  }
-  P.bc = to_dev(b);
-  P.h[0] = (T)hx(level);
-  P.h[1] = (T)hy(level);
-  P.h[2] = (T)hz(level);
-  P.rc = make_relax_coef_d<T>(relax_params(level));
-  const double hh = h[level];
-  P.res.fxh = (T)(fx / (hh * hh));
-  P.res.fyh = (T)(fy / (hh * hh));
-  P.res.fzh = (T)(fz / (hh * hh));
-  P.res.dg = (T)(2 * (fx + fy + fz) / (hh * hh));
-  P.cu = origin<T>(grids_u[level + 1]);
-  P.cb = origin<T>(grids_b[level + 1]);
-  P.cxs = lay[level + 1].xstride;
-  P.cys = lay[level + 1].ystride;
-  P.cu_base = static_cast<T *>(grids_u[level + 1]->buf);
-  P.c_alloc = lay[level + 1].allocated;
-  return P;
-}
-
-// relax(level, nu1, RO_RED_BLACK), clear_level(level + 1), restriction: u moves to the second
-// buffer until the up-leg brings it back
-template <typename T>
-ocu_status MGCore<T>::leg_down(int level, int nu1) {
-  LegLevel<T> P = leg_level(level, u0(level), origin<T>(grids_uleg[level]));
-  P.passes = 2 * nu1;
-  P.order = RO_RED_BLACK;
-  return launch_leg<T>(P, false, stream);
-}
-
-// prolong(level + 1, level), relax(level, nu2, order)
-template <typename T>
-ocu_status MGCore<T>::leg_up(int level, int nu2, int order) {
-  LegLevel<T> P = leg_level(level, origin<T>(grids_uleg[level]), u0(level));
-  P.passes = 2 * nu2;
-  P.order = order;
-  return launch_leg<T>(P, true, stream);
 }
 
 template <typename T>
@@ -545,11 +461,6 @@ ocu_status MGCore<T>::cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool
     bo[l] = b0(l);
   }
   fill_tail_params(P, s, nu1, nu2, coarse_iters, symmetric, uo.data(), bo.data());
-  if (tail_ctas >= 2) {  // the cluster form needs fused ghost writes on every tail level
-    bool all_emit = true;
-    for (int l = s; l <= coarse; l++) all_emit = all_emit && emit_ok(l);
-    if (all_emit) return launch_coarse_tail_cluster<T>(P, tail_ctas, stream);
-  }
   return launch_coarse_tail<T>(P, stream);
 }
 
@@ -636,10 +547,6 @@ enum { SEG_INIT = 0, SEG_RAMP = 8, SEG_PRE0 = 16, SEG_REST0 = 24, SEG_FINAL = 32
 // levels [a, b) of a down-leg without norm checks
 ocu_status MGSolver::enq_down(CoreOps *c, int a, int b) {
   for (int level = a; level < b; level++) {
-    if (c->leg_ok(level, prm.nu1) && c->leg_ok(level, prm.nu2)) {
-      OCU_TRY(c->leg_down(level, prm.nu1));
-      continue;
-    }
     OCU_TRY(c->relax(level, prm.nu1, RO_RED_BLACK));
     OCU_TRY(c->clear_and_restrict(level, false, false));
   }
@@ -651,10 +558,6 @@ ocu_status MGSolver::enq_tail_up(CoreOps *c, int s, int f) {
   const bool sym = prm.make_symmetric_operator != 0;
   OCU_TRY(c->cycle_tail(s, prm.nu1, prm.nu2, coarse_iters(), sym));
   for (int level = s - 1; level >= f; level--) {
-    if (c->leg_ok(level, prm.nu1) && c->leg_ok(level, prm.nu2)) {
-      OCU_TRY(c->leg_up(level, prm.nu2, sym ? RO_BLACK_RED : RO_RED_BLACK));
-      continue;
-    }
     OCU_TRY(c->prolong(level + 1, level));
     if (level > 0) OCU_TRY(c->relax(level, prm.nu2, sym ? RO_BLACK_RED : RO_RED_BLACK));
   }
@@ -802,10 +705,6 @@ ocu_status MGSolver::cycle(CoreOps *c, int fine_level, double tolerance, double 
   const int s = c->tail_start() > fine_level ? c->tail_start() : fine_level;
   *converged = false;
   for (int level = fine_level; level < s; level++) {
-    if (c->leg_ok(level, prm.nu1) && c->leg_ok(level, prm.nu2)) {
-      OCU_TRY(c->leg_down(level, prm.nu1));
-      continue;
-    }
     OCU_TRY(c->relax(level, prm.nu1, RO_RED_BLACK));
     if (level == 0) {
       double *l2 = (conv & OCU_CONVERGENCE_CALC_L2) ? rl2 : nullptr;
@@ -826,10 +725,6 @@ ocu_status MGSolver::cycle(CoreOps *c, int fine_level, double tolerance, double 
   OCU_TRY(c->cycle_tail(s, prm.nu1, prm.nu2, coarse_iters(), sym));
   (void)coarse_level;
   for (int level = s - 1; level >= fine_level; level--) {
-    if (c->leg_ok(level, prm.nu1) && c->leg_ok(level, prm.nu2)) {
-      OCU_TRY(c->leg_up(level, prm.nu2, sym ? RO_BLACK_RED : RO_RED_BLACK));
-      continue;
-    }
     OCU_TRY(c->prolong(level + 1, level));
     if (level > 0) OCU_TRY(c->relax(level, prm.nu2, sym ? RO_BLACK_RED : RO_RED_BLACK));
   }
@@ -1096,11 +991,7 @@ ocu_status MGSolver::apply_knobs() {
   cf.sweep_cells = cd.sweep_cells = prm.sweep_cells <= 0 ? kDefaultSweepCells : prm.sweep_cells;
   if (cf.sweep_cells > 0 && cf.num_levels > 0) OCU_TRY(cf.ensure_sweep_buffers());
   if (cd.sweep_cells > 0 && cd.num_levels > 0) OCU_TRY(cd.ensure_sweep_buffers());
-  cf.leg_cells = cd.leg_cells = prm.leg_cells <= 0 ? kDefaultLegCells : prm.leg_cells;
-  cf.tail_ctas = cd.tail_ctas = prm.tail_ctas <= 0 ? kDefaultTailCtas : (prm.tail_ctas > 8 ? 8 : prm.tail_ctas);
   cf.wait_limit = cd.wait_limit = prm.wait_limit;
-  if (cf.leg_cells > 0 && cf.num_levels > 0) OCU_TRY(cf.ensure_leg_buffers());
-  if (cd.leg_cells > 0 && cd.num_levels > 0) OCU_TRY(cd.ensure_leg_buffers());
   return OCU_OK;
 }
 

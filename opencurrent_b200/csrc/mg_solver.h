@@ -28,19 +28,6 @@ constexpr int kDefaultTailCells = 64;
 // against 124 us for the two colour launches, but it is instruction-bound, slower in FP64, and a
 // whole solve is not faster with it yet.
 constexpr int kDefaultSweepCells = 0;
-// Levels below 0 with at most this many cells can run each V-cycle leg as one launch (smoothing
-// + restriction, prolongation + smoothing over shared-memory boxes with a redundant halo).  Off
-// by default: measured V-cycle times (FP32 / FP64, 1024-thread boxes) with the legs on the 32^3,
-// 16^3 and 8^3 levels are 137 / 153 us from 64^3 against 125 / 151 us with the per-operation
-// launches (98 / 108 against 96 / 113 us from 32^3): the redundant halo work (about 7 updates
-// per cell) costs what the saved launches do.
-constexpr long long kDefaultLegCells = 0;
-// CTAs of the thread-block cluster that runs the tail kernel (1 = a single CTA).  One by
-// default: with the tail phases spread over a cluster (global memory, cluster barriers) a
-// 256^3 FP32 V-cycle takes 488 / 517 us with the tail at 4096 / 32768 cells against 476 us with
-// the per-operation launches down to the 4^3 level (FP64: 796 / 828 against 775 us) -- a phase
-// costs about what a launch with programmatic dependencies does.
-constexpr int kDefaultTailCtas = 1;
 double mg_optimal_omega(double fx, double fy, double fz);
 
 // The virtual level operations of Sol_MultigridPressure3DBase (sol_mgpressure3d.h:76-80).
@@ -63,11 +50,6 @@ struct CoreOps {
   // levels tail_start()..L-1 of a V-cycle in one launch
   virtual int tail_start() const = 0;
   virtual ocu_status cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool symmetric) = 0;
-  // one-launch V-cycle legs of a small level (kernels_mg_legs.cu); leg_ok is the same for both
-  // legs of a level, so the level's u returns to its own buffer after the up-leg
-  virtual bool leg_ok(int level, int nu) const = 0;
-  virtual ocu_status leg_down(int level, int nu1) = 0;
-  virtual ocu_status leg_up(int level, int nu2, int order) = 0;
 };
 
 // Level hierarchy of one precision (Sol_MultigridPressure3DDevice<T> storage).
@@ -93,9 +75,6 @@ struct MGCore : CoreOps {
   bool store_residuals = false;   // keep r_grid filled (reference kernels) for read_r
   int tail_cells = kDefaultTailCells;    // levels with at most this many cells run in the tail kernel
   int sweep_cells = kDefaultSweepCells;  // levels with at least this many cells use the two-colour pass
-  long long leg_cells = kDefaultLegCells;  // levels below 0 with at most this many cells run one-launch legs
-  std::vector<ocu_grid *> grids_uleg;      // their second u buffer
-  int tail_ctas = kDefaultTailCtas;        // CTAs of the cluster that runs the tail kernel
   // two-colour pass: per level a second u buffer (ping-pong) and the TMA maps of u, u2 and b
   std::vector<ocu_grid *> grids_u2;
   std::vector<SweepTmap> tm_u, tm_u2, tm_b;
@@ -108,11 +87,6 @@ struct MGCore : CoreOps {
   bool sweep2_ok(int level) const;
   ocu_status ensure_sweep_buffers();
   ocu_status relax_pairs(int level, int iterations, int order);
-  ocu_status ensure_leg_buffers();
-  bool leg_ok(int level, int nu) const override;
-  ocu_status leg_down(int level, int nu1) override;
-  ocu_status leg_up(int level, int nu2, int order) override;
-  LegLevel<T> leg_level(int level, const T *u_in, T *u_out) const;
   ocu_status enqueue_restrict_residuals(int fine, int coarse, bool want_l2, bool want_linf) override;
   ocu_status clear_and_restrict(int fine, bool want_l2, bool want_linf) override;
   ocu_status finish_norms(int fine, double *l2, double *linf) override;

@@ -57,15 +57,6 @@ __device__ __forceinline__ T relax_value(T uc, T bv, T zm, T zp, T ym, T yp, T x
   return uc + c.omega * res / dg;
 }
 
-// Global load; CG = true reads through L2 only (ld.global.cg): data written by other CTAs of a
-// cluster earlier in the same launch (the cluster-wide coarse tail) must not come from a
-// non-coherent path.
-template <bool CG, typename T>
-__device__ __forceinline__ T gld(const T *p) {
-  if constexpr (CG) return __ldcg(p);
-  else return *p;
-}
-
 template <typename T>
 __device__ __forceinline__ T relax_point(const T *__restrict__ u, const T *__restrict__ b, long long id, long long xs,
                                          long long ys, int i, int j, int k, int nx, int ny, int nz,
@@ -81,23 +72,6 @@ __device__ __forceinline__ T residual_at(const T *__restrict__ u, const T *__res
                                          long long ys, const ResCoefT<T> &c) {
   return b[id] - (c.fzh * (u[id - 1] + u[id + 1]) + c.fyh * (u[id - ys] + u[id + ys]) +
                   c.fxh * (u[id - xs] + u[id + xs]) - c.dg * u[id]);
-}
-
-// The same two with coherent (L2) loads, for the cluster-wide tail.
-template <typename T>
-__device__ __forceinline__ T relax_point_cg(const T *u, const T *b, long long id, long long xs, long long ys, int i,
-                                            int j, int k, int nx, int ny, int nz, const RelaxCoefD<T> &c) {
-  return relax_value<T>(__ldcg(u + id), __ldcg(b + id), __ldcg(u + id - 1), __ldcg(u + id + 1), __ldcg(u + id - ys),
-                        __ldcg(u + id + ys), __ldcg(u + id - xs), __ldcg(u + id + xs), i, j, k, nx, ny, nz, c,
-                        nullptr);
-}
-
-template <typename T>
-__device__ __forceinline__ T residual_at_cg(const T *u, const T *b, long long id, long long xs, long long ys,
-                                            const ResCoefT<T> &c) {
-  return __ldcg(b + id) - (c.fzh * (__ldcg(u + id - 1) + __ldcg(u + id + 1)) +
-                           c.fyh * (__ldcg(u + id - ys) + __ldcg(u + id + ys)) +
-                           c.fxh * (__ldcg(u + id - xs) + __ldcg(u + id + xs)) - c.dg * __ldcg(u + id));
 }
 
 }  // namespace ocub

@@ -45,9 +45,7 @@ def pair(dt, shape, h, bcname, seed=0, sym=0, disable_host=0, conv=0x05, **knobs
 
 
 KNOBS = [dict(), dict(unfused=True), dict(tail_cells=-1), dict(tail_cells=40000), dict(tail_cells=4096),
-         dict(store_residual_grids=True), dict(sweep_cells=1), dict(sweep_cells=-1), dict(leg_cells=32768),
-         dict(leg_cells=1 << 20), dict(tail_cells=40000, tail_ctas=8), dict(tail_cells=4096, tail_ctas=3),
-         dict(tail_cells=40000, tail_ctas=1)]
+         dict(store_residual_grids=True), dict(sweep_cells=1), dict(sweep_cells=-1)]
 
 
 @pytest.mark.parametrize("dt", [F32, F64])
