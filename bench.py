@@ -420,6 +420,7 @@ def run_secondary(torch, ocu, _capi, lib, stream, sh):
     out["ns_128x128x64_fp32_fp64_pressure_steps_per_s"] = round(steps / (ms * 1e-3), 2)
     out["ns_fp64_pressure_steps_projection_above_tol"] = unconverged
     out.update(run_ensemble(torch, ocu, stream, sh))
+    out.update(run_persistent_ensemble(torch, ocu, stream, sh))
     out.update(run_differentiable(torch, ocu))
     return out
 
@@ -545,6 +546,58 @@ def run_ensemble(torch, ocu, stream, sh, count=512):
             "ensemble_classes": [{"n": c["dims"][0], "members": c["members"], "nu": [c["nu1"], c["nu2"]],
                                   "relax_block": list(c["relax_block"]), "tuned_ms": round(c["ms"], 3)}
                                  for c in ens.classes()]}
+
+
+def run_persistent_ensemble(torch, ocu, stream, sh, count=512):
+    """The same 512 members (sizes from {32,48,64,96}^3, seed 1; rhs U[-1,1] mean-removed, seed
+    1000 + index; each to 1e-6 relative L2) solved by the persistent refinement ensemble: ONE
+    kernel launch in which each block runs whole member solves (FP64 residual, FP32 split-layout
+    multigrid corrections), autotuned first (not timed), then timed from a zero guess."""
+    sizes = ensemble_sizes(count, 1)
+    dims = [(n, n, n) for n in sizes]
+    ens = ocu.PersistentEnsemble(dims, [(1.0 / n,) * 3 for n in sizes])
+    ens.set_stream(stream.cuda_stream)
+    tols = []
+    for m, n in enumerate(sizes):
+        b = np.random.default_rng(1000 + m).uniform(-1.0, 1.0, (n, n, n))
+        b -= b.mean()
+        L = ocu.layout(n, n, n)
+        ens.rhs(m).copy_from_host(padded(b, L, np.float64))
+        tols.append(1e-6 * float(np.sqrt(np.mean(b ** 2))))
+    ens.autotune(tols)
+    pressures = [ens.pressure(m) for m in range(count)]
+
+    def zero():
+        for g in pressures:
+            _capi.check(ocu.load().ocu_grid_clear(g.handle, 0.0, sh))
+
+    zero()
+    ens.solve(tols)  # graph recorded
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps, total = 3, 0.0
+    for _ in range(reps):
+        zero()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        conv = ens.solve(tols)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total += e0.elapsed_time(e1)
+    ms = total / reps
+    p = ens.params()
+    stats = [ens.member_stats(m) for m in range(count)]
+    corr = [st.corrections for st in stats]
+    # per member and correction: the FP32 V-cycles (cycles + the nested-iteration ramp ~ 1/7
+    # cycle) at 12.57 N 4 bytes each, the FP64 residual (x, b read, float r written: 20 N) and
+    # the correction update (x read and written, e read: 20 N); plus the final residual check
+    alg = sum((c * ((p.cycles + 1.0 / 7.0) * 12.57 * 4 + 40) + 20) * n ** 3 for c, n in zip(corr, sizes))
+    blocks, threads, scratch = ens.launch_shape()
+    return {"pens_512_ms": round(ms, 3), "pens_members_converged": conv,
+            "pens_alg_gbs": round(alg / (ms * 1e-3) / 1e9, 1),
+            "pens_corrections_mean": round(float(np.mean(corr)), 2),
+            "pens_max_rel_residual": float(f"{max(st.l2 / t for st, t in zip(stats, tols)) * 1e-6:.3e}"),
+            "pens_tuning": {"threads": p.threads, "cycles": p.cycles, "nu": [p.nu1, p.nu2], "blocks": blocks,
+                            "scratch_mb": round(scratch / 2 ** 20, 1)}}
 
 
 # --------------------------------------------------------------------------- CPU arms ---

@@ -306,6 +306,58 @@ ocu_status ocu_ens_set_tuning(ocu_ens *e, int cls, const ocu_ens_tuning *tuning)
  * shapes and keeps the fastest that converges every member; leaves every pressure zeroed. */
 ocu_status ocu_ens_autotune(ocu_ens *e, const double *tol, int max_iter);
 
+/* ---- persistent refinement ensembles ----------------------------------------------------
+ * No reference counterpart as a whole: many Sol_MultigridPressure3DBase::solve calls
+ * (sol_mgpressure3d.cpp:332-370: sqrt(sum r^2 / N) of the residual against an absolute
+ * tolerance) on right-hand sides of uneven sizes, run as ONE persistent kernel launch (replayed
+ * from a CUDA graph).  Each block takes the next member (largest first) from a device counter
+ * and runs its whole solve: an FP64 iterative refinement (FP64 residual and pressure) whose
+ * corrections are FP32 multigrid solves on the library's red/black split levels (nested
+ * iteration + `cycles` V-cycles), until the FP64 residual's L2 norm is at most the member's
+ * tolerance or max_outer corrections were applied.  No block waits for another block.
+ * Results are checked against FP64 multigrid solutions at the tolerance, not bit for bit. */
+typedef struct ocu_pens ocu_pens;
+typedef struct ocu_pens_params {
+  ocu_bc_set bc;       /* every member's boundary conditions (fixed at creation); faces Neumann,
+                          Dirichlet, periodic (even sizes on every level) or none */
+  int nu1, nu2;        /* red-black iterations before / after the coarse correction */
+  int cycles;          /* V-cycles at level 0 per correction, after the nested iteration
+                          (0: the nested iteration alone) */
+  int ramp_iters;      /* iterations per level on the way up the nested iteration (0 = nu1+nu2) */
+  int max_outer;       /* corrections at most (0 = 10) */
+  int threads;         /* threads per block: 256, 512 or 1024 */
+  int tail_cells;      /* levels with at most this many cells are solved in shared memory
+                          (0 = 512; fixed at creation) */
+  double ms;           /* autotuner: measured solve time of the chosen setting */
+} ocu_pens_params;
+typedef struct ocu_pens_stats {
+  int converged;       /* 1 when the last solve reached the member's tolerance */
+  int corrections;     /* FP32 correction solves applied */
+  int vcycles;         /* level-0 V-cycles run by them */
+  double l2;           /* FP64 residual norm sqrt(sum r^2 / N) at the last check */
+} ocu_pens_stats;
+void ocu_pens_params_default(ocu_pens_params *p);
+/* dims: 3 ints per member; h: 3 doubles per member. */
+ocu_status ocu_pens_create(int members, const int *dims, const double *h, const ocu_pens_params *params,
+                           ocu_pens **out);
+void ocu_pens_destroy(ocu_pens *e);
+ocu_status ocu_pens_set_stream(ocu_pens *e, ocu_stream s);
+/* FP64 views (standard layout, ghost 1) owned by the ensemble; the pressure is the initial guess
+ * of the next solve and its result. */
+ocu_status ocu_pens_rhs(ocu_pens *e, int member, ocu_grid **out);
+ocu_status ocu_pens_pressure(ocu_pens *e, int member, ocu_grid **out);
+/* tol: one absolute L2 tolerance per member.  *converged gets the members that reached it;
+ * OCU_ERR_NOT_CONVERGED if some did not. */
+ocu_status ocu_pens_solve(ocu_pens *e, const double *tol, int *converged);
+ocu_status ocu_pens_member_stats(const ocu_pens *e, int member, ocu_pens_stats *stats);
+ocu_status ocu_pens_get_params(const ocu_pens *e, ocu_pens_params *p);
+ocu_status ocu_pens_set_params(ocu_pens *e, const ocu_pens_params *p);
+/* blocks of the persistent launch, threads per block, bytes of the per-block FP32 hierarchies */
+ocu_status ocu_pens_launch_shape(const ocu_pens *e, int *blocks, int *threads, long long *scratch_bytes);
+/* Times whole solves from a zero guess over thread counts, cycles and smoothing pairs; keeps the
+ * fastest that converges every member (ms set); leaves every pressure zeroed. */
+ocu_status ocu_pens_autotune(ocu_pens *e, const double *tol);
+
 /* ---- projection (Sol_ProjectDivergence3DDevice<T>, sol_project3d.h:29-129) ------------- */
 ocu_status ocu_project_create(ocu_dtype dtype, ocu_project **out);
 /* The same with the pressure solver's kind chosen: OCU_MG_F32 / OCU_MG_F64 are

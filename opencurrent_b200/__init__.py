@@ -17,6 +17,7 @@ from ._capi import *  # noqa: F401,F403  (enums, structs)
 from ._capi import OcuError, check, load
 
 __all__ = [
+    "PersistentEnsemble",
     "BoundaryCondition", "BoundaryConditionSet", "Grid3DDevice", "Sol_MultigridPressure3DDevice",
     "Sol_MultigridPressure3DDeviceF", "Sol_MultigridPressure3DDeviceD",
     "Sol_MultigridPressureMixed3DDeviceD", "Sol_ProjectDivergence3DDevice",
@@ -408,6 +409,87 @@ class PressureEnsemble:
         try:
             if self._h:
                 load().ocu_ens_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+class PersistentEnsemble:
+    """Many independent pressure solves of uneven sizes in one persistent kernel launch
+    (ocu_pens_* in the C ABI).
+
+    Each block of the launch takes the next member (largest first) and runs its whole solve: an
+    FP64 iterative refinement whose corrections are FP32 multigrid solves on the library's
+    red/black split levels, until sqrt(sum r^2 / N) of the FP64 residual is at most the member's
+    tolerance.  Right-hand sides and pressures are FP64 grids.
+    """
+
+    def __init__(self, dims, spacings, bc=None, nu1=2, nu2=2, cycles=2, ramp_iters=0, max_outer=10,
+                 threads=512, tail_cells=0):
+        lib = load()
+        n = len(dims)
+        d = (C.c_int * (3 * n))(*[int(v) for t in dims for v in t])
+        h = (C.c_double * (3 * n))(*[float(v) for t in spacings for v in t])
+        p = PensParams()
+        lib.ocu_pens_params_default(C.byref(p))
+        if bc is not None:
+            p.bc = bc.to_c()
+        p.nu1, p.nu2, p.cycles, p.ramp_iters = nu1, nu2, cycles, ramp_iters
+        p.max_outer, p.threads, p.tail_cells = max_outer, threads, tail_cells
+        handle = C.c_void_p()
+        check(lib.ocu_pens_create(n, d, h, C.byref(p), C.byref(handle)))
+        self._h = handle.value
+        self.count = n
+
+    def rhs(self, m):
+        out = C.c_void_p()
+        check(load().ocu_pens_rhs(self._h, m, C.byref(out)))
+        return Grid3DDevice._borrow(out.value, self)
+
+    def pressure(self, m):
+        out = C.c_void_p()
+        check(load().ocu_pens_pressure(self._h, m, C.byref(out)))
+        return Grid3DDevice._borrow(out.value, self)
+
+    def set_stream(self, stream_handle):
+        check(load().ocu_pens_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    def solve(self, tol):
+        """tol: absolute L2 tolerance per member.  Returns the number of members converged."""
+        t = (C.c_double * self.count)(*[float(v) for v in tol])
+        conv = C.c_int()
+        check(load().ocu_pens_solve(self._h, t, C.byref(conv)), allow=(ERR_NOT_CONVERGED,))
+        return conv.value
+
+    def member_stats(self, m):
+        st = PensStats()
+        check(load().ocu_pens_member_stats(self._h, m, C.byref(st)))
+        return st
+
+    def params(self):
+        p = PensParams()
+        check(load().ocu_pens_get_params(self._h, C.byref(p)))
+        return p
+
+    def set_params(self, **kw):
+        p = self.params()
+        for k, v in kw.items():
+            setattr(p, k, v)
+        check(load().ocu_pens_set_params(self._h, C.byref(p)))
+
+    def launch_shape(self):
+        b, t, s = C.c_int(), C.c_int(), C.c_longlong()
+        check(load().ocu_pens_launch_shape(self._h, C.byref(b), C.byref(t), C.byref(s)))
+        return b.value, t.value, s.value
+
+    def autotune(self, tol):
+        t = (C.c_double * self.count)(*[float(v) for v in tol])
+        check(load().ocu_pens_autotune(self._h, t))
+
+    def __del__(self):
+        try:
+            if self._h:
+                load().ocu_pens_destroy(self._h)
                 self._h = None
         except Exception:
             pass

@@ -66,6 +66,16 @@ class EnsTuning(C.Structure):
     _fields_ = [("nu1", C.c_int), ("nu2", C.c_int), ("relax_block", C.c_int * 3), ("ms", C.c_double)]
 
 
+class PensParams(C.Structure):
+    _fields_ = [("bc", BCSet), ("nu1", C.c_int), ("nu2", C.c_int), ("cycles", C.c_int),
+                ("ramp_iters", C.c_int), ("max_outer", C.c_int), ("threads", C.c_int),
+                ("tail_cells", C.c_int), ("ms", C.c_double)]
+
+
+class PensStats(C.Structure):
+    _fields_ = [("converged", C.c_int), ("corrections", C.c_int), ("vcycles", C.c_int), ("l2", C.c_double)]
+
+
 class NSParams(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double),
@@ -142,6 +152,18 @@ SIGNATURES = {
     "ocu_ens_class_info": (I, [P, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(EnsTuning)]),
     "ocu_ens_set_tuning": (I, [P, I, C.POINTER(EnsTuning)]),
     "ocu_ens_autotune": (I, [P, C.POINTER(D), I]),
+    "ocu_pens_params_default": (None, [C.POINTER(PensParams)]),
+    "ocu_pens_create": (I, [I, C.POINTER(C.c_int), C.POINTER(D), C.POINTER(PensParams), PP]),
+    "ocu_pens_destroy": (None, [P]),
+    "ocu_pens_set_stream": (I, [P, P]),
+    "ocu_pens_rhs": (I, [P, I, PP]),
+    "ocu_pens_pressure": (I, [P, I, PP]),
+    "ocu_pens_solve": (I, [P, C.POINTER(D), C.POINTER(C.c_int)]),
+    "ocu_pens_member_stats": (I, [P, I, C.POINTER(PensStats)]),
+    "ocu_pens_get_params": (I, [P, C.POINTER(PensParams)]),
+    "ocu_pens_set_params": (I, [P, C.POINTER(PensParams)]),
+    "ocu_pens_launch_shape": (I, [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_longlong)]),
+    "ocu_pens_autotune": (I, [P, C.POINTER(D)]),
     "ocu_project_create": (I, [I, PP]),
     "ocu_project_create_with": (I, [I, PP]),
     "ocu_project_create_fields": (I, [I, I, PP]),
