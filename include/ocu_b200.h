@@ -326,6 +326,8 @@ typedef struct ocu_pens_params {
   int ramp_iters;      /* iterations per level on the way up the nested iteration (0 = nu1+nu2) */
   int max_outer;       /* corrections at most (0 = 10) */
   int threads;         /* threads per block: 256, 512 or 1024 */
+  int dense;           /* 1: 1536 threads per SM at up to 42 registers (threads 256 or 512);
+                          0: 1024 threads per SM at up to 64 */
   int tail_cells;      /* levels with at most this many cells are solved in shared memory
                           (0 = 512; fixed at creation) */
   double ms;           /* autotuner: measured solve time of the chosen setting */

@@ -425,7 +425,7 @@ class PersistentEnsemble:
     """
 
     def __init__(self, dims, spacings, bc=None, nu1=2, nu2=2, cycles=2, ramp_iters=0, max_outer=10,
-                 threads=512, tail_cells=0):
+                 threads=512, dense=False, tail_cells=0):
         lib = load()
         n = len(dims)
         d = (C.c_int * (3 * n))(*[int(v) for t in dims for v in t])
@@ -435,7 +435,7 @@ class PersistentEnsemble:
         if bc is not None:
             p.bc = bc.to_c()
         p.nu1, p.nu2, p.cycles, p.ramp_iters = nu1, nu2, cycles, ramp_iters
-        p.max_outer, p.threads, p.tail_cells = max_outer, threads, tail_cells
+        p.max_outer, p.threads, p.dense, p.tail_cells = max_outer, threads, int(bool(dense)), tail_cells
         handle = C.c_void_p()
         check(lib.ocu_pens_create(n, d, h, C.byref(p), C.byref(handle)))
         self._h = handle.value

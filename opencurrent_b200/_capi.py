@@ -69,7 +69,7 @@ class EnsTuning(C.Structure):
 class PensParams(C.Structure):
     _fields_ = [("bc", BCSet), ("nu1", C.c_int), ("nu2", C.c_int), ("cycles", C.c_int),
                 ("ramp_iters", C.c_int), ("max_outer", C.c_int), ("threads", C.c_int),
-                ("tail_cells", C.c_int), ("ms", C.c_double)]
+                ("dense", C.c_int), ("tail_cells", C.c_int), ("ms", C.c_double)]
 
 
 class PensStats(C.Structure):

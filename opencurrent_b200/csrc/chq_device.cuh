@@ -33,10 +33,40 @@ struct ChqK {
   float fxh, fyh, fzh, dgh;  // residual: f / h^2, ld / h^2
 };
 
+// Division of a non-negative int by a run-time constant d: a shift and a mask when d is a power
+// of two, else a multiply-high by a precomputed magic number (Granlund and Montgomery, "Division
+// by invariant integers using multiplication", 1994: l = ceil(log2 d),
+// m = floor(2^32 (2^l - d) / d) + 1, q = (umulhi(m, t) + t) >> l, exact for 0 <= t < 2^31).
+struct FDiv {
+  int d, sh;    // divisor; log2 d when a power of two, else -1
+  unsigned m;   // magic multiplier
+  int l;        // ceil(log2 d)
+};
+
+inline FDiv make_fdiv(int d) {
+  FDiv f;
+  f.d = d;
+  f.l = 0;
+  while ((1LL << f.l) < d) f.l++;
+  f.sh = ((1LL << f.l) == d) ? f.l : -1;
+  f.m = (unsigned)((((unsigned long long)1 << 32) * (((unsigned long long)1 << f.l) - d)) / d + 1);
+  return f;
+}
+
+__device__ __forceinline__ void split(const FDiv &f, int t, int &quot, int &rem) {
+  if (f.sh >= 0) {
+    quot = t >> f.sh;
+    rem = t & (f.d - 1);
+  } else {
+    quot = (int)(((unsigned long long)__umulhi((unsigned)t, f.m) + (unsigned)t) >> f.l);
+    rem = t - quot * f.d;
+  }
+}
+
 struct ChqG {
   float *u0, *u1, *b0, *b1;
   int nx, ny, nz, rz;
-  int qsh, ysh, zsh;  // log2 of rz/4, ny, nz when powers of two, else -1
+  FDiv fq, fy;  // division by rz/4 (float4 groups per row) and by ny
 };
 
 inline int log2_exact(int v) {
@@ -85,15 +115,6 @@ __device__ __forceinline__ float residual_cell(float u, float b, float sx, float
   return b - __fmaf_rn(k.fzh, sz, __fmaf_rn(k.fyh, sy, __fmaf_rn(k.fxh, sx, -k.dgh * u)));
 }
 
-__device__ __forceinline__ void split_index(int t, int div, int sh, int &quot, int &rem) {
-  if (sh >= 0) {
-    quot = t >> sh;
-    rem = t & (div - 1);
-  } else {
-    quot = t / div;
-    rem = t - quot * div;
-  }
-}
 
 // One colour of a red-black SOR iteration.  A thread owns four consecutive entries m of one
 // colour row (one float4); the z neighbours are the other colour's entries m - 1 + p .. m + p
@@ -115,10 +136,9 @@ __device__ __forceinline__ void split_index(int t, int div, int sh, int &quot, i
 #endif
 template <bool NC>
 __device__ __forceinline__ void chq_relax_item(const ChqG &g, const ChqK &k, const ChqBC &bc, int color, int t) {
-  const int qpr = g.rz >> 2;
   int row, q, i, j;
-  split_index(t, qpr, g.qsh, row, q);
-  split_index(row, g.ny, g.ysh, i, j);
+  split(g.fq, t, row, q);
+  split(g.fy, row, i, j);
   const int p = (i + j + color) & 1;
   const float *__restrict__ o = color ? g.u0 : g.u1;
   float *__restrict__ u = color ? g.u1 : g.u0;
@@ -206,11 +226,11 @@ __device__ __forceinline__ void load4(const FRow &r, int m2, float v[4]) {
 // coarse pair's u is zeroed (the next V-cycle leg starts from zero).  All lanes of a warp share
 // (I, J), so every row and boundary decision is uniform across the warp.
 template <bool NC>
-__device__ __forceinline__ void chq_restrict_item(const ChqG &f, const ChqG &c, const ChqK &k, const ChqBC &bc, int cm,
-                                                  int cmsh, int t) {
+__device__ __forceinline__ void chq_restrict_item(const ChqG &f, const ChqG &c, const ChqK &k, const ChqBC &bc,
+                                                  const FDiv &fcm, int t) {
   int r, mp, I, J;
-  split_index(t, cm, cmsh, r, mp);
-  split_index(r, c.ny, c.ysh, I, J);
+  split(fcm, t, r, mp);
+  split(c.fy, r, I, J);
   const int x0 = 2 * I, y0 = 2 * J, m2 = 2 * mp;
   const bool second = 2 * mp + 1 < c.nz;  // coarse K = 2m' + 1 exists
   float u[2][2][6], bv[2][2][4];           // u[a][b][1 + e], e = -1..4
@@ -290,11 +310,11 @@ __device__ __forceinline__ void chq_restrict_item(const ChqG &f, const ChqG &c, 
 // follow the homogeneous rules axis by axis (a corner is the product of the face signs times the
 // cell).  Rows are warp-uniform; the eight fine float2 pairs are loaded before the first store.
 template <bool NC>
-__device__ __forceinline__ void chq_prolong_item(const ChqG &c, const ChqG &f, const ChqBC &bc, int cm, int cmsh,
+__device__ __forceinline__ void chq_prolong_item(const ChqG &c, const ChqG &f, const ChqBC &bc, const FDiv &fcm,
                                                  int t) {
   int r, mp, I, J;
-  split_index(t, cm, cmsh, r, mp);
-  split_index(r, c.ny, c.ysh, I, J);
+  split(fcm, t, r, mp);
+  split(c.fy, r, I, J);
   const int K0 = 2 * mp;
   const bool second = K0 + 1 < c.nz;
   // V[di][dj][q]: coarse value at (I + di - 1, J + dj - 1, K0 - 1 + q), q = 0..3
@@ -636,9 +656,8 @@ inline ChqG make_g(const ChqLevel &l) {
   ChqG g;
   g.u0 = l.u[0]; g.u1 = l.u[1]; g.b0 = l.b[0]; g.b1 = l.b[1];
   g.nx = l.nx; g.ny = l.ny; g.nz = l.nz; g.rz = l.rz;
-  g.qsh = log2_exact(l.rz / 4);
-  g.ysh = log2_exact(l.ny);
-  g.zsh = log2_exact(l.nz);
+  g.fq = make_fdiv(l.rz / 4);
+  g.fy = make_fdiv(l.ny);
   return g;
 }
 

@@ -41,8 +41,9 @@ constexpr int kPensMaxLevels = 12;
 // b1) in the block's scratch hierarchy, its coarse-pair count and operator coefficients.
 struct PensLevel {
   int nx, ny, nz, rz;
-  int qsh, ysh, zsh;
-  int cm, cmsh;  // pairs per row of this level (as the coarse level of a transfer)
+  int ysh, zsh;  // log2 of ny, nz when powers of two, else -1 (the shared-memory tail)
+  FDiv fq, fy;   // division by rz/4 and by ny
+  FDiv fcm;      // pairs per row of this level (as the coarse level of a transfer)
   long long off;
   ChqK k;
 };
@@ -56,7 +57,7 @@ struct PensMember {
   const double *b;    // origin of the FP64 right-hand side
   long long xs, ys;
   int nx, ny, nz, M;  // M = pairs per row at level 0
-  int msh, ysh;       // log2 of M and ny when powers of two, else -1
+  FDiv fM, fY;        // division by M and by ny
   int nlev, ts;       // FP32 levels; first level of the shared-memory tail
   int vec;            // FP64 rows allow 16-byte pairs
   int pad_;
@@ -94,12 +95,18 @@ __device__ __forceinline__ ChqG level_g(const PensLevel &L, float *H) {
   g.b0 = g.u0 + 2 * n;
   g.b1 = g.u0 + 3 * n;
   g.nx = L.nx; g.ny = L.ny; g.nz = L.nz; g.rz = L.rz;
-  g.qsh = L.qsh; g.ysh = L.ysh; g.zsh = L.zsh;
+  g.fq = L.fq; g.fy = L.fy;
   return g;
 }
 
+// The phases take their level records by value and copy them into locals: a record read through
+// a reference (to the caller's stack or to shared memory) would be re-read after every global
+// store, which the compiler cannot prove does not alias it.
 template <int NT>
-__device__ __noinline__ void b_relax(const ChqG &g, const ChqK &k, const ChqBC &bc, int iterations) {
+__device__ __noinline__ void b_relax(const ChqG g_, const ChqK k_, const ChqBC bc_, int iterations) {
+  const ChqG g = g_;
+  const ChqK k = k_;
+  const ChqBC bc = bc_;
   const int n = g.nx * g.ny * (g.rz >> 2);
   for (int it = 0; it < iterations; it++)
     for (int color = 0; color < 2; color++) {
@@ -109,55 +116,78 @@ __device__ __noinline__ void b_relax(const ChqG &g, const ChqK &k, const ChqBC &
 }
 
 template <int NT>
-__device__ __noinline__ void b_restrict(const ChqG &f, const ChqG &c, const ChqK &k, const ChqBC &bc, int cm, int cmsh) {
-  const int n = c.nx * c.ny * cm;
-  for (int t = threadIdx.x; t < n; t += NT) chq_restrict_item<false>(f, c, k, bc, cm, cmsh, t);
+__device__ __noinline__ void b_restrict(const ChqG f_, const ChqG c_, const ChqK k_, const ChqBC bc_, const FDiv fcm_) {
+  const ChqG f = f_, c = c_;
+  const ChqK k = k_;
+  const ChqBC bc = bc_;
+  const FDiv fcm = fcm_;
+  const int n = c.nx * c.ny * fcm.d;
+  for (int t = threadIdx.x; t < n; t += NT) chq_restrict_item<false>(f, c, k, bc, fcm, t);
   __syncthreads();
 }
 
 template <int NT>
-__device__ __noinline__ void b_prolong(const ChqG &c, const ChqG &f, const ChqBC &bc, int cm, int cmsh) {
-  const int n = c.nx * c.ny * cm;
-  for (int t = threadIdx.x; t < n; t += NT) chq_prolong_item<false>(c, f, bc, cm, cmsh, t);
+__device__ __noinline__ void b_prolong(const ChqG c_, const ChqG f_, const ChqBC bc_, const FDiv fcm_) {
+  const ChqG c = c_, f = f_;
+  const ChqBC bc = bc_;
+  const FDiv fcm = fcm_;
+  const int n = c.nx * c.ny * fcm.d;
+  for (int t = threadIdx.x; t < n; t += NT) chq_prolong_item<false>(c, f, bc, fcm, t);
   __syncthreads();
 }
 
 template <int NT>
-__device__ __noinline__ void b_clear_u(const ChqG &g) {  // u0 and u1 are adjacent, rz a multiple of 4
+__device__ __noinline__ void b_clear_u(const ChqG g) {  // u0 and u1 are adjacent, rz a multiple of 4
   const int n4 = g.nx * g.ny * g.rz / 2;
   float4 *p = reinterpret_cast<float4 *>(g.u0);
   for (int t = threadIdx.x; t < n4; t += NT) p[t] = make_float4(0.f, 0.f, 0.f, 0.f);
   __syncthreads();
 }
 
-__device__ __forceinline__ void pair_index(const PensMember &D, int t, int &i, int &j, int &m, int &row) {
-  split_index(t, D.M, D.msh, row, m);
-  split_index(row, D.ny, D.ysh, i, j);
-}
 
 // r = b - A x in FP64 (the reference operator with the ghost values of x), written as float into
 // the level-0 colour arrays; returns the block's sum of r^2 (every thread gets it).
+// The FP64 level-0 record of a member, in registers.
+struct Fine64 {
+  double *x;
+  const double *b;
+  long long xs, ys;
+  int nx, ny, nz, M, vec;
+  FDiv fM, fY;
+};
+
+__device__ __forceinline__ Fine64 fine64(const PensMember &D) {
+  Fine64 F;
+  F.x = D.x; F.b = D.b; F.xs = D.xs; F.ys = D.ys;
+  F.nx = D.nx; F.ny = D.ny; F.nz = D.nz; F.M = D.M; F.vec = D.vec;
+  F.fM = D.fM; F.fY = D.fY;
+  return F;
+}
+
 template <int NT>
-__device__ __noinline__ double b_residual(const PensMember &D, const ChqG &g0, double *red) {
-  const int n = D.nx * D.ny * D.M;
-  const double *__restrict__ x = D.x;
-  const double *__restrict__ b = D.b;
-  const PensOuter c = D.oc;
+__device__ __noinline__ double b_residual(const Fine64 F_, const PensOuter c_, const ChqG g0_, double *red) {
+  const Fine64 F = F_;
+  const PensOuter c = c_;
+  const ChqG g0 = g0_;
+  const int n = F.nx * F.ny * F.M;
+  const double *__restrict__ x = F.x;
+  const double *__restrict__ b = F.b;
   double acc = 0;
   for (int t = threadIdx.x; t < n; t += NT) {
     int i, j, m, row;
-    pair_index(D, t, i, j, m, row);
-    const long long id = (long long)i * D.xs + (long long)j * D.ys + 2 * m;
+    split(F.fM, t, row, m);
+    split(F.fY, row, i, j);
+    const long long id = (long long)i * F.xs + (long long)j * F.ys + 2 * m;
     const long long cid = (long long)row * g0.rz + m;
     const bool s = (i + j) & 1;
     float *Bs = s ? g0.b1 : g0.b0;
     float *Bo = s ? g0.b0 : g0.b1;
-    if (D.vec) {
+    if (F.vec) {
       const double2 X = *reinterpret_cast<const double2 *>(x + id), B = *reinterpret_cast<const double2 *>(b + id);
-      const double2 YM = *reinterpret_cast<const double2 *>(x + id - D.ys);
-      const double2 YP = *reinterpret_cast<const double2 *>(x + id + D.ys);
-      const double2 XM = *reinterpret_cast<const double2 *>(x + id - D.xs);
-      const double2 XP = *reinterpret_cast<const double2 *>(x + id + D.xs);
+      const double2 YM = *reinterpret_cast<const double2 *>(x + id - F.ys);
+      const double2 YP = *reinterpret_cast<const double2 *>(x + id + F.ys);
+      const double2 XM = *reinterpret_cast<const double2 *>(x + id - F.xs);
+      const double2 XP = *reinterpret_cast<const double2 *>(x + id + F.xs);
       const double zl = x[id - 1], zr = x[id + 2];
       const double r0 = B.x - (c.fzh * (zl + X.y) + c.fyh * (YM.x + YP.x) + c.fxh * (XM.x + XP.x) - c.dg * X.x);
       const double r1 = B.y - (c.fzh * (X.x + zr) + c.fyh * (YM.y + YP.y) + c.fxh * (XM.y + XP.y) - c.dg * X.y);
@@ -168,10 +198,10 @@ __device__ __noinline__ double b_residual(const PensMember &D, const ChqG &g0, d
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const int k = 2 * m + h;
-        if (k < D.nz) {
+        if (k < F.nz) {
           const long long q = id + h;
-          const double r = b[q] - (c.fzh * (x[q - 1] + x[q + 1]) + c.fyh * (x[q - D.ys] + x[q + D.ys]) +
-                                   c.fxh * (x[q - D.xs] + x[q + D.xs]) - c.dg * x[q]);
+          const double r = b[q] - (c.fzh * (x[q - 1] + x[q + 1]) + c.fyh * (x[q - F.ys] + x[q + F.ys]) +
+                                   c.fxh * (x[q - F.xs] + x[q + F.xs]) - c.dg * x[q]);
           (h ? Bo : Bs)[cid] = (float)r;
           acc += r * r;
         }
@@ -192,23 +222,27 @@ __device__ __noinline__ double b_residual(const PensMember &D, const ChqG &g0, d
 
 // x += (double) e on the interior (e: the level-0 colour arrays of u)
 template <int NT>
-__device__ __noinline__ void b_add_correction(const PensMember &D, const ChqG &g0) {
-  const int n = D.nx * D.ny * D.M;
+__device__ __noinline__ void b_add_correction(const Fine64 F_, const ChqG g0_) {
+  const Fine64 F = F_;
+  const ChqG g0 = g0_;
+  const int n = F.nx * F.ny * F.M;
+  double *__restrict__ x = F.x;
   for (int t = threadIdx.x; t < n; t += NT) {
     int i, j, m, row;
-    pair_index(D, t, i, j, m, row);
-    const long long id = (long long)i * D.xs + (long long)j * D.ys + 2 * m;
+    split(F.fM, t, row, m);
+    split(F.fY, row, i, j);
+    const long long id = (long long)i * F.xs + (long long)j * F.ys + 2 * m;
     const long long cid = (long long)row * g0.rz + m;
     const bool s = (i + j) & 1;
     const float e0 = (s ? g0.u1 : g0.u0)[cid], e1 = (s ? g0.u0 : g0.u1)[cid];
-    if (D.vec) {
-      double2 X = *reinterpret_cast<double2 *>(D.x + id);
+    if (F.vec) {
+      double2 X = *reinterpret_cast<double2 *>(x + id);
       X.x = X.x + (double)e0;
       X.y = X.y + (double)e1;
-      *reinterpret_cast<double2 *>(D.x + id) = X;
+      *reinterpret_cast<double2 *>(x + id) = X;
     } else {
-      D.x[id] = D.x[id] + (double)e0;
-      if (2 * m + 1 < D.nz) D.x[id + 1] = D.x[id + 1] + (double)e1;
+      x[id] = x[id] + (double)e0;
+      if (2 * m + 1 < F.nz) x[id + 1] = x[id + 1] + (double)e1;
     }
   }
   __syncthreads();
@@ -231,33 +265,34 @@ __device__ void b_correction(PensMember &D, float *H, float *sm, const PensArgs 
   const int ts = D.ts;
   if (ts > 0) b_clear_u<NT>(level_g(D.lv[0], H));
   for (int l = 0; l < ts; l++)
-    b_restrict<NT>(level_g(D.lv[l], H), level_g(D.lv[l + 1], H), D.lv[l].k, D.bc, D.lv[l + 1].cm, D.lv[l + 1].cmsh);
+    b_restrict<NT>(level_g(D.lv[l], H), level_g(D.lv[l + 1], H), D.lv[l].k, D.bc, D.lv[l + 1].fcm);
   b_tail<NT>(D, sm, 1);
   if (ts == 0) {
     for (int c = 1; c < A.cycles; c++) b_tail<NT>(D, sm, 0);
     return;
   }
   for (int f = ts - 1; f >= 1; f--) {
-    b_prolong<NT>(level_g(D.lv[f + 1], H), level_g(D.lv[f], H), D.bc, D.lv[f + 1].cm, D.lv[f + 1].cmsh);
+    b_prolong<NT>(level_g(D.lv[f + 1], H), level_g(D.lv[f], H), D.bc, D.lv[f + 1].fcm);
     b_relax<NT>(level_g(D.lv[f], H), D.lv[f].k, D.bc, A.ramp);
   }
-  b_prolong<NT>(level_g(D.lv[1], H), level_g(D.lv[0], H), D.bc, D.lv[1].cm, D.lv[1].cmsh);
+  b_prolong<NT>(level_g(D.lv[1], H), level_g(D.lv[0], H), D.bc, D.lv[1].fcm);
   for (int c = 0; c < A.cycles; c++) {
     for (int l = 0; l < ts; l++) {
       b_relax<NT>(level_g(D.lv[l], H), D.lv[l].k, D.bc, A.nu1);
-      b_restrict<NT>(level_g(D.lv[l], H), level_g(D.lv[l + 1], H), D.lv[l].k, D.bc, D.lv[l + 1].cm,
-                     D.lv[l + 1].cmsh);
+      b_restrict<NT>(level_g(D.lv[l], H), level_g(D.lv[l + 1], H), D.lv[l].k, D.bc, D.lv[l + 1].fcm);
     }
     b_tail<NT>(D, sm, 0);
     for (int l = ts - 1; l >= 0; l--) {
-      b_prolong<NT>(level_g(D.lv[l + 1], H), level_g(D.lv[l], H), D.bc, D.lv[l + 1].cm, D.lv[l + 1].cmsh);
+      b_prolong<NT>(level_g(D.lv[l + 1], H), level_g(D.lv[l], H), D.bc, D.lv[l + 1].fcm);
       if (l > 0) b_relax<NT>(level_g(D.lv[l], H), D.lv[l].k, D.bc, A.nu2);
     }
   }
 }
 
-template <int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT) k_pens_solve(const __grid_constant__ PensArgs A) {
+// MINB blocks of NT threads per SM: 1024 threads at up to 64 registers, or (dense) 1536 threads
+// at up to 42 registers (the transfer phases then spill a little more)
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_pens_solve(const __grid_constant__ PensArgs A) {
   extern __shared__ float sm[];
   __shared__ PensMember D;
   __shared__ double red[NT / 32 + 1];
@@ -294,11 +329,11 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_pens_solve(const __grid_const
     for (;;) {
       level1_fill_block<double>(D.x, D.xs, D.ys, D.nx, D.ny, D.nz, D.bcd, D.hx, D.hy, D.hz);
       __syncthreads();
-      l2 = sqrt(b_residual<NT>(D, g0, red) * D.inv_n);
+      l2 = sqrt(b_residual<NT>(fine64(D), D.oc, g0, red) * D.inv_n);
       if (l2 <= tol) { conv = 1; break; }
       if (corr >= A.max_outer || !(l2 == l2)) break;
       b_correction<NT>(D, H, sm, A);
-      b_add_correction<NT>(D, g0);
+      b_add_correction<NT>(fine64(D), g0);
       corr++;
     }
     if (threadIdx.x == 0) {
@@ -317,9 +352,9 @@ __global__ void k_pens_reset(int *queue, int *nconv) {
   *nconv = 0;
 }
 
-template <int NT>
+template <int NT, int MINB>
 void *pens_kernel() {
-  return reinterpret_cast<void *>(&k_pens_solve<NT>);
+  return reinterpret_cast<void *>(&k_pens_solve<NT, MINB>);
 }
 
 }  // namespace
@@ -342,7 +377,6 @@ struct PersistentEnsemble {
   int blocks = 0;
   cudaStream_t user = nullptr;
   cudaGraphExec_t graph = nullptr;
-  int graph_threads = 0;
 
   ~PersistentEnsemble() {
     if (user) cudaStreamSynchronize(user);
@@ -386,8 +420,8 @@ struct PersistentEnsemble {
     D.ys = L.ystride;
     D.nx = nx; D.ny = ny; D.nz = nz;
     D.M = (nz + 1) / 2;
-    D.msh = log2_exact(D.M);
-    D.ysh = log2_exact(ny);
+    D.fM = make_fdiv(D.M);
+    D.fY = make_fdiv(ny);
     D.nlev = L_;
     D.vec = (nz % 2 == 0 && L.shift % 2 == 0 && L.xstride % 2 == 0 && L.ystride % 2 == 0) ? 1 : 0;
     D.inv_n = 1.0 / ((double)nx * ny * nz);
@@ -404,11 +438,11 @@ struct PersistentEnsemble {
       PensLevel &P = D.lv[l];
       P.nx = geo.dim[l][0]; P.ny = geo.dim[l][1]; P.nz = geo.dim[l][2];
       P.rz = round4((P.nz + 1) / 2);
-      P.qsh = log2_exact(P.rz / 4);
       P.ysh = log2_exact(P.ny);
       P.zsh = log2_exact(P.nz);
-      P.cm = (P.nz + 1) / 2;
-      P.cmsh = log2_exact(P.cm);
+      P.fq = make_fdiv(P.rz / 4);
+      P.fy = make_fdiv(P.ny);
+      P.fcm = make_fdiv((P.nz + 1) / 2);
       P.off = off;
       P.k = make_k(geo.h[l], geo.fx, geo.fy, geo.fz, geo.omega);
       off += 4LL * P.nx * P.ny * P.rz;
@@ -496,10 +530,11 @@ struct PersistentEnsemble {
   }
 
   void *kernel() const {
+    if (prm.dense) return prm.threads == 256 ? pens_kernel<256, 6>() : pens_kernel<512, 3>();
     switch (prm.threads) {
-      case 256: return pens_kernel<256>();
-      case 1024: return pens_kernel<1024>();
-      default: return pens_kernel<512>();
+      case 256: return pens_kernel<256, 4>();
+      case 1024: return pens_kernel<1024, 1>();
+      default: return pens_kernel<512, 2>();
     }
   }
 
@@ -507,6 +542,8 @@ struct PersistentEnsemble {
   ocu_status configure() {
     if (prm.threads != 256 && prm.threads != 512 && prm.threads != 1024)
       return fail(OCU_ERR_INVALID_VALUE, "[ERROR] ocu_pens - threads must be 256, 512 or 1024 (got %d)", prm.threads);
+    if (prm.dense && prm.threads == 1024)
+      return fail(OCU_ERR_INVALID_VALUE, "[ERROR] ocu_pens - the dense build takes 256 or 512 threads");
     void *k = kernel();
     OCU_TRY(check_cuda(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tail_smem),
                        "cudaFuncSetAttribute (persistent ensemble)"));
@@ -574,7 +611,7 @@ struct PersistentEnsemble {
       s = own;
     }
     ocu_status st = OCU_OK;
-    if (!graph || graph_threads != prm.threads) {
+    if (!graph) {
       if (graph) cudaGraphExecDestroy(graph);
       graph = nullptr;
       cudaGraph_t g = nullptr;
@@ -587,7 +624,6 @@ struct PersistentEnsemble {
         st = se != OCU_OK ? se : check_cuda(e, "cudaStreamEndCapture");
         if (st == OCU_OK) st = check_cuda(cudaGraphInstantiate(&graph, g, 0), "cudaGraphInstantiate");
         if (g) cudaGraphDestroy(g);
-        graph_threads = prm.threads;
       }
     }
     if (st == OCU_OK) st = check_cuda(cudaGraphLaunch(graph, s), "cudaGraphLaunch");
@@ -625,12 +661,13 @@ struct PersistentEnsemble {
   // pairs; keeps the fastest that converges every member; leaves every pressure zeroed.
   ocu_status autotune(const double *tol) {
     const ocu_pens_params base = prm;
-    struct Cand { int threads, cycles, nu1, nu2; };
+    struct Cand { int threads, dense, cycles, nu1, nu2; };
     std::vector<Cand> cands;
-    for (int th : {256, 512, 1024})
+    for (auto sh : {std::make_pair(256, 0), std::make_pair(512, 0), std::make_pair(1024, 0), std::make_pair(256, 1),
+                    std::make_pair(512, 1)})
       for (int cy : {0, 1, 2, 3})
         for (auto nu : {std::make_pair(2, 2), std::make_pair(2, 1), std::make_pair(1, 1)})
-          cands.push_back({th, cy, nu.first, nu.second});
+          cands.push_back({sh.first, sh.second, cy, nu.first, nu.second});
     cudaStream_t s = user;
     double best = 1e300;
     ocu_pens_params best_p = base;
@@ -641,6 +678,7 @@ struct PersistentEnsemble {
     for (const Cand &c : cands) {
       prm = base;
       prm.threads = c.threads;
+      prm.dense = c.dense;
       prm.cycles = c.cycles;
       prm.nu1 = c.nu1;
       prm.nu2 = c.nu2;
@@ -682,14 +720,14 @@ struct PersistentEnsemble {
     if (p.tail_cells != prm.tail_cells)
       return fail(OCU_ERR_INVALID_VALUE, "[ERROR] ocu_pens_set_params - tail_cells is fixed at creation");
     const ocu_bc_set bc = prm.bc;
-    const int old_threads = prm.threads;
+    const int old_threads = prm.threads, old_dense = prm.dense;
     prm = p;
     prm.bc = bc;  // fixed at creation
     if (graph) {  // counts are launch arguments baked into the graph
       cudaGraphExecDestroy(graph);
       graph = nullptr;
     }
-    if (prm.threads != old_threads) return configure();
+    if (prm.threads != old_threads || prm.dense != old_dense) return configure();
     return OCU_OK;
   }
 };
@@ -721,6 +759,7 @@ void ocu_pens_params_default(ocu_pens_params *p) {
   p->ramp_iters = 0;
   p->max_outer = 10;
   p->threads = 512;
+  p->dense = 0;
   p->tail_cells = 0;
   p->ms = 0;
 }

@@ -25,18 +25,18 @@ __global__ void __launch_bounds__(CHQ_RELAX_THREADS) k_chq_relax(ChqG g, ChqK k,
   chq_relax_item<true>(g, k, bc, color, (int)t);
 }
 
-__global__ void __launch_bounds__(256, CHQ_RESTRICT_MINB) k_chq_restrict(ChqG f, ChqG c, ChqK k, ChqBC bc, int cm, int cmsh) {
+__global__ void __launch_bounds__(256, CHQ_RESTRICT_MINB) k_chq_restrict(ChqG f, ChqG c, ChqK k, ChqBC bc, FDiv fcm) {
   pdl_entry();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)c.nx * c.ny * cm) return;
-  chq_restrict_item<true>(f, c, k, bc, cm, cmsh, (int)t);
+  if (t >= (long long)c.nx * c.ny * fcm.d) return;
+  chq_restrict_item<true>(f, c, k, bc, fcm, (int)t);
 }
 
-__global__ void __launch_bounds__(256, CHQ_PROLONG_MINB) k_chq_prolong(ChqG c, ChqG f, ChqBC bc, int cm, int cmsh) {
+__global__ void __launch_bounds__(256, CHQ_PROLONG_MINB) k_chq_prolong(ChqG c, ChqG f, ChqBC bc, FDiv fcm) {
   pdl_entry();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long long)c.nx * c.ny * cm) return;
-  chq_prolong_item<true>(c, f, bc, cm, cmsh, (int)t);
+  if (t >= (long long)c.nx * c.ny * fcm.d) return;
+  chq_prolong_item<true>(c, f, bc, fcm, (int)t);
 }
 
 __global__ void k_chq_zero(float *p, long long n) {
@@ -241,7 +241,7 @@ ocu_status ChequerMG::restrict_to(int l, cudaStream_t s) {
   const int cm = (Cl.nz + 1) / 2;  // coarse pairs per row
   const long long n = (long long)Cl.nx * Cl.ny * cm;
   launch_pdl(k_chq_restrict, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, s, make_g(F), make_g(Cl),
-             make_k(F.h, fx, fy, fz, omega), make_bc(bc, fx, fy, fz), cm, log2_exact(cm));
+             make_k(F.h, fx, fy, fz, omega), make_bc(bc, fx, fy, fz), make_fdiv(cm));
   return check_launch("k_chq_restrict");
 }
 
@@ -250,7 +250,7 @@ ocu_status ChequerMG::prolong_from(int l, cudaStream_t s) {
   const int cm = (Cl.nz + 1) / 2;
   const long long n = (long long)Cl.nx * Cl.ny * cm;
   launch_pdl(k_chq_prolong, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, s, make_g(Cl), make_g(F),
-             make_bc(bc, fx, fy, fz), cm, log2_exact(cm));
+             make_bc(bc, fx, fy, fz), make_fdiv(cm));
   return check_launch("k_chq_prolong");
 }
 
