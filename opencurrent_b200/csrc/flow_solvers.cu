@@ -243,14 +243,15 @@ ocu_status NSSolver::set_parameters(const ocu_ns_params &p, const void *iu, cons
 // get_max_stable_timestep (eqn_incompressns3d.cu:301-328)
 ocu_status NSSolver::get_max_stable_timestep(double *out) {
   if (!initialized) return fail(OCU_ERR_NOT_INITIALIZED, "[ERROR] get_max_stable_timestep - not initialized");
+  // max |u|, max |v|, max |w| in one launch (the reference's three reduce_maxabs calls; a maximum
+  // is the same in any fold order)
+  const ocu_layout *lays[3] = {&u->L, &v->L, &w->L};
   if (dtype == OCU_F64) {
-    OCU_TRY(launch_reduce<double>(origin<double>(u), u->L, OCU_REDUCE_MAXABS, scratch, d_red, stream));
-    OCU_TRY(launch_reduce<double>(origin<double>(v), v->L, OCU_REDUCE_MAXABS, scratch, d_red + 1, stream));
-    OCU_TRY(launch_reduce<double>(origin<double>(w), w->L, OCU_REDUCE_MAXABS, scratch, d_red + 2, stream));
+    const double *o[3] = {origin<double>(u), origin<double>(v), origin<double>(w)};
+    OCU_TRY(launch_minmax<double>(o, lays, 3, OCU_REDUCE_MAXABS, scratch, d_red, stream));
   } else {
-    OCU_TRY(launch_reduce<float>(origin<float>(u), u->L, OCU_REDUCE_MAXABS, scratch, d_red, stream));
-    OCU_TRY(launch_reduce<float>(origin<float>(v), v->L, OCU_REDUCE_MAXABS, scratch, d_red + 1, stream));
-    OCU_TRY(launch_reduce<float>(origin<float>(w), w->L, OCU_REDUCE_MAXABS, scratch, d_red + 2, stream));
+    const float *o[3] = {origin<float>(u), origin<float>(v), origin<float>(w)};
+    OCU_TRY(launch_minmax<float>(o, lays, 3, OCU_REDUCE_MAXABS, scratch, d_red, stream));
   }
   OCU_TRY(check_cuda(cudaMemcpyAsync(h_red, d_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream), "maxabs"));
   OCU_TRY(check_cuda(cudaStreamSynchronize(stream), "maxabs"));

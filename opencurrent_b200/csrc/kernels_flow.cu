@@ -4,6 +4,9 @@
 // All grids handed to one kernel share a padded layout (the reference requires it,
 // sol_selfadvection3ddev.cu:616-620), so one index serves every array.  Expression order is
 // the reference's; built with --fmad=false.
+#include <cstdint>
+#include <initializer_list>
+
 #include "ocu_internal.h"
 
 namespace ocub {
@@ -158,11 +161,296 @@ __global__ void k_thermal_force(T *__restrict__ dvdt, T c, const T *__restrict__
   CELL_LOOP_END
 }
 
+// ---- FP32 forms on 16-byte groups along k ---------------------------------------------------
+// A thread owns four consecutive cells of a row (one float4) at CI consecutive i; its z
+// neighbours k - 1 and k + 4 come from the adjacent lanes (warp shuffles), the first / last
+// group of a block row loads them itself.  Each cell's expression is the scalar kernel's, in its
+// order, so results are bit-identical; only the loads are wider (a quarter of the load
+// instructions, 16-byte transactions).  Used when nz, both strides and the interior origin are
+// multiples of four floats.
+#ifndef OCU_FLOW_CELLS_I
+#define OCU_FLOW_CELLS_I 4
+#endif
+constexpr int kCellsIV = OCU_FLOW_CELLS_I;
+
+struct Row4 {
+  float v[6];  // cells k - 1 .. k + 4
+};
+
+__device__ __forceinline__ float4 ld4g(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ void st4g(float *p, float a, float b, float c, float d) {
+  *reinterpret_cast<float4 *>(p) = make_float4(a, b, c, d);
+}
+
+// the group at id with its k - 1 and k + 4 neighbours; every lane of the warp calls it
+__device__ __forceinline__ Row4 row4(const float *__restrict__ p, long long id, bool ok, bool first, bool last) {
+  const float4 c = ok ? ld4g(p + id) : make_float4(0.f, 0.f, 0.f, 0.f);
+  Row4 r;
+  r.v[1] = c.x; r.v[2] = c.y; r.v[3] = c.z; r.v[4] = c.w;
+  r.v[0] = __shfl_up_sync(0xffffffffu, c.w, 1);
+  r.v[5] = __shfl_down_sync(0xffffffffu, c.x, 1);
+  if (ok && first) r.v[0] = p[id - 1];
+  if (ok && last) r.v[5] = p[id + 4];
+  return r;
+}
+
+#define V4_BEGIN_CI(CI)                                                                          \
+  const int k4 = blockIdx.x * blockDim.x + threadIdx.x;                                          \
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;                                           \
+  const bool ok = k4 < nz4 && j < ny;                                                            \
+  const bool first = threadIdx.x == 0, last = threadIdx.x == blockDim.x - 1 || k4 == nz4 - 1;    \
+  _Pragma("unroll") for (int ci = 0; ci < (CI); ci++) {                                           \
+    const int i = blockIdx.z * (CI) + ci;                                                        \
+    if (i >= nx) break;                                                                          \
+    const long long id = (long long)i * xs + (long long)j * ys + 4 * k4;
+#define V4_BEGIN V4_BEGIN_CI(kCellsIV)
+#define V4_END }
+// Cells per thread along i of the passive advection's group form: one (measured at
+// 256x256x128: 35.8 us against 39.8 with four; the other group kernels measured best at four).
+constexpr int kCellsIPassive = 1;
+
+// nr (0..3): cells past the last group of a row (rows of nz = 4 nz4 + nr cells); the lane of the
+// last group computes them with the scalar expression.
+// nr (0..3): cells past the last group of a row (rows of nz = 4 nz4 + nr cells); the blocks
+// holding the rows' last groups compute them afterwards, one cell per thread, with the scalar
+// expression (handled by the last lane of each row they measured slower: its warp waited).
+__global__ void __launch_bounds__(256) k_laplacian_v4(const float *__restrict__ phi, float *__restrict__ dphidt,
+                                                      float ihx2, float ihy2, float ihz2, float c, long long xs,
+                                                      long long ys, int nx, int ny, int nz4, int nr) {
+  if (nr > 0 && blockIdx.x == gridDim.x - 1) {
+    const int nt = blockDim.x * blockDim.y, cnt = nr * blockDim.y * kCellsIV;
+    for (int t = threadIdx.y * blockDim.x + threadIdx.x; t < cnt; t += nt) {
+      const int e = t % nr, ry = (t / nr) % blockDim.y, cr = t / (nr * blockDim.y);
+      const int jr = blockIdx.y * blockDim.y + ry, ir = blockIdx.z * kCellsIV + cr;
+      if (jr >= ny || ir >= nx) continue;
+      const long long q = (long long)ir * xs + (long long)jr * ys + 4 * nz4 + e;
+      const float p = phi[q];
+      const float lap = ihz2 * (phi[q + 1] + phi[q - 1] - 2.f * p) + ihy2 * (phi[q + ys] + phi[q - ys] - 2.f * p) +
+                        ihx2 * (phi[q + xs] + phi[q - xs] - 2.f * p);
+      dphidt[q] = dphidt[q] + c * lap;
+    }
+  }
+  V4_BEGIN
+  const Row4 P = row4(phi, id, ok, first, last);
+  if (!ok) continue;
+  const float4 D = ld4g(dphidt + id), YP = ld4g(phi + id + ys), YM = ld4g(phi + id - ys);
+  const float4 XP = ld4g(phi + id + xs), XM = ld4g(phi + id - xs);
+  const float yp[4] = {YP.x, YP.y, YP.z, YP.w}, ym[4] = {YM.x, YM.y, YM.z, YM.w};
+  const float xp[4] = {XP.x, XP.y, XP.z, XP.w}, xm[4] = {XM.x, XM.y, XM.z, XM.w};
+  const float d[4] = {D.x, D.y, D.z, D.w};
+  float o[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const float p = P.v[e + 1];
+    const float lap = ihz2 * (P.v[e + 2] + P.v[e] - 2.f * p) + ihy2 * (yp[e] + ym[e] - 2.f * p) +
+                      ihx2 * (xp[e] + xm[e] - 2.f * p);
+    o[e] = d[e] + c * lap;
+  }
+  st4g(dphidt + id, o[0], o[1], o[2], o[3]);
+  V4_END
+}
+
+__global__ void __launch_bounds__(256) k_divergence_v4(const float *__restrict__ u, const float *__restrict__ v,
+                                                       const float *__restrict__ w, float *__restrict__ div,
+                                                       float ihx, float ihy, float ihz, long long xs, long long ys,
+                                                       int nx, int ny, int nz4) {
+  V4_BEGIN
+  const Row4 W = row4(w, id, ok, first, last);
+  if (!ok) continue;
+  const float4 U = ld4g(u + id), UP = ld4g(u + id + xs), V = ld4g(v + id), VP = ld4g(v + id + ys);
+  const float uu[4] = {U.x, U.y, U.z, U.w}, up[4] = {UP.x, UP.y, UP.z, UP.w};
+  const float vv[4] = {V.x, V.y, V.z, V.w}, vp[4] = {VP.x, VP.y, VP.z, VP.w};
+  float o[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) o[e] = ihx * (up[e] - uu[e]) + ihy * (vp[e] - vv[e]) + ihz * (W.v[e + 2] - W.v[e + 1]);
+  st4g(div + id, o[0], o[1], o[2], o[3]);
+  V4_END
+}
+
+__global__ void __launch_bounds__(256) k_gradient_v4(float *__restrict__ u, float *__restrict__ v,
+                                                     float *__restrict__ w, const float *__restrict__ phi, float c,
+                                                     float ihx, float ihy, float ihz, long long xs, long long ys,
+                                                     int nx, int ny, int nz4) {
+  V4_BEGIN
+  const Row4 P = row4(phi, id, ok, first, last);
+  if (!ok) continue;
+  const float4 XM = ld4g(phi + id - xs), YM = ld4g(phi + id - ys);
+  const float4 U = ld4g(u + id), V = ld4g(v + id), W = ld4g(w + id);
+  const float xm[4] = {XM.x, XM.y, XM.z, XM.w}, ym[4] = {YM.x, YM.y, YM.z, YM.w};
+  float uu[4] = {U.x, U.y, U.z, U.w}, vv[4] = {V.x, V.y, V.z, V.w}, ww[4] = {W.x, W.y, W.z, W.w};
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const float p = P.v[e + 1];
+    uu[e] += c * ihx * (p - xm[e]);
+    vv[e] += c * ihy * (p - ym[e]);
+    ww[e] += c * ihz * (p - P.v[e]);
+  }
+  st4g(u + id, uu[0], uu[1], uu[2], uu[3]);
+  st4g(v + id, vv[0], vv[1], vv[2], vv[3]);
+  st4g(w + id, ww[0], ww[1], ww[2], ww[3]);
+  V4_END
+}
+
+// the vertical neighbour along k (nbr = 1) from the lanes, or a whole group (nbr a multiple of 4)
+__global__ void __launch_bounds__(256) k_thermal_force_v4(float *__restrict__ dvdt, float c,
+                                                          const float *__restrict__ temp, long long nbr,
+                                                          long long xs, long long ys, int nx, int ny, int nz4) {
+  V4_BEGIN
+  const Row4 Tc = row4(temp, id, ok, first, last);
+  if (!ok) continue;
+  float tn[4];
+  if (nbr == 1) {
+#pragma unroll
+    for (int e = 0; e < 4; e++) tn[e] = Tc.v[e];
+  } else {
+    const float4 N = ld4g(temp + id - nbr);
+    tn[0] = N.x; tn[1] = N.y; tn[2] = N.z; tn[3] = N.w;
+  }
+  const float4 D = ld4g(dvdt + id);
+  float d[4] = {D.x, D.y, D.z, D.w};
+#pragma unroll
+  for (int e = 0; e < 4; e++) d[e] += 0.5f * c * (Tc.v[e + 1] + tn[e]);
+  st4g(dvdt + id, d[0], d[1], d[2], d[3]);
+  V4_END
+}
+
+template <int IT>
+__global__ void __launch_bounds__(256) k_advect_passive_v4(const float *__restrict__ u, const float *__restrict__ v,
+                                                           const float *__restrict__ w, const float *__restrict__ phi,
+                                                           float *__restrict__ dphidt, float ihx, float ihy, float ihz,
+                                                           long long xs, long long ys, int nx, int ny, int nz4) {
+  V4_BEGIN_CI(kCellsIPassive)
+  const Row4 P = row4(phi, id, ok, first, last);
+  const Row4 W = row4(w, id, ok, first, last);
+  if (!ok) continue;
+  const float4 UP = ld4g(u + id + xs), U = ld4g(u + id), PXP = ld4g(phi + id + xs), PXM = ld4g(phi + id - xs);
+  const float4 VP = ld4g(v + id + ys), V = ld4g(v + id), PYP = ld4g(phi + id + ys), PYM = ld4g(phi + id - ys);
+  const float up[4] = {UP.x, UP.y, UP.z, UP.w}, uu[4] = {U.x, U.y, U.z, U.w};
+  const float pxp[4] = {PXP.x, PXP.y, PXP.z, PXP.w}, pxm[4] = {PXM.x, PXM.y, PXM.z, PXM.w};
+  const float vp[4] = {VP.x, VP.y, VP.z, VP.w}, vv[4] = {V.x, V.y, V.z, V.w};
+  const float pyp[4] = {PYP.x, PYP.y, PYP.z, PYP.w}, pym[4] = {PYM.x, PYM.y, PYM.z, PYM.w};
+  float o[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const float p = P.v[e + 1];
+    const float du = up[e] * interp<float, IT>(up[e], p, pxp[e]) - uu[e] * interp<float, IT>(uu[e], pxm[e], p);
+    const float dv = vp[e] * interp<float, IT>(vp[e], p, pyp[e]) - vv[e] * interp<float, IT>(vv[e], pym[e], p);
+    const float wpk = W.v[e + 2], wij = W.v[e + 1];
+    const float dw = wpk * interp<float, IT>(wpk, p, P.v[e + 2]) - wij * interp<float, IT>(wij, P.v[e], p);
+    o[e] = (-du * ihx) - (dv * ihy) - (dw * ihz);
+  }
+  st4g(dphidt + id, o[0], o[1], o[2], o[3]);
+  V4_END
+}
+
+// Self-advection on groups of four cells along k: the 17 rows it reads (u, v, w at the cell and
+// its face neighbours) as 16-byte loads, the k-shifted values from the adjacent lanes; each
+// component's expression is the scalar kernel's, in its order.
+template <int IT>
+__global__ void __launch_bounds__(256, 2) k_advect_self_v4(const float *__restrict__ u, const float *__restrict__ v,
+                                                           const float *__restrict__ w, float *__restrict__ dudt,
+                                                           float *__restrict__ dvdt, float *__restrict__ dwdt, float ihx,
+                                                           float ihy, float ihz, long long xs, long long ys, int nx,
+                                                           int ny, int nz4) {
+  V4_BEGIN
+  // rows with their k - 1 / k + 4 neighbours (every lane takes part in the shuffles)
+  const Row4 U00 = row4(u, id, ok, first, last), Up0 = row4(u, id + xs, ok, first, last);
+  const Row4 V00 = row4(v, id, ok, first, last), V0p = row4(v, id + ys, ok, first, last);
+  const Row4 W00 = row4(w, id, ok, first, last), Wm0 = row4(w, id - xs, ok, first, last);
+  const Row4 W0m = row4(w, id - ys, ok, first, last);
+  if (!ok) continue;
+  const float4 Um0 = ld4g(u + id - xs), U0p = ld4g(u + id + ys), U0m = ld4g(u + id - ys), Upm = ld4g(u + id + xs - ys);
+  const float4 Vm0 = ld4g(v + id - xs), Vp0 = ld4g(v + id + xs), V0m = ld4g(v + id - ys), Vmp = ld4g(v + id - xs + ys);
+  const float4 Wp0 = ld4g(w + id + xs), W0p = ld4g(w + id + ys);
+  const float um0[4] = {Um0.x, Um0.y, Um0.z, Um0.w}, u0p[4] = {U0p.x, U0p.y, U0p.z, U0p.w};
+  const float u0m[4] = {U0m.x, U0m.y, U0m.z, U0m.w}, upm[4] = {Upm.x, Upm.y, Upm.z, Upm.w};
+  const float vm0[4] = {Vm0.x, Vm0.y, Vm0.z, Vm0.w}, vp0[4] = {Vp0.x, Vp0.y, Vp0.z, Vp0.w};
+  const float v0m[4] = {V0m.x, V0m.y, V0m.z, V0m.w}, vmp[4] = {Vmp.x, Vmp.y, Vmp.z, Vmp.w};
+  const float wp0[4] = {Wp0.x, Wp0.y, Wp0.z, Wp0.w}, w0p[4] = {W0p.x, W0p.y, W0p.z, W0p.w};
+  const float half = 0.5f;
+  float ou[4], ov[4], ow[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    // cell k = 4 k4 + e: Row4 index e + 1 is k, e + 2 is k + 1, e is k - 1
+    const float ui = U00.v[e + 1], vi = V00.v[e + 1], wi = W00.v[e + 1];
+    const float u_pi = Up0.v[e + 1], u_mi = um0[e], u_pj = u0p[e], u_mj = u0m[e], u_pk = U00.v[e + 2],
+                u_mk = U00.v[e];
+    const float v_pi = vp0[e], v_mi = vm0[e], v_pj = V0p.v[e + 1], v_mj = v0m[e], v_pk = V00.v[e + 2],
+                v_mk = V00.v[e];
+    const float w_pi = wp0[e], w_mi = Wm0.v[e + 1], w_pj = w0p[e], w_mj = W0m.v[e + 1], w_pk = W00.v[e + 2],
+                w_mk = W00.v[e];
+    float a, b, d1, d2, d3;
+    a = half * (ui + u_pi);
+    b = half * (ui + u_mi);
+    d1 = (a * interp<float, IT>(a, ui, u_pi)) - (b * interp<float, IT>(b, u_mi, ui));
+    a = half * (v_pj + vmp[e]);
+    b = half * (vi + v_mi);
+    d2 = (a * interp<float, IT>(a, ui, u_pj)) - (b * interp<float, IT>(b, u_mj, ui));
+    a = half * (w_pk + Wm0.v[e + 2]);
+    b = half * (wi + w_mi);
+    d3 = (a * interp<float, IT>(a, ui, u_pk)) - (b * interp<float, IT>(b, u_mk, ui));
+    ou[e] = -d1 * ihx - d2 * ihy - d3 * ihz;
+
+    a = half * (u_pi + upm[e]);
+    b = half * (ui + u_mj);
+    d1 = (a * interp<float, IT>(a, vi, v_pi)) - (b * interp<float, IT>(b, v_mi, vi));
+    a = half * (vi + v_pj);
+    b = half * (vi + v_mj);
+    d2 = (a * interp<float, IT>(a, vi, v_pj)) - (b * interp<float, IT>(b, v_mj, vi));
+    a = half * (w_pk + W0m.v[e + 2]);
+    b = half * (wi + w_mj);
+    d3 = (a * interp<float, IT>(a, vi, v_pk)) - (b * interp<float, IT>(b, v_mk, vi));
+    ov[e] = -d1 * ihx - d2 * ihy - d3 * ihz;
+
+    a = half * (u_pi + Up0.v[e]);
+    b = half * (ui + u_mk);
+    d1 = (a * interp<float, IT>(a, wi, w_pi)) - (b * interp<float, IT>(b, w_mi, wi));
+    a = half * (v_pj + V0p.v[e]);
+    b = half * (vi + v_mk);
+    d2 = (a * interp<float, IT>(a, wi, w_pj)) - (b * interp<float, IT>(b, w_mj, wi));
+    a = half * (wi + w_pk);
+    b = half * (wi + w_mk);
+    d3 = (a * interp<float, IT>(a, wi, w_pk)) - (b * interp<float, IT>(b, w_mk, wi));
+    ow[e] = -d1 * ihx - d2 * ihy - d3 * ihz;
+  }
+  st4g(dudt + id, ou[0], ou[1], ou[2], ou[3]);
+  st4g(dvdt + id, ov[0], ov[1], ov[2], ov[3]);
+  st4g(dwdt + id, ow[0], ow[1], ow[2], ow[3]);
+  V4_END
+}
+
+// whether the FP32 group form applies: nz, the strides and every array's interior origin on
+// 16-byte boundaries
+static bool v4_ok(int nz, const ocu_layout &L, std::initializer_list<const void *> origins) {
+  if (nz % 4 || L.xstride % 4 || L.ystride % 4) return false;
+  for (const void *p : origins)
+    if (reinterpret_cast<uintptr_t>(p) % 16) return false;
+  return true;
+}
+
+// Blocks of 256 threads, whole warps: a block row is the row's nz/4 groups when that divides 32
+// (a warp then holds several rows), else 32 (lanes past the row's end idle).  Every lane of a
+// warp takes part in the shuffles.
+static inline void shape_v4(int nx, int ny, int nz, dim3 *grid, dim3 *block, int ci = kCellsIV) {
+  const int nz4 = nz / 4;
+  const int bx = (nz4 < 32 && 32 % nz4 == 0) ? nz4 : 32;
+  *block = dim3(bx, 256 / bx);
+  *grid = dim3((nz4 + bx - 1) / bx, (ny + block->y - 1) / block->y, (nx + ci - 1) / ci);
+}
+
 template <typename T>
 ocu_status launch_divergence(const T *u, const T *v, const T *w, T *div, const ocu_layout &L,
                              int nx, int ny, int nz, double hx, double hy, double hz,
                              cudaStream_t s) {
   dim3 g, b;
+  if constexpr (sizeof(T) == 4) {
+    if (v4_ok(nz, L, {u, v, w, div})) {
+      shape_v4(nx, ny, nz, &g, &b);
+      k_divergence_v4<<<g, b, 0, s>>>(u, v, w, div, (T)(1 / hx), (T)(1 / hy), (T)(1 / hz), L.xstride, L.ystride, nx,
+                                      ny, nz / 4);
+      return check_launch("k_divergence_v4");
+    }
+  }
   shape(nx, ny, nz, &g, &b);
   k_divergence<T><<<g, b, 0, s>>>(u, v, w, div, (T)(1 / hx), (T)(1 / hy), (T)(1 / hz), L.xstride, L.ystride, nx,
                                   ny, nz);
@@ -174,6 +462,14 @@ ocu_status launch_gradient(T *u, T *v, T *w, const T *phi, const ocu_layout &L, 
                            int nz, double hx, double hy, double hz, T coefficient,
                            cudaStream_t s) {
   dim3 g, b;
+  if constexpr (sizeof(T) == 4) {
+    if (v4_ok(nz, L, {u, v, w, phi})) {
+      shape_v4(nx, ny, nz, &g, &b);
+      k_gradient_v4<<<g, b, 0, s>>>(u, v, w, phi, coefficient, (T)(1 / hx), (T)(1 / hy), (T)(1 / hz), L.xstride,
+                                    L.ystride, nx, ny, nz / 4);
+      return check_launch("k_gradient_v4");
+    }
+  }
   shape(nx, ny, nz, &g, &b);
   k_gradient<T><<<g, b, 0, s>>>(u, v, w, phi, coefficient, (T)(1 / hx), (T)(1 / hy), (T)(1 / hz), L.xstride,
                                 L.ystride, nx, ny, nz);
@@ -194,6 +490,16 @@ ocu_status launch_laplacian(const T *phi, T *dphidt, const ocu_layout &L, int nx
                             int nz, double hx, double hy, double hz, T coefficient,
                             cudaStream_t s) {
   dim3 g, b;
+  if constexpr (sizeof(T) == 4) {
+    const int nz4 = nz / 4, nr = nz - 4 * nz4;
+    if (nz4 > 0 && v4_ok(4 * nz4, L, {phi, dphidt})) {
+      const T ihx2 = (T)(1 / (hx * hx)), ihy2 = (T)(1 / (hy * hy)), ihz2 = (T)(1 / (hz * hz));
+      shape_v4(nx, ny, 4 * nz4, &g, &b);
+      k_laplacian_v4<<<g, b, 0, s>>>(phi, dphidt, ihx2, ihy2, ihz2, coefficient, L.xstride, L.ystride, nx, ny, nz4,
+                                     nr);
+      return check_launch("k_laplacian_v4");
+    }
+  }
   shape(nx, ny, nz, &g, &b);
   k_laplacian<T><<<g, b, 0, s>>>(phi, dphidt, (T)(1 / (hx * hx)), (T)(1 / (hy * hy)), (T)(1 / (hz * hz)),
                                  coefficient, L.xstride, L.ystride, nx, ny, nz);
@@ -205,8 +511,20 @@ ocu_status launch_advect_self(const T *u, const T *v, const T *w, T *du, T *dv, 
                               const ocu_layout &L, int nx, int ny, int nz, double hx, double hy,
                               double hz, int it, cudaStream_t s) {
   dim3 g, b;
-  shape(nx, ny, nz, &g, &b, 1);
   const T ihx = (T)(1 / hx), ihy = (T)(1 / hy), ihz = (T)(1 / hz);
+  if constexpr (sizeof(T) == 4) {
+    if ((it == OCU_IT_FIRST_ORDER_UPWIND || it == OCU_IT_SECOND_ORDER_CENTERED) && v4_ok(nz, L, {u, v, w, du, dv, dw})) {
+      shape_v4(nx, ny, nz, &g, &b);
+      if (it == OCU_IT_FIRST_ORDER_UPWIND)
+        k_advect_self_v4<OCU_IT_FIRST_ORDER_UPWIND><<<g, b, 0, s>>>(u, v, w, du, dv, dw, ihx, ihy, ihz, L.xstride,
+                                                                   L.ystride, nx, ny, nz / 4);
+      else
+        k_advect_self_v4<OCU_IT_SECOND_ORDER_CENTERED><<<g, b, 0, s>>>(u, v, w, du, dv, dw, ihx, ihy, ihz,
+                                                                      L.xstride, L.ystride, nx, ny, nz / 4);
+      return check_launch("k_advect_self_v4");
+    }
+  }
+  shape(nx, ny, nz, &g, &b, 1);
   if (it == OCU_IT_FIRST_ORDER_UPWIND)
     k_advect_self<T, OCU_IT_FIRST_ORDER_UPWIND><<<g, b, 0, s>>>(u, v, w, du, dv, dw, ihx, ihy, ihz, L.xstride,
                                                                L.ystride, nx, ny, nz);
@@ -223,8 +541,20 @@ ocu_status launch_advect_passive(const T *u, const T *v, const T *w, const T *ph
                                  const ocu_layout &L, int nx, int ny, int nz, double hx,
                                  double hy, double hz, int it, cudaStream_t s) {
   dim3 g, b;
-  shape(nx, ny, nz, &g, &b);
   const T ihx = (T)(1 / hx), ihy = (T)(1 / hy), ihz = (T)(1 / hz);
+  if constexpr (sizeof(T) == 4) {
+    if ((it == OCU_IT_FIRST_ORDER_UPWIND || it == OCU_IT_SECOND_ORDER_CENTERED) && v4_ok(nz, L, {u, v, w, phi, dphi})) {
+      shape_v4(nx, ny, nz, &g, &b, kCellsIPassive);
+      if (it == OCU_IT_FIRST_ORDER_UPWIND)
+        k_advect_passive_v4<OCU_IT_FIRST_ORDER_UPWIND><<<g, b, 0, s>>>(u, v, w, phi, dphi, ihx, ihy, ihz, L.xstride,
+                                                                      L.ystride, nx, ny, nz / 4);
+      else
+        k_advect_passive_v4<OCU_IT_SECOND_ORDER_CENTERED><<<g, b, 0, s>>>(u, v, w, phi, dphi, ihx, ihy, ihz,
+                                                                         L.xstride, L.ystride, nx, ny, nz / 4);
+      return check_launch("k_advect_passive_v4");
+    }
+  }
+  shape(nx, ny, nz, &g, &b);
   if (it == OCU_IT_FIRST_ORDER_UPWIND)
     k_advect_passive<T, OCU_IT_FIRST_ORDER_UPWIND><<<g, b, 0, s>>>(u, v, w, phi, dphi, ihx, ihy, ihz, L.xstride,
                                                                   L.ystride, nx, ny, nz);
@@ -240,6 +570,13 @@ template <typename T>
 ocu_status launch_thermal_force(T *dvdt, T coefficient, const T *temp, const ocu_layout &L,
                                 int nbr_stride, int nx, int ny, int nz, cudaStream_t s) {
   dim3 g, b;
+  if constexpr (sizeof(T) == 4) {
+    if ((nbr_stride == 1 || nbr_stride % 4 == 0) && v4_ok(nz, L, {dvdt, temp})) {
+      shape_v4(nx, ny, nz, &g, &b);
+      k_thermal_force_v4<<<g, b, 0, s>>>(dvdt, coefficient, temp, nbr_stride, L.xstride, L.ystride, nx, ny, nz / 4);
+      return check_launch("k_thermal_force_v4");
+    }
+  }
   shape(nx, ny, nz, &g, &b);
   k_thermal_force<T><<<g, b, 0, s>>>(dvdt, coefficient, temp, nbr_stride, L.xstride, L.ystride, nx, ny, nz);
   return check_launch("k_thermal_force");

@@ -2,8 +2,11 @@
 //
 // All arithmetic reproduces the reference expression order; the library is compiled with
 // --fmad=false so every product and sum is rounded exactly as written.
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
+
+#include <type_traits>
 
 #include "bc_device.cuh"
 #include "ocu_internal.h"
@@ -428,9 +431,12 @@ __device__ __forceinline__ void block_tree_256(T *sh, const RedOp<T> &op) {
 
 constexpr int kReduceThreads = 512;  // 16 warps, 16 of a block's 256 rows each; two blocks per SM
 
-template <typename T>
-__global__ void __launch_bounds__(kReduceThreads, 2) k_reduce(const T *origin, long long xs, long long ys, int nx, int ny, int nz,
-                                                RedOp<T> op, T *partial, unsigned *counter, double *result) {
+// DOT: the folded value of cell k is origin[k] * origin2[k] rounded to T (a pointwise product
+// grid reduced with the sum, without storing the product grid).
+template <typename T, bool DOT = false>
+__global__ void __launch_bounds__(kReduceThreads, 2) k_reduce(const T *origin, const T *origin2, long long xs, long long ys,
+                                                              int nx, int ny, int nz, RedOp<T> op, T *partial,
+                                                              unsigned *counter, double *result) {
   pdl_entry();
   __shared__ T sh[256];
   __shared__ bool last;
@@ -441,11 +447,12 @@ __global__ void __launch_bounds__(kReduceThreads, 2) k_reduce(const T *origin, l
   // the shuffle tree), the loads of the RB rows interleaved so that they are in flight
   // together.  Rows beyond nrows carry the identity, as in reduce_per_cta.
   constexpr int RW = 256 / (kReduceThreads / 32);  // rows of a warp
-  constexpr int RB = 8;
+  constexpr int RB = (DOT && sizeof(T) == 8) ? 4 : 8;  // rows in flight; each row keeps its own fold
   static_assert(RW % RB == 0, "rows of a warp in whole groups");
   for (int r0 = 0; r0 < RW; r0 += RB) {
     T acc[RB];
     const T *base[RB];
+    const T *base2[RB];
     bool ok[RB];
     // consecutive rows: one division for the first, then step j (wrapping into i)
     const long long qb = row0 + warp * RW + r0;
@@ -455,6 +462,7 @@ __global__ void __launch_bounds__(kReduceThreads, 2) k_reduce(const T *origin, l
       ok[r] = qb + r < nrows;
       acc[r] = op.identity();
       base[r] = ok[r] ? origin + (long long)i * xs + (long long)j * ys : origin;
+      base2[r] = DOT ? (ok[r] ? origin2 + (long long)i * xs + (long long)j * ys : origin2) : nullptr;
       if (++j == ny) {
         j = 0;
         ++i;
@@ -465,7 +473,7 @@ __global__ void __launch_bounds__(kReduceThreads, 2) k_reduce(const T *origin, l
     for (int k = lane; k < nz; k += 32) {
       T v[RB];
 #pragma unroll
-      for (int r = 0; r < RB; r++) v[r] = base[r][k];
+      for (int r = 0; r < RB; r++) v[r] = DOT ? base[r][k] * base2[r][k] : base[r][k];
 #pragma unroll
       for (int r = 0; r < RB; r++)
         if (ok[r]) acc[r] = k == lane ? op.process(v[r]) : op.reduce(op.process(v[r]), acc[r]);
@@ -512,6 +520,228 @@ __global__ void __launch_bounds__(kReduceThreads, 2) k_reduce(const T *origin, l
   }
 }
 
+// Max, min and max-abs in one pass: exact in any fold order, so no partials are kept.  Each warp
+// folds one group of rows (read with 16-byte loads along k, a ragged row end with scalar loads,
+// all the group's loads in flight together), the block folds its warps, and the block's value
+// enters an unsigned key in the scratch header with atomicMax (an order-preserving encoding of
+// the float; min as its complement); the last block decodes it and clears the key and the
+// ticket for the next launch.  Folds start from NaN (fmax / fmin drop a NaN operand), so the
+// result is the extremum of the grid's non-NaN values -- what the reference-order fold gives
+// whenever the grid holds one -- and NaN when it holds none.
+template <typename T>
+__device__ __forceinline__ T red_nan();
+template <>
+__device__ __forceinline__ float red_nan<float>() { return __int_as_float(0x7fffffff); }
+template <>
+__device__ __forceinline__ double red_nan<double>() { return __longlong_as_double(0x7fffffffffffffffLL); }
+
+template <typename T>
+struct MMKey;
+template <>
+struct MMKey<float> {
+  using K = unsigned;
+  __device__ static K enc(float f) {
+    const unsigned b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+  }
+  __device__ static float dec(K k) { return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k); }
+};
+template <>
+struct MMKey<double> {
+  using K = unsigned long long;
+  __device__ static K enc(double f) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(f);
+    return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+  }
+  __device__ static double dec(K k) {
+    return __longlong_as_double((long long)((k & 0x8000000000000000ull) ? (k & 0x7fffffffffffffffull) : ~k));
+  }
+};
+
+// the operation fixed at compile time (a run-time switch in the unrolled loads spilled)
+template <typename T, int OP>
+struct MinMaxOp {
+  __device__ __forceinline__ T process(T a) const { return OP == OCU_REDUCE_MAXABS ? fabs(a) : a; }
+  __device__ __forceinline__ T reduce(T a, T b) const { return OP == OCU_REDUCE_MIN ? fmin(a, b) : fmax(a, b); }
+};
+
+constexpr int kMMThreads = 256;
+
+template <typename T, bool VEC>
+constexpr int mm_rows() { return (VEC && sizeof(T) == 4) ? 6 : 4; }  // rows of a warp (no spills)
+
+// Up to three grids in one launch (the CFL step reduces u, v and w): blocks [b0[g], b0[g+1])
+// fold grid g into key g; one ticket for the launch.
+template <typename T>
+struct MMGrids {
+  const T *o0, *o1, *o2;
+  long long xs, ys;       // shared strides
+  int nx0, nx1, nx2, ny0, ny1, ny2, nz0, nz1, nz2;
+  unsigned b1, b2;        // first blocks of grids 1 and 2
+  int n;                  // grids
+};
+
+template <typename T, bool VEC, int OP>
+__global__ void __launch_bounds__(kMMThreads, 4) k_reduce_mm(const __grid_constant__ MMGrids<T> G, unsigned *counter,
+                                                          typename MMKey<T>::K *keys, double *results) {
+  pdl_entry();
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  using K = typename MMKey<T>::K;
+  constexpr int W = sizeof(V) / sizeof(T);
+  constexpr int NW = kMMThreads / 32, RB = mm_rows<T, VEC>();
+  const MinMaxOp<T, OP> op;
+  __shared__ T sh[NW];
+  __shared__ bool last;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // this block's grid (selects: an indexed parameter array would go to local memory)
+  const int g = blockIdx.x >= G.b2 ? 2 : (blockIdx.x >= G.b1 ? 1 : 0);
+  const T *origin = g == 2 ? G.o2 : (g == 1 ? G.o1 : G.o0);
+  const int ny = g == 2 ? G.ny2 : (g == 1 ? G.ny1 : G.ny0);
+  const int nz = g == 2 ? G.nz2 : (g == 1 ? G.nz1 : G.nz0);
+  const int nx = g == 2 ? G.nx2 : (g == 1 ? G.nx1 : G.nx0);
+  const unsigned blk = blockIdx.x - (g == 2 ? G.b2 : (g == 1 ? G.b1 : 0u));
+  const unsigned nblk = (g == 2 ? gridDim.x : (g == 1 ? G.b2 : G.b1)) - (g == 2 ? G.b2 : (g == 1 ? G.b1 : 0u));
+  const long long xs = G.xs, ys = G.ys;
+  const long long nrows = (long long)nx * ny;
+  T acc = red_nan<T>();
+  // the grid's blocks take the groups of RB consecutive rows in turn (one resident wave: the
+  // atomic and the ticket at a block's end are paid once per block)
+  for (long long grp = (long long)blk * NW + warp; grp * RB < nrows; grp += (long long)nblk * NW) {
+  const T *base[RB];
+  bool ok[RB];
+  // consecutive rows: one division for the first, then step j (wrapping into i)
+  const long long qb = grp * RB;
+  int i = (int)(qb / ny), j = (int)(qb - (long long)i * ny);
+#pragma unroll
+  for (int r = 0; r < RB; r++) {
+    ok[r] = qb + r < nrows;
+    base[r] = ok[r] ? origin + (long long)i * xs + (long long)j * ys : origin;
+    if (++j == ny) {
+      j = 0;
+      ++i;
+    }
+  }
+  if (VEC) {
+    const int nzv = nz - nz % W;  // whole vectors; the ragged end of each row below
+    for (int k = nzv + lane; k < nz; k += 32)
+#pragma unroll
+      for (int r = 0; r < RB; r++)
+        if (ok[r]) acc = op.reduce(acc, op.process(base[r][k]));
+    for (int k = lane * W; k < nzv; k += 32 * W) {
+      V v[RB];
+#pragma unroll
+      for (int r = 0; r < RB; r++)
+        if (ok[r]) v[r] = *reinterpret_cast<const V *>(base[r] + k);
+#pragma unroll
+      for (int r = 0; r < RB; r++)
+        if (ok[r]) {
+          const T *e = reinterpret_cast<const T *>(&v[r]);
+#pragma unroll
+          for (int c = 0; c < W; c++) acc = op.reduce(acc, op.process(e[c]));
+        }
+    }
+  } else {
+    for (int k = lane; k < nz; k += 32) {
+      T v[RB];
+#pragma unroll
+      for (int r = 0; r < RB; r++)
+        if (ok[r]) v[r] = base[r][k];
+#pragma unroll
+      for (int r = 0; r < RB; r++)
+        if (ok[r]) acc = op.reduce(acc, op.process(v[r]));
+    }
+  }
+  }
+  for (int o = 16; o > 0; o >>= 1) acc = op.reduce(acc, __shfl_down_sync(0xffffffffu, acc, o));
+  if (lane == 0) sh[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T a = sh[0];
+    for (int w = 1; w < NW; w++) a = op.reduce(a, sh[w]);
+    if (a == a) {  // a block of NaNs only contributes nothing
+      const K kv = MMKey<T>::enc(a);
+      atomicMax(keys + g, OP == OCU_REDUCE_MIN ? ~kv : kv);
+    }
+    __threadfence();
+    const unsigned ticket = atomicAdd(counter, 1u);
+    last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last || threadIdx.x >= G.n) return;
+  __threadfence();
+  const K kv = atomicMax(keys + threadIdx.x, (K)0);  // the final key (max with the empty key leaves it)
+  results[threadIdx.x] = kv == 0 ? (double)red_nan<T>() : (double)MMKey<T>::dec(OP == OCU_REDUCE_MIN ? ~kv : kv);
+  keys[threadIdx.x] = 0;
+  if (threadIdx.x == 0) *counter = 0;
+}
+
+// n (1..3) grids sharing strides: min, max or max-abs of each into results[0..n); scratch: the
+// ticket at +0, the n keys from +8 (inside the 64-byte header every reduction scratch has), all
+// zero between launches.
+template <typename T>
+ocu_status launch_minmax(const T *const *origins, const ocu_layout *const *lays, int n, int op, void *d_scratch,
+                         double *d_results, cudaStream_t s) {
+  using K = typename MMKey<T>::K;
+  static_assert(sizeof(K) <= 8, "key slots are 8 bytes");
+  if (n < 1 || n > 3) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] reduce - %d grids", n);
+  constexpr int W = 16 / sizeof(T);
+  bool vec = true;
+  MMGrids<T> G{};
+  G.n = n;
+  G.xs = lays[0]->xstride;
+  G.ys = lays[0]->ystride;
+  unsigned start[3] = {0, 0, 0}, total = 0;
+  for (int g = 0; g < n; g++) {
+    if (lays[g]->xstride != G.xs || lays[g]->ystride != G.ys)
+      return fail(OCU_ERR_LAYOUT, "[ERROR] reduce - grids of one launch must share strides");
+    vec = vec && G.xs % W == 0 && G.ys % W == 0 && reinterpret_cast<uintptr_t>(origins[g]) % 16 == 0;
+  }
+  // one resident wave, shared among the grids in proportion to their rows (at least one block,
+  // at most one per block's worth of rows each)
+  static int wave = 0;
+  if (!wave) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_reduce_mm<T, true, OCU_REDUCE_MAXABS>, kMMThreads, 0);
+    wave = sms > 0 && per > 0 ? sms * per : 148 * 8;
+  }
+  const long long rpb = (long long)(kMMThreads / 32) * (vec ? mm_rows<T, true>() : mm_rows<T, false>());
+  long long rows[3] = {0, 0, 0}, all = 0;
+  for (int g = 0; g < n; g++) {
+    rows[g] = (long long)lays[g]->nx * lays[g]->ny;
+    if (rows[g] < 1) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] reduce_with_operator - empty grid");
+    all += rows[g];
+  }
+  for (int g = 0; g < n; g++) {
+    long long b = (long long)((double)wave * rows[g] / all);
+    b = std::max(1LL, std::min(b, (rows[g] + rpb - 1) / rpb));
+    start[g] = total;
+    total += (unsigned)b;
+  }
+  G.o0 = origins[0]; G.o1 = n > 1 ? origins[1] : origins[0]; G.o2 = n > 2 ? origins[2] : origins[0];
+  G.nx0 = lays[0]->nx; G.ny0 = lays[0]->ny; G.nz0 = lays[0]->nz;
+  G.nx1 = lays[n > 1 ? 1 : 0]->nx; G.ny1 = lays[n > 1 ? 1 : 0]->ny; G.nz1 = lays[n > 1 ? 1 : 0]->nz;
+  G.nx2 = lays[n > 2 ? 2 : 0]->nx; G.ny2 = lays[n > 2 ? 2 : 0]->ny; G.nz2 = lays[n > 2 ? 2 : 0]->nz;
+  G.b1 = n > 1 ? start[1] : total;
+  G.b2 = n > 2 ? start[2] : total;
+  unsigned *counter = reinterpret_cast<unsigned *>(d_scratch);
+  K *keys = reinterpret_cast<K *>(reinterpret_cast<char *>(d_scratch) + 8);
+#define OCU_MM_LAUNCH(V, O) \
+  launch_pdl(k_reduce_mm<T, V, O>, total, kMMThreads, 0, s, G, counter, keys, d_results)
+  if (vec) {
+    if (op == OCU_REDUCE_MAXABS) OCU_MM_LAUNCH(true, OCU_REDUCE_MAXABS);
+    else if (op == OCU_REDUCE_MAX) OCU_MM_LAUNCH(true, OCU_REDUCE_MAX);
+    else OCU_MM_LAUNCH(true, OCU_REDUCE_MIN);
+  } else {
+    if (op == OCU_REDUCE_MAXABS) OCU_MM_LAUNCH(false, OCU_REDUCE_MAXABS);
+    else if (op == OCU_REDUCE_MAX) OCU_MM_LAUNCH(false, OCU_REDUCE_MAX);
+    else OCU_MM_LAUNCH(false, OCU_REDUCE_MIN);
+  }
+#undef OCU_MM_LAUNCH
+  return check_launch("k_reduce_mm");
+}
+
 size_t reduce_scratch_bytes(const ocu_layout &L, size_t elem) {
   const long long nrows = (long long)L.nx * L.ny;
   const long long blocks = (nrows + 255) / 256;
@@ -529,9 +759,29 @@ ocu_status launch_reduce(const T *origin, const ocu_layout &L, int op, void *d_s
   unsigned *counter = reinterpret_cast<unsigned *>(d_scratch);
   T *partial = reinterpret_cast<T *>(reinterpret_cast<char *>(d_scratch) + 64);
   RedOp<T> r{op};
-  launch_pdl(k_reduce<T>, (unsigned)blocks, kReduceThreads, 0, s, origin, L.xstride, L.ystride, L.nx, L.ny, L.nz, r, partial,
-             counter, d_result);
+  if (op == OCU_REDUCE_MAX || op == OCU_REDUCE_MIN || op == OCU_REDUCE_MAXABS) {
+    const T *o[1] = {origin};
+    const ocu_layout *l[1] = {&L};
+    return launch_minmax<T>(o, l, 1, op, d_scratch, d_result, s);
+  }
+  launch_pdl(k_reduce<T, false>, (unsigned)blocks, kReduceThreads, 0, s, origin, (const T *)nullptr, L.xstride,
+             L.ystride, L.nx, L.ny, L.nz, r, partial, counter, d_result);
   return check_launch("k_reduce");
+}
+
+// sum over the interior of a * b (both in layout L), in the reference fold order of
+// reduce_sum over the product grid (sol_pcgpressure3d.cu:257-287)
+template <typename T>
+ocu_status launch_dot(const T *a, const T *b, const ocu_layout &L, void *d_scratch, double *d_result, cudaStream_t s) {
+  const long long nrows = (long long)L.nx * L.ny;
+  const long long blocks = (nrows + 255) / 256;
+  if (blocks < 1) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] dot product - empty grid");
+  unsigned *counter = reinterpret_cast<unsigned *>(d_scratch);
+  T *partial = reinterpret_cast<T *>(reinterpret_cast<char *>(d_scratch) + 64);
+  RedOp<T> r{OCU_REDUCE_SUM};
+  launch_pdl(k_reduce<T, true>, (unsigned)blocks, kReduceThreads, 0, s, a, b, L.xstride, L.ystride, L.nx, L.ny, L.nz,
+             r, partial, counter, d_result);
+  return check_launch("k_reduce_dot");
 }
 
 #define INST(T)                                                                                               \
@@ -544,7 +794,10 @@ ocu_status launch_reduce(const T *origin, const ocu_layout &L, int op, void *d_s
   template ocu_status launch_clear<T>(T *, long long, T, cudaStream_t);                                        \
   template ocu_status launch_lincomb1<T>(T *, T, const T *, long long, cudaStream_t);                          \
   template ocu_status launch_lincomb2<T>(T *, const ocu_layout &, T, const T *, T, const T *, cudaStream_t);   \
-  template ocu_status launch_reduce<T>(const T *, const ocu_layout &, int, void *, double *, cudaStream_t);
+  template ocu_status launch_reduce<T>(const T *, const ocu_layout &, int, void *, double *, cudaStream_t);    \
+  template ocu_status launch_dot<T>(const T *, const T *, const ocu_layout &, void *, double *, cudaStream_t);  \
+  template ocu_status launch_minmax<T>(const T *const *, const ocu_layout *const *, int, int, void *, double *,  \
+                                       cudaStream_t);
 INST(float)
 INST(double)
 #undef INST

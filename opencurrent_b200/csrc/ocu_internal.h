@@ -134,6 +134,12 @@ ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, T a2,
 // as double at *d_result (device pointer).  d_scratch: >= reduce_scratch_elems(L) elements of
 // T plus one unsigned counter (see kernels_grid.cu).
 size_t reduce_scratch_bytes(const ocu_layout &L, size_t elem);
+// min, max or max-abs (op) of n <= 3 grids sharing strides, one launch, into results[0..n)
+template <typename T>
+ocu_status launch_minmax(const T *const *origins, const ocu_layout *const *lays, int n, int op, void *d_scratch,
+                         double *d_results, cudaStream_t s);
+template <typename T>
+ocu_status launch_dot(const T *a, const T *b, const ocu_layout &L, void *d_scratch, double *d_result, cudaStream_t s);
 template <typename T>
 ocu_status launch_reduce(const T *origin, const ocu_layout &L, int op, void *d_scratch,
                          double *d_result, cudaStream_t s);
