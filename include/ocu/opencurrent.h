@@ -53,6 +53,10 @@ enum InterpolationType {
   IT_THIRD_ORDER_VAN_LEER_FLUX_LIMITED = OCU_IT_THIRD_ORDER_VAN_LEER_FLUX_LIMITED
 };
 
+enum PreconditionerType {
+  PRECOND_NONE = OCU_PRECOND_NONE, PRECOND_JACOBI = OCU_PRECOND_JACOBI,
+  PRECOND_MULTIGRID = OCU_PRECOND_MULTIGRID, PRECOND_BFBT = OCU_PRECOND_BFBT
+};
 enum TimeStepType { TS_ERROR = OCU_TS_ERROR, TS_FORWARD_EULER = OCU_TS_FORWARD_EULER, TS_ADAMS_BASHFORD2 = OCU_TS_ADAMS_BASHFORD2 };
 
 enum DirectionType {
@@ -521,6 +525,61 @@ typedef Eqn_IncompressibleNS3D<float> Eqn_IncompressibleNS3DF;
 typedef Eqn_IncompressibleNS3D<double> Eqn_IncompressibleNS3DD;
 typedef Eqn_IncompressibleNS3DParams<float> Eqn_IncompressibleNS3DParamsF;
 typedef Eqn_IncompressibleNS3DParams<double> Eqn_IncompressibleNS3DParamsD;
+
+// Sol_PCGPressure3DDevice<T> (sol_pcgpressure3d.h:41-97): conjugate gradients on
+// -div(coefficient grad p) = rhs; the public fields are read at initialize_storage and at each
+// solve (bc only at initialize_storage).
+template <typename T>
+class Sol_PCGPressure3DDevice : public ErrorHandler {
+  ocu_pcg *_s = nullptr;
+  Grid3DDevice<T> _pressure;
+  ocu_pcg_params params() const {
+    ocu_pcg_params p;
+    ocu_pcg_params_default(&p);
+    p.bc = bc.c();
+    p.convergence = convergence;
+    p.preconditioner = preconditioner;
+    p.multigrid_cycles = multigrid_cycles;
+    p.multigrid_use_fmg = multigrid_use_fmg ? 1 : 0;
+    return p;
+  }
+ public:
+  BoundaryConditionSet bc;
+  ConvergenceType convergence = CONVERGENCE_L2;
+  PreconditionerType preconditioner = PRECOND_BFBT;
+  int multigrid_cycles = 2;
+  bool multigrid_use_fmg = true;
+  Grid3DDevice<T> *rhs_grid = nullptr, *coefficient_grid = nullptr;
+  ~Sol_PCGPressure3DDevice() { ocu_pcg_destroy(_s); }
+  bool initialize_storage(int nx, int ny, int nz, float hx, float hy, float hz, Grid3DDevice<T> *rhs,
+                          Grid3DDevice<T> *coefficient) {
+    rhs_grid = rhs;
+    coefficient_grid = coefficient;
+    ocu_pcg_params p = params();
+    if (!_s && !check_ok(ocu_pcg_create(detail::dtype_of<T>::value, &p, &_s))) return false;
+    ocu_pcg_set_stream(_s, detail::stream());
+    if (!check_ok(ocu_pcg_initialize_storage(_s, nx, ny, nz, hx, hy, hz, rhs->handle(), coefficient->handle())))
+      return false;
+    ocu_grid *g = nullptr;
+    if (!check_ok(ocu_pcg_pressure(_s, &g))) return false;
+    _pressure.attach(g);
+    return true;
+  }
+  bool solve(double &residual, double tolerance = 1e-6, int max_iter = 1000) {
+    clear_error();
+    ocu_pcg_params p = params();
+    if (!check_ok(ocu_pcg_set_params(_s, &p))) return false;
+    ocu_status st = ocu_pcg_solve(_s, &residual, tolerance, max_iter);
+    if (st == OCU_ERR_NOT_CONVERGED) return false;
+    return check_ok(st);
+  }
+  Grid3DDevice<T> &pressure() { return _pressure; }
+  Grid3DDevice<T> &rhs() { return *rhs_grid; }
+  Grid3DDevice<T> &coefficient() { return *coefficient_grid; }
+};
+
+typedef Sol_PCGPressure3DDevice<float> Sol_PCGPressure3DDeviceF;
+typedef Sol_PCGPressure3DDevice<double> Sol_PCGPressure3DDeviceD;
 
 }  // namespace ocu
 

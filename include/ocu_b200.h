@@ -306,6 +306,42 @@ ocu_status ocu_ens_set_tuning(ocu_ens *e, int cls, const ocu_ens_tuning *tuning)
  * shapes and keeps the fastest that converges every member; leaves every pressure zeroed. */
 ocu_status ocu_ens_autotune(ocu_ens *e, const double *tol, int max_iter);
 
+/* ---- preconditioned conjugate gradients (Sol_PCGPressure3DDevice<T>, sol_pcgpressure3d.h:41-97) --
+ * Solves L p = rhs, L = -div(c grad) with a cell coefficient grid c (the variable-coefficient
+ * pressure equation), by CG with no preconditioner, Jacobi, multigrid (FMG or V-cycles of the
+ * constant-coefficient multigrid solver on the residual, sign flipped) or BFBT (multigrid then
+ * Jacobi), restarting the residual from rhs - L p every 25 iterations, as the reference does
+ * (sol_pcgpressure3d.cu:335-457).  Faces must be periodic or Neumann.  solve() returns
+ * OCU_ERR_NOT_CONVERGED (the reference's false) when sqrt(<r, M^-1 r>) stays at or above the
+ * tolerance after max_iter + 1 iterations; *residual is that norm (OCU_CONVERGENCE_L2) or
+ * max |r|.  Bit-identical to the CPU oracle's restatement. */
+typedef struct ocu_pcg ocu_pcg;
+typedef struct ocu_pcg_params {
+  ocu_bc_set bc;
+  int convergence;        /* OCU_CONVERGENCE_L2 (default) or OCU_CONVERGENCE_LINF */
+  int preconditioner;     /* ocu_precond; default OCU_PRECOND_BFBT */
+  int multigrid_cycles;   /* default 2 */
+  int multigrid_use_fmg;  /* default 1; 0 = V-cycles */
+} ocu_pcg_params;
+/* The reference constructor's defaults (sol_pcgpressure3d.cu:160-171), faces Neumann. */
+void ocu_pcg_params_default(ocu_pcg_params *p);
+ocu_status ocu_pcg_create(ocu_dtype dtype, const ocu_pcg_params *params, ocu_pcg **out);
+void ocu_pcg_destroy(ocu_pcg *s);
+ocu_status ocu_pcg_set_stream(ocu_pcg *s, ocu_stream stream);
+/* convergence, preconditioner and the multigrid counts take effect at the next solve; bc only
+ * before initialize_storage */
+ocu_status ocu_pcg_set_params(ocu_pcg *s, const ocu_pcg_params *params);
+/* initialize_storage(nx, ny, nz, hx, hy, hz, rhs, coefficient) (sol_pcgpressure3d.cu:604-654):
+ * spacings are float, as in the reference; rhs and coefficient share one layout (ghost >= 1) and
+ * are borrowed (the coefficient's face ghosts are written at each solve); the pressure is
+ * allocated congruent and cleared. */
+ocu_status ocu_pcg_initialize_storage(ocu_pcg *s, int nx, int ny, int nz, float hx, float hy, float hz,
+                                      ocu_grid *rhs, ocu_grid *coefficient);
+ocu_status ocu_pcg_solve(ocu_pcg *s, double *residual, double tolerance, int max_iter);
+ocu_status ocu_pcg_pressure(ocu_pcg *s, ocu_grid **out);
+/* CG iterations of the last solve */
+ocu_status ocu_pcg_iterations(const ocu_pcg *s, int *out);
+
 /* ---- persistent refinement ensembles ----------------------------------------------------
  * No reference counterpart as a whole: many Sol_MultigridPressure3DBase::solve calls
  * (sol_mgpressure3d.cpp:332-370: sqrt(sum r^2 / N) of the residual against an absolute

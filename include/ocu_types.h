@@ -57,6 +57,14 @@ typedef enum ocu_convergence {
   OCU_CONVERGENCE_NONE_CALC_L2LINF = 0x10 | 0x01 | 0x02
 } ocu_convergence;
 
+/* Preconditioners of the conjugate-gradient pressure solver (ocuequation/sol_pcgpressure3d.h:34-39). */
+typedef enum ocu_precond {
+  OCU_PRECOND_NONE = 0,
+  OCU_PRECOND_JACOBI = 1,
+  OCU_PRECOND_MULTIGRID = 2,
+  OCU_PRECOND_BFBT = 3
+} ocu_precond;
+
 /* Advection interpolants (ocuutil/interpolation.h:26-31). */
 typedef enum ocu_interpolation {
   OCU_IT_ERROR = 0,

@@ -17,6 +17,7 @@ from ._capi import *  # noqa: F401,F403  (enums, structs)
 from ._capi import OcuError, check, load
 
 __all__ = [
+    "Sol_PCGPressure3DDevice",
     "PersistentEnsemble",
     "BoundaryCondition", "BoundaryConditionSet", "Grid3DDevice", "Sol_MultigridPressure3DDevice",
     "Sol_MultigridPressure3DDeviceF", "Sol_MultigridPressure3DDeviceD",
@@ -490,6 +491,74 @@ class PersistentEnsemble:
         try:
             if self._h:
                 load().ocu_pens_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+class Sol_PCGPressure3DDevice:
+    """Preconditioned conjugate gradients on L p = rhs, L = -div(c grad) with a cell coefficient
+    grid c (Sol_PCGPressure3DDevice<T>, sol_pcgpressure3d.h:41-97).  preconditioner: one of
+    PRECOND_NONE, PRECOND_JACOBI, PRECOND_MULTIGRID, PRECOND_BFBT (the reference's default);
+    faces periodic or Neumann.  Bit-identical to the CPU oracle's restatement."""
+
+    def __init__(self, dtype):
+        p = PCGParams()
+        load().ocu_pcg_params_default(C.byref(p))
+        self.dtype = dtype
+        self.bc = BoundaryConditionSet(BoundaryCondition(BC_NEUMANN, 0.0))
+        self.convergence = p.convergence
+        self.preconditioner = p.preconditioner
+        self.multigrid_cycles = p.multigrid_cycles
+        self.multigrid_use_fmg = bool(p.multigrid_use_fmg)
+        self._h = None
+        self._keep = ()
+
+    def _params(self):
+        p = PCGParams()
+        p.bc = self.bc.to_c()
+        p.convergence = int(self.convergence)
+        p.preconditioner = int(self.preconditioner)
+        p.multigrid_cycles = int(self.multigrid_cycles)
+        p.multigrid_use_fmg = int(bool(self.multigrid_use_fmg))
+        return p
+
+    def initialize_storage(self, nx, ny, nz, hx, hy, hz, rhs, coefficient):
+        lib = load()
+        h = C.c_void_p()
+        p = self._params()
+        check(lib.ocu_pcg_create(self.dtype, C.byref(p), C.byref(h)))
+        self._h = h.value
+        self._keep = (rhs, coefficient)  # borrowed, as in the reference
+        check(lib.ocu_pcg_initialize_storage(self._h, nx, ny, nz, hx, hy, hz, rhs._h, coefficient._h))
+        return True
+
+    def solve(self, tolerance=1e-6, max_iter=1000):
+        """solve (sol_pcgpressure3d.cu:571-601) -> (converged, residual)."""
+        p = self._params()
+        check(load().ocu_pcg_set_params(self._h, C.byref(p)))
+        r = C.c_double()
+        st = check(load().ocu_pcg_solve(self._h, C.byref(r), tolerance, max_iter), allow=(ERR_NOT_CONVERGED,))
+        return st == OK, r.value
+
+    def pressure(self):
+        out = C.c_void_p()
+        check(load().ocu_pcg_pressure(self._h, C.byref(out)))
+        return Grid3DDevice._borrow(out.value, self)
+
+    @property
+    def iterations(self):
+        n = C.c_int()
+        check(load().ocu_pcg_iterations(self._h, C.byref(n)))
+        return n.value
+
+    def set_stream(self, stream_handle):
+        check(load().ocu_pcg_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    def __del__(self):
+        try:
+            if self._h:
+                load().ocu_pcg_destroy(self._h)
                 self._h = None
         except Exception:
             pass

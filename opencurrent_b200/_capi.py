@@ -26,6 +26,7 @@ DIR_XPOS, DIR_XNEG, DIR_YPOS, DIR_YNEG, DIR_ZPOS, DIR_ZNEG = 0x05, 0x06, 0x09, 0
 REDUCE_MAXABS, REDUCE_MAX, REDUCE_MIN, REDUCE_SUM, REDUCE_SQRSUM, REDUCE_CHECKNAN = range(6)
 BC_LEVEL1, BC_LEVEL1_NOCORNERS = 0, 1
 MG_F32, MG_F64, MG_MIXED_IR, MG_MIXED_WARMSTART = 0, 1, 2, 3
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_MULTIGRID, PRECOND_BFBT = 0, 1, 2, 3
 
 OK, ERR_INVALID_VALUE, ERR_LAYOUT, ERR_CUDA, ERR_NOT_CONVERGED = 0, 1, 2, 3, 4
 ERR_NOT_INITIALIZED, ERR_ALLOC, ERR_UNSUPPORTED, ERR_TIMEOUT = 5, 6, 7, 8
@@ -74,6 +75,11 @@ class PensParams(C.Structure):
 
 class PensStats(C.Structure):
     _fields_ = [("converged", C.c_int), ("corrections", C.c_int), ("vcycles", C.c_int), ("l2", C.c_double)]
+
+
+class PCGParams(C.Structure):
+    _fields_ = [("bc", BCSet), ("convergence", C.c_int), ("preconditioner", C.c_int),
+                ("multigrid_cycles", C.c_int), ("multigrid_use_fmg", C.c_int)]
 
 
 class NSParams(C.Structure):
@@ -152,6 +158,15 @@ SIGNATURES = {
     "ocu_ens_class_info": (I, [P, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(EnsTuning)]),
     "ocu_ens_set_tuning": (I, [P, I, C.POINTER(EnsTuning)]),
     "ocu_ens_autotune": (I, [P, C.POINTER(D), I]),
+    "ocu_pcg_params_default": (None, [C.POINTER(PCGParams)]),
+    "ocu_pcg_create": (I, [I, C.POINTER(PCGParams), PP]),
+    "ocu_pcg_destroy": (None, [P]),
+    "ocu_pcg_set_stream": (I, [P, P]),
+    "ocu_pcg_set_params": (I, [P, C.POINTER(PCGParams)]),
+    "ocu_pcg_initialize_storage": (I, [P, I, I, I, C.c_float, C.c_float, C.c_float, P, P]),
+    "ocu_pcg_solve": (I, [P, C.POINTER(D), D, I]),
+    "ocu_pcg_pressure": (I, [P, PP]),
+    "ocu_pcg_iterations": (I, [P, C.POINTER(C.c_int)]),
     "ocu_pens_params_default": (None, [C.POINTER(PensParams)]),
     "ocu_pens_create": (I, [I, C.POINTER(C.c_int), C.POINTER(D), C.POINTER(PensParams), PP]),
     "ocu_pens_destroy": (None, [P]),

@@ -48,7 +48,7 @@ SOURCES=(
   ocuequation/sol_mgpressure3ddevf.cu ocuequation/sol_project3ddev.cu
   ocuequation/sol_projectmixed3d.cu ocuequation/sol_project3d.cpp
   ocuequation/sol_laplaciancent3ddev.cu ocuequation/sol_divergence3ddev.cu
-  ocuequation/sol_gradient3ddev.cu
+  ocuequation/sol_gradient3ddev.cu ocuequation/sol_pcgpressure3d.cu
 )
 LOCAL=(grid3d_reduce.cu ref_driver.cu)
 

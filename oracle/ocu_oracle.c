@@ -610,6 +610,178 @@ void *orc_project_divergence(orc_project *p) { return p->div; }
 orc_mg *orc_project_pressure_solver(orc_project *p) { return p->mg; }
 
 /* ------------------------------------------------------------------------------------------
+ * Sol_PCGPressure3DDevice<T> (ocuequation/sol_pcgpressure3d.cu:289-654).
+ * ---------------------------------------------------------------------------------------- */
+struct orc_pcg {
+  int dtype;
+  orc_pcg_params prm;
+  int nx, ny, nz;
+  double h, fx, fy, fz;
+  ocu_layout L;
+  void *rhs, *coef;          /* borrowed */
+  void *p, *r, *y, *d;       /* pressure, residual (the multigrid's rhs), L d, search direction */
+  orc_mg *mg;
+  int iterations;
+};
+
+orc_pcg *orc_pcg_create(int dtype, const orc_pcg_params *prm, int nx, int ny, int nz, double hx_d, double hy_d,
+                        double hz_d, void *rhs, void *coefficient, const ocu_layout *L)
+{
+  const float hx = (float)hx_d, hy = (float)hy_d, hz = (float)hz_d;
+  const size_t es = dtype == OCU_F64 ? 8 : 4;
+  orc_mg_params mp;
+  orc_pcg *p;
+  int f;
+  const ocu_bc *faces[6];
+  if (L->gx < 1 || L->gy < 1 || L->gz < 1) return 0;
+  faces[0] = &prm->bc.xpos; faces[1] = &prm->bc.xneg; faces[2] = &prm->bc.ypos;
+  faces[3] = &prm->bc.yneg; faces[4] = &prm->bc.zpos; faces[5] = &prm->bc.zneg;
+  for (f = 0; f < 6; f++) /* bc.check_type(BC_PERIODIC, BC_NEUMANN) */
+    if (faces[f]->type != OCU_BC_PERIODIC && faces[f]->type != OCU_BC_NEUMANN) return 0;
+  p = (orc_pcg *)calloc(1, sizeof(orc_pcg));
+  p->dtype = dtype;
+  p->prm = *prm;
+  p->nx = nx; p->ny = ny; p->nz = nz;
+  p->h = orc_min3(hx, hy, hz);
+  p->fx = (p->h * p->h) / ((double)hx * hx);
+  p->fy = (p->h * p->h) / ((double)hy * hy);
+  p->fz = (p->h * p->h) / ((double)hz * hz);
+  p->L = *L;
+  p->rhs = rhs;
+  p->coef = coefficient;
+  p->p = calloc((size_t)L->allocated, es);
+  p->r = calloc((size_t)L->allocated, es);
+  p->y = calloc((size_t)L->allocated, es);
+  p->d = calloc((size_t)L->allocated, es);
+  memset(&mp, 0, sizeof(mp));
+  mp.bc = prm->bc;
+  mp.nu1 = 2;
+  mp.nu2 = 2;
+  mp.convergence = OCU_CONVERGENCE_NONE_CALC_L2LINF;
+  p->mg = orc_mg_create(dtype, &mp, nx, ny, nz, hx, hy, hz, p->r, L);
+  return p;
+}
+
+void orc_pcg_destroy(orc_pcg *p)
+{
+  if (!p) return;
+  orc_mg_destroy(p->mg);
+  free(p->p); free(p->r); free(p->y); free(p->d);
+  free(p);
+}
+
+void *orc_pcg_pressure(orc_pcg *p) { return p->p; }
+int orc_pcg_iterations(const orc_pcg *p) { return p->iterations; }
+
+/* f / h^2 as the reference's host code has them: rounded to T */
+static double pcg_fh(const orc_pcg *p, double f)
+{
+  return p->dtype == OCU_F64 ? f / (p->h * p->h) : (double)(float)(f / (p->h * p->h));
+}
+
+static void pcg_bc(orc_pcg *p, void *g)
+{
+  const double hx = p->h / sqrt(p->fx), hy = p->h / sqrt(p->fy), hz = p->h / sqrt(p->fz);
+  if (p->dtype == OCU_F64) orc_bc_nocorners_dev_d((double *)g, &p->L, &p->prm.bc, hx, hy, hz);
+  else orc_bc_nocorners_dev_f((float *)g, &p->L, &p->prm.bc, hx, hy, hz);
+}
+
+/* invoke_kernel_apply_laplacian: src's face ghosts first, then the stencil */
+static void pcg_apply_laplacian(orc_pcg *p, void *dst, void *src)
+{
+  const double fxh = pcg_fh(p, p->fx), fyh = pcg_fh(p, p->fy), fzh = pcg_fh(p, p->fz);
+  pcg_bc(p, src);
+  if (p->dtype == OCU_F64)
+    orc_pcg_laplacian_d((double *)dst, (const double *)src, (const double *)p->coef, &p->L, fxh, fyh, fzh);
+  else orc_pcg_laplacian_f((float *)dst, (const float *)src, (const float *)p->coef, &p->L, fxh, fyh, fzh);
+}
+
+static void pcg_diag(orc_pcg *p, void *dst, const void *src)
+{
+  const double fxh = pcg_fh(p, p->fx), fyh = pcg_fh(p, p->fy), fzh = pcg_fh(p, p->fz);
+  if (p->dtype == OCU_F64)
+    orc_pcg_diag_d((double *)dst, (const double *)src, (const double *)p->coef, &p->L, fxh, fyh, fzh);
+  else orc_pcg_diag_f((float *)dst, (const float *)src, (const float *)p->coef, &p->L, fxh, fyh, fzh);
+}
+
+static double pcg_dot(orc_pcg *p, const void *a, const void *b)
+{
+  return p->dtype == OCU_F64 ? orc_pcg_dot_d((const double *)a, (const double *)b, &p->L)
+                             : orc_pcg_dot_f((const float *)a, (const float *)b, &p->L);
+}
+
+static void pcg_lincomb2(orc_pcg *p, void *res, double a1, const void *g1, double a2, const void *g2)
+{
+  if (p->dtype == OCU_F64) orc_lincomb2_d((double *)res, &p->L, a1, (const double *)g1, a2, (const double *)g2);
+  else orc_lincomb2_f((float *)res, &p->L, a1, (const float *)g1, a2, (const float *)g2);
+}
+
+/* apply_preconditioner (sol_pcgpressure3d.cu:289-331); the multigrid solves for its own rhs,
+ * the residual grid, whatever src is */
+static void pcg_precondition(orc_pcg *p, void *dst, const void *src)
+{
+  const int pc = p->prm.preconditioner;
+  const size_t es = p->dtype == OCU_F64 ? 8 : 4;
+  if (pc == OCU_PRECOND_JACOBI) {
+    pcg_diag(p, dst, src);
+  } else if (pc == OCU_PRECOND_MULTIGRID || pc == OCU_PRECOND_BFBT) {
+    void *u = orc_mg_grid(p->mg, 'u', 0, 0);
+    memset(u, 0, es * (size_t)p->L.allocated);
+    if (p->prm.multigrid_use_fmg) orc_mg_run_fmg(p->mg, p->prm.multigrid_cycles);
+    else orc_mg_run_vcycles(p->mg, p->prm.multigrid_cycles);
+    if (p->dtype == OCU_F64) orc_lincomb1_d((double *)dst, &p->L, -1.0, (const double *)u);
+    else orc_lincomb1_f((float *)dst, &p->L, -1.0, (const float *)u);
+    if (pc == OCU_PRECOND_BFBT) pcg_diag(p, dst, dst);
+  } else {
+    memcpy(dst, src, es * (size_t)p->L.allocated);
+  }
+}
+
+/* the host scalars of do_pcg are T */
+static double pcg_round(const orc_pcg *p, double x) { return p->dtype == OCU_F64 ? x : (double)(float)x; }
+
+/* do_pcg (sol_pcgpressure3d.cu:335-457) and solve (:571-601) */
+int orc_pcg_solve(orc_pcg *p, double *residual, double tolerance, int max_iter)
+{
+  double delta0, deltanew, deltaold, d_dot_y, alpha, beta, l2, linf;
+  int it = 0, converged, ok;
+  if (!orc_check_float((float)tolerance) || tolerance < 0 || max_iter <= 0) return 0;
+  pcg_bc(p, p->coef);
+  pcg_apply_laplacian(p, p->y, p->p);
+  pcg_lincomb2(p, p->r, 1.0, p->rhs, -1.0, p->y);
+  pcg_precondition(p, p->d, p->r);
+  delta0 = pcg_dot(p, p->r, p->d);
+  deltanew = delta0;
+  converged = (it > max_iter) || (delta0 < tolerance * tolerance);
+  while (!converged) {
+    pcg_apply_laplacian(p, p->y, p->d);
+    d_dot_y = pcg_dot(p, p->d, p->y);
+    alpha = pcg_round(p, deltanew / d_dot_y);
+    pcg_lincomb2(p, p->p, 1.0, p->p, alpha, p->d);
+    if (it % 25 == 0) {
+      pcg_apply_laplacian(p, p->y, p->p);
+      pcg_lincomb2(p, p->r, 1.0, p->rhs, -1.0, p->y);
+    } else {
+      pcg_lincomb2(p, p->r, 1.0, p->r, -alpha, p->y);
+    }
+    pcg_precondition(p, p->y, p->r);
+    deltaold = deltanew;
+    deltanew = pcg_dot(p, p->r, p->y);
+    beta = pcg_round(p, deltanew / deltaold);
+    pcg_lincomb2(p, p->d, beta, p->d, 1.0, p->y);
+    it++;
+    converged = (it > max_iter) || (deltanew < tolerance * tolerance);
+  }
+  ok = deltanew <= tolerance * tolerance;
+  p->iterations = it;
+  l2 = sqrt(deltanew);
+  linf = p->dtype == OCU_F64 ? orc_reduce_d((const double *)p->r, &p->L, OCU_REDUCE_MAXABS)
+                             : orc_reduce_f((const float *)p->r, &p->L, OCU_REDUCE_MAXABS);
+  *residual = p->prm.convergence == OCU_CONVERGENCE_L2 ? l2 : linf;
+  return ok;
+}
+
+/* ------------------------------------------------------------------------------------------
  * Eqn_IncompressibleNS3D<T> (eqn_incompressns3d.cu:164-399) and Equation::advance
  * (equation.cpp:31-56).  Parameters that the reference stores as T are rounded to T here.
  * ---------------------------------------------------------------------------------------- */

@@ -60,7 +60,12 @@ double orc_optimal_omega(double fx, double fy, double fz);
                              const ocu_layout *L, int nx, int ny, int nz, double hx, double hy,   \
                              double hz, int interp);                                              \
   void orc_thermal_force##S(T *dvdt, double coefficient, const T *temp, const ocu_layout *L,      \
-                            int nbr_stride, int nx, int ny, int nz);
+                            int nbr_stride, int nx, int ny, int nz);                              \
+  void orc_pcg_laplacian##S(T *dst, const T *src, const T *coef, const ocu_layout *L, double fxh, \
+                            double fyh, double fzh);                                              \
+  void orc_pcg_diag##S(T *dst, const T *src, const T *coef, const ocu_layout *L, double fxh,      \
+                       double fyh, double fzh);                                                   \
+  double orc_pcg_dot##S(const T *a, const T *b, const ocu_layout *L);
 
 ORC_DECLARE(float, _f)
 ORC_DECLARE(double, _d)
@@ -131,6 +136,30 @@ int orc_project_solve(orc_project *p, double tolerance);
 int orc_project_solve_divergence_only(orc_project *p);
 void *orc_project_divergence(orc_project *p);
 orc_mg *orc_project_pressure_solver(orc_project *p);
+
+/* ------------------------------------------------------------------------------------------
+ * Preconditioned conjugate gradients (Sol_PCGPressure3DDevice<T>,
+ * ocuequation/sol_pcgpressure3d.cu:289-654): L p = rhs with L = -div(c grad), c a cell
+ * coefficient grid; preconditioner none, Jacobi, multigrid (FMG or V-cycles on the constant-
+ * coefficient operator, sign flipped) or BFBT (multigrid then Jacobi).  Borrows rhs and
+ * coefficient (one layout, ghost >= 1); owns the pressure and the CG vectors.
+ * ---------------------------------------------------------------------------------------- */
+typedef struct orc_pcg_params {
+  ocu_bc_set bc;
+  int convergence;       /* OCU_CONVERGENCE_L2 (default) or _LINF: which norm solve() returns */
+  int preconditioner;    /* ocu_precond (default OCU_PRECOND_BFBT) */
+  int multigrid_cycles;  /* default 2 */
+  int multigrid_use_fmg; /* default 1 */
+} orc_pcg_params;
+typedef struct orc_pcg orc_pcg;
+/* hx, hy, hz are rounded to float (the reference's initialize_storage takes float). */
+orc_pcg *orc_pcg_create(int dtype, const orc_pcg_params *prm, int nx, int ny, int nz, double hx, double hy,
+                        double hz, void *rhs, void *coefficient, const ocu_layout *layout);
+void orc_pcg_destroy(orc_pcg *p);
+/* solve (sol_pcgpressure3d.cu:571-601); returns 1 when converged, *residual the chosen norm. */
+int orc_pcg_solve(orc_pcg *p, double *residual, double tolerance, int max_iter);
+void *orc_pcg_pressure(orc_pcg *p);
+int orc_pcg_iterations(const orc_pcg *p);
 
 /* ------------------------------------------------------------------------------------------
  * Incompressible Navier-Stokes / Boussinesq (Eqn_IncompressibleNS3D<T>,

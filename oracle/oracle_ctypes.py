@@ -36,6 +36,11 @@ class MGParams(C.Structure):
                 ("make_symmetric_operator", C.c_int), ("disable_relax_on_host", C.c_int)]
 
 
+class PCGParams(C.Structure):
+    _fields_ = [("bc", BCSet), ("convergence", C.c_int), ("preconditioner", C.c_int),
+                ("multigrid_cycles", C.c_int), ("multigrid_use_fmg", C.c_int)]
+
+
 class NSParams(C.Structure):
     _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
                 ("hx", C.c_double), ("hy", C.c_double), ("hz", C.c_double),
@@ -134,6 +139,18 @@ def _setup(L):
     L.orc_ns_grid.restype = P
     L.orc_ns_layout.argtypes = [P, LP]
     L.orc_ns_set_omp_threads.argtypes = [i]
+    for s in ("_f", "_d"):
+        getattr(L, "orc_pcg_laplacian" + s).argtypes = [P, P, P, LP, d, d, d]
+        getattr(L, "orc_pcg_diag" + s).argtypes = [P, P, P, LP, d, d, d]
+        getattr(L, "orc_pcg_dot" + s).argtypes = [P, P, LP]
+        getattr(L, "orc_pcg_dot" + s).restype = d
+    L.orc_pcg_create.argtypes = [i, C.POINTER(PCGParams), i, i, i, d, d, d, P, P, LP]
+    L.orc_pcg_create.restype = P
+    L.orc_pcg_destroy.argtypes = [P]
+    L.orc_pcg_solve.argtypes = [P, C.POINTER(d), d, i]
+    L.orc_pcg_pressure.argtypes = [P]
+    L.orc_pcg_pressure.restype = P
+    L.orc_pcg_iterations.argtypes = [P]
 
 
 def np_dtype(dtype):
@@ -254,3 +271,48 @@ def region(a, L, i0, i1, j0, j1, k0, k1):
     return np.lib.stride_tricks.as_strided(
         a[base:], shape=(i1 - i0, j1 - j0, k1 - k0),
         strides=(L.xstride * a.itemsize, L.ystride * a.itemsize, a.itemsize))
+
+
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_MULTIGRID, PRECOND_BFBT = 0, 1, 2, 3
+
+
+def pcg_params(bc, preconditioner=PRECOND_BFBT, convergence=0x05, cycles=2, fmg=True):
+    p = PCGParams()
+    p.bc = bc
+    p.convergence = convergence
+    p.preconditioner = preconditioner
+    p.multigrid_cycles = cycles
+    p.multigrid_use_fmg = int(bool(fmg))
+    return p
+
+
+class OraclePCG:
+    """Oracle preconditioned CG (Sol_PCGPressure3DDevice); rhs and coefficient are borrowed."""
+
+    def __init__(self, dtype, prm, nx, ny, nz, hx, hy, hz, rhs, coef, L):
+        self.lib = lib()
+        self.rhs, self.coef, self.L, self.dtype = rhs, coef, L, dtype
+        self.h = self.lib.orc_pcg_create(dtype, C.byref(prm), nx, ny, nz, hx, hy, hz, ptr(rhs), ptr(coef),
+                                         C.byref(L))
+        if not self.h:
+            raise RuntimeError("oracle PCG create failed")
+
+    def solve(self, tol, max_iter=1000):
+        r = C.c_double(0)
+        ok = self.lib.orc_pcg_solve(self.h, C.byref(r), tol, max_iter)
+        return bool(ok), r.value
+
+    def pressure(self):
+        return wrap(self.lib.orc_pcg_pressure(self.h), self.L, self.dtype).copy()
+
+    @property
+    def iterations(self):
+        return self.lib.orc_pcg_iterations(self.h)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                self.lib.orc_pcg_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass

@@ -25,6 +25,7 @@
 #include "ocuequation/sol_mgpressure3d.h"
 #include "ocuequation/sol_mgpressuremixed3d.h"
 #include "ocuequation/sol_passiveadvection3d.h"
+#include "ocuequation/sol_pcgpressure3d.h"
 #include "ocuequation/sol_project3d.h"
 #include "ocuequation/sol_projectmixed3d.h"
 #include "ocuequation/sol_selfadvection3d.h"
@@ -461,6 +462,70 @@ int ref_ns_download(void *h, char which, void *host, ocu_layout *layout_out) {
   if (layout_out) fill_layout(*g, layout_out);
   return cudaMemcpy(host, g->buffer(), 4 * (size_t)g->num_allocated_elements(),
                     cudaMemcpyDeviceToHost) == cudaSuccess;
+}
+
+/* Sol_PCGPressure3DDevice<T> (sol_pcgpressure3d.cu): rhs and coefficient are reference grids of
+ * one layout; the pressure is borrowed from the solver. */
+struct RefPCG {
+  int dtype;
+  Sol_PCGPressure3DDevice<float> *f;
+  Sol_PCGPressure3DDevice<double> *d;
+  RefGrid *pressure;
+};
+
+void *ref_pcg_create(const orc_pcg_params *prm, int nx, int ny, int nz, double hx, double hy, double hz,
+                     void *rhs, void *coefficient) {
+  if (!ready()) return nullptr;
+  RefGrid *r = (RefGrid *)rhs, *c = (RefGrid *)coefficient;
+  if (r->dtype != c->dtype) return nullptr;
+  RefPCG *s = new RefPCG{r->dtype, nullptr, nullptr, nullptr};
+  bool ok;
+  if (r->dtype == OCU_F32) {
+    s->f = new Sol_PCGPressure3DDevice<float>();
+    s->f->bc = to_bcset(prm->bc);
+    s->f->convergence = (ConvergenceType)prm->convergence;
+    s->f->preconditioner = (PreconditionerType)prm->preconditioner;
+    s->f->multigrid_cycles = prm->multigrid_cycles;
+    s->f->multigrid_use_fmg = prm->multigrid_use_fmg != 0;
+    ok = s->f->initialize_storage(nx, ny, nz, (float)hx, (float)hy, (float)hz, r->f, c->f);
+    if (ok) s->pressure = borrow(s->f->pressure());
+  } else {
+    s->d = new Sol_PCGPressure3DDevice<double>();
+    s->d->bc = to_bcset(prm->bc);
+    s->d->convergence = (ConvergenceType)prm->convergence;
+    s->d->preconditioner = (PreconditionerType)prm->preconditioner;
+    s->d->multigrid_cycles = prm->multigrid_cycles;
+    s->d->multigrid_use_fmg = prm->multigrid_use_fmg != 0;
+    ok = s->d->initialize_storage(nx, ny, nz, (float)hx, (float)hy, (float)hz, r->d, c->d);
+    if (ok) s->pressure = borrow(s->d->pressure());
+  }
+  if (!ok) {
+    delete s->f;
+    delete s->d;
+    delete s;
+    return nullptr;
+  }
+  return s;
+}
+
+int ref_pcg_solve(void *h, double *residual, double tol, int max_iter) {
+  RefPCG *s = (RefPCG *)h;
+  double r = 0;
+  const bool ok = s->f ? s->f->solve(r, tol, max_iter) : s->d->solve(r, tol, max_iter);
+  cudaDeviceSynchronize();
+  *residual = r;
+  return ok ? 1 : 0;
+}
+
+void *ref_pcg_pressure(void *h) { return ((RefPCG *)h)->pressure; }
+
+void ref_pcg_destroy(void *h) {
+  RefPCG *s = (RefPCG *)h;
+  if (!s) return;
+  ref_grid_destroy(s->pressure);
+  delete s->f;
+  delete s->d;
+  delete s;
 }
 
 }  // extern "C"

@@ -48,6 +48,12 @@ def _setup(L):
     L.ref_mg_run_fmg.argtypes = [P, i]
     L.ref_mg_pressure.argtypes = [P]
     L.ref_mg_pressure.restype = P
+    L.ref_pcg_create.argtypes = [C.POINTER(O.PCGParams), i, i, i, d, d, d, P, P]
+    L.ref_pcg_create.restype = P
+    L.ref_pcg_solve.argtypes = [P, C.POINTER(d), d, i]
+    L.ref_pcg_pressure.argtypes = [P]
+    L.ref_pcg_pressure.restype = P
+    L.ref_pcg_destroy.argtypes = [P]
     L.ref_project_create.argtypes = [i, C.POINTER(O.BCSet), i, i, i, d, d, d, P, P, P]
     L.ref_project_create.restype = P
     L.ref_project_destroy.argtypes = [P]
@@ -142,6 +148,35 @@ class RefMG:
         try:
             if self.h:
                 lib().ref_mg_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class RefPCG:
+    """Sol_PCGPressure3DDevice<T> over reference grids made from host rhs / coefficient buffers."""
+
+    def __init__(self, dtype, prm, nx, ny, nz, hx, hy, hz, rhs_host, coef_host, L):
+        self.dtype = dtype
+        self.rhs = RefGrid(dtype, L, rhs_host)
+        self.coef = RefGrid(dtype, L, coef_host)
+        self.L = L
+        self.h = lib().ref_pcg_create(C.byref(prm), nx, ny, nz, hx, hy, hz, self.rhs.h, self.coef.h)
+        if not self.h:
+            raise RuntimeError("reference initialize_storage failed")
+
+    def solve(self, tol, max_iter=1000):
+        r = C.c_double(0)
+        ok = lib().ref_pcg_solve(self.h, C.byref(r), tol, max_iter)
+        return bool(ok), r.value
+
+    def pressure(self):
+        return RefGrid(self.dtype, self.L, handle=lib().ref_pcg_pressure(self.h)).download()
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().ref_pcg_destroy(self.h)
                 self.h = None
         except Exception:
             pass

@@ -240,6 +240,48 @@ static void ns_smoke() {
   CHECK(eqn.num_steps() == 5);
 }
 
+// Sol_PCGPressure3DDevice: a variable coefficient, multigrid-preconditioned CG to 1e-8 (FP64)
+static void pcg(PreconditionerType pc) {
+  const int n = 16;
+  const float h = 1.0f / n;
+  Grid3DDeviceD rhs, coef;
+  REQUIRE(rhs.init(n, n, n, 1, 1, 1));
+  REQUIRE(coef.init_congruent(rhs));
+  Grid3DHostD hr, hc;
+  REQUIRE(hr.init_congruent(rhs));
+  REQUIRE(hc.init_congruent(rhs));
+  double mean = 0;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+      for (int k = 0; k < n; k++) {
+        hr.at(i, j, k) = std::sin(6.28318530718 * (i + 0.5) / n) * std::cos(3.14159265359 * (k + 0.5) / n) + 0.01 * j;
+        mean += hr.at(i, j, k);
+        hc.at(i, j, k) = 1.0 + 0.5 * std::sin(6.28318530718 * (j + 0.5) / n);
+      }
+  mean /= (double)n * n * n;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+      for (int k = 0; k < n; k++) hr.at(i, j, k) -= mean;
+  CHECK(rhs.copy_all_data(hr));
+  CHECK(coef.copy_all_data(hc));
+  Sol_PCGPressure3DDeviceD solver;
+  BoundaryCondition per, neu;
+  per.type = BC_PERIODIC;
+  neu.type = BC_NEUMANN;
+  solver.bc = BoundaryConditionSet(neu);
+  solver.bc.xpos = solver.bc.xneg = per;
+  solver.preconditioner = pc;
+  REQUIRE(solver.initialize_storage(n, n, n, h, h, h, &rhs, &coef));
+  double residual = 0;
+  CHECK(solver.solve(residual, 1e-8, 300));
+  CHECK(residual < 1e-8);
+  CHECK(!solver.any_error());
+  // max_iter too small: solve() returns false, as the reference does
+  double r2 = 0;
+  solver.pressure().clear_zero();
+  CHECK(!solver.solve(r2, 1e-14, 2));
+}
+
 int main() {
   all_dirichlet(0.0);
   all_dirichlet(0.5);
@@ -249,6 +291,8 @@ int main() {
   projection_mixed(true);
   failure_paths();
   ns_smoke();
+  pcg(PRECOND_MULTIGRID);
+  pcg(PRECOND_JACOBI);
   if (failures) {
     std::printf("FACADE FAILED (%d)\n", failures);
     return 1;
