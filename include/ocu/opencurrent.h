@@ -26,6 +26,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../ocu_b200.h"
@@ -57,6 +58,12 @@ enum PreconditionerType {
   PRECOND_NONE = OCU_PRECOND_NONE, PRECOND_JACOBI = OCU_PRECOND_JACOBI,
   PRECOND_MULTIGRID = OCU_PRECOND_MULTIGRID, PRECOND_BFBT = OCU_PRECOND_BFBT
 };
+enum GridStaggering {
+  GS_CENTER_POINT = OCU_GS_CENTER_POINT, GS_U_FACE = OCU_GS_U_FACE, GS_V_FACE = OCU_GS_V_FACE,
+  GS_W_FACE = OCU_GS_W_FACE, GS_CUSTOM = OCU_GS_CUSTOM
+};
+typedef int nc_type;
+enum { NC_INT = OCU_NC_INT, NC_FLOAT = OCU_NC_FLOAT, NC_DOUBLE = OCU_NC_DOUBLE };
 enum TimeStepType { TS_ERROR = OCU_TS_ERROR, TS_FORWARD_EULER = OCU_TS_FORWARD_EULER, TS_ADAMS_BASHFORD2 = OCU_TS_ADAMS_BASHFORD2 };
 
 enum DirectionType {
@@ -580,6 +587,103 @@ class Sol_PCGPressure3DDevice : public ErrorHandler {
 
 typedef Sol_PCGPressure3DDevice<float> Sol_PCGPressure3DDeviceF;
 typedef Sol_PCGPressure3DDevice<double> Sol_PCGPressure3DDeviceD;
+
+// NetCDFGrid3DWriter / NetCDFGrid3DReader (gridnetcdf.h:67-183): the reference's grid files in the
+// NetCDF classic format, without libnetcdf; the writer writes the file at close().
+namespace detail {
+template <typename T> struct nc_of;
+template <> struct nc_of<float> { static const int value = OCU_NC_FLOAT; };
+template <> struct nc_of<double> { static const int value = OCU_NC_DOUBLE; };
+template <> struct nc_of<int> { static const int value = OCU_NC_INT; };
+}  // namespace detail
+
+class NetCDFGrid3DWriter {
+  ocu_nc_writer *_w = nullptr;
+  std::vector<float> _times;
+ public:
+  ~NetCDFGrid3DWriter() { if (_w) close(); }
+  bool is_open() const { return _w != nullptr; }
+  bool open(const char *filename, int nx, int ny, int nz, float hx = 1.0f, float hy = 1.0f, float hz = 1.0f) {
+    return !_w && ocu_nc_writer_open(filename, nx, ny, nz, hx, hy, hz, &_w) == OCU_OK;
+  }
+  bool define_variable(const char *name, nc_type var_type, GridStaggering stag, float offsetx = 0.5f,
+                       float offsety = 0.5f, float offsetz = 0.5f) {
+    return ocu_nc_writer_define_variable(_w, name, var_type, stag, offsetx, offsety, offsetz) == OCU_OK;
+  }
+  bool add_time_level(float time, size_t &level) {
+    int l = 0;
+    if (ocu_nc_writer_add_time_level(_w, time, &l) != OCU_OK) return false;
+    _times.push_back(time);
+    level = (size_t)l;
+    return true;
+  }
+  int get_time_level(float time) const {
+    for (size_t i = 0; i < _times.size(); i++)
+      if (_times[i] == time) return (int)i;
+    return -1;
+  }
+  float get_time(int time_level) const { return _times[time_level]; }
+  template <typename T>
+  bool add_data(const char *name, const Grid3DHost<T> &grid, int time_level = 0) {
+    if (time_level == 0 && _times.empty()) _times.push_back(0.0f);
+    return ocu_nc_writer_add_data(_w, name, &grid.at(0, 0, 0), detail::nc_of<T>::value, grid.xstride(), grid.ystride(),
+                                  grid.nx(), grid.ny(), grid.nz(), time_level) == OCU_OK;
+  }
+  bool close() {
+    const bool ok = ocu_nc_writer_close(_w) == OCU_OK;
+    _w = nullptr;
+    _times.clear();
+    return ok;
+  }
+};
+
+class NetCDFGrid3DReader {
+  ocu_nc_reader *_r = nullptr;
+  int _nx = 0, _ny = 0, _nz = 0, _nt = 0;
+  float _hx = 0, _hy = 0, _hz = 0;
+  bool find(const char *name, int &t, int &x, int &y, int &z) const {
+    int n = 0;
+    ocu_nc_reader_num_variables(_r, &n);
+    char buf[1024];
+    for (int q = 0; q < n; q++)
+      if (ocu_nc_reader_variable(_r, q, buf, (int)sizeof(buf), &t, &x, &y, &z) == OCU_OK && std::strcmp(buf, name) == 0)
+        return true;
+    return false;
+  }
+ public:
+  ~NetCDFGrid3DReader() { close(); }
+  bool is_open() const { return _r != nullptr; }
+  bool open(const char *filename) {
+    if (_r || ocu_nc_reader_open(filename, &_r) != OCU_OK) return false;
+    return ocu_nc_reader_info(_r, &_nx, &_ny, &_nz, &_hx, &_hy, &_hz, &_nt) == OCU_OK;
+  }
+  int nx() const { return _nx; } int ny() const { return _ny; } int nz() const { return _nz; }
+  float hx() const { return _hx; } float hy() const { return _hy; } float hz() const { return _hz; }
+  int num_time_levels() const { return _nt; }
+  float get_time(int time_level) const { float t = 0; ocu_nc_reader_get_time(_r, time_level, &t); return t; }
+  std::vector<std::string> list_variables() const {
+    std::vector<std::string> out;
+    int n = 0;
+    ocu_nc_reader_num_variables(_r, &n);
+    char buf[1024];
+    for (int q = 0; q < n; q++)
+      if (ocu_nc_reader_variable(_r, q, buf, (int)sizeof(buf), nullptr, nullptr, nullptr, nullptr) == OCU_OK)
+        out.push_back(buf);
+    return out;
+  }
+  bool variable_type(const char *name, nc_type &type) const { int x, y, z; return find(name, type, x, y, z); }
+  bool variable_size(const char *name, int &nx, int &ny, int &nz) const { int t; return find(name, t, nx, ny, nz); }
+  template <typename T>
+  bool read_variable(const char *name, Grid3DHost<T> &grid, int time_level = 0) const {
+    return ocu_nc_reader_read(_r, name, &grid.at(0, 0, 0), detail::nc_of<T>::value, grid.xstride(), grid.ystride(),
+                              grid.nx(), grid.ny(), grid.nz(), time_level) == OCU_OK;
+  }
+  bool close() {
+    if (_r) ocu_nc_reader_close(_r);
+    _r = nullptr;
+    return true;
+  }
+};
 
 }  // namespace ocu
 

@@ -342,6 +342,43 @@ ocu_status ocu_pcg_pressure(ocu_pcg *s, ocu_grid **out);
 /* CG iterations of the last solve */
 ocu_status ocu_pcg_iterations(const ocu_pcg *s, int *out);
 
+/* ---- grid files (NetCDFGrid3DWriter / NetCDFGrid3DReader, gridnetcdf.h:67-183) -------------
+ * The reference's NetCDF grid files, written and read without libnetcdf in the NetCDF classic
+ * format (CDF-1, or CDF-2 when the data passes 2 GB): an unlimited "Time" dimension and float
+ * "Time" variable, global attributes nx, ny, nz, hx, hy, hz, one coordinate dimension + float
+ * variable per axis offset (XAxisCentered, XAxisUFace, XAxisOffset%.4f, ...), and each grid
+ * variable on (Time, X, Y, Z).  Data are host grids: the interior origin, the x and y strides
+ * in elements (z contiguous) and the interior extents, of the variable's type.  The writer keeps
+ * the data in memory and writes the file at close. */
+typedef struct ocu_nc_writer ocu_nc_writer;
+typedef struct ocu_nc_reader ocu_nc_reader;
+/* open (gridnetcdf.cpp: nc_create with NC_CLOBBER): creates / truncates the file now */
+ocu_status ocu_nc_writer_open(const char *path, int nx, int ny, int nz, float hx, float hy, float hz,
+                              ocu_nc_writer **out);
+/* define_variable(name, nc_type, staggering, offsets used for OCU_GS_CUSTOM) */
+ocu_status ocu_nc_writer_define_variable(ocu_nc_writer *w, const char *name, int nc_type, int staggering,
+                                         float offsetx, float offsety, float offsetz);
+ocu_status ocu_nc_writer_add_time_level(ocu_nc_writer *w, float time, int *level);
+/* add_data: level 0 of a file without time levels adds time 0 first, as the reference does */
+ocu_status ocu_nc_writer_add_data(ocu_nc_writer *w, const char *name, const void *origin, int nc_type,
+                                  long long xstride, long long ystride, int nx, int ny, int nz, int time_level);
+/* the same from a device grid (downloaded first) */
+ocu_status ocu_nc_writer_add_grid(ocu_nc_writer *w, const char *name, const ocu_grid *g, int time_level);
+/* writes the file and frees the writer */
+ocu_status ocu_nc_writer_close(ocu_nc_writer *w);
+ocu_status ocu_nc_reader_open(const char *path, ocu_nc_reader **out);
+void ocu_nc_reader_close(ocu_nc_reader *r);
+ocu_status ocu_nc_reader_info(const ocu_nc_reader *r, int *nx, int *ny, int *nz, float *hx, float *hy, float *hz,
+                              int *num_time_levels);
+ocu_status ocu_nc_reader_get_time(const ocu_nc_reader *r, int time_level, float *time);
+/* list_variables / variable_type / variable_size: the grid variables in file order */
+ocu_status ocu_nc_reader_num_variables(const ocu_nc_reader *r, int *n);
+ocu_status ocu_nc_reader_variable(const ocu_nc_reader *r, int index, char *name, int name_size, int *nc_type,
+                                  int *nx, int *ny, int *nz);
+/* read_variable into a host grid of the variable's type and extents */
+ocu_status ocu_nc_reader_read(const ocu_nc_reader *r, const char *name, void *origin, int nc_type, long long xstride,
+                              long long ystride, int nx, int ny, int nz, int time_level);
+
 /* ---- persistent refinement ensembles ----------------------------------------------------
  * No reference counterpart as a whole: many Sol_MultigridPressure3DBase::solve calls
  * (sol_mgpressure3d.cpp:332-370: sqrt(sum r^2 / N) of the residual against an absolute

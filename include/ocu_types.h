@@ -65,6 +65,18 @@ typedef enum ocu_precond {
   OCU_PRECOND_BFBT = 3
 } ocu_precond;
 
+/* Grid staggering of a NetCDF grid variable (ocustorage/gridnetcdf.h:32-38). */
+typedef enum ocu_grid_staggering {
+  OCU_GS_CENTER_POINT = 0,
+  OCU_GS_U_FACE = 1,
+  OCU_GS_V_FACE = 2,
+  OCU_GS_W_FACE = 3,
+  OCU_GS_CUSTOM = 4
+} ocu_grid_staggering;
+
+/* Value types of NetCDF variables (the netCDF library's nc_type codes). */
+typedef enum ocu_nc_type { OCU_NC_INT = 4, OCU_NC_FLOAT = 5, OCU_NC_DOUBLE = 6 } ocu_nc_type;
+
 /* Advection interpolants (ocuutil/interpolation.h:26-31). */
 typedef enum ocu_interpolation {
   OCU_IT_ERROR = 0,

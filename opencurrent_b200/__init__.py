@@ -9,6 +9,7 @@ Where the reference returns bool and fills a double& (solve), the Python method 
 (ok, residual).  Every compute call runs on the device; nothing falls back to the CPU.
 """
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -17,6 +18,7 @@ from ._capi import *  # noqa: F401,F403  (enums, structs)
 from ._capi import OcuError, check, load
 
 __all__ = [
+    "NetCDFGrid3DWriter", "NetCDFGrid3DReader",
     "Sol_PCGPressure3DDevice",
     "PersistentEnsemble",
     "BoundaryCondition", "BoundaryConditionSet", "Grid3DDevice", "Sol_MultigridPressure3DDevice",
@@ -560,6 +562,124 @@ class Sol_PCGPressure3DDevice:
             if self._h:
                 load().ocu_pcg_destroy(self._h)
                 self._h = None
+        except Exception:
+            pass
+
+
+_NC_NP = {NC_FLOAT: np.float32, NC_DOUBLE: np.float64, NC_INT: np.int32}
+
+
+class NetCDFGrid3DWriter:
+    """The reference's NetCDF grid files (ocustorage/gridnetcdf.h:67-123), written without
+    libnetcdf in the NetCDF classic format.  add_data takes a Grid3DDevice or an (nx, ny, nz)
+    numpy array of the variable's type; the file is written at close()."""
+
+    def __init__(self):
+        self._h = None
+
+    def open(self, filename, nx, ny, nz, hx=1.0, hy=1.0, hz=1.0):
+        h = C.c_void_p()
+        check(load().ocu_nc_writer_open(os.fsencode(filename), nx, ny, nz, hx, hy, hz, C.byref(h)))
+        self._h = h.value
+        return True
+
+    def is_open(self):
+        return self._h is not None
+
+    def define_variable(self, name, var_type, stag=GS_CENTER_POINT, offsetx=0.5, offsety=0.5, offsetz=0.5):
+        check(load().ocu_nc_writer_define_variable(self._h, name.encode(), var_type, stag, offsetx, offsety, offsetz))
+        return True
+
+    def add_time_level(self, time):
+        lvl = C.c_int()
+        check(load().ocu_nc_writer_add_time_level(self._h, time, C.byref(lvl)))
+        return lvl.value
+
+    def add_data(self, name, grid, time_level=0):
+        if isinstance(grid, Grid3DDevice):
+            check(load().ocu_nc_writer_add_grid(self._h, name.encode(), grid._h, time_level))
+            return True
+        a = np.ascontiguousarray(grid)
+        t = {np.dtype(np.float32): NC_FLOAT, np.dtype(np.float64): NC_DOUBLE, np.dtype(np.int32): NC_INT}[a.dtype]
+        nx, ny, nz = a.shape
+        check(load().ocu_nc_writer_add_data(self._h, name.encode(), a.ctypes.data_as(C.c_void_p), t, ny * nz, nz,
+                                            nx, ny, nz, time_level))
+        return True
+
+    def close(self):
+        h, self._h = self._h, None
+        check(load().ocu_nc_writer_close(h))
+        return True
+
+
+class NetCDFGrid3DReader:
+    """Reader of those files (ocustorage/gridnetcdf.h:126-183); read_variable returns an
+    (nx, ny, nz) numpy array of the variable's type."""
+
+    def __init__(self):
+        self._h = None
+
+    def open(self, filename):
+        h = C.c_void_p()
+        check(load().ocu_nc_reader_open(os.fsencode(filename), C.byref(h)))
+        self._h = h.value
+        nx, ny, nz, nt = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        hx, hy, hz = C.c_float(), C.c_float(), C.c_float()
+        check(load().ocu_nc_reader_info(self._h, C.byref(nx), C.byref(ny), C.byref(nz), C.byref(hx), C.byref(hy),
+                                        C.byref(hz), C.byref(nt)))
+        self.nx, self.ny, self.nz = nx.value, ny.value, nz.value
+        self.hx, self.hy, self.hz = hx.value, hy.value, hz.value
+        self._nt = nt.value
+        return True
+
+    def is_open(self):
+        return self._h is not None
+
+    def num_time_levels(self):
+        return self._nt
+
+    def get_time(self, time_level):
+        t = C.c_float()
+        check(load().ocu_nc_reader_get_time(self._h, time_level, C.byref(t)))
+        return t.value
+
+    def _vars(self):
+        n = C.c_int()
+        check(load().ocu_nc_reader_num_variables(self._h, C.byref(n)))
+        out = {}
+        for q in range(n.value):
+            buf = C.create_string_buffer(1024)
+            t, x, y, z = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+            check(load().ocu_nc_reader_variable(self._h, q, buf, 1024, C.byref(t), C.byref(x), C.byref(y),
+                                                C.byref(z)))
+            out[buf.value.decode()] = (t.value, (x.value, y.value, z.value))
+        return out
+
+    def list_variables(self):
+        return list(self._vars())
+
+    def variable_type(self, name):
+        return self._vars()[name][0]
+
+    def variable_size(self, name):
+        return self._vars()[name][1]
+
+    def read_variable(self, name, time_level=0):
+        t, (nx, ny, nz) = self._vars()[name]
+        a = np.empty((nx, ny, nz), _NC_NP[t])
+        check(load().ocu_nc_reader_read(self._h, name.encode(), a.ctypes.data_as(C.c_void_p), t, ny * nz, nz, nx, ny,
+                                        nz, time_level))
+        return a
+
+    def close(self):
+        if self._h:
+            load().ocu_nc_reader_close(self._h)
+            self._h = None
+        return True
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass
 

@@ -27,6 +27,8 @@ REDUCE_MAXABS, REDUCE_MAX, REDUCE_MIN, REDUCE_SUM, REDUCE_SQRSUM, REDUCE_CHECKNA
 BC_LEVEL1, BC_LEVEL1_NOCORNERS = 0, 1
 MG_F32, MG_F64, MG_MIXED_IR, MG_MIXED_WARMSTART = 0, 1, 2, 3
 PRECOND_NONE, PRECOND_JACOBI, PRECOND_MULTIGRID, PRECOND_BFBT = 0, 1, 2, 3
+GS_CENTER_POINT, GS_U_FACE, GS_V_FACE, GS_W_FACE, GS_CUSTOM = 0, 1, 2, 3, 4
+NC_INT, NC_FLOAT, NC_DOUBLE = 4, 5, 6
 
 OK, ERR_INVALID_VALUE, ERR_LAYOUT, ERR_CUDA, ERR_NOT_CONVERGED = 0, 1, 2, 3, 4
 ERR_NOT_INITIALIZED, ERR_ALLOC, ERR_UNSUPPORTED, ERR_TIMEOUT = 5, 6, 7, 8
@@ -158,6 +160,22 @@ SIGNATURES = {
     "ocu_ens_class_info": (I, [P, I, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(EnsTuning)]),
     "ocu_ens_set_tuning": (I, [P, I, C.POINTER(EnsTuning)]),
     "ocu_ens_autotune": (I, [P, C.POINTER(D), I]),
+    "ocu_nc_writer_open": (I, [C.c_char_p, I, I, I, C.c_float, C.c_float, C.c_float, PP]),
+    "ocu_nc_writer_define_variable": (I, [P, C.c_char_p, I, I, C.c_float, C.c_float, C.c_float]),
+    "ocu_nc_writer_add_time_level": (I, [P, C.c_float, C.POINTER(C.c_int)]),
+    "ocu_nc_writer_add_data": (I, [P, C.c_char_p, P, I, C.c_longlong, C.c_longlong, I, I, I, I]),
+    "ocu_nc_writer_add_grid": (I, [P, C.c_char_p, P, I]),
+    "ocu_nc_writer_close": (I, [P]),
+    "ocu_nc_reader_open": (I, [C.c_char_p, PP]),
+    "ocu_nc_reader_close": (None, [P]),
+    "ocu_nc_reader_info": (I, [P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                               C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                               C.POINTER(C.c_int)]),
+    "ocu_nc_reader_get_time": (I, [P, I, C.POINTER(C.c_float)]),
+    "ocu_nc_reader_num_variables": (I, [P, C.POINTER(C.c_int)]),
+    "ocu_nc_reader_variable": (I, [P, I, C.c_char_p, I, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "ocu_nc_reader_read": (I, [P, C.c_char_p, P, I, C.c_longlong, C.c_longlong, I, I, I, I]),
     "ocu_pcg_params_default": (None, [C.POINTER(PCGParams)]),
     "ocu_pcg_create": (I, [I, C.POINTER(PCGParams), PP]),
     "ocu_pcg_destroy": (None, [P]),

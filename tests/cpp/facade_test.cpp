@@ -282,6 +282,45 @@ static void pcg(PreconditionerType pc) {
   CHECK(!solver.solve(r2, 1e-14, 2));
 }
 
+// NetCDFGrid3DWriter / Reader: a cell-centred and a u-face grid over two time levels, read back
+static void netcdf_round_trip() {
+  const char *path = "facade_test_grids.nc";
+  Grid3DHostF t;
+  Grid3DHostD u;
+  REQUIRE(t.init(5, 4, 3, 1, 1, 1));
+  REQUIRE(u.init(6, 4, 3, 1, 1, 1));
+  for (int i = 0; i < 6; i++)
+    for (int j = 0; j < 4; j++)
+      for (int k = 0; k < 3; k++) {
+        if (i < 5) t.at(i, j, k) = (float)(i * 100 + j * 10 + k);
+        u.at(i, j, k) = 0.5 * i - 0.25 * j + 0.125 * k;
+      }
+  NetCDFGrid3DWriter w;
+  REQUIRE(w.open(path, 5, 4, 3, 0.2f, 0.25f, 1.0f / 3));
+  CHECK(w.define_variable("temp", NC_FLOAT, GS_CENTER_POINT));
+  CHECK(w.define_variable("u", NC_DOUBLE, GS_U_FACE));
+  CHECK(w.add_data("temp", t, 0));
+  size_t level = 0;
+  CHECK(w.add_time_level(0.5f, level) && level == 1);
+  CHECK(w.add_data("u", u, 1));
+  CHECK(w.close());
+  NetCDFGrid3DReader r;
+  REQUIRE(r.open(path));
+  CHECK(r.nx() == 5 && r.ny() == 4 && r.nz() == 3 && r.num_time_levels() == 2 && r.get_time(1) == 0.5f);
+  CHECK(r.list_variables().size() == 2);
+  int nx = 0, ny = 0, nz = 0;
+  CHECK(r.variable_size("u", nx, ny, nz) && nx == 6);
+  Grid3DHostF t2;
+  Grid3DHostD u2;
+  REQUIRE(t2.init(5, 4, 3, 1, 1, 1));
+  REQUIRE(u2.init(6, 4, 3, 1, 1, 1));
+  CHECK(r.read_variable("temp", t2, 0));
+  CHECK(r.read_variable("u", u2, 1));
+  CHECK(t2.at(4, 3, 2) == 432.0f && u2.at(5, 0, 1) == 2.625);
+  r.close();
+  std::remove(path);
+}
+
 int main() {
   all_dirichlet(0.0);
   all_dirichlet(0.5);
@@ -293,6 +332,7 @@ int main() {
   ns_smoke();
   pcg(PRECOND_MULTIGRID);
   pcg(PRECOND_JACOBI);
+  netcdf_round_trip();
   if (failures) {
     std::printf("FACADE FAILED (%d)\n", failures);
     return 1;
