@@ -282,12 +282,31 @@ ocu_status NSSolver::step_t(double dtv) {
   num_steps++;
   OCU_TRY(launch_advect_self<T>(origin<T>(u), origin<T>(v), origin<T>(w), origin<T>(du), origin<T>(dv), origin<T>(dw),
                                 Lu, nx, ny, nz, prm.hx, prm.hy, prm.hz, prm.advection_scheme, stream));
+  // viscosity, then buoyancy on the vertical component; in FP32 the vertical component's two
+  // passes are one kernel (same arithmetic, in the same order)
+  bool buoyancy_done = false;
   if (T_nu > 0) {
-    OCU_TRY(launch_laplacian<T>(origin<T>(u), origin<T>(du), Lu, nx + 1, ny, nz, prm.hx, prm.hy, prm.hz, (T)T_nu, stream));
-    OCU_TRY(launch_laplacian<T>(origin<T>(v), origin<T>(dv), Lu, nx, ny + 1, nz, prm.hx, prm.hy, prm.hz, (T)T_nu, stream));
-    OCU_TRY(launch_laplacian<T>(origin<T>(w), origin<T>(dw), Lu, nx, ny, nz + 1, prm.hx, prm.hy, prm.hz, (T)T_nu, stream));
+    ocu_grid *st3[3] = {u, v, w}, *ds3[3] = {du, dv, dw};
+    for (int c = 0; c < 3; c++) {
+      const int ex = nx + (c == 0), ey = ny + (c == 1), ez = nz + (c == 2);
+      if constexpr (sizeof(T) == 4) {
+        if (ds3[c] == vert) {
+          const ocu_status fs = launch_laplacian_thermal(origin<float>(st3[c]), origin<float>(ds3[c]), Lu, ex, ey, ez,
+                                                         prm.hx, prm.hy, prm.hz, (float)T_nu, origin<float>(t),
+                                                         (float)coef, nbr, nx, ny, nz, stream);
+          if (fs == OCU_OK) {
+            buoyancy_done = true;
+            continue;
+          }
+          if (fs != OCU_ERR_UNSUPPORTED) return fs;
+        }
+      }
+      OCU_TRY(launch_laplacian<T>(origin<T>(st3[c]), origin<T>(ds3[c]), Lu, ex, ey, ez, prm.hx, prm.hy, prm.hz,
+                                  (T)T_nu, stream));
+    }
   }
-  OCU_TRY(launch_thermal_force<T>(origin<T>(vert), coef, origin<T>(t), t->L, nbr, nx, ny, nz, stream));
+  if (!buoyancy_done)
+    OCU_TRY(launch_thermal_force<T>(origin<T>(vert), coef, origin<T>(t), t->L, nbr, nx, ny, nz, stream));
   OCU_TRY(launch_advect_passive<T>(origin<T>(u), origin<T>(v), origin<T>(w), origin<T>(t), origin<T>(dt), t->L, nx, ny,
                                    nz, prm.hx, prm.hy, prm.hz, prm.advection_scheme, stream));
   if (T_kappa > 0)
@@ -301,6 +320,16 @@ ocu_status NSSolver::step_t(double dtv) {
   }
   OCU_TRY(launch_bc_nocorners_dev<T>(origin<T>(t), t->L, prm.temp_bc, prm.hx, prm.hy, prm.hz, stream));
   ocu_grid *st[3] = {u, v, w}, *ds[3] = {du, dv, dw}, *ls[3] = {ldu, ldv, ldw};
+  // u, v, w updated in one pass when they take the interior 16-byte form
+  {
+    T *x3[3] = {(T *)u->buf, (T *)v->buf, (T *)w->buf};
+    const T *d3[3] = {(const T *)du->buf, (const T *)dv->buf, (const T *)dw->buf};
+    const T *l3[3] = {(const T *)ldu->buf, (const T *)ldv->buf, (const T *)ldw->buf};
+    const ocu_status us = ab2 ? launch_update3<T>(x3, d3, l3, Lu, (T)(dtv - ab), ab, stream)
+                              : launch_update3<T>(x3, d3, nullptr, Lu, (T)dtv, (T)0, stream);
+    if (us == OCU_OK) goto updated;
+    if (us != OCU_ERR_UNSUPPORTED) return us;
+  }
   for (int c = 0; c < 3; c++) {
     T *x = (T *)st[c]->buf;
     if (ab2) {
@@ -310,6 +339,7 @@ ocu_status NSSolver::step_t(double dtv) {
       OCU_TRY(launch_lincomb2<T>(x, st[c]->L, (T)1.0, x, (T)dtv, (const T *)ds[c]->buf, stream));
     }
   }
+updated:
   if (prm.time_step == OCU_TS_ADAMS_BASHFORD2) {
     // this step's derivatives become the previous ones by exchanging the buffers, where the
     // reference copies them (eqn_incompressns3d.cu:390-396).  The derivative kernels overwrite

@@ -214,9 +214,20 @@ constexpr int kCellsIPassive = 1;
 // nr (0..3): cells past the last group of a row (rows of nz = 4 nz4 + nr cells); the blocks
 // holding the rows' last groups compute them afterwards, one cell per thread, with the scalar
 // expression (handled by the last lane of each row they measured slower: its warp waited).
+// TH: the buoyancy term of the same component added after the diffusion term, in the order of
+// the reference's two kernels (d + c lap, then + 0.5 ct (T + T_nbr)), on the cells i < tnx,
+// j < tny, k < tnz (the temperature's extent; the velocity component has one face layer more).
+struct ThermalArgs {
+  const float *temp;
+  float ct;
+  long long nbr;
+  int tnx, tny, tnz;
+};
+
+template <bool TH>
 __global__ void __launch_bounds__(256) k_laplacian_v4(const float *__restrict__ phi, float *__restrict__ dphidt,
                                                       float ihx2, float ihy2, float ihz2, float c, long long xs,
-                                                      long long ys, int nx, int ny, int nz4, int nr) {
+                                                      long long ys, int nx, int ny, int nz4, int nr, ThermalArgs th) {
   if (nr > 0 && blockIdx.x == gridDim.x - 1) {
     const int nt = blockDim.x * blockDim.y, cnt = nr * blockDim.y * kCellsIV;
     for (int t = threadIdx.y * blockDim.x + threadIdx.x; t < cnt; t += nt) {
@@ -227,11 +238,17 @@ __global__ void __launch_bounds__(256) k_laplacian_v4(const float *__restrict__ 
       const float p = phi[q];
       const float lap = ihz2 * (phi[q + 1] + phi[q - 1] - 2.f * p) + ihy2 * (phi[q + ys] + phi[q - ys] - 2.f * p) +
                         ihx2 * (phi[q + xs] + phi[q - xs] - 2.f * p);
-      dphidt[q] = dphidt[q] + c * lap;
+      float o = dphidt[q] + c * lap;
+      if (TH && ir < th.tnx && jr < th.tny && 4 * nz4 + e < th.tnz)
+        o += 0.5f * th.ct * (th.temp[q] + th.temp[q - th.nbr]);
+      dphidt[q] = o;
     }
   }
   V4_BEGIN
   const Row4 P = row4(phi, id, ok, first, last);
+  // the temperature group (its k - 1 neighbour from the lanes when the vertical is z)
+  Row4 TT;
+  if (TH) TT = row4(th.temp, id, ok && i < th.tnx && j < th.tny, first, last);
   if (!ok) continue;
   const float4 D = ld4g(dphidt + id), YP = ld4g(phi + id + ys), YM = ld4g(phi + id - ys);
   const float4 XP = ld4g(phi + id + xs), XM = ld4g(phi + id - xs);
@@ -245,6 +262,19 @@ __global__ void __launch_bounds__(256) k_laplacian_v4(const float *__restrict__ 
     const float lap = ihz2 * (P.v[e + 2] + P.v[e] - 2.f * p) + ihy2 * (yp[e] + ym[e] - 2.f * p) +
                       ihx2 * (xp[e] + xm[e] - 2.f * p);
     o[e] = d[e] + c * lap;
+  }
+  if (TH && i < th.tnx && j < th.tny) {
+    float t1[4];
+    if (th.nbr == 1) {
+#pragma unroll
+      for (int e = 0; e < 4; e++) t1[e] = TT.v[e];
+    } else {  // a multiple of 4: a whole group
+      const float4 T1 = ld4g(th.temp + id - th.nbr);
+      t1[0] = T1.x; t1[1] = T1.y; t1[2] = T1.z; t1[3] = T1.w;
+    }
+#pragma unroll
+    for (int e = 0; e < 4; e++)
+      if (4 * k4 + e < th.tnz) o[e] += 0.5f * th.ct * (TT.v[e + 1] + t1[e]);
   }
   st4g(dphidt + id, o[0], o[1], o[2], o[3]);
   V4_END
@@ -495,8 +525,8 @@ ocu_status launch_laplacian(const T *phi, T *dphidt, const ocu_layout &L, int nx
     if (nz4 > 0 && v4_ok(4 * nz4, L, {phi, dphidt})) {
       const T ihx2 = (T)(1 / (hx * hx)), ihy2 = (T)(1 / (hy * hy)), ihz2 = (T)(1 / (hz * hz));
       shape_v4(nx, ny, 4 * nz4, &g, &b);
-      k_laplacian_v4<<<g, b, 0, s>>>(phi, dphidt, ihx2, ihy2, ihz2, coefficient, L.xstride, L.ystride, nx, ny, nz4,
-                                     nr);
+      k_laplacian_v4<false><<<g, b, 0, s>>>(phi, dphidt, ihx2, ihy2, ihz2, coefficient, L.xstride, L.ystride, nx, ny,
+                                            nz4, nr, ThermalArgs{});
       return check_launch("k_laplacian_v4");
     }
   }
@@ -504,6 +534,23 @@ ocu_status launch_laplacian(const T *phi, T *dphidt, const ocu_layout &L, int nx
   k_laplacian<T><<<g, b, 0, s>>>(phi, dphidt, (T)(1 / (hx * hx)), (T)(1 / (hy * hy)), (T)(1 / (hz * hz)),
                                  coefficient, L.xstride, L.ystride, nx, ny, nz);
   return check_launch("k_laplacian");
+}
+
+// The diffusion of the vertical velocity component and its buoyancy in one pass (FP32 group
+// form only); OCU_ERR_UNSUPPORTED when it does not apply, and the caller launches the two.
+ocu_status launch_laplacian_thermal(const float *phi, float *dphidt, const ocu_layout &L, int nx, int ny, int nz,
+                                    double hx, double hy, double hz, float coefficient, const float *temp, float ct,
+                                    long long nbr, int tnx, int tny, int tnz, cudaStream_t s) {
+  const int nz4 = nz / 4, nr = nz - 4 * nz4;
+  // the temperature is read at the velocity's index (one layout), and its vertical neighbour one
+  // cell down (from the lanes) or a whole group away
+  if (nz4 == 0 || (nbr != 1 && nbr % 4 != 0) || !v4_ok(4 * nz4, L, {phi, dphidt, temp})) return OCU_ERR_UNSUPPORTED;
+  dim3 g, b;
+  shape_v4(nx, ny, 4 * nz4, &g, &b);
+  k_laplacian_v4<true><<<g, b, 0, s>>>(phi, dphidt, (float)(1 / (hx * hx)), (float)(1 / (hy * hy)),
+                                       (float)(1 / (hz * hz)), coefficient, L.xstride, L.ystride, nx, ny, nz4, nr,
+                                       ThermalArgs{temp, ct, nbr, tnx, tny, tnz});
+  return check_launch("k_laplacian_v4");
 }
 
 template <typename T>

@@ -340,6 +340,56 @@ __global__ void k_lincomb2_3dv(T *res, T a1, const T *g1, T a2, const T *g2, lon
   }
 }
 
+// The velocity update of a time step over u, v and w (one layout) in one pass: x = x * 1 + d * a2,
+// then, with Adams-Bashforth history, x = x * 1 + l * a3 -- the reference's one or two
+// linear_combination calls per component, each rounded as there (grid3ddev.cu:283-349).
+template <typename T>
+struct UpdateSet {
+  T *x[3];
+  const T *d[3], *l[3];
+};
+
+template <typename T, bool AB2>
+__global__ void k_update3_3dv(const __grid_constant__ UpdateSet<T> S, T a2, T a3, long long xs, long long ys, int ny,
+                              int nz, int cpr, long long nchunks) {
+  pdl_entry();
+  constexpr int V = 16 / (int)sizeof(T);
+  using Vec = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < 3 * nchunks;
+       c += (long long)gridDim.x * blockDim.x) {
+    const int f = (int)(c / nchunks);
+    const long long cc = c - f * nchunks;
+    T *x = f == 0 ? S.x[0] : (f == 1 ? S.x[1] : S.x[2]);
+    const T *d = f == 0 ? S.d[0] : (f == 1 ? S.d[1] : S.d[2]);
+    const T *l = f == 0 ? S.l[0] : (f == 1 ? S.l[1] : S.l[2]);
+    const long long row = cc / cpr;
+    const int k0 = (int)(cc - row * cpr) * V;
+    const int i = (int)(row / ny), j = (int)(row - (long long)i * ny);
+    const long long id = (long long)i * xs + (long long)j * ys + k0;
+    if (k0 + V <= nz) {
+      Vec xv = *reinterpret_cast<const Vec *>(x + id);
+      const Vec dv = *reinterpret_cast<const Vec *>(d + id);
+      T *xe = reinterpret_cast<T *>(&xv);
+      const T *de = reinterpret_cast<const T *>(&dv);
+#pragma unroll
+      for (int e = 0; e < V; e++) xe[e] = xe[e] * (T)1 + de[e] * a2;
+      if (AB2) {
+        const Vec lv = *reinterpret_cast<const Vec *>(l + id);
+        const T *le = reinterpret_cast<const T *>(&lv);
+#pragma unroll
+        for (int e = 0; e < V; e++) xe[e] = xe[e] * (T)1 + le[e] * a3;
+      }
+      *reinterpret_cast<Vec *>(x + id) = xv;
+    } else {
+      for (int e = 0; k0 + e < nz; e++) {
+        T v = x[id + e] * (T)1 + d[id + e] * a2;
+        if (AB2) v = v * (T)1 + l[id + e] * a3;
+        x[id + e] = v;
+      }
+    }
+  }
+}
+
 static unsigned grid_for(long long n, int threads) {
   long long b = (n + threads - 1) / threads;
   if (b > 148LL * 32) b = 148LL * 32;
@@ -363,6 +413,36 @@ template <typename T>
 ocu_status launch_lincomb1(T *res, T a1, const T *g1, long long n, cudaStream_t s) {
   launch_pdl(k_lincomb1<T>, grid_for(n, 256), 256, 0, s, res, a1, g1, n);
   return check_launch("k_lincomb1");
+}
+
+// OCU_ERR_UNSUPPORTED when the interior-only 16-byte form would not be the one the separate
+// linear combinations take (the caller then launches those).
+template <typename T>
+ocu_status launch_update3(T *const *x, const T *const *d, const T *const *l, const ocu_layout &L, T a2, T a3,
+                          cudaStream_t s) {
+  const long long waste = L.allocated - (long long)L.nx * L.ny * L.nz;
+  const auto a16 = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+  bool ok = (double)waste > 0.03 * (double)L.allocated && (L.ystride * sizeof(T)) % 16 == 0 &&
+            (L.xstride * sizeof(T)) % 16 == 0 && L.nx > 0 && L.ny > 0 && L.nz > 0;
+  for (int f = 0; f < 3 && ok; f++)
+    ok = a16(x[f] + L.shift) && a16(d[f] + L.shift) && (!l || a16(l[f] + L.shift));
+  if (!ok) return OCU_ERR_UNSUPPORTED;
+  constexpr int V = 16 / (int)sizeof(T);
+  const int cpr = (L.nz + V - 1) / V;
+  const long long nchunks = (long long)L.nx * L.ny * cpr;
+  UpdateSet<T> S;
+  for (int f = 0; f < 3; f++) {
+    S.x[f] = x[f] + L.shift;
+    S.d[f] = d[f] + L.shift;
+    S.l[f] = l ? l[f] + L.shift : nullptr;
+  }
+  if (l)
+    launch_pdl(k_update3_3dv<T, true>, grid_for(3 * nchunks, 256), 256, 0, s, S, a2, a3, (long long)L.xstride,
+               (long long)L.ystride, L.ny, L.nz, cpr, nchunks);
+  else
+    launch_pdl(k_update3_3dv<T, false>, grid_for(3 * nchunks, 256), 256, 0, s, S, a2, a3, (long long)L.xstride,
+               (long long)L.ystride, L.ny, L.nz, cpr, nchunks);
+  return check_launch("k_update3_3dv");
 }
 
 // The reference switches to the interior-only kernel when more than 3% of the buffer is
@@ -795,6 +875,8 @@ ocu_status launch_dot(const T *a, const T *b, const ocu_layout &L, void *d_scrat
   template ocu_status launch_lincomb1<T>(T *, T, const T *, long long, cudaStream_t);                          \
   template ocu_status launch_lincomb2<T>(T *, const ocu_layout &, T, const T *, T, const T *, cudaStream_t);   \
   template ocu_status launch_reduce<T>(const T *, const ocu_layout &, int, void *, double *, cudaStream_t);    \
+  template ocu_status launch_update3<T>(T *const *, const T *const *, const T *const *, const ocu_layout &, T, T, \
+                                        cudaStream_t);                                                        \
   template ocu_status launch_dot<T>(const T *, const T *, const ocu_layout &, void *, double *, cudaStream_t);  \
   template ocu_status launch_minmax<T>(const T *const *, const ocu_layout *const *, int, int, void *, double *,  \
                                        cudaStream_t);

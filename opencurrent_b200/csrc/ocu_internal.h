@@ -187,6 +187,14 @@ ocu_status launch_gradient(T *u, T *v, T *w, const T *phi, const ocu_layout &L, 
 // u, v, w (float) -= c grad(phi) with phi in double
 ocu_status launch_gradient_p64(float *u, float *v, float *w, const double *phi, const ocu_layout &L, int nx, int ny,
                               int nz, double hx, double hy, double hz, double coefficient, cudaStream_t s);
+// u, v, w (one layout) += a2 d [then += a3 l]: one launch, or OCU_ERR_UNSUPPORTED
+template <typename T>
+ocu_status launch_update3(T *const *x, const T *const *d, const T *const *l, const ocu_layout &L, T a2, T a3,
+                          cudaStream_t s);
+// diffusion + buoyancy of the vertical velocity in one pass (FP32), or OCU_ERR_UNSUPPORTED
+ocu_status launch_laplacian_thermal(const float *phi, float *dphidt, const ocu_layout &L, int nx, int ny, int nz,
+                                    double hx, double hy, double hz, float coefficient, const float *temp, float ct,
+                                    long long nbr, int tnx, int tny, int tnz, cudaStream_t s);
 template <typename T>
 ocu_status launch_laplacian(const T *phi, T *dphidt, const ocu_layout &L, int nx, int ny,
                             int nz, double hx, double hy, double hz, T coefficient,
