@@ -376,8 +376,11 @@ __global__ void __launch_bounds__(256) k_advect_passive_v4(const float *__restri
 // Self-advection on groups of four cells along k: the 17 rows it reads (u, v, w at the cell and
 // its face neighbours) as 16-byte loads, the k-shifted values from the adjacent lanes; each
 // component's expression is the scalar kernel's, in its order.
+#ifndef OCU_ADVECT_SELF_MINB
+#define OCU_ADVECT_SELF_MINB 2
+#endif
 template <int IT>
-__global__ void __launch_bounds__(256, 2) k_advect_self_v4(const float *__restrict__ u, const float *__restrict__ v,
+__global__ void __launch_bounds__(256, OCU_ADVECT_SELF_MINB) k_advect_self_v4(const float *__restrict__ u, const float *__restrict__ v,
                                                            const float *__restrict__ w, float *__restrict__ dudt,
                                                            float *__restrict__ dvdt, float *__restrict__ dwdt, float ihx,
                                                            float ihy, float ihz, long long xs, long long ys, int nx,
