@@ -231,7 +231,8 @@ ocu_status ChequerMG::relax(int l, int iterations, bool reverse, cudaStream_t s)
 ocu_status ChequerMG::sweep_level(int l, int color, cudaStream_t s) {
   const ChqLevel &L = lv[l];
   const long long threads = (long long)L.nx * L.ny * (L.rz / 4);
-  launch_pdl(k_chq_relax, dim3((unsigned)((threads + 255) / 256)), dim3(256), 0, s, make_g(L),
+  launch_pdl(k_chq_relax, dim3((unsigned)((threads + CHQ_RELAX_THREADS - 1) / CHQ_RELAX_THREADS)),
+             dim3(CHQ_RELAX_THREADS), 0, s, make_g(L),
              make_k(L.h, fx, fy, fz, omega), make_bc(bc, fx, fy, fz), color & 1);
   return check_launch("k_chq_relax");
 }

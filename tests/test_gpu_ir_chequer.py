@@ -112,3 +112,36 @@ def test_ir_odd_periodic_hierarchy_uses_exact_inner():
     print(f"IRCHQ odd-periodic fallback rel_res={res / rms:.3e} err_vs_fp64_oracle={e:.3e}")
     assert ok and res <= 1e-10 * rms
     assert e <= 1e-7
+
+
+def test_split_level_operations_run_on_every_level():
+    """The split hierarchy's level operations of the C ABI (core 2: a colour sweep, red-black
+    iterations, residual + restriction into the next level, prolongation from it) launch on
+    every level, and levels out of range or norms requested from the split hierarchy are refused."""
+    shape, h, bcname = CASES[1]
+    L, rhs, rms = problem(shape, 13)
+    g = dev_grid(rhs, F64, L)
+    dm = ocu.Sol_MultigridPressureMixed3DDeviceD("ir")
+    dm.bc = to_ocu_bc(bc_from(SCALAR_BCS[bcname]))
+    dm.initialize_storage(*shape, *h, g)
+    levels = dm.stats.num_levels
+    assert levels >= 3
+    for lv in range(levels):
+        dm.relax_sweep(lv, 0, core=2)
+        dm.relax_sweep(lv, 1, core=2)
+        dm.relax(lv, 2, order=1, core=2)
+        if lv + 1 < levels:
+            dm.restrict_residuals(lv, lv + 1, core=2)
+            dm.prolong(lv + 1, lv, core=2)
+    dm.synchronize()
+    with pytest.raises(ocu.OcuError):
+        dm.relax_sweep(levels, 0, core=2)
+    with pytest.raises(ocu.OcuError):
+        dm.restrict_residuals(0, 2, core=2)
+    with pytest.raises(ocu.OcuError):
+        dm.restrict_residuals(0, 1, norms=True, core=2)
+    with pytest.raises(ocu.OcuError):
+        dm.prolong(levels, levels - 1, core=2)
+    # the solve afterwards is unaffected by the level operations (they work on its scratch levels)
+    ok, res = dm.solve(1e-10 * rms, 20)
+    assert ok and res <= 1e-10 * rms
