@@ -232,6 +232,45 @@ ocu_status ocu_mg_prolong(ocu_mg *mg, int core, int coarse, int fine);
 /* Wait for all work the solver enqueued. */
 ocu_status ocu_mg_synchronize(ocu_mg *mg);
 
+/* ---- multi-image multigrid (Sol_MultigridPressure3DDeviceCo<T>) ---------------------------
+ * sol_mgpressure3d.h:184-242, sol_mgpressure3dco.cu:39-529.  The domain is split along x into
+ * `num_images` slabs of nx_local x ny x nz, one per image; an image lives on a device (several
+ * images may share one).  The reference runs one host thread per image with host-staged
+ * barrier exchanges (coarray.h:50-113); here one host thread drives every image in lockstep:
+ * each image has its own stream, the one-plane x halo is copied device to device into the
+ * receiving image's ghost plane (peer access over NVLink across devices) after every ghost
+ * refresh, ordered by events, so no kernel waits on another.  Levels whose global cell count
+ * is at most the cutoff (grid_size_for_cutoff, 64^3 by default) are gathered onto image 0 and
+ * scattered back before the prolongation, as in the reference.  Norms are each image's
+ * reduction folded in image order on the host.  The handle is an ocu_mg of kind OCU_MG_F32 or
+ * OCU_MG_F64: ocu_mg_solve / run_vcycles / run_fmg / set_params / get_stats / set_stream (image
+ * 0's stream, on devices[0]) / synchronize / destroy apply, and core 0 of the level operations
+ * acts on all images. */
+typedef struct ocu_mgco_plan {
+  int num_levels;     /* levels of the global hierarchy */
+  int cutoff_level;   /* first level held whole by image 0 (num_levels: none) */
+  int neg_image;      /* image across the x- face, -1 at the domain's face */
+  int pos_image;      /* image across the x+ face, -1 at the domain's face */
+  ocu_bc_set local_bc;  /* this image's faces at level 0: BC_NONE where a neighbour's plane lands */
+} ocu_mgco_plan;
+/* Host-only: the decomposition of one image (sol_mgpressure3dco.cu:242-300, 420-435). */
+ocu_status ocu_mgco_plan_compute(int nx_local, int ny, int nz, int num_images, int image,
+                                 long long cutoff_cells, const ocu_bc_set *bc, ocu_mgco_plan *out);
+/* kind: OCU_MG_F32 or OCU_MG_F64.  devices: num_images device ordinals (NULL: all 0). */
+ocu_status ocu_mgco_create(ocu_mg_kind kind, const ocu_mg_params *params, int num_images,
+                           const int *devices, ocu_mg **out);
+/* grid_size_for_cutoff (sol_mgpressure3dco.cu:223); before initialize_storage. */
+ocu_status ocu_mgco_set_cutoff_cells(ocu_mg *mg, long long cells);
+/* initialize_storage (sol_mgpressure3dco.cu:240-520): rhs[i] is image i's slab (borrowed),
+ * all with the same layout, ghost >= 1.  The global grid is (nx_local * num_images) x ny x nz;
+ * every level above the cutoff must split evenly across the images. */
+ocu_status ocu_mgco_initialize_storage(ocu_mg *mg, int nx_local, int ny, int nz, double hx,
+                                       double hy, double hz, ocu_grid *const *rhs);
+/* co_pressure() of an image (its slab of u at level 0); owned by the solver. */
+ocu_grid *ocu_mgco_pressure(ocu_mg *mg, int image);
+int ocu_mgco_num_images(const ocu_mg *mg);
+int ocu_mgco_cutoff_level(const ocu_mg *mg);
+
 /* ---- differentiable advection + projection (periodic MAC grid) ----------------------------
  * No single counterpart in the reference: the transposes of Sol_SelfAdvection3DDevice /
  * Sol_PassiveAdvection3DDevice (sol_selfadvection3ddev.cu:135-337,

@@ -23,6 +23,7 @@ __all__ = [
     "PersistentEnsemble",
     "BoundaryCondition", "BoundaryConditionSet", "Grid3DDevice", "Sol_MultigridPressure3DDevice",
     "Sol_MultigridPressure3DDeviceF", "Sol_MultigridPressure3DDeviceD",
+    "Sol_MultigridPressure3DDeviceCo", "mgco_plan",
     "Sol_MultigridPressureMixed3DDeviceD", "Sol_ProjectDivergence3DDevice",
     "Sol_SelfAdvection3DDevice", "Sol_PassiveAdvection3DDevice", "Sol_LaplacianCentered3DDevice",
     "Eqn_IncompressibleNS3DParams", "Eqn_IncompressibleNS3D", "layout", "OcuError",
@@ -330,6 +331,63 @@ def Sol_MultigridPressure3DDeviceF():
 
 def Sol_MultigridPressure3DDeviceD():
     return Sol_MultigridPressure3DDevice(F64)
+
+
+class Sol_MultigridPressure3DDeviceCo(_MGBase):
+    """Sol_MultigridPressure3DDeviceCo<T> (sol_mgpressure3d.h:184-242, sol_mgpressure3dco.cu).
+
+    The domain is split along x into `num_images` slabs, image i on device devices[i] (several
+    images may share a device).  initialize_storage takes the slab size and one rhs grid per
+    image; co_pressure(i) is image i's slab of the pressure.  One host thread drives every image:
+    the x halo planes are copied device to device after each ghost refresh, and the levels of at
+    most grid_size_for_cutoff cells are held whole by image 0.  solve / run_vcycles / run_fmg and
+    the parameters are those of Sol_MultigridPressure3DDevice.
+    """
+
+    def __init__(self, dtype=F32, num_images=1, devices=None):
+        super().__init__()
+        self.kind = MG_F64 if dtype == F64 else MG_F32
+        self.num_images = int(num_images)
+        self.devices = [int(d) for d in devices] if devices is not None else [0] * self.num_images
+        if len(self.devices) != self.num_images:
+            raise ValueError("one device per image")
+        self.grid_size_for_cutoff = 64 * 64 * 64
+
+    def initialize_storage(self, nx, ny, nz, hx, hy, hz, rhs):
+        """nx: the slab's cells along x; rhs: one grid per image (borrowed)."""
+        rhs = list(rhs)
+        if len(rhs) != self.num_images:
+            raise ValueError("one rhs grid per image")
+        lib = load()
+        h = C.c_void_p()
+        p = self._params()
+        devs = (C.c_int * self.num_images)(*self.devices)
+        check(lib.ocu_mgco_create(self.kind, C.byref(p), self.num_images, devs, C.byref(h)))
+        self._h = h.value
+        self._rhs = rhs
+        check(lib.ocu_mgco_set_cutoff_cells(self._h, int(self.grid_size_for_cutoff)))
+        arr = (C.c_void_p * self.num_images)(*[g._h for g in rhs])
+        check(lib.ocu_mgco_initialize_storage(self._h, nx, ny, nz, hx, hy, hz, arr))
+        return True
+
+    def co_pressure(self, image=0):
+        return Grid3DDevice._borrow(load().ocu_mgco_pressure(self._h, int(image)), self)
+
+    @property
+    def cutoff_level(self):
+        return load().ocu_mgco_cutoff_level(self._h)
+
+
+def mgco_plan(nx_local, ny, nz, num_images, image, bc, cutoff_cells=64 * 64 * 64):
+    """The decomposition of one image of a Sol_MultigridPressure3DDeviceCo (host only):
+    level count, cutoff level, x neighbours (-1 at the domain's face) and the image's faces."""
+    out = _capi.MGCoPlan()
+    b = bc.to_c()
+    check(load().ocu_mgco_plan_compute(nx_local, ny, nz, num_images, image, int(cutoff_cells), C.byref(b),
+                                       C.byref(out)))
+    return {"num_levels": out.num_levels, "cutoff_level": out.cutoff_level, "neg_image": out.neg_image,
+            "pos_image": out.pos_image,
+            "local_bc": {f: getattr(out.local_bc, f).type for f in ("xpos", "xneg", "ypos", "yneg", "zpos", "zneg")}}
 
 
 class PressureEnsemble:

@@ -60,6 +60,11 @@ class MGParams(C.Structure):
                 ("ir_inner_exact", C.c_int), ("wait_limit", C.c_int)]
 
 
+class MGCoPlan(C.Structure):
+    _fields_ = [("num_levels", C.c_int), ("cutoff_level", C.c_int), ("neg_image", C.c_int),
+                ("pos_image", C.c_int), ("local_bc", BCSet)]
+
+
 class MGStats(C.Structure):
     _fields_ = [("num_levels", C.c_int), ("vcycles", C.c_int), ("outer_iterations", C.c_int),
                 ("last_l2", C.c_double), ("last_linf", C.c_double), ("omega", C.c_double)]
@@ -141,6 +146,13 @@ SIGNATURES = {
     "ocu_mg_restrict_residuals": (I, [P, I, I, I, C.POINTER(D), C.POINTER(D)]),
     "ocu_mg_prolong": (I, [P, I, I, I]),
     "ocu_mg_synchronize": (I, [P]),
+    "ocu_mgco_plan_compute": (I, [I, I, I, I, I, C.c_longlong, C.POINTER(BCSet), C.POINTER(MGCoPlan)]),
+    "ocu_mgco_create": (I, [I, C.POINTER(MGParams), I, C.POINTER(C.c_int), PP]),
+    "ocu_mgco_set_cutoff_cells": (I, [P, C.c_longlong]),
+    "ocu_mgco_initialize_storage": (I, [P, I, I, I, D, D, D, C.POINTER(P)]),
+    "ocu_mgco_pressure": (P, [P, I]),
+    "ocu_mgco_num_images": (I, [P]),
+    "ocu_mgco_cutoff_level": (I, [P]),
     "ocu_advect_passive_adjoint": (I, [P] * 9 + [I, I, I, D, D, D, D, I, P]),
     "ocu_advect_self_adjoint": (I, [P] * 9 + [I, I, I, D, D, D, D, I, P]),
     "ocu_adj_create": (I, [I, I, I, I, D, D, D, I, I, D, I, D, PP]),

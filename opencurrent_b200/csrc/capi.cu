@@ -348,7 +348,8 @@ static ocu_status pick_core(ocu_mg *mg, int core, int level, CoreOps **out) {
       return fail(OCU_ERR_INVALID_VALUE, "[ERROR] level operation - solver has no FP32 hierarchy");
     c = &mg->s.cf;
   } else if (core == 0) {
-    c = mg->s.kind == OCU_MG_F32 ? (CoreOps *)&mg->s.cf : (CoreOps *)&mg->s.cd;
+    if (mg->s.co) c = mg->s.co->ops();
+    else c = mg->s.kind == OCU_MG_F32 ? (CoreOps *)&mg->s.cf : (CoreOps *)&mg->s.cd;
   } else {
     return fail(OCU_ERR_INVALID_VALUE, "[ERROR] level operation - bad core %d", core);
   }
@@ -421,6 +422,7 @@ ocu_status ocu_mg_prolong(ocu_mg *mg, int core, int coarse, int fine) {
 
 ocu_status ocu_mg_synchronize(ocu_mg *mg) {
   OCU_NOT_NULL(mg, "solver");
+  if (mg->s.co) OCU_TRY(mg->s.co->ops()->join());
   return check_cuda(cudaStreamSynchronize(mg->s.stream), "synchronize");
 }
 

@@ -470,11 +470,15 @@ template struct MGCore<double>;
 // ------------------------------------------------------------------------------------------
 // Driver (Sol_MultigridPressure3DBase)
 // ------------------------------------------------------------------------------------------
-CoreOps *MGSolver::active() { return double_mode ? (CoreOps *)&cd : (CoreOps *)&cf; }
+CoreOps *MGSolver::active() {
+  if (co) return co->ops();
+  return double_mode ? (CoreOps *)&cd : (CoreOps *)&cf;
+}
 
 int MGSolver::coarse_iters() const {
   const int cl = num_levels - 1;
-  const auto &d = (kind == OCU_MG_F32) ? cf.dim[cl] : cd.dim[cl];
+  int d[3];
+  for (int q = 0; q < 3; q++) d[q] = co ? co->coarse_dim()[q] : (kind == OCU_MG_F32) ? cf.dim[cl][q] : cd.dim[cl][q];
   const int a = d[0] * d[1], b = d[1] * d[2], c = d[0] * d[2];
   const int mx = a > b ? (a > c ? a : c) : (b > c ? b : c);
   return mx / 2;
@@ -499,6 +503,7 @@ static double pick(int conv, double l2, double linf) {
 // solver's inner solve) runs as a chain of graph launches without a host wait.
 // ------------------------------------------------------------------------------------------
 MGSolver::~MGSolver() {
+  co.reset();  // waits for every image's stream; image 0's pressure is freed below
   clear_graphs();
   if (stream) cudaStreamSynchronize(stream);
   if (pressure) { cudaFree(pressure->buf); delete pressure; }
@@ -907,6 +912,7 @@ ocu_status MGSolver::solve(double *residual, double tolerance, int max_iter) {
     OCU_TRY(active()->clear_zero(0));
     st = fmg_dispatch(tolerance, max_iter, &l2, &linf);
   }
+  if (co && (st == OCU_OK || st == OCU_ERR_NOT_CONVERGED)) OCU_TRY(co->ops()->join());
   *residual = (prm.convergence == OCU_CONVERGENCE_L2) ? l2 : linf;
   stats.last_l2 = l2;
   stats.last_linf = linf;
@@ -921,6 +927,7 @@ ocu_status MGSolver::run_vcycles(int count) {
   double l2, linf;
   ocu_status st = do_vcycle(0, count, &l2, &linf);
   if (st == OCU_ERR_NOT_CONVERGED) st = OCU_OK;
+  if (st == OCU_OK && co) st = co->ops()->join();
   if (st == OCU_OK) st = check_cuda(cudaStreamSynchronize(stream), "run_vcycles");
   return st;
 }
@@ -931,12 +938,15 @@ ocu_status MGSolver::run_fmg(int count) {
   double l2, linf;
   ocu_status st = do_fmg(0, count, &l2, &linf);
   if (st == OCU_ERR_NOT_CONVERGED) st = OCU_OK;
+  if (st == OCU_OK && co) st = co->ops()->join();
   if (st == OCU_OK) st = check_cuda(cudaStreamSynchronize(stream), "run_fmg");
   return st;
 }
 
 ocu_status MGSolver::initialize_storage(int nx, int ny, int nz, double hx, double hy, double hz, ocu_grid *rhs) {
   if (initialized) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] initialize_storage - already initialized");
+  if (co_images > 0)
+    return fail(OCU_ERR_INVALID_VALUE, "[ERROR] initialize_storage - a multi-image solver takes one rhs per image (ocu_mgco_initialize_storage)");
   if (!stream) set_stream(nullptr);
   if (!check_float((float)hx) || !check_float((float)hy) || !check_float((float)hz))
     return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_MultigridPressure3DBase::initialize_storage - garbage hx,hy,hz value %f %f %f", hx, hy, hz);
@@ -1003,6 +1013,7 @@ ocu_status MGSolver::set_params(const ocu_mg_params &p) {
   cd.bc = p.bc;
   if (kind == OCU_MG_MIXED_IR) bc_make_homogeneous(&cf.bc);
   cf.disable_relax_on_host = cd.disable_relax_on_host = p.disable_relax_on_host != 0;
+  if (co) co->ops()->on_params(p);
   clear_graphs();  // captured schedules depend on every parameter
   return apply_knobs();
 }
@@ -1018,10 +1029,55 @@ void MGSolver::set_stream(cudaStream_t s) {
   stream = s;
   cf.stream = s;
   cd.stream = s;
+  if (co) co->ops()->on_stream(s);
+}
+
+// Sol_MultigridPressure3DDeviceCo::initialize_storage (sol_mgpressure3dco.cu:240-520)
+ocu_status MGSolver::initialize_storage_co(int nxl, int ny, int nz, double hx, double hy, double hz,
+                                           ocu_grid *const *rhs) {
+  if (initialized) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] initialize_storage - already initialized");
+  if (!rhs) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_MultigridPressure3DDeviceCo::initialize_storage - null rhs");
+  const ocu_dtype want = kind == OCU_MG_F32 ? OCU_F32 : OCU_F64;
+  for (int i = 0; i < co_images; i++) {
+    const ocu_grid *r = rhs[i];
+    if (!r) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_MultigridPressure3DDeviceCo::initialize_storage - null rhs of image %d", i);
+    if (r->dtype != want) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_MultigridPressure3DDeviceCo::initialize_storage - rhs dtype mismatch (image %d)", i);
+    if (r->L.gx < 1 || r->L.gy < 1 || r->L.gz < 1)
+      return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_MultigridPressure3DDevice::initialize_storage - rhs has invalid ghost cells (%d,%d,%d), must be >= 1", r->L.gx, r->L.gy, r->L.gz);
+    if (r->L.nx != nxl || r->L.ny != ny || r->L.nz != nz)
+      return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_MultigridPressure3DDevice::initialize_storage - rhs dimension mismatch (%d,%d,%d) != (%d,%d,%d)", r->L.nx, r->L.ny, r->L.nz, nxl, ny, nz);
+    const ocu_layout &a = r->L, &b = rhs[0]->L;
+    if (a.gx != b.gx || a.gy != b.gy || a.gz != b.gz || a.pnx != b.pnx || a.pny != b.pny || a.pnz != b.pnz)
+      return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_MultigridPressure3DDeviceCo::initialize_storage - the images' rhs layouts differ (image %d)", i);
+  }
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(co_devices[0]);
+  if (!stream) set_stream(nullptr);
+  ocu_status st = OCU_OK;
+  pressure = alloc_grid(want, rhs[0]->L, &st);
+  if (pressure) st = mgco_create(want, co_images, co_devices.data(), nxl, ny, nz, hx, hy, hz, rhs, pressure, prm,
+                                 co_cutoff_cells, stream, &co);
+  cudaSetDevice(prev);
+  if (st != OCU_OK) {
+    co.reset();
+    return st;
+  }
+  num_levels = co->ops()->levels();
+  double_mode = kind != OCU_MG_F32;
+  use_graphs = false;  // the schedule spans several streams (and devices)
+  stats.num_levels = num_levels;
+  {
+    const double h0 = hx < hy ? (hx < hz ? hx : hz) : (hy < hz ? hy : hz);
+    stats.omega = mg_optimal_omega(h0 * h0 / (hx * hx), h0 * h0 / (hy * hy), h0 * h0 / (hz * hz));
+  }
+  initialized = true;
+  return OCU_OK;
 }
 
 ocu_grid *MGSolver::level_grid(char which, int level) {
   if (!initialized || level < 0 || level >= num_levels) return nullptr;
+  if (co) return co->ops()->grid(which, level);
   auto &core = (kind == OCU_MG_F32) ? (CoreOps &)cf : (CoreOps &)cd;
   return core.grid(which, level);
 }

@@ -8,6 +8,7 @@
 #include <memory>
 #include <vector>
 
+#include "co_mg.h"
 #include "ir_chequer.h"
 #include "mg_fused.h"
 #include "ocu_internal.h"
@@ -50,6 +51,10 @@ struct CoreOps {
   // levels tail_start()..L-1 of a V-cycle in one launch
   virtual int tail_start() const = 0;
   virtual ocu_status cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool symmetric) = 0;
+  // hierarchies spread over several streams: make the solver's stream wait for all of them
+  virtual ocu_status join() { return OCU_OK; }
+  virtual void on_stream(cudaStream_t) {}
+  virtual void on_params(const ocu_mg_params &) {}
 };
 
 // Level hierarchy of one precision (Sol_MultigridPressure3DDevice<T> storage).
@@ -140,6 +145,12 @@ struct MGSolver {
   };
   std::unique_ptr<ocu_grid, GridDeleter> pressure_f;  // FP32 u0 of the mixed solvers
   std::unique_ptr<ChequerMG> chq;  // split-layout FP32 correction solver (OCU_MG_MIXED_IR)
+  // multi-image solver (Sol_MultigridPressure3DDeviceCo): images, their devices, the cutoff
+  // (grid_size_for_cutoff) and, once initialized, the hierarchy that replaces cf / cd
+  int co_images = 0;
+  std::vector<int> co_devices;
+  long long co_cutoff_cells = 64LL * 64 * 64;
+  std::unique_ptr<CoOps> co;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;  // used when the caller's stream is the legacy NULL stream
   ocu_mg_stats stats{};
@@ -166,6 +177,8 @@ struct MGSolver {
   CoreOps *active();
   int coarse_iters() const;
   ocu_status initialize_storage(int nx, int ny, int nz, double hx, double hy, double hz, ocu_grid *rhs);
+  ocu_status initialize_storage_co(int nx_local, int ny, int nz, double hx, double hy, double hz,
+                                   ocu_grid *const *rhs);
   ocu_status set_params(const ocu_mg_params &p);
   ocu_status apply_knobs();
   void set_stream(cudaStream_t s);
