@@ -419,10 +419,52 @@ def run_secondary(torch, ocu, _capi, lib, stream, sh):
     steps, ms, unconverged = ns_run(True)
     out["ns_128x128x64_fp32_fp64_pressure_steps_per_s"] = round(steps / (ms * 1e-3), 2)
     out["ns_fp64_pressure_steps_projection_above_tol"] = unconverged
+    out.update(run_coarray(torch, ocu, _capi, lib, stream, sh))
     out.update(run_ensemble(torch, ocu, stream, sh))
     out.update(run_persistent_ensemble(torch, ocu, stream, sh))
     out.update(run_differentiable(torch, ocu))
     return out
+
+
+def run_coarray(torch, ocu, _capi, lib, stream, sh, n=256, images=2):
+    """The headline FP64 solve (256^3 Neumann, 16 modes, to 1e-10 relative RMS residual) through
+    the multi-image solver: `images` x-slabs on this one device, halo planes copied device to
+    device after every ghost refresh, levels of at most 64^3 cells on image 0."""
+    L = ocu.layout(n // images, n, n)
+    b = fourier_rhs(n)
+    rms = float(np.sqrt(np.mean(b ** 2)))
+    nxl = n // images
+    rhs = []
+    for i in range(images):
+        g = ocu.Grid3DDevice(ocu.F64)
+        g.init(nxl, n, n)
+        g.copy_from_host(padded(b[i * nxl:(i + 1) * nxl], L, np.float64))
+        rhs.append(g)
+    s = ocu.Sol_MultigridPressure3DDeviceCo(ocu.F64, images)
+    s.bc = ocu.BoundaryConditionSet(ocu.BoundaryCondition(ocu.BC_NEUMANN, 0.0))
+    s.initialize_storage(nxl, n, n, 1.0 / n, 1.0 / n, 1.0 / n, rhs)
+    _capi.check(lib.ocu_mg_set_stream(s._h, sh))
+
+    def solve():
+        for i in range(images):
+            _capi.check(lib.ocu_grid_clear(s.co_pressure(i).handle, 0.0, sh))
+        ok, res = s.solve(TOL_REL * rms, 30)
+        if not ok:
+            raise RuntimeError(f"multi-image solve did not reach tolerance: {res / rms:.3e}")
+        return res
+    for _ in range(2):
+        solve()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record(stream)
+    for _ in range(reps):
+        res = solve()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return {"coarray_256_fp64_images": images, "coarray_256_fp64_solve_ms": round(e0.elapsed_time(e1) / reps, 4),
+            "coarray_256_fp64_vcycles": s.stats.vcycles, "coarray_256_fp64_rel_residual": res / rms,
+            "coarray_256_fp64_cutoff_level": s.cutoff_level}
 
 
 def run_differentiable(torch, ocu, n=96, steps=32, every=8, directions=8):

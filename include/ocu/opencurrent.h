@@ -7,6 +7,7 @@
  *   Grid3DDevice<T> / Grid3DHost<T>               ocustorage/grid3d.h:151-264
  *   apply_3d_(mac_)boundary_conditions_level1*    ocustorage/grid3dboundary.h:26-70
  *   Sol_MultigridPressure3DDevice<T>              ocuequation/sol_mgpressure3d.h:104-181
+ *   Sol_MultigridPressure3DDeviceCo<T>            ocuequation/sol_mgpressure3d.h:184-242
  *   Sol_MultigridPressureMixed3DDeviceD           ocuequation/sol_mgpressuremixed3d.h:28-55
  *   Sol_ProjectDivergence3DDevice<T>              ocuequation/sol_project3d.h:74-93
  *   Sol_SelfAdvection3DDevice<T>                  ocuequation/sol_selfadvection3d.h:33-73
@@ -26,6 +27,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -313,6 +315,43 @@ class Sol_MultigridPressure3DDevice : public Sol_MultigridPressure3DBase {
 
 typedef Sol_MultigridPressure3DDevice<float> Sol_MultigridPressure3DDeviceF;
 typedef Sol_MultigridPressure3DDevice<double> Sol_MultigridPressure3DDeviceD;
+
+// Sol_MultigridPressure3DDeviceCo<T> (sol_mgpressure3d.h:184-242).  The reference builds one
+// object per image thread; here one object drives all `num_images` slabs (image i on
+// devices[i], several images may share a device).  initialize_storage takes the slab size along
+// x and one rhs per image; co_pressure(i) is image i's slab of the pressure.  solve / run_vcycles
+// / run_fmg and the parameters are Sol_MultigridPressure3DBase's.
+template <typename T>
+class Sol_MultigridPressure3DDeviceCo : public Sol_MultigridPressure3DBase {
+  std::string _id;
+  int _images;
+  std::vector<int> _devices;
+  std::unique_ptr<Grid3DDevice<T>[]> _co_pressure;
+ public:
+  long long grid_size_for_cutoff = 64 * 64 * 64;  // sol_mgpressure3dco.cu:223
+  Sol_MultigridPressure3DDeviceCo(const char *id, int num_images, const int *devices = nullptr)
+      : Sol_MultigridPressure3DBase(sizeof(T) == 8 ? OCU_MG_F64 : OCU_MG_F32), _id(id ? id : ""),
+        _images(num_images), _devices(num_images > 0 ? num_images : 0, 0) {
+    if (devices)
+      for (int i = 0; i < num_images; i++) _devices[i] = devices[i];
+  }
+  bool initialize_storage(int nx, int ny, int nz, double hx, double hy, double hz, Grid3DDevice<T> *const *rhs) {
+    ocu_mg_params p = params();
+    if (!check_ok(ocu_mgco_create(_kind, &p, _images, _devices.data(), &_mg))) return false;
+    ocu_mg_set_stream(_mg, detail::stream());
+    if (!check_ok(ocu_mgco_set_cutoff_cells(_mg, grid_size_for_cutoff))) return false;
+    std::vector<ocu_grid *> h(_images);
+    for (int i = 0; i < _images; i++) h[i] = rhs[i]->handle();
+    if (!check_ok(ocu_mgco_initialize_storage(_mg, nx, ny, nz, hx, hy, hz, h.data()))) return false;
+    _co_pressure.reset(new Grid3DDevice<T>[_images]);
+    for (int i = 0; i < _images; i++) _co_pressure[i].attach(ocu_mgco_pressure(_mg, i));
+    return true;
+  }
+  int num_images() const { return _images; }
+  int cutoff_level() const { return ocu_mgco_cutoff_level(_mg); }
+  Grid3DDevice<T> &co_pressure(int image) { return _co_pressure[image]; }
+  const Grid3DDevice<T> &co_pressure(int image) const { return _co_pressure[image]; }
+};
 
 // FP64 interface; the default algorithm is FP32 V-cycles inside FP64 iterative refinement,
 // use_reference_algorithm() selects the reference FP32 warm start + FP64 FMG.

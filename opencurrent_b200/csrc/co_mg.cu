@@ -122,6 +122,30 @@ struct CoMG : CoOps, CoreOps {
   bool sliced(int level) const { return level < cutoff; }
   Image &zero() { return *im[0]; }
 
+  // Fused kernels (ghost writes inside the colour sweep and the prolongation, residual and
+  // restriction in one pass, the single-CTA coarse tail on image 0's levels); off with the
+  // unfused parameter.  All of them give the same bits as the separate kernels.
+  bool fused = true;
+
+  // Ghost writes can ride in a slab's kernels when each BC_NONE face of the slab is one whose
+  // ghost plane the halo copy then overwrites whole (a neighbour's face), and no periodic axis
+  // of the slab is odd (the single-image rule).
+  bool slab_emit(int level) const {
+    if (!fused) return false;
+    for (auto &m : im) {
+      const ocu_bc_set b = m->slab.bc_at_level(level);
+      if (b.ypos.type == OCU_BC_NONE || b.yneg.type == OCU_BC_NONE || b.zpos.type == OCU_BC_NONE ||
+          b.zneg.type == OCU_BC_NONE)
+        return false;
+      if ((b.xneg.type == OCU_BC_NONE && m->neg < 0) || (b.xpos.type == OCU_BC_NONE && m->pos < 0)) return false;
+      if (b.xneg.type == OCU_BC_PERIODIC || b.xpos.type == OCU_BC_PERIODIC) return false;
+      const auto &d = m->slab.dim[level];
+      if ((b.ypos.type == OCU_BC_PERIODIC || b.yneg.type == OCU_BC_PERIODIC) && (d[1] & 1)) return false;
+      if ((b.zpos.type == OCU_BC_PERIODIC || b.zneg.type == OCU_BC_PERIODIC) && (d[2] & 1)) return false;
+    }
+    return true;
+  }
+
   // ---- halo exchange (CoArrayManager::barrier_exchange of the u planes,
   //      sol_mgpressure3dco.cu:44-58, 440-470) ----
   ocu_status exchange(int level) {
@@ -230,7 +254,7 @@ struct CoMG : CoOps, CoreOps {
 
   // ---- CoreOps ----
   int levels() const override { return L; }
-  int tail_start() const override { return L - 1; }
+  int tail_start() const override { return fused ? cutoff + top.tail_start() : L - 1; }
 
   ocu_grid *grid(char which, int level) override {
     if (level < 0 || level >= L) return nullptr;
@@ -269,12 +293,15 @@ struct CoMG : CoOps, CoreOps {
   ocu_status relax(int level, int iterations, int order) override {
     DevGuard g;
     PdlSuppress np_;
+    // On the fused path every operation leaves the ghosts current, so the refresh the
+    // reference makes first would rewrite the same values.
     if (!sliced(level)) {
       cudaSetDevice(zero().dev);
-      OCU_TRY(top.apply_bc(level - cutoff));
+      if (!fused) OCU_TRY(top.apply_bc(level - cutoff));
       return top.relax(level - cutoff, iterations, order);
     }
-    OCU_TRY(apply_bc(level));
+    const bool emit = slab_emit(level);
+    if (!emit) OCU_TRY(apply_bc(level));
     if (order == RO_SYMMETRIC) {
       if (iterations % 2 == 1) iterations++;
       if (iterations < 4) iterations = 4;
@@ -283,8 +310,19 @@ struct CoMG : CoOps, CoreOps {
       for (int rb = 0; rb < 2; rb++) {
         int color = rb;
         if (order == RO_BLACK_RED || (order == RO_SYMMETRIC && it >= iterations / 2)) color = !rb;
-        OCU_TRY(sweep_all(level, color));
-        OCU_TRY(apply_bc(level));
+        if (emit) {
+          for (auto &m : im) {
+            cudaSetDevice(m->dev);
+            MGCore<T> &q = m->slab;
+            const T *dg = q.diag.empty() ? nullptr : (const T *)q.diag[level];
+            OCU_TRY(launch_relax_color_emit<T>(q.u0(level), q.b0(level), q.lay[level], dg, color, q.relax_params(level),
+                                               q.hx(level), q.hy(level), q.hz(level), m->stream));
+          }
+          OCU_TRY(exchange(level));
+        } else {
+          OCU_TRY(sweep_all(level, color));
+          OCU_TRY(apply_bc(level));
+        }
       }
     return OCU_OK;
   }
@@ -325,6 +363,11 @@ struct CoMG : CoOps, CoreOps {
   // restrict_residuals (sol_mgpressure3dco.cu:112-178)
   int norm_mode = 0;  // 0: none pending, 1: images, 2: image 0's whole levels
   ocu_status enqueue_restrict_residuals(int fine, int coarse, bool want_l2, bool want_linf) override {
+    return restrict_images(fine, coarse, want_l2, want_linf, false);
+  }
+
+  // zero_coarse: clear the coarse level's u too (in the restriction kernel when fused)
+  ocu_status restrict_images(int fine, int coarse, bool want_l2, bool want_linf, bool zero_coarse) {
     DevGuard g;
     PdlSuppress np_;
     const bool do_restrict = fine != coarse;
@@ -332,9 +375,39 @@ struct CoMG : CoOps, CoreOps {
     if ((!do_restrict && coarse == cutoff) || fine >= cutoff) {
       cudaSetDevice(zero().dev);
       norm_mode = norms ? 2 : 0;
+      if (zero_coarse) return top.clear_and_restrict(fine - cutoff, want_l2, want_linf);
       return top.enqueue_restrict_residuals(fine - cutoff, coarse - cutoff, want_l2, want_linf);
     }
     norm_mode = norms ? 1 : 0;
+    if (zero_coarse && (coarse == cutoff || !fused)) OCU_TRY(clear_zero(coarse));
+    if (fused) {
+      for (auto &m : im) {
+        cudaSetDevice(m->dev);
+        MGCore<T> &q = m->slab;
+        T *rows2 = want_l2 ? (T *)q.rows : nullptr;
+        T *rowsinf = want_linf ? (T *)q.rows + q.rows_stride : nullptr;
+        if (do_restrict) {
+          const bool to_cut = coarse == cutoff;
+          T *zu = (zero_coarse && !to_cut) ? static_cast<T *>(q.grids_u[coarse]->buf) : nullptr;
+          const long long zn = zu ? q.lay[coarse].allocated : 0;
+          OCU_TRY(launch_residual_restrict<T>(q.u0(fine), q.b0(fine), q.lay[fine],
+                                              to_cut ? origin<T>(m->b_restrict) : q.b0(coarse),
+                                              to_cut ? m->b_restrict->L : q.lay[coarse], q.h[fine], q.fx, q.fy, q.fz,
+                                              rows2, rowsinf, m->stream, zu, zn));
+        } else if (norms) {
+          OCU_TRY(launch_residual_rows<T>(q.u0(fine), q.b0(fine), nullptr, nullptr, q.lay[fine], q.h[fine], q.fx, q.fy,
+                                          q.fz, rows2, rowsinf, m->stream));
+        }
+        const long long nrows = (long long)q.dim[fine][0] * q.dim[fine][1];
+        if (want_l2) OCU_TRY(launch_fold_rows<T>(rows2, nrows, false, q.red_scratch, q.d_norms, m->stream));
+        if (want_linf) OCU_TRY(launch_fold_rows<T>(rowsinf, nrows, true, q.red_scratch, q.d_norms + 1, m->stream));
+        if (norms)
+          CO_CK(cudaMemcpyAsync(q.h_norms, q.d_norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, m->stream),
+                "norm readback");
+      }
+      if (do_restrict && coarse == cutoff) OCU_TRY(gather_b());
+      return OCU_OK;
+    }
     for (auto &m : im) {
       cudaSetDevice(m->dev);
       MGCore<T> &s = m->slab;
@@ -393,9 +466,9 @@ struct CoMG : CoOps, CoreOps {
     return OCU_OK;
   }
 
+  // clear_level(fine + 1) then the restriction into it (level fine + 1 >= 1: no ghost refresh)
   ocu_status clear_and_restrict(int fine, bool want_l2, bool want_linf) override {
-    OCU_TRY(clear_level(fine + 1));
-    return enqueue_restrict_residuals(fine, fine + 1, want_l2, want_linf);
+    return restrict_images(fine, fine + 1, want_l2, want_linf, true);
   }
 
   // prolong (sol_mgpressure3dco.cu:180-201)
@@ -407,20 +480,27 @@ struct CoMG : CoOps, CoreOps {
       return top.prolong(coarse - cutoff, fine - cutoff);
     }
     if (coarse == cutoff) OCU_TRY(scatter_u());
+    const bool emit = slab_emit(fine);
     for (auto &m : im) {
       cudaSetDevice(m->dev);
       MGCore<T> &s = m->slab;
-      if (coarse == cutoff)
-        OCU_TRY(launch_prolong<T>(origin<T>(m->u_prolong), m->u_prolong->L, s.u0(fine), s.lay[fine], m->stream));
+      const T *uc = coarse == cutoff ? origin<T>(m->u_prolong) : s.u0(coarse);
+      const ocu_layout &Lc = coarse == cutoff ? m->u_prolong->L : s.lay[coarse];
+      if (emit)
+        OCU_TRY(launch_prolong_emit<T>(uc, Lc, s.u0(fine), s.lay[fine], s.bc_at_level(fine), s.hx(fine), s.hy(fine),
+                                       s.hz(fine), m->stream));
       else
-        OCU_TRY(launch_prolong<T>(s.u0(coarse), s.lay[coarse], s.u0(fine), s.lay[fine], m->stream));
+        OCU_TRY(launch_prolong<T>(uc, Lc, s.u0(fine), s.lay[fine], m->stream));
     }
-    return apply_bc(fine);
+    return emit ? exchange(fine) : apply_bc(fine);
   }
 
+  // the levels from s down, all on image 0 (s >= cutoff): its tail kernel or coarse relax
   ocu_status cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool symmetric) override {
-    (void)s; (void)nu1; (void)nu2;
-    return relax(L - 1, coarse_iters, symmetric ? RO_SYMMETRIC : RO_RED_BLACK);
+    DevGuard g;
+    PdlSuppress np_;
+    cudaSetDevice(zero().dev);
+    return top.cycle_tail(s - cutoff, nu1, nu2, coarse_iters, symmetric);
   }
 
   ocu_status join() override {
@@ -435,21 +515,27 @@ struct CoMG : CoOps, CoreOps {
     top.stream = s;
   }
 
-  void on_params(const ocu_mg_params &p) override { top.disable_relax_on_host = p.disable_relax_on_host != 0; }
+  void on_params(const ocu_mg_params &p) override {
+    top.disable_relax_on_host = p.disable_relax_on_host != 0;
+    fused = top.fused = p.unfused == 0;
+    top.tail_cells = p.tail_cells == 0 ? kDefaultTailCells : (p.tail_cells < 0 ? 0 : p.tail_cells);
+  }
 };
 
 // Geometry of levels [first, last) of the global hierarchy G into core C, x extent divided by
 // div; storage of level 0 of C supplied by the caller (u0, b0), the rest allocated here.
 template <typename T>
 ocu_status co_fill_core(MGCore<T> &C, const MGCore<T> &G, int first, int last, int div, const ocu_bc_set &bc,
-                        ocu_grid *u0, ocu_grid *b0, const ocu_layout &L0, bool disable_host, cudaStream_t s) {
+                        ocu_grid *u0, ocu_grid *b0, const ocu_layout &L0, bool disable_host, bool fused,
+                        int tail_cells, cudaStream_t s) {
   const ocu_dtype dt = sizeof(T) == 8 ? OCU_F64 : OCU_F32;
   const int n = last - first;
   C.stream = s;
   C.bc = bc;
   C.disable_relax_on_host = disable_host;
   C.update_bc_between_colors = true;  // sol_mgpressure3dco.cu:290
-  C.fused = false;
+  C.fused = fused;
+  C.tail_cells = tail_cells;
   C.num_levels = n;
   C.fx = G.fx; C.fy = G.fy; C.fz = G.fz;
   C.omega = G.omega;
@@ -487,6 +573,8 @@ ocu_status co_fill_core(MGCore<T> &C, const MGCore<T> &G, int first, int last, i
   const size_t rs = reduce_scratch_bytes(C.lay[0], sizeof(T));
   OCU_TRY(check_cuda(cudaMalloc(&C.red_scratch, rs), "cudaMalloc(reduce)"));
   OCU_TRY(check_cuda(cudaMemset(C.red_scratch, 0, rs), "cudaMemset(reduce)"));
+  C.rows_stride = ((long long)C.dim[0][0] * C.dim[0][1] + 63) / 64 * 64;
+  OCU_TRY(check_cuda(cudaMalloc(&C.rows, 2 * sizeof(T) * C.rows_stride), "cudaMalloc(norm rows)"));
   OCU_TRY(check_cuda(cudaMalloc(&C.d_norms, 4 * sizeof(double)), "cudaMalloc(norms)"));
   OCU_TRY(check_cuda(cudaMemset(C.d_norms, 0, 4 * sizeof(double)), "cudaMemset(norms)"));
   OCU_TRY(check_cuda(cudaMallocHost(&C.h_norms, 4 * sizeof(double)), "cudaMallocHost(norms)"));
@@ -504,6 +592,8 @@ ocu_status co_build(int N, const int *devices, int nxl, int ny, int nz, double h
   std::unique_ptr<CoMG<T>> c(new CoMG<T>());
   c->dt = dt;
   c->N = N;
+  c->fused = prm.unfused == 0;
+  const int tail_cells = prm.tail_cells == 0 ? kDefaultTailCells : (prm.tail_cells < 0 ? 0 : prm.tail_cells);
   MGCore<T> G;  // the global geometry (no storage)
   OCU_TRY(G.set_geometry(prm.bc, prm.disable_relax_on_host != 0, nxl * N, ny, nz, hx, hy, hz, rhs[0]->L));
   ocu_mgco_plan plan0;
@@ -558,7 +648,7 @@ ocu_status co_build(int N, const int *devices, int nxl, int ny, int nz, double h
       m.own_pressure = true;
     }
     OCU_TRY(co_fill_core<T>(m.slab, G, 0, c->cutoff, N, p.local_bc, m.pressure, rhs[i], rhs[i]->L,
-                            true, m.stream));
+                            true, c->fused, tail_cells, m.stream));
     m.u_prolong = co_alloc(dt, Lc, &st);
     if (!m.u_prolong) return st;
     m.b_restrict = co_alloc(dt, Lc, &st);
@@ -581,7 +671,7 @@ ocu_status co_build(int N, const int *devices, int nxl, int ny, int nz, double h
     c->top.grids_u.assign(1, u0);  // owned by CoMG from here on, whatever happens below
     c->top.grids_b.assign(1, b0);
     OCU_TRY(co_fill_core<T>(c->top, G, c->cutoff, c->L, 1, hb, u0, b0, Lt, prm.disable_relax_on_host != 0,
-                            stream0));
+                            c->fused, tail_cells, stream0));
   }
   for (auto &m : c->im) {
     cudaSetDevice(m->dev);

@@ -95,6 +95,22 @@ def test_fixed_schedule_bit_identical_to_oracle(dt, case):
         assert_same(s.read_b(lev).copy_to_host(), om.grid("b", lev)[0], f"b level {lev}")
 
 
+@pytest.mark.parametrize("dt", [F32, F64])
+@pytest.mark.parametrize("case", [0, 2, 5, 7])
+def test_unfused_kernels_bit_identical_to_oracle(dt, case):
+    """The reference's separate kernels (ghost fill after every colour, residual stored, then
+    restricted) instead of the fused ones: the same bits."""
+    shape, h, bcname, N, cutoff = CASES[case]
+    b = rhs_field(shape, bcname, 60 + case)
+    s, Ls, keep = co_solver(dt, shape, h, bcname, N, cutoff, b, unfused=True)
+    om, L, keep_o = oracle_solver(dt, shape, h, bcname, b)
+    s.run_fmg(1)
+    om.run_fmg(1)
+    s.run_vcycles(1)
+    om.run_vcycles(1)
+    assert_same(whole(s, N, Ls), O.interior(om.grid("u", 0)[0], L), f"unfused {bcname} N={N}")
+
+
 @pytest.mark.parametrize("dt,tol", [(F32, 1e-4), (F64, 1e-9)])
 @pytest.mark.parametrize("conv", [0x05, 0x0A])
 def test_solve_to_tolerance(dt, tol, conv):
