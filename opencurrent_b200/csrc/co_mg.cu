@@ -402,8 +402,7 @@ struct CoMG : CoOps, CoreOps {
         if (want_l2) OCU_TRY(launch_fold_rows<T>(rows2, nrows, false, q.red_scratch, q.d_norms, m->stream));
         if (want_linf) OCU_TRY(launch_fold_rows<T>(rowsinf, nrows, true, q.red_scratch, q.d_norms + 1, m->stream));
         if (norms)
-          CO_CK(cudaMemcpyAsync(q.h_norms, q.d_norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, m->stream),
-                "norm readback");
+          OCU_TRY(launch_readback(q.d_norms, q.h_norms, 2, m->stream));
       }
       if (do_restrict && coarse == cutoff) OCU_TRY(gather_b());
       return OCU_OK;
@@ -423,8 +422,7 @@ struct CoMG : CoOps, CoreOps {
       if (want_linf)
         OCU_TRY(launch_reduce<T>(s.r0(fine), s.lay[fine], OCU_REDUCE_MAXABS, s.red_scratch, s.d_norms + 1, m->stream));
       if (norms)
-        CO_CK(cudaMemcpyAsync(s.h_norms, s.d_norms, 2 * sizeof(double), cudaMemcpyDeviceToHost, m->stream),
-              "norm readback");
+        OCU_TRY(launch_readback(s.d_norms, s.h_norms, 2, m->stream));
     }
     if (do_restrict && coarse == cutoff) OCU_TRY(gather_b());
     return OCU_OK;

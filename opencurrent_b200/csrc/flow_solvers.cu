@@ -253,7 +253,7 @@ ocu_status NSSolver::get_max_stable_timestep(double *out) {
     const float *o[3] = {origin<float>(u), origin<float>(v), origin<float>(w)};
     OCU_TRY(launch_minmax<float>(o, lays, 3, OCU_REDUCE_MAXABS, scratch, d_red, stream));
   }
-  OCU_TRY(check_cuda(cudaMemcpyAsync(h_red, d_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream), "maxabs"));
+  OCU_TRY(launch_readback(d_red, h_red, 3, stream));
   OCU_TRY(check_cuda(cudaStreamSynchronize(stream), "maxabs"));
   double ut = prm.hx / h_red[0], vt = prm.hy / h_red[1], wt = prm.hz / h_red[2];
   if (!check_float((float)ut)) ut = 1e10;

@@ -822,6 +822,23 @@ ocu_status launch_minmax(const T *const *origins, const ocu_layout *const *lays,
   return check_launch("k_reduce_mm");
 }
 
+// A few doubles from device memory into pinned host memory by a one-warp kernel.  Pinned host
+// memory is mapped into the device's address space under unified addressing, so the stores
+// cross PCIe as the kernel's own writes: a host-blocking readback of a norm is not queued on
+// the device-to-host copy engine behind a large transfer that another stream has issued.
+__global__ void k_readback(const double *__restrict__ src, double *dst, int n) {
+  pdl_entry();
+  const int i = threadIdx.x;
+  if (i < n) dst[i] = src[i];
+  __threadfence_system();
+}
+
+ocu_status launch_readback(const double *src, double *host_pinned, int n, cudaStream_t s) {
+  if (n < 1 || n > 32) return fail(OCU_ERR_INVALID_VALUE, "[ERROR] readback - bad count %d", n);
+  launch_pdl(k_readback, dim3(1), dim3(32), 0, s, src, host_pinned, n);
+  return check_launch("k_readback");
+}
+
 size_t reduce_scratch_bytes(const ocu_layout &L, size_t elem) {
   const long long nrows = (long long)L.nx * L.ny;
   const long long blocks = (nrows + 255) / 256;

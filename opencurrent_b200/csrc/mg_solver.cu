@@ -314,8 +314,7 @@ ocu_status MGCore<T>::enqueue_restrict_residuals(int fine, int coarse, bool want
     if (want_linf) OCU_TRY(launch_fold_rows<T>(rowsinf, nrows, true, red_scratch, d_norms + 1, stream));
   }
   if (norms)
-    OCU_TRY(check_cuda(cudaMemcpyAsync(h_norms, d_norms, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream),
-                       "norm readback"));
+    OCU_TRY(launch_readback(d_norms, h_norms, 3, stream));
   return OCU_OK;
 }
 
@@ -339,8 +338,7 @@ ocu_status MGCore<T>::clear_and_restrict(int fine, bool want_l2, bool want_linf)
   if (want_l2) OCU_TRY(launch_fold_rows<T>(rows2, nrows, false, red_scratch, d_norms, stream));
   if (want_linf) OCU_TRY(launch_fold_rows<T>(rowsinf, nrows, true, red_scratch, d_norms + 1, stream));
   if (norms)
-    OCU_TRY(check_cuda(cudaMemcpyAsync(h_norms, d_norms, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream),
-                       "norm readback"));
+    OCU_TRY(launch_readback(d_norms, h_norms, 3, stream));
   return OCU_OK;
 }
 
@@ -834,8 +832,7 @@ ocu_status MGSolver::ir_chequer_residual_tail() {
   OCU_TRY(chq->enqueue_residual(cd.u0(0), cd.b0(0), L, cd.h[0], cd.fx, cd.fy, cd.fz, rows2, rowsinf, stream));
   OCU_TRY(launch_fold_rows<double>(rows2, nrows, false, cd.red_scratch, cd.d_norms, stream));
   OCU_TRY(launch_fold_rows<double>(rowsinf, nrows, true, cd.red_scratch, cd.d_norms + 1, stream));
-  return check_cuda(cudaMemcpyAsync(cd.h_norms, cd.d_norms, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream),
-                    "norm readback");
+  return launch_readback(cd.d_norms, cd.h_norms, 3, stream);
 }
 
 ocu_status MGSolver::ir_solve_chequer(double tolerance, int max_outer, double *rl2, double *rlinf) {
@@ -885,8 +882,7 @@ ocu_status MGSolver::ir_residual(double *l2, double *linf) {
   const long long nrows = (long long)L.nx * L.ny;
   OCU_TRY(launch_fold_rows<double>(rows2, nrows, false, cd.red_scratch, cd.d_norms, stream));
   OCU_TRY(launch_fold_rows<double>(rowsinf, nrows, true, cd.red_scratch, cd.d_norms + 1, stream));
-  OCU_TRY(check_cuda(cudaMemcpyAsync(cd.h_norms, cd.d_norms, 3 * sizeof(double), cudaMemcpyDeviceToHost, stream),
-                     "norm readback"));
+  OCU_TRY(launch_readback(cd.d_norms, cd.h_norms, 3, stream));
   return cd.finish_norms(0, l2, linf);
 }
 

@@ -134,6 +134,9 @@ ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, T a2,
 // as double at *d_result (device pointer).  d_scratch: >= reduce_scratch_elems(L) elements of
 // T plus one unsigned counter (see kernels_grid.cu).
 size_t reduce_scratch_bytes(const ocu_layout &L, size_t elem);
+// n <= 32 doubles from device memory into pinned (cudaMallocHost) host memory by a kernel's
+// stores instead of a copy-engine transfer (see kernels_grid.cu)
+ocu_status launch_readback(const double *src, double *host_pinned, int n, cudaStream_t s);
 // min, max or max-abs (op) of n <= 3 grids sharing strides, one launch, into results[0..n)
 template <typename T>
 ocu_status launch_minmax(const T *const *origins, const ocu_layout *const *lays, int n, int op, void *d_scratch,

@@ -186,7 +186,7 @@ struct PCGSolver {
   template <typename T>
   ocu_status dot(ocu_grid *a, ocu_grid *b, double *out) {
     OCU_TRY(launch_dot<T>(origin<T>(a), origin<T>(b), a->L, scratch, d_red, stream));
-    OCU_TRY(check_cuda(cudaMemcpyAsync(h_red, d_red, sizeof(double), cudaMemcpyDeviceToHost, stream), "dot"));
+    OCU_TRY(launch_readback(d_red, h_red, 1, stream));
     OCU_TRY(check_cuda(cudaStreamSynchronize(stream), "dot"));
     *out = h_red[0];
     return OCU_OK;
@@ -250,7 +250,7 @@ struct PCGSolver {
     }
     iterations = it;
     OCU_TRY(launch_reduce<T>(origin<T>(r), r->L, OCU_REDUCE_MAXABS, scratch, d_red + 1, stream));
-    OCU_TRY(check_cuda(cudaMemcpyAsync(h_red + 1, d_red + 1, sizeof(double), cudaMemcpyDeviceToHost, stream), "linf"));
+    OCU_TRY(launch_readback(d_red + 1, h_red + 1, 1, stream));
     OCU_TRY(check_cuda(cudaStreamSynchronize(stream), "linf"));
     *rl2 = std::sqrt(deltanew);
     *rlinf = h_red[1];
