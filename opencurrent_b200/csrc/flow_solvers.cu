@@ -2,6 +2,7 @@
 // (Eqn_IncompressibleNS3D<T>) over the sm_100a stencil kernels and the multigrid solver.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "flow_solvers.h"
@@ -234,6 +235,7 @@ ocu_status NSSolver::set_parameters(const ocu_ns_params &p, const void *iu, cons
     OCU_TRY(check_cuda(cudaMalloc(&scratch, reduce_scratch_bytes(Lu, 8) * 3), "cudaMalloc(ns scratch)"));
     OCU_TRY(check_cuda(cudaMemset(scratch, 0, reduce_scratch_bytes(Lu, 8) * 3), "cudaMemset"));
     OCU_TRY(check_cuda(cudaMalloc(&d_red, 4 * sizeof(double)), "cudaMalloc"));
+    OCU_TRY(check_cuda(cudaMemset(d_red, 0, 4 * sizeof(double)), "cudaMemset"));
     OCU_TRY(check_cuda(cudaMallocHost(&h_red, 4 * sizeof(double)), "cudaMallocHost"));
   }
   initialized = true;
@@ -253,8 +255,14 @@ ocu_status NSSolver::get_max_stable_timestep(double *out) {
     const float *o[3] = {origin<float>(u), origin<float>(v), origin<float>(w)};
     OCU_TRY(launch_minmax<float>(o, lays, 3, OCU_REDUCE_MAXABS, scratch, d_red, stream));
   }
-  OCU_TRY(launch_readback(d_red, h_red, 3, stream));
+  // d_red[3] holds the timeout word of the TMA-fed advection (read with the maxima)
+  OCU_TRY(launch_readback(d_red, h_red, 4, stream));
   OCU_TRY(check_cuda(cudaStreamSynchronize(stream), "maxabs"));
+  if (*reinterpret_cast<const int *>(h_red + 3) != 0) {
+    OCU_TRY(check_cuda(cudaMemsetAsync(d_red + 3, 0, sizeof(double), stream), "clear timeout word"));
+    *reinterpret_cast<int *>(h_red + 3) = 0;
+    return fail(OCU_ERR_TIMEOUT, "[ERROR] Eqn_IncompressibleNS3D - a load wait of the TMA-fed advection gave up (previous step)");
+  }
   double ut = prm.hx / h_red[0], vt = prm.hy / h_red[1], wt = prm.hz / h_red[2];
   if (!check_float((float)ut)) ut = 1e10;
   if (!check_float((float)vt)) vt = 1e10;
@@ -280,8 +288,19 @@ ocu_status NSSolver::step_t(double dtv) {
   const T ab = (T)(-dtv * dtv / (2 * lastdt));
   const bool ab2 = prm.time_step == OCU_TS_ADAMS_BASHFORD2 && lastdt > 0;
   num_steps++;
-  OCU_TRY(launch_advect_self<T>(origin<T>(u), origin<T>(v), origin<T>(w), origin<T>(du), origin<T>(dv), origin<T>(dw),
-                                Lu, nx, ny, nz, prm.hx, prm.hy, prm.hz, prm.advection_scheme, stream));
+  // FP32 on a large grid: the TMA-fed form (bit-identical), its timeout word in d_red[3]
+  ocu_status adv = OCU_ERR_UNSUPPORTED;
+  if constexpr (sizeof(T) == 4) {
+    const char *st = std::getenv("OCU_B200_TMA_STALL_TEST");  // polls; testing the timeout path
+    adv = launch_advect_self_tma(origin<float>(u), origin<float>(v), origin<float>(w), origin<float>(du),
+                                 origin<float>(dv), origin<float>(dw), Lu, nx, ny, nz, prm.hx, prm.hy, prm.hz,
+                                 prm.advection_scheme, reinterpret_cast<int *>(d_red + 3), st ? -std::atoi(st) : 0,
+                                 stream);
+    if (adv != OCU_OK && adv != OCU_ERR_UNSUPPORTED) return adv;
+  }
+  if (adv == OCU_ERR_UNSUPPORTED)
+    OCU_TRY(launch_advect_self<T>(origin<T>(u), origin<T>(v), origin<T>(w), origin<T>(du), origin<T>(dv),
+                                  origin<T>(dw), Lu, nx, ny, nz, prm.hx, prm.hy, prm.hz, prm.advection_scheme, stream));
   // viscosity, then buoyancy on the vertical component; in FP32 the vertical component's two
   // passes are one kernel (same arithmetic, in the same order)
   bool buoyancy_done = false;

@@ -5,9 +5,12 @@
 // sol_selfadvection3ddev.cu:616-620), so one index serves every array.  Expression order is
 // the reference's; built with --fmad=false.
 #include <cstdint>
+#include <cstdlib>
+#include <mutex>
 #include <initializer_list>
 
 #include "ocu_internal.h"
+#include "tma_ptx.cuh"
 
 namespace ocub {
 
@@ -379,29 +382,26 @@ __global__ void __launch_bounds__(256) k_advect_passive_v4(const float *__restri
 #ifndef OCU_ADVECT_SELF_MINB
 #define OCU_ADVECT_SELF_MINB 2
 #endif
+// Neighbourhood of four cells k..k+3 of row (i, j) for the self-advection: rows with their
+// k - 1 / k + 4 cells (Row4) and plain groups (float4); the suffixes give the (i, j) offsets
+// (0, p = +1, m = -1).
+struct SelfNbr {
+  Row4 U00, Up0, V00, V0p, W00, Wm0, W0m;
+  float4 Um0, U0p, U0m, Upm, Vm0, Vp0, V0m, Vmp, Wp0, W0p;
+};
+
+// The advection terms of u, v and w on the four cells (sol_selfadvection3ddev.cu:135-337 per
+// cell, in its operand order), shared by the group kernel and the TMA-fed kernel.
 template <int IT>
-__global__ void __launch_bounds__(256, OCU_ADVECT_SELF_MINB) k_advect_self_v4(const float *__restrict__ u, const float *__restrict__ v,
-                                                           const float *__restrict__ w, float *__restrict__ dudt,
-                                                           float *__restrict__ dvdt, float *__restrict__ dwdt, float ihx,
-                                                           float ihy, float ihz, long long xs, long long ys, int nx,
-                                                           int ny, int nz4) {
-  V4_BEGIN
-  // rows with their k - 1 / k + 4 neighbours (every lane takes part in the shuffles)
-  const Row4 U00 = row4(u, id, ok, first, last), Up0 = row4(u, id + xs, ok, first, last);
-  const Row4 V00 = row4(v, id, ok, first, last), V0p = row4(v, id + ys, ok, first, last);
-  const Row4 W00 = row4(w, id, ok, first, last), Wm0 = row4(w, id - xs, ok, first, last);
-  const Row4 W0m = row4(w, id - ys, ok, first, last);
-  if (!ok) continue;
-  const float4 Um0 = ld4g(u + id - xs), U0p = ld4g(u + id + ys), U0m = ld4g(u + id - ys), Upm = ld4g(u + id + xs - ys);
-  const float4 Vm0 = ld4g(v + id - xs), Vp0 = ld4g(v + id + xs), V0m = ld4g(v + id - ys), Vmp = ld4g(v + id - xs + ys);
-  const float4 Wp0 = ld4g(w + id + xs), W0p = ld4g(w + id + ys);
-  const float um0[4] = {Um0.x, Um0.y, Um0.z, Um0.w}, u0p[4] = {U0p.x, U0p.y, U0p.z, U0p.w};
-  const float u0m[4] = {U0m.x, U0m.y, U0m.z, U0m.w}, upm[4] = {Upm.x, Upm.y, Upm.z, Upm.w};
-  const float vm0[4] = {Vm0.x, Vm0.y, Vm0.z, Vm0.w}, vp0[4] = {Vp0.x, Vp0.y, Vp0.z, Vp0.w};
-  const float v0m[4] = {V0m.x, V0m.y, V0m.z, V0m.w}, vmp[4] = {Vmp.x, Vmp.y, Vmp.z, Vmp.w};
-  const float wp0[4] = {Wp0.x, Wp0.y, Wp0.z, Wp0.w}, w0p[4] = {W0p.x, W0p.y, W0p.z, W0p.w};
+__device__ __forceinline__ void advect_self_group(const SelfNbr &n, float ihx, float ihy, float ihz, float ou[4],
+                                                  float ov[4], float ow[4]) {
+  const Row4 &U00 = n.U00, &Up0 = n.Up0, &V00 = n.V00, &V0p = n.V0p, &W00 = n.W00, &Wm0 = n.Wm0, &W0m = n.W0m;
+  const float um0[4] = {n.Um0.x, n.Um0.y, n.Um0.z, n.Um0.w}, u0p[4] = {n.U0p.x, n.U0p.y, n.U0p.z, n.U0p.w};
+  const float u0m[4] = {n.U0m.x, n.U0m.y, n.U0m.z, n.U0m.w}, upm[4] = {n.Upm.x, n.Upm.y, n.Upm.z, n.Upm.w};
+  const float vm0[4] = {n.Vm0.x, n.Vm0.y, n.Vm0.z, n.Vm0.w}, vp0[4] = {n.Vp0.x, n.Vp0.y, n.Vp0.z, n.Vp0.w};
+  const float v0m[4] = {n.V0m.x, n.V0m.y, n.V0m.z, n.V0m.w}, vmp[4] = {n.Vmp.x, n.Vmp.y, n.Vmp.z, n.Vmp.w};
+  const float wp0[4] = {n.Wp0.x, n.Wp0.y, n.Wp0.z, n.Wp0.w}, w0p[4] = {n.W0p.x, n.W0p.y, n.W0p.z, n.W0p.w};
   const float half = 0.5f;
-  float ou[4], ov[4], ow[4];
 #pragma unroll
   for (int e = 0; e < 4; e++) {
     // cell k = 4 k4 + e: Row4 index e + 1 is k, e + 2 is k + 1, e is k - 1
@@ -446,6 +446,30 @@ __global__ void __launch_bounds__(256, OCU_ADVECT_SELF_MINB) k_advect_self_v4(co
     d3 = (a * interp<float, IT>(a, wi, w_pk)) - (b * interp<float, IT>(b, w_mk, wi));
     ow[e] = -d1 * ihx - d2 * ihy - d3 * ihz;
   }
+}
+
+template <int IT>
+__global__ void __launch_bounds__(256, OCU_ADVECT_SELF_MINB) k_advect_self_v4(const float *__restrict__ u, const float *__restrict__ v,
+                                                           const float *__restrict__ w, float *__restrict__ dudt,
+                                                           float *__restrict__ dvdt, float *__restrict__ dwdt, float ihx,
+                                                           float ihy, float ihz, long long xs, long long ys, int nx,
+                                                           int ny, int nz4) {
+  V4_BEGIN
+  // rows with their k - 1 / k + 4 neighbours (every lane takes part in the shuffles)
+  SelfNbr n;
+  n.U00 = row4(u, id, ok, first, last);
+  n.Up0 = row4(u, id + xs, ok, first, last);
+  n.V00 = row4(v, id, ok, first, last);
+  n.V0p = row4(v, id + ys, ok, first, last);
+  n.W00 = row4(w, id, ok, first, last);
+  n.Wm0 = row4(w, id - xs, ok, first, last);
+  n.W0m = row4(w, id - ys, ok, first, last);
+  if (!ok) continue;
+  n.Um0 = ld4g(u + id - xs); n.U0p = ld4g(u + id + ys); n.U0m = ld4g(u + id - ys); n.Upm = ld4g(u + id + xs - ys);
+  n.Vm0 = ld4g(v + id - xs); n.Vp0 = ld4g(v + id + xs); n.V0m = ld4g(v + id - ys); n.Vmp = ld4g(v + id - xs + ys);
+  n.Wp0 = ld4g(w + id + xs); n.W0p = ld4g(w + id + ys);
+  float ou[4], ov[4], ow[4];
+  advect_self_group<IT>(n, ihx, ihy, ihz, ou, ov, ow);
   st4g(dudt + id, ou[0], ou[1], ou[2], ou[3]);
   st4g(dvdt + id, ov[0], ov[1], ov[2], ov[3]);
   st4g(dwdt + id, ow[0], ow[1], ow[2], ow[3]);
@@ -584,6 +608,277 @@ ocu_status launch_advect_self(const T *u, const T *v, const T *w, T *du, T *dv, 
   else
     return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Sol_SelfAdvection3DDevice::solve_tex - invalid interpolation type %d", it);
   return check_launch("k_advect_self");
+}
+
+// ---- self-advection fed by TMA ----------------------------------------------------------------
+// A CTA owns a (j, k) tile -- TY rows of TZ cells -- and marches along i over a run of planes.
+// Each plane of u, v and w over the tile with a one-row halo in j and a 16-byte halo in k comes
+// into shared memory by one 3-D TMA box load per field (cp.async.bulk.tensor, mbarrier
+// completion), issued by one thread three planes ahead of its use; a thread then computes four
+// cells of the tile's plane i from planes i-1, i and i+1 in shared memory and stores the three
+// results as 16-byte writes.  Every operand is the group kernel's (advect_self_group), so the
+// results are bit-identical to it.  Work split: the (tile, plane) steps of the grid are cut
+// into equal contiguous ranges, one per resident CTA (tile-major: a range is one or two runs of
+// planes), so a tile's halo planes are loaded twice per run only.
+#ifndef OCU_ADV_TMA_NS
+#define OCU_ADV_TMA_NS 4
+#endif
+#ifndef OCU_ADV_TMA_MINB
+#define OCU_ADV_TMA_MINB 3
+#endif
+template <int TZ>
+struct AdvTile {
+  static constexpr int BX = TZ / 4;                        // threads along k (a float4 group each)
+  static constexpr int TY = 256 / BX;                      // rows (j)
+  static constexpr int H = 4;                              // k halo: one 16-byte granule
+  static constexpr int W = TZ + 2 * H;                     // shared row pitch (floats)
+  static constexpr int R = TY + 2;                         // rows j0-1 .. j0+TY
+  static constexpr int PLANE = (W * R + 31) / 32 * 32;     // floats, a multiple of 128 bytes
+  static constexpr int NS = OCU_ADV_TMA_NS;                // buffers per field: i-1, i, i+1, the rest ahead
+  static constexpr int THREADS = 256;
+  // plane buffers, NS mbarriers, the abort word (8 bytes), the barrier of the timeout test
+  // (8 bytes); +128 to align the base by hand
+  static constexpr size_t SMEM = (size_t)3 * NS * PLANE * sizeof(float) + NS * 8 + 16 + 128;
+};
+
+struct AdvArgs {
+  long long xs, ys;   // strides of the interior-origin pointers (elements)
+  int nx, ny, nz;
+  int gx, gy;         // ghost widths (view coordinates)
+  int ntz;            // tiles along k
+  long long steps;    // tiles * nx
+  int wait_limit;     // polls of a load wait before the launch gives up
+  int stall_test;     // testing the timeout path: the first wait is on a barrier nothing completes
+};
+
+template <int TZ, int IT>
+__global__ void __launch_bounds__(256, OCU_ADV_TMA_MINB) k_advect_self_tma(
+    const __grid_constant__ CUtensorMap tm_u, const __grid_constant__ CUtensorMap tm_v,
+    const __grid_constant__ CUtensorMap tm_w, float *__restrict__ dudt, float *__restrict__ dvdt,
+    float *__restrict__ dwdt, float ihx, float ihy, float ihz, AdvArgs a, int *__restrict__ err) {
+  using S = AdvTile<TZ>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // TMA destinations must be 128-byte aligned: align the base explicitly
+  float *sm = reinterpret_cast<float *>(smem_raw + ((128 - (smem_addr(smem_raw) & 127)) & 127));
+  constexpr int FIELD = S::NS * S::PLANE;  // field f's buffers start at sm + f * FIELD
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sm + 3 * FIELD);
+  int &abort_flag = *reinterpret_cast<int *>(bar + S::NS);
+  unsigned long long *stall_bar = bar + S::NS + 1;  // never arrived at: only the timeout test waits on it
+
+  const unsigned bytes = 3u * S::W * S::R * (unsigned)sizeof(float);
+  const long long lo = a.steps * blockIdx.x / gridDim.x, hi = a.steps * (blockIdx.x + 1) / gridDim.x;
+  const int tx = threadIdx.x % S::BX, ty = threadIdx.x / S::BX;
+
+  if (threadIdx.x == 0) {
+    abort_flag = 0;
+    for (int q = 0; q < S::NS; q++) mbar_init(&bar[q], 1);
+    mbar_init(stall_bar, 1);
+    mbar_init_fence();
+    tma_prefetch_map(&tm_u);
+    tma_prefetch_map(&tm_v);
+    tma_prefetch_map(&tm_w);
+  }
+  __syncthreads();
+  if (a.stall_test) {
+    // the timeout path without a fault: a wait that nothing completes runs out of polls before
+    // any load is issued, so the CTA has nothing in flight when it returns
+    if (threadIdx.x == 0 && !mbar_wait_bounded(stall_bar, 0u, a.wait_limit)) {
+      atomicOr(err, 1);
+      abort_flag = 1;
+    }
+    __syncthreads();
+    if (abort_flag) return;
+  }
+
+  int gbase = 0;   // loads are numbered across this CTA's runs: buffer = g % NS
+  int issued = 0;  // (thread 0) loads issued in the current run
+  for (long long idx = lo; idx < hi;) {
+    const int tile = (int)(idx / a.nx);
+    const int ia = (int)(idx % a.nx);
+    const int ib = (int)((long long)ia + (hi - idx) < a.nx ? ia + (hi - idx) : a.nx);
+    idx += ib - ia;
+    const int k0 = (tile % a.ntz) * TZ, j0 = (tile / a.ntz) * S::TY;
+    const int nload = ib - ia + 2;  // planes ia-1 .. ib
+    auto issue = [&](int m) {       // load m of this run: plane ia-1+m of u, v and w
+      const int g = gbase + m;
+      unsigned long long *bm = &bar[g % S::NS];
+      float *dst = sm + (g % S::NS) * S::PLANE;
+      const int pz = ia - 1 + m + a.gx, py = j0 - 1 + a.gy;
+      mbar_expect_tx(bm, bytes);
+      // view x = k + H: the box starts at k = k0 - H
+      tma_load_3d(dst, &tm_u, k0, py, pz, bm);
+      tma_load_3d(dst + FIELD, &tm_v, k0, py, pz, bm);
+      tma_load_3d(dst + 2 * FIELD, &tm_w, k0, py, pz, bm);
+    };
+    // the previous run's buffers are no longer read; order those reads before the new loads
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (issued = 0; issued < nload && issued < S::NS; issued++) issue(issued);
+
+    for (int n = 0; n < ib - ia; n++) {
+      const int s = ia + n;  // plane computed: loads n (plane s-1), n+1 (s), n+2 (s+1)
+      if (threadIdx.x == 0) {
+        for (int m = (n == 0 ? 0 : n + 2); m <= n + 2; m++) {
+          const int g = gbase + m;
+          if (!mbar_wait_bounded(&bar[g % S::NS], (unsigned)((g / S::NS) & 1), a.wait_limit)) {
+            atomicOr(err, 1);
+            abort_flag = 1;
+            // let the copies already issued -- the one waited for included -- land before the
+            // CTA's shared memory goes away (each wait again bounded, by the default limit)
+            for (int q = m; q < issued; q++)
+              mbar_wait_bounded(&bar[(gbase + q) % S::NS], (unsigned)(((gbase + q) / S::NS) & 1), kWaitLimit);
+            break;
+          }
+        }
+      }
+      __syncthreads();
+      if (abort_flag) return;
+      const int g = gbase + n;
+      const float *um = sm + (g % S::NS) * S::PLANE, *uc = sm + ((g + 1) % S::NS) * S::PLANE;
+      const float *up = sm + ((g + 2) % S::NS) * S::PLANE;
+      const float *vm = um + FIELD, *vc = uc + FIELD, *vp = up + FIELD;
+      const float *wm = um + 2 * FIELD, *wc = uc + 2 * FIELD, *wp = up + 2 * FIELD;
+      const int j = j0 + ty, k = k0 + 4 * tx;
+      if (j < a.ny && k < a.nz) {
+        const int r = ty + 1, cb = 4 * tx + S::H;
+        // a row's group with its k - 1 / k + 4 cells (warp shuffles for these measured slower:
+        // 61.6 against 55.9 us at 256x256x128)
+        auto row6 = [&](const float *p, int rr) {
+          const float *q = p + rr * S::W + cb;
+          const float4 c = *reinterpret_cast<const float4 *>(q);
+          Row4 o;
+          o.v[0] = q[-1]; o.v[1] = c.x; o.v[2] = c.y; o.v[3] = c.z; o.v[4] = c.w; o.v[5] = q[4];
+          return o;
+        };
+        auto grp = [&](const float *p, int rr) { return *reinterpret_cast<const float4 *>(p + rr * S::W + cb); };
+        SelfNbr nb;
+        nb.U00 = row6(uc, r); nb.Up0 = row6(up, r);
+        nb.V00 = row6(vc, r); nb.V0p = row6(vc, r + 1);
+        nb.W00 = row6(wc, r); nb.Wm0 = row6(wm, r); nb.W0m = row6(wc, r - 1);
+        nb.Um0 = grp(um, r); nb.U0p = grp(uc, r + 1); nb.U0m = grp(uc, r - 1); nb.Upm = grp(up, r - 1);
+        nb.Vm0 = grp(vm, r); nb.Vp0 = grp(vp, r); nb.V0m = grp(vc, r - 1); nb.Vmp = grp(vm, r + 1);
+        nb.Wp0 = grp(wp, r); nb.W0p = grp(wc, r + 1);
+        float ou[4], ov[4], ow[4];
+        advect_self_group<IT>(nb, ihx, ihy, ihz, ou, ov, ow);
+        const long long id = (long long)s * a.xs + (long long)j * a.ys + k;
+        st4g(dudt + id, ou[0], ou[1], ou[2], ou[3]);
+        st4g(dvdt + id, ov[0], ov[1], ov[2], ov[3]);
+        st4g(dwdt + id, ow[0], ow[1], ow[2], ow[3]);
+      }
+      // every thread is done with plane s-1's buffers: the next load reuses them
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (threadIdx.x == 0 && issued < nload) issue(issued++);
+    }
+    gbase += nload;
+  }
+}
+
+// View of a field for the TMA loads: x = k + H (base = row (i=-gx, j=-gy) at k = -H, which is
+// pre-padding of that row), dims {nz+H+1, pny, pnx}: both z ghosts inside, and the view's last
+// element inside the allocation (pnz >= nz + H + 1); box = one plane of a tile with its halos.
+template <int TZ>
+static ocu_status make_adv_tmap(const float *origin_ptr, const ocu_layout &L, CUtensorMap *out) {
+  using S = AdvTile<TZ>;
+  auto fn = encode_fn();
+  if (!fn) return fail(OCU_ERR_CUDA, "[ERROR] cuTensorMapEncodeTiled is not available");
+  const float *base = origin_ptr - (long long)L.gx * L.xstride - (long long)L.gy * L.ystride - S::H;
+  cuuint64_t dims[3] = {(cuuint64_t)(L.nz + S::H + 1), (cuuint64_t)L.pny, (cuuint64_t)L.pnx};
+  cuuint64_t strides[2] = {(cuuint64_t)L.ystride * sizeof(float), (cuuint64_t)L.xstride * sizeof(float)};
+  cuuint32_t box[3] = {(cuuint32_t)S::W, (cuuint32_t)S::R, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(OCU_ERR_CUDA, "[ERROR] cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return OCU_OK;
+}
+
+// Resident CTAs of the TMA kernel per device, computed once per (device, tile width).
+template <int TZ, int IT>
+static ocu_status adv_slots(int *slots) {
+  using S = AdvTile<TZ>;
+  static int cache[64] = {0};
+  static std::mutex mu;
+  int dev = 0;
+  OCU_TRY(check_cuda(cudaGetDevice(&dev), "cudaGetDevice"));
+  std::lock_guard<std::mutex> lock(mu);
+  if (!cache[dev & 63]) {
+    OCU_TRY(check_cuda(cudaFuncSetAttribute(k_advect_self_tma<TZ, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)S::SMEM),
+                       "cudaFuncSetAttribute (advection)"));
+    int per_sm = 0, sms = 0;
+    OCU_TRY(check_cuda(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_advect_self_tma<TZ, IT>, S::THREADS,
+                                                                     S::SMEM),
+                       "cudaOccupancyMaxActiveBlocksPerMultiprocessor"));
+    OCU_TRY(check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute"));
+    cache[dev & 63] = per_sm * sms > 0 ? per_sm * sms : 1;
+  }
+  *slots = cache[dev & 63];
+  return OCU_OK;
+}
+
+// OCU_B200_ADVECT_TMA=0 never takes the TMA form, =1 takes it wherever it applies (for tests);
+// unset: where every CTA gets at least kAdvTmaMinSteps planes (below that the halo planes
+// cost more than they save, and the grid's fields fit in L2 anyway).
+constexpr long long kAdvTmaMinSteps = 16;
+
+template <int TZ, int IT>
+static ocu_status launch_adv_tma_t(const float *u, const float *v, const float *w, float *du, float *dv, float *dw,
+                                   const ocu_layout &L, int nx, int ny, int nz, float ihx, float ihy, float ihz,
+                                   int force, int *err, int wait_limit, cudaStream_t s) {
+  using S = AdvTile<TZ>;
+  AdvArgs a;
+  a.xs = L.xstride; a.ys = L.ystride;
+  a.nx = nx; a.ny = ny; a.nz = nz;
+  a.gx = L.gx; a.gy = L.gy;
+  a.ntz = (nz + TZ - 1) / TZ;
+  a.steps = (long long)a.ntz * ((ny + S::TY - 1) / S::TY) * nx;
+  a.stall_test = wait_limit < 0;
+  a.wait_limit = wait_limit < 0 ? -wait_limit : (wait_limit > 0 ? wait_limit : kWaitLimit);
+  int slots = 1;
+  OCU_TRY((adv_slots<TZ, IT>(&slots)));
+  if (!force && a.steps < kAdvTmaMinSteps * slots) return OCU_ERR_UNSUPPORTED;
+  const long long grid = a.steps < slots ? a.steps : slots;
+  CUtensorMap tu, tv, tw;
+  OCU_TRY(make_adv_tmap<TZ>(u, L, &tu));
+  OCU_TRY(make_adv_tmap<TZ>(v, L, &tv));
+  OCU_TRY(make_adv_tmap<TZ>(w, L, &tw));
+  k_advect_self_tma<TZ, IT><<<(unsigned)grid, S::THREADS, S::SMEM, s>>>(tu, tv, tw, du, dv, dw, ihx, ihy, ihz, a, err);
+  return check_launch("k_advect_self_tma");
+}
+
+ocu_status launch_advect_self_tma(const float *u, const float *v, const float *w, float *du, float *dv, float *dw,
+                                  const ocu_layout &L, int nx, int ny, int nz, double hx, double hy, double hz,
+                                  int it, int *err, int wait_limit, cudaStream_t s) {
+  const char *e = std::getenv("OCU_B200_ADVECT_TMA");
+  const int mode = e ? std::atoi(e) : -1;
+  if (mode == 0 || !err) return OCU_ERR_UNSUPPORTED;
+  if (it != OCU_IT_FIRST_ORDER_UPWIND && it != OCU_IT_SECOND_ORDER_CENTERED) return OCU_ERR_UNSUPPORTED;
+  // one ghost layer on every side, 16-byte groups along k, and the view's conditions
+  if (L.gx != 1 || L.gy != 1 || L.gz != 1 || nz % 4 || nz < 32 || L.pnz < nz + AdvTile<32>::H + 1) return OCU_ERR_UNSUPPORTED;
+  if (!v4_ok(nz, L, {u, v, w, du, dv, dw})) return OCU_ERR_UNSUPPORTED;
+  const float ihx = (float)(1 / hx), ihy = (float)(1 / hy), ihz = (float)(1 / hz);
+  const int force = mode == 1;
+  if (it == OCU_IT_FIRST_ORDER_UPWIND) {
+    if (nz >= 128)
+      return launch_adv_tma_t<128, OCU_IT_FIRST_ORDER_UPWIND>(u, v, w, du, dv, dw, L, nx, ny, nz, ihx, ihy, ihz, force,
+                                                              err, wait_limit, s);
+    if (nz >= 64)
+      return launch_adv_tma_t<64, OCU_IT_FIRST_ORDER_UPWIND>(u, v, w, du, dv, dw, L, nx, ny, nz, ihx, ihy, ihz, force,
+                                                             err, wait_limit, s);
+    return launch_adv_tma_t<32, OCU_IT_FIRST_ORDER_UPWIND>(u, v, w, du, dv, dw, L, nx, ny, nz, ihx, ihy, ihz, force,
+                                                           err, wait_limit, s);
+  }
+  if (nz >= 128)
+    return launch_adv_tma_t<128, OCU_IT_SECOND_ORDER_CENTERED>(u, v, w, du, dv, dw, L, nx, ny, nz, ihx, ihy, ihz,
+                                                               force, err, wait_limit, s);
+  if (nz >= 64)
+    return launch_adv_tma_t<64, OCU_IT_SECOND_ORDER_CENTERED>(u, v, w, du, dv, dw, L, nx, ny, nz, ihx, ihy, ihz,
+                                                              force, err, wait_limit, s);
+  return launch_adv_tma_t<32, OCU_IT_SECOND_ORDER_CENTERED>(u, v, w, du, dv, dw, L, nx, ny, nz, ihx, ihy, ihz, force,
+                                                            err, wait_limit, s);
 }
 
 template <typename T>

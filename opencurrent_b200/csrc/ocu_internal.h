@@ -210,6 +210,14 @@ template <typename T>
 ocu_status launch_advect_passive(const T *u, const T *v, const T *w, const T *phi, T *dphi,
                                  const ocu_layout &L, int nx, int ny, int nz, double hx,
                                  double hy, double hz, int interp, cudaStream_t s);
+// FP32 self-advection fed by TMA (kernels_flow.cu), bit-identical to launch_advect_self;
+// OCU_ERR_UNSUPPORTED where it does not apply (the caller then uses launch_advect_self).  err:
+// device word set when a load wait gives up (nullptr: never taken); wait_limit: polls per wait
+// (0: the default; negative: the timeout test, a first wait that nothing completes).
+ocu_status launch_advect_self_tma(const float *u, const float *v, const float *w, float *du, float *dv,
+                                  float *dw, const ocu_layout &L, int nx, int ny, int nz, double hx,
+                                  double hy, double hz, int interp, int *err, int wait_limit,
+                                  cudaStream_t s);
 template <typename T>
 ocu_status launch_thermal_force(T *dvdt, T coefficient, const T *temp, const ocu_layout &L,
                                 int nbr_stride, int nx, int ny, int nz, cudaStream_t s);
