@@ -1,6 +1,7 @@
 // PTX wrappers for TMA tile loads into shared memory with mbarrier completion (sm_90+ forms that
-// sm_100a keeps), and the driver entry point that encodes tensor maps.  No cluster multicast:
-// every load's tensor map covers this GPU's own memory and lands in the issuing CTA.
+// sm_100a keeps), and the driver entry point that encodes tensor maps.  Every load's tensor map
+// covers this GPU's own memory, and each load lands in the shared memory of the CTA that issues
+// it only.
 #pragma once
 
 #include <cuda.h>
