@@ -4,8 +4,12 @@
 // Forward step n (fixed dt): dphi = A(u_n, phi_n) (passive advection), du = S(u_n) (self
 // advection), phi_{n+1} = phi_n + dt dphi, u*_{n+1} = u_n + dt du, u_{n+1} = P u*_{n+1} with P
 // the projection of Sol_ProjectDivergence3DDevice (divergence, multigrid pressure solve,
-// gradient subtraction; sol_project3ddev.cu:58-71).  The pressure solve starts from zero every
-// step, so a recomputed step reproduces the stored one exactly.
+// gradient subtraction; sol_project3ddev.cu:58-71).  Each projection's pressure solve starts from
+// the previous step's pressure, as the reference's projection solver keeps its pressure between
+// solves; the forward chain starts from a zero pressure, and every checkpoint stores the pressure
+// with the state, so a recomputed step starts from the same guess and reproduces the stored one
+// exactly.  The adjoint chain's projections likewise start from the previous adjoint projection
+// (from zero at the start of the backward pass).
 //
 // Adjoint step, given the cotangents (Lu', Lphi') of (u_{n+1}, phi_{n+1}):
 //   Lu*   = P^T Lu' = P Lu'          (on the periodic grid D^T = -G, so P = I - G (DG)^-1 D is
@@ -55,6 +59,7 @@ struct AdjChain {
   using State = std::array<ocu_grid *, 4>;  // u, v, w, phi
   State W{}, D{}, Lam{}, Pl{}, nphi{};       // work state, derivatives, cotangents, projected, spare
   std::vector<State> ckpt, seg;
+  std::vector<ocu_grid *> ckpt_p;  // the forward projection's pressure at each checkpoint
   std::unique_ptr<ProjectSolver> proj, proj_adj;
   bool have_forward = false;
 
@@ -69,6 +74,8 @@ struct AdjChain {
     drop(W); drop(D); drop(Lam); drop(Pl); drop(nphi);
     for (auto &s : ckpt) drop(s);
     for (auto &s : seg) drop(s);
+    for (ocu_grid *g : ckpt_p)
+      if (g) { cudaFree(g->buf); delete g; }
   }
 
   ocu_status make(const char which, ocu_grid **out) {
@@ -106,6 +113,17 @@ struct AdjChain {
     proj->dtype = dtype;
     proj->set_stream(stream);
     OCU_TRY(proj->initialize_storage(nx, ny, nz, hx, hy, hz, W[0], W[1], W[2], bc));
+    const ocu_layout &Lp = pressure(*proj)->L;
+    ckpt_p.assign(ckpt.size(), nullptr);
+    for (auto &g : ckpt_p) {
+      g = new ocu_grid{dtype, Lp, nullptr, true};
+      cudaError_t e = cudaMalloc(&g->buf, dtype_size(dtype) * Lp.allocated);
+      if (e != cudaSuccess) {
+        delete g;
+        g = nullptr;
+        return check_cuda(e, "cudaMalloc(adjoint chain checkpoint pressure)");
+      }
+    }
     proj_adj.reset(new ProjectSolver());
     proj_adj->dtype = dtype;
     proj_adj->set_stream(stream);
@@ -133,9 +151,13 @@ struct AdjChain {
     return launch_bc_level1<T>(origin<T>(s[3]), s[3]->L, bc, hx, hy, hz, stream);
   }
 
+  static ocu_grid *pressure(ProjectSolver &p) { return p.mg->s.pressure; }
+  ocu_status clear_pressure(ProjectSolver &p) {
+    return check_cuda(cudaMemsetAsync(pressure(p)->buf, 0, dtype_size(dtype) * pressure(p)->L.allocated, stream),
+                      "clear pressure");
+  }
+  // the solve starts from the pressure the solver holds (the previous projection's)
   ocu_status project(ProjectSolver &p, double tolerance) {
-    OCU_TRY(check_cuda(cudaMemsetAsync(p.mg->s.pressure->buf, 0,
-                                       dtype_size(dtype) * p.mg->s.pressure->L.allocated, stream), "clear pressure"));
     ocu_status st = p.solve(tolerance);
     return st == OCU_ERR_NOT_CONVERGED ? OCU_OK : st;
   }
@@ -161,8 +183,12 @@ struct AdjChain {
   template <typename T> ocu_status forward(const State &in, ocu_grid *phi_out) {
     OCU_TRY(copy_state(W, in));
     OCU_TRY(ghosts<T>(W));
+    OCU_TRY(clear_pressure(*proj));
     for (int n = 0; n < steps; n++) {
-      if (n % every == 0) OCU_TRY(copy_state(ckpt[n / every], W));
+      if (n % every == 0) {
+        OCU_TRY(copy_state(ckpt[n / every], W));
+        OCU_TRY(copy(ckpt_p[n / every], pressure(*proj)));
+      }
       OCU_TRY(step<T>(W));
     }
     OCU_TRY(copy(phi_out, W[3]));
@@ -200,10 +226,12 @@ struct AdjChain {
     for (int c = 0; c < 3; c++)
       OCU_TRY(check_cuda(cudaMemsetAsync(Lam[c]->buf, 0, dtype_size(dtype) * Lam[c]->L.allocated, stream), "clear"));
     OCU_TRY(copy(Lam[3], lam_phi));
+    OCU_TRY(clear_pressure(*proj_adj));
     const int nseg = (int)ckpt.size();
     for (int sg = nseg - 1; sg >= 0; sg--) {
       const int n0 = sg * every, len = (steps - n0) < every ? steps - n0 : every;
       OCU_TRY(copy_state(W, ckpt[sg]));
+      OCU_TRY(copy(pressure(*proj), ckpt_p[sg]));
       for (int j = 0; j < len; j++) {
         if (j > 0) OCU_TRY(step<T>(W));
         OCU_TRY(copy_state(seg[j], W));
