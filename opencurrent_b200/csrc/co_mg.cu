@@ -507,6 +507,11 @@ struct CoMG : CoOps, CoreOps {
     return zero_waits_all();
   }
 
+  ocu_status fork() override {
+    DevGuard g;
+    return fence_with_zero();
+  }
+
   void on_stream(cudaStream_t s) override {
     zero().stream = s;
     zero().slab.stream = s;

@@ -523,7 +523,9 @@ ocu_status MGSolver::run_segment(const void *core, int seg, F &&enqueue) {
     OCU_TRY(check_cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture"));
     set_capturing(true);
     const unsigned long long n0 = launch_count_captured();
-    ocu_status st = enqueue();
+    ocu_status st = co ? co->ops()->fork() : OCU_OK;
+    if (st == OCU_OK) st = enqueue();
+    if (st == OCU_OK && co) st = co->ops()->join();
     const int kernels = (int)(launch_count_captured() - n0);
     set_capturing(false);
     cudaGraph_t g = nullptr;
@@ -1061,7 +1063,10 @@ ocu_status MGSolver::initialize_storage_co(int nxl, int ny, int nz, double hx, d
   }
   num_levels = co->ops()->levels();
   double_mode = kind != OCU_MG_F32;
-  use_graphs = false;  // the schedule spans several streams (and devices)
+  // segments are captured across the images' streams (fork / join) when the images share one
+  // device; images on several devices run without replay
+  for (int d : co_devices)
+    if (d != co_devices[0]) use_graphs = false;
   stats.num_levels = num_levels;
   {
     const double h0 = hx < hy ? (hx < hz ? hx : hz) : (hy < hz ? hy : hz);

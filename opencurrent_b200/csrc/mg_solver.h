@@ -52,7 +52,10 @@ struct CoreOps {
   virtual int tail_start() const = 0;
   virtual ocu_status cycle_tail(int s, int nu1, int nu2, int coarse_iters, bool symmetric) = 0;
   // hierarchies spread over several streams: make the solver's stream wait for all of them
+  // (join), and all of them wait for the solver's stream (fork: at the start of a stream capture,
+  // so that their work joins the captured graph)
   virtual ocu_status join() { return OCU_OK; }
+  virtual ocu_status fork() { return OCU_OK; }
   virtual void on_stream(cudaStream_t) {}
   virtual void on_params(const ocu_mg_params &) {}
 };
