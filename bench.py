@@ -100,18 +100,19 @@ class ClockSampler:
 # --------------------------------------------------------------------------- helpers ----
 def ir_alg_bytes(n, cycles, outer, ramp_iters=4):
     """Compulsory HBM bytes of the refinement solve with the split-layout FP32 inner solver
-    (s = 4): per refinement step `cycles` level-0 V-cycles (12.57 N s each, as in
-    solve_alg_bytes), the right-hand side restricted down ((2 + 1/8) N_l s per level) and the
-    nested-iteration ramp (prolongation (2 + 1/8) N_l s + ramp_iters red-black iterations of
-    3 N_l s on each level >= 1, and the prolongation into level 0); plus the FP64 residual + FP32
-    right-hand side per step and the initial residual (2N*8 + N*4 each) and the update per step
-    (2N*8 + N*4)."""
+    (s = 4).  Per refinement step: `cycles` level-0 V-cycles (12.57 N s each, as in
+    solve_alg_bytes); the right-hand side restricted down from a zero correction (b read, the
+    coarse b written and its u cleared: (1 + 1/4) N_l s per level); the nested-iteration ramp
+    (a prolongation that assigns, (1 + 1/8) N_l s, + ramp_iters red-black iterations of 3 N_l s
+    on each level >= 1, and the assigning prolongation into level 0); x += e fused into the last
+    prolongation (x read and written, 2N*8, and e not written back: - N s).  Plus the FP64
+    residual + FP32 right-hand side per step and the initial residual (2N*8 + N*4 each)."""
     N = float(n) ** 3
     s = 4
     coarse = N / 7.0  # sum over levels >= 1
-    ramp = 2.125 * N * s + 2.125 * coarse * s + (2.125 + 3 * ramp_iters) * coarse * s + 2.125 * N * s
-    b = outer * (cycles * 12.57 * N * s + ramp)
-    b += (outer + 1) * (2 * N * 8 + N * 4) + outer * (2 * N * 8 + N * 4)
+    ramp = 1.25 * N * s + 1.25 * coarse * s + (1.125 + 3 * ramp_iters) * coarse * s + 1.125 * N * s
+    b = outer * (cycles * 12.57 * N * s + ramp + 2 * N * 8 - N * s)
+    b += (outer + 1) * (2 * N * 8 + N * 4)
     return b
 
 

@@ -225,7 +225,10 @@ __device__ __forceinline__ void load4(const FRow &r, int m2, float v[4]) {
 // row (I, J)), restricted (the mean of each cell's eight) into the coarse right-hand side; the
 // coarse pair's u is zeroed (the next V-cycle leg starts from zero).  All lanes of a warp share
 // (I, J), so every row and boundary decision is uniform across the warp.
-template <bool NC>
+// ZU: the fine u is zero (a correction solve's first descent), so only b is read: with every u
+// term zero residual_cell returns b itself (each product is +0, and b - (+0) == b, signed
+// zeros included), so the sums are the general path's, bit for bit.
+template <bool NC, bool ZU = false>
 __device__ __forceinline__ void chq_restrict_item(const ChqG &f, const ChqG &c, const ChqK &k, const ChqBC &bc,
                                                   const FDiv &fcm, int t) {
   int r, mp, I, J;
@@ -233,6 +236,27 @@ __device__ __forceinline__ void chq_restrict_item(const ChqG &f, const ChqG &c, 
   split(c.fy, r, I, J);
   const int x0 = 2 * I, y0 = 2 * J, m2 = 2 * mp;
   const bool second = 2 * mp + 1 < c.nz;  // coarse K = 2m' + 1 exists
+  const long long cid = ((long long)I * c.ny + J) * c.rz + mp;
+  const bool sc = (I + J) & 1;  // coarse row parity: K = 2m' is colour sc entry m', K = 2m' + 1 colour sc^1
+  if (ZU) {
+    float sum[2] = {0.f, 0.f};
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+      for (int b = 0; b < 2; b++) {
+        float bv[4];
+        load4<NC>(fine_row(f.b0, f.b1, f, x0 + a, y0 + b), m2, bv);
+#pragma unroll
+        for (int e = 0; e < 4; e++) sum[e >> 1] += bv[e];
+      }
+    (sc ? c.b1 : c.b0)[cid] = 0.125f * sum[0];
+    (sc ? c.u1 : c.u0)[cid] = 0.f;
+    if (second) {
+      (sc ? c.b0 : c.b1)[cid] = 0.125f * sum[1];
+      (sc ? c.u0 : c.u1)[cid] = 0.f;
+    }
+    return;
+  }
   float u[2][2][6], bv[2][2][4];           // u[a][b][1 + e], e = -1..4
 #pragma unroll
   for (int a = 0; a < 2; a++)
@@ -293,9 +317,6 @@ __device__ __forceinline__ void chq_restrict_item(const ChqG &f, const ChqG &c, 
         const float yp = b ? yo[a][1][e] : u[a][1][1 + e];
         sum[e >> 1] += residual_cell(u[a][b][1 + e], bv[a][b][e], xm + xp, ym + yp, u[a][b][e] + u[a][b][2 + e], k);
       }
-  // coarse row parity sc: K = 2m' is colour sc entry m', K = 2m' + 1 colour sc^1 entry m'
-  const long long cid = ((long long)I * c.ny + J) * c.rz + mp;
-  const bool sc = (I + J) & 1;
   (sc ? c.b1 : c.b0)[cid] = 0.125f * sum[0];
   (sc ? c.u1 : c.u0)[cid] = 0.f;
   if (second) {
@@ -305,13 +326,27 @@ __device__ __forceinline__ void chq_restrict_item(const ChqG &f, const ChqG &c, 
 }
 
 
+// Where a prolongation's result goes.  ADD: added to the fine u.  ASSIGN: the fine u is zero
+// (the first ascent of a correction solve) and is not read; the result is fma(p, 1/64, 0), the
+// ADD result for a zero fine u, bit for bit.  X64 / X64V: the fine u (the refinement's FP32
+// correction e) is read, e + p/64 is formed as in ADD and added in double to the FP64 solution
+// x instead of being stored (the correction solve's last step fused with x += e); X64V moves
+// x as 16-byte double pairs (k even, pairs 16-byte aligned).
+enum { CHQ_P_ADD = 0, CHQ_P_ASSIGN = 1, CHQ_P_X64 = 2, CHQ_P_X64V = 3 };
+
+struct ChqX {
+  double *x;       // the FP64 level-0 grid at its interior origin
+  long long xs, ys;
+};
+
 // Trilinear prolongation (weights 27, 9, 3, 1 / 64) of a coarse pair (K = 2m', 2m' + 1 of coarse
-// row (I, J)) into its sixteen children, added to the fine u.  Coarse values outside the domain
-// follow the homogeneous rules axis by axis (a corner is the product of the face signs times the
-// cell).  Rows are warp-uniform; the eight fine float2 pairs are loaded before the first store.
-template <bool NC>
+// row (I, J)) into its sixteen children, added to the fine u (MODE: see above).  Coarse values
+// outside the domain follow the homogeneous rules axis by axis (a corner is the product of the
+// face signs times the cell).  Rows are warp-uniform; the eight fine float2 pairs are loaded
+// before the first store.
+template <bool NC, int MODE = CHQ_P_ADD>
 __device__ __forceinline__ void chq_prolong_item(const ChqG &c, const ChqG &f, const ChqBC &bc, const FDiv &fcm,
-                                                 int t) {
+                                                 int t, ChqX X = ChqX{nullptr, 0, 0}) {
   int r, mp, I, J;
   split(fcm, t, r, mp);
   split(c.fy, r, I, J);
@@ -351,8 +386,13 @@ __device__ __forceinline__ void chq_prolong_item(const ChqG &c, const ChqG &f, c
       const FRow R = fine_row(f.u0, f.u1, f, 2 * I + a, 2 * J + b);
       dA[a][b] = reinterpret_cast<float2 *>(const_cast<float *>(R.a) + 2 * mp);
       dO[a][b] = reinterpret_cast<float2 *>(const_cast<float *>(R.o) + 2 * mp);
-      fa[a][b] = *dA[a][b];
-      fo[a][b] = *dO[a][b];
+      if (MODE == CHQ_P_ASSIGN) {
+        fa[a][b] = make_float2(0.f, 0.f);
+        fo[a][b] = make_float2(0.f, 0.f);
+      } else {
+        fa[a][b] = *dA[a][b];
+        fo[a][b] = *dO[a][b];
+      }
     }
 #pragma unroll
   for (int a = 0; a < 2; a++)
@@ -375,8 +415,33 @@ __device__ __forceinline__ void chq_prolong_item(const ChqG &c, const ChqG &f, c
         A.y = __fmaf_rn(out[2], 0.015625f, A.y);
         O.y = __fmaf_rn(out[3], 0.015625f, O.y);
       }
-      *dA[a][b] = A;
-      *dO[a][b] = O;
+      if (MODE == CHQ_P_ADD || MODE == CHQ_P_ASSIGN) {
+        *dA[a][b] = A;
+        *dO[a][b] = O;
+      } else {
+        // fine k = 4m' + e: e = 0 A.x, 1 O.x, 2 A.y, 3 O.y (k = 4m' + 2, + 3 only with `second`)
+        double *px = X.x + (long long)(2 * I + a) * X.xs + (long long)(2 * J + b) * X.ys + 4 * mp;
+        if (MODE == CHQ_P_X64V) {
+          double2 *p2 = reinterpret_cast<double2 *>(px);
+          double2 v = p2[0];
+          v.x = v.x + (double)A.x;
+          v.y = v.y + (double)O.x;
+          p2[0] = v;
+          if (second) {
+            double2 w = p2[1];
+            w.x = w.x + (double)A.y;
+            w.y = w.y + (double)O.y;
+            p2[1] = w;
+          }
+        } else {
+          px[0] = px[0] + (double)A.x;
+          px[1] = px[1] + (double)O.x;
+          if (second) {
+            px[2] = px[2] + (double)A.y;
+            px[3] = px[3] + (double)O.y;
+          }
+        }
+      }
     }
 }
 

@@ -25,24 +25,20 @@ __global__ void __launch_bounds__(CHQ_RELAX_THREADS) k_chq_relax(ChqG g, ChqK k,
   chq_relax_item<true>(g, k, bc, color, (int)t);
 }
 
+template <bool ZU>
 __global__ void __launch_bounds__(256, CHQ_RESTRICT_MINB) k_chq_restrict(ChqG f, ChqG c, ChqK k, ChqBC bc, FDiv fcm) {
   pdl_entry();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)c.nx * c.ny * fcm.d) return;
-  chq_restrict_item<true>(f, c, k, bc, fcm, (int)t);
+  chq_restrict_item<true, ZU>(f, c, k, bc, fcm, (int)t);
 }
 
-__global__ void __launch_bounds__(256, CHQ_PROLONG_MINB) k_chq_prolong(ChqG c, ChqG f, ChqBC bc, FDiv fcm) {
+template <int MODE>
+__global__ void __launch_bounds__(256, CHQ_PROLONG_MINB) k_chq_prolong(ChqG c, ChqG f, ChqBC bc, FDiv fcm, ChqX X) {
   pdl_entry();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)c.nx * c.ny * fcm.d) return;
-  chq_prolong_item<true>(c, f, bc, fcm, (int)t);
-}
-
-__global__ void k_chq_zero(float *p, long long n) {
-  pdl_entry();
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) p[q] = 0.f;
+  chq_prolong_item<true, MODE>(c, f, bc, fcm, (int)t, X);
 }
 
 __global__ void __launch_bounds__(1024) k_chq_tail(ChqTail T) {
@@ -147,6 +143,11 @@ __global__ void __launch_bounds__(256) k_chq_add_correction(double *__restrict__
 
 }  // namespace
 
+// the FP64 grid's pairs (k, k+1), k even, are 16-byte aligned double2
+static bool vec_ok(const ocu_layout &L) {
+  return L.nz % 2 == 0 && L.shift % 2 == 0 && L.xstride % 2 == 0 && L.ystride % 2 == 0;
+}
+
 bool ChequerMG::suits(const std::vector<std::array<int, 3>> &dims, const ocu_bc_set &bc) {
   if (dims.size() < 2) return false;
   const ocu_bc *f[6] = {&bc.xpos, &bc.xneg, &bc.ypos, &bc.yneg, &bc.zpos, &bc.zneg};
@@ -205,14 +206,6 @@ ocu_status ChequerMG::init(const std::vector<std::array<int, 3>> &dims, const st
   return OCU_OK;
 }
 
-ocu_status ChequerMG::clear_u(int l, cudaStream_t s) {
-  const ChqLevel &L = lv[l];
-  const long long n = 2LL * L.nx * L.ny * L.rz;  // u[0] and u[1] are adjacent
-  const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
-  launch_pdl(k_chq_zero, dim3(blocks), dim3(256), 0, s, L.u[0], n);
-  return check_launch("k_chq_zero");
-}
-
 ocu_status ChequerMG::relax(int l, int iterations, bool reverse, cudaStream_t s) {
   const ChqLevel &L = lv[l];
   const ChqG g = make_g(L);
@@ -237,21 +230,35 @@ ocu_status ChequerMG::sweep_level(int l, int color, cudaStream_t s) {
   return check_launch("k_chq_relax");
 }
 
-ocu_status ChequerMG::restrict_to(int l, cudaStream_t s) {
+ocu_status ChequerMG::restrict_to(int l, cudaStream_t s, bool zero_u) {
   const ChqLevel &F = lv[l], &Cl = lv[l + 1];
   const int cm = (Cl.nz + 1) / 2;  // coarse pairs per row
   const long long n = (long long)Cl.nx * Cl.ny * cm;
-  launch_pdl(k_chq_restrict, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, s, make_g(F), make_g(Cl),
-             make_k(F.h, fx, fy, fz, omega), make_bc(bc, fx, fy, fz), make_fdiv(cm));
+  const dim3 grid((unsigned)((n + 255) / 256));
+  if (zero_u)
+    launch_pdl(k_chq_restrict<true>, grid, dim3(256), 0, s, make_g(F), make_g(Cl), make_k(F.h, fx, fy, fz, omega),
+               make_bc(bc, fx, fy, fz), make_fdiv(cm));
+  else
+    launch_pdl(k_chq_restrict<false>, grid, dim3(256), 0, s, make_g(F), make_g(Cl), make_k(F.h, fx, fy, fz, omega),
+               make_bc(bc, fx, fy, fz), make_fdiv(cm));
   return check_launch("k_chq_restrict");
 }
 
-ocu_status ChequerMG::prolong_from(int l, cudaStream_t s) {
+ocu_status ChequerMG::prolong_from(int l, cudaStream_t s, int mode, double *x, const ocu_layout *Lx) {
   const ChqLevel &Cl = lv[l], &F = lv[l - 1];
   const int cm = (Cl.nz + 1) / 2;
   const long long n = (long long)Cl.nx * Cl.ny * cm;
-  launch_pdl(k_chq_prolong, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, s, make_g(Cl), make_g(F),
-             make_bc(bc, fx, fy, fz), make_fdiv(cm));
+  const dim3 grid((unsigned)((n + 255) / 256));
+  ChqX X{x, Lx ? (long long)Lx->xstride : 0, Lx ? (long long)Lx->ystride : 0};
+  const ChqG cg = make_g(Cl), fg = make_g(F);
+  const ChqBC b = make_bc(bc, fx, fy, fz);
+  const FDiv d = make_fdiv(cm);
+  switch (mode) {
+    case CHQ_P_ASSIGN: launch_pdl(k_chq_prolong<CHQ_P_ASSIGN>, grid, dim3(256), 0, s, cg, fg, b, d, X); break;
+    case CHQ_P_X64: launch_pdl(k_chq_prolong<CHQ_P_X64>, grid, dim3(256), 0, s, cg, fg, b, d, X); break;
+    case CHQ_P_X64V: launch_pdl(k_chq_prolong<CHQ_P_X64V>, grid, dim3(256), 0, s, cg, fg, b, d, X); break;
+    default: launch_pdl(k_chq_prolong<CHQ_P_ADD>, grid, dim3(256), 0, s, cg, fg, b, d, X); break;
+  }
   return check_launch("k_chq_prolong");
 }
 
@@ -292,20 +299,27 @@ ocu_status ChequerMG::tail(bool fmg, int nu1, int nu2, int citers, cudaStream_t 
 // and ramp_iters red-black iterations (no V-cycle: measured at 256^3, a refinement solve takes
 // 3.87 ms this way against 4.61 ms with one V-cycle per ramp level, at the same residual after
 // the same two refinement steps), and level 0 gets `cycles` V-cycles.
-ocu_status ChequerMG::enqueue_fmg(int nu1, int nu2, int cycles, int coarse_iters, int ramp_iters, cudaStream_t s) {
+// The correction starts from zero, so the first descent restricts b alone (the residual of a
+// zero u is b) and each level's first prolongation assigns instead of adding: level 0 is never
+// cleared or read before it is written.  With x given, the last prolongation into level 0 adds
+// e + p/64 to x (in double) instead of storing it -- level 0 then does not hold the final
+// correction -- otherwise x += e follows as its own pass.
+ocu_status ChequerMG::enqueue_fmg(int nu1, int nu2, int cycles, int coarse_iters, int ramp_iters, cudaStream_t s,
+                                  double *x, const ocu_layout *Lx) {
   const int ts = tail_s;
-  if (ts > 0) OCU_TRY(clear_u(0, s));
-  for (int l = 0; l < ts; l++) OCU_TRY(restrict_to(l, s));
-  OCU_TRY(tail(true, nu1, nu2, coarse_iters, s));
-  if (ts == 0) {
+  if (ts == 0) {  // the whole hierarchy in the single-CTA tail
+    OCU_TRY(tail(true, nu1, nu2, coarse_iters, s));
     for (int c = 1; c < cycles; c++) OCU_TRY(tail(false, nu1, nu2, coarse_iters, s));
-    return OCU_OK;
+    return x ? enqueue_add_correction(x, *Lx, s) : OCU_OK;
   }
+  for (int l = 0; l < ts; l++) OCU_TRY(restrict_to(l, s, true));
+  OCU_TRY(tail(true, nu1, nu2, coarse_iters, s));
   for (int f = ts - 1; f >= 1; f--) {
-    OCU_TRY(prolong_from(f + 1, s));
+    OCU_TRY(prolong_from(f + 1, s, CHQ_P_ASSIGN));
     OCU_TRY(relax(f, ramp_iters, false, s));
   }
-  OCU_TRY(prolong_from(1, s));
+  OCU_TRY(prolong_from(1, s, CHQ_P_ASSIGN));
+  const int xmode = x && vec_ok(*Lx) ? CHQ_P_X64V : CHQ_P_X64;
   for (int c = 0; c < cycles; c++) {
     for (int l = 0; l < ts; l++) {
       OCU_TRY(relax(l, nu1, false, s));
@@ -313,16 +327,12 @@ ocu_status ChequerMG::enqueue_fmg(int nu1, int nu2, int cycles, int coarse_iters
     }
     OCU_TRY(tail(false, nu1, nu2, coarse_iters, s));
     for (int l = ts - 1; l >= 0; l--) {
+      if (l == 0 && x && c == cycles - 1) return prolong_from(1, s, xmode, x, Lx);
       OCU_TRY(prolong_from(l + 1, s));
       if (l > 0) OCU_TRY(relax(l, nu2, false, s));
     }
   }
-  return OCU_OK;
-}
-
-// the FP64 grid's pairs (k, k+1), k even, are 16-byte aligned double2
-static bool vec_ok(const ocu_layout &L) {
-  return L.nz % 2 == 0 && L.shift % 2 == 0 && L.xstride % 2 == 0 && L.ystride % 2 == 0;
+  return x ? enqueue_add_correction(x, *Lx, s) : OCU_OK;
 }
 
 ocu_status ChequerMG::enqueue_residual(const double *x, const double *b, const ocu_layout &L, double h, double fx_,

@@ -35,11 +35,14 @@ class ChequerMG {
   // dims / h: the FP64 hierarchy's levels; fx, fy, fz, omega: its operator factors.
   ocu_status init(const std::vector<std::array<int, 3>> &dims, const std::vector<double> &h, double fx,
                   double fy, double fz, double omega, const ocu_bc_set &bc_homogeneous);
-  // Enqueue: u(0) = 0; the right-hand side restricted to the coarsest levels, solved there,
-  // carried up level by level with ramp_iters red-black iterations each (nested iteration),
-  // then `cycles` V-cycles at level 0 (nu1 pre-smoothing iterations on every level, nu2
-  // post-smoothing on levels > 0, the coarsest level relaxed coarse_iters times).
-  ocu_status enqueue_fmg(int nu1, int nu2, int cycles, int coarse_iters, int ramp_iters, cudaStream_t s);
+  // Enqueue the correction solve from u(0) = 0: the right-hand side restricted to the coarsest
+  // levels, solved there, carried up level by level with ramp_iters red-black iterations each
+  // (nested iteration), then `cycles` V-cycles at level 0 (nu1 pre-smoothing iterations on every
+  // level, nu2 post-smoothing on levels > 0, the coarsest level relaxed coarse_iters times).
+  // With x (the FP64 level-0 grid at its interior origin, layout *Lx): then x += e, the last
+  // prolongation adding into x directly where it can (u(0) is then left without it).
+  ocu_status enqueue_fmg(int nu1, int nu2, int cycles, int coarse_iters, int ramp_iters, cudaStream_t s,
+                         double *x = nullptr, const ocu_layout *Lx = nullptr);
   // Enqueue: b(0) = (float) (b - A x) from the FP64 level-0 grids (ghosts filled), with the
   // per-row sum of squares and max |r| of the FP64 residual in rows2 / rowsinf.
   ocu_status enqueue_residual(const double *x, const double *b, const ocu_layout &L, double h, double fx,
@@ -62,12 +65,13 @@ class ChequerMG {
   double fx = 1, fy = 1, fz = 1, omega = 1;
   ocu_bc_set bc{};
   ocu_status relax(int l, int iterations, bool reverse, cudaStream_t s);
-  ocu_status restrict_to(int l, cudaStream_t s);
-  ocu_status prolong_from(int l, cudaStream_t s);
+  // zero_u: level l's u is zero and is not read (only b is restricted)
+  ocu_status restrict_to(int l, cudaStream_t s, bool zero_u = false);
+  // mode: CHQ_P_ADD / ASSIGN / X64 / X64V (chq_device.cuh); x, Lx for the X64 modes
+  ocu_status prolong_from(int l, cudaStream_t s, int mode = 0, double *x = nullptr, const ocu_layout *Lx = nullptr);
   // levels tail_s..L-1 in one single-CTA launch: FMG (fmg) or one V-cycle from tail_s
   ocu_status tail(bool fmg, int nu1, int nu2, int citers, cudaStream_t s);
   int tail_s = 0;
-  ocu_status clear_u(int l, cudaStream_t s);
 };
 
 }  // namespace ocub

@@ -821,8 +821,8 @@ ocu_status MGSolver::ir_solve(double tolerance, int max_outer, double *rl2, doub
 }
 
 // The same refinement with the split-layout FP32 correction solver (ir_chequer.cu).  One
-// captured graph per refinement step: clear the correction, FMG ramp + ir_inner_cycles fine-level
-// V-cycles, x += e, the level-0 ghost refresh with the caller's boundary values, the FP64
+// captured graph per refinement step: FMG ramp + ir_inner_cycles fine-level V-cycles from a zero
+// correction, x += e (fused into the last prolongation), the level-0 ghost refresh with the caller's boundary values, the FP64
 // residual (written as float into the correction's right-hand side) and its norms.  The host
 // waits once per step, for the norms.
 enum { SEG_CHQ_FIRST = 0, SEG_CHQ_STEP = 1 };
@@ -855,8 +855,7 @@ ocu_status MGSolver::ir_solve_chequer(double tolerance, int max_outer, double *r
   const int citers = coarse_iters();
   for (int outer = 1; outer <= max_outer; outer++) {
     OCU_TRY(run_segment(chq.get(), SEG_CHQ_STEP, [&]() -> ocu_status {
-      OCU_TRY(chq->enqueue_fmg(prm.nu1, prm.nu2, inner, citers, prm.nu1 + prm.nu2, stream));
-      OCU_TRY(chq->enqueue_add_correction(cd.u0(0), cd.lay[0], stream));
+      OCU_TRY(chq->enqueue_fmg(prm.nu1, prm.nu2, inner, citers, prm.nu1 + prm.nu2, stream, cd.u0(0), &cd.lay[0]));
       OCU_TRY(cd.apply_bc(0));
       return ir_chequer_residual_tail();
     }));
