@@ -702,8 +702,9 @@ def run_persistent_ensemble(torch, ocu, stream, sh, count=512):
     corr = [st.corrections for st in stats]
     # per member and correction: the FP32 V-cycles (cycles + the nested-iteration ramp ~ 1/7
     # cycle) at 12.57 N 4 bytes each, the FP64 residual (x, b read, float r written: 20 N) and
-    # the correction update (x read and written, e read: 20 N); plus the final residual check
-    alg = sum((c * ((p.cycles + 1.0 / 7.0) * 12.57 * 4 + 40) + 20) * n ** 3 for c, n in zip(corr, sizes))
+    # x += e fused into the last prolongation (x read and written: 16 N; e not written back:
+    # - 4 N); plus the final residual check
+    alg = sum((c * ((p.cycles + 1.0 / 7.0) * 12.57 * 4 + 32) + 20) * n ** 3 for c, n in zip(corr, sizes))
     blocks, threads, scratch = ens.launch_shape()
     return {"pens_512_ms": round(ms, 3), "pens_members_converged": conv,
             "pens_alg_gbs": round(alg / (ms * 1e-3) / 1e9, 1),

@@ -112,25 +112,20 @@ __device__ __noinline__ void b_relax(const ChqG &g, const ChqK &k, const ChqBC &
     }
 }
 
-template <int NT>
+// ZU: the fine u is zero and only b is read (chq_restrict_item)
+template <int NT, bool ZU = false>
 __device__ __noinline__ void b_restrict(const ChqG &f, const ChqG &c, const ChqK &k, const ChqBC &bc, const FDiv &fcm) {
   const int n = c.nx * c.ny * fcm.d;
-  for (int t = threadIdx.x; t < n; t += NT) chq_restrict_item<false>(f, c, k, bc, fcm, t);
+  for (int t = threadIdx.x; t < n; t += NT) chq_restrict_item<false, ZU>(f, c, k, bc, fcm, t);
   __syncthreads();
 }
 
-template <int NT>
-__device__ __noinline__ void b_prolong(const ChqG &c, const ChqG &f, const ChqBC &bc, const FDiv &fcm) {
+// MODE: add into the fine u, assign it, or add the result into the FP64 x (chq_prolong_item)
+template <int NT, int MODE = CHQ_P_ADD>
+__device__ __noinline__ void b_prolong(const ChqG &c, const ChqG &f, const ChqBC &bc, const FDiv &fcm,
+                                       ChqX X = ChqX{nullptr, 0, 0}) {
   const int n = c.nx * c.ny * fcm.d;
-  for (int t = threadIdx.x; t < n; t += NT) chq_prolong_item<false>(c, f, bc, fcm, t);
-  __syncthreads();
-}
-
-template <int NT>
-__device__ __noinline__ void b_clear_u(const ChqG &g) {  // u0 and u1 are adjacent, rz a multiple of 4
-  const int n4 = g.nx * g.ny * g.rz / 2;
-  float4 *p = reinterpret_cast<float4 *>(g.u0);
-  for (int t = threadIdx.x; t < n4; t += NT) p[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int t = threadIdx.x; t < n; t += NT) chq_prolong_item<false, MODE>(c, f, bc, fcm, t, X);
   __syncthreads();
 }
 
@@ -241,35 +236,48 @@ __device__ __noinline__ void b_tail(PensMember &D, float *sm, int fmg) {
   __syncthreads();
 }
 
-// One FP32 correction solve of A e = r (r already in level 0's b): u(0) = 0, r restricted to the
-// tail, the tail solved, nested iteration up (prolongation + ramp iterations per level), then
-// `cycles` V-cycles at level 0 (none: the nested iteration alone) -- the schedule of
+// One FP32 correction solve of A e = r (r already in level 0's b) and x += e: from a zero
+// correction, r restricted to the tail (b alone is read), the tail solved, nested iteration up
+// (an assigning prolongation + ramp iterations per level), then `cycles` V-cycles at level 0
+// (none: the nested iteration alone), the last prolongation adding into x -- the schedule of
 // ChequerMG::enqueue_fmg, block-wide.
 template <int NT>
 __device__ void b_correction(PensMember &D, float *H, float *sm, const PensArgs &A) {
   const int ts = D.ts;
-  if (ts > 0) b_clear_u<NT>(level_g(D.lv[0], H));
-  for (int l = 0; l < ts; l++)
-    b_restrict<NT>(level_g(D.lv[l], H), level_g(D.lv[l + 1], H), D.lv[l].k, D.bc, D.lv[l + 1].fcm);
-  b_tail<NT>(D, sm, 1);
-  if (ts == 0) {
+  if (ts == 0) {  // the whole hierarchy in the tail
+    b_tail<NT>(D, sm, 1);
     for (int c = 1; c < A.cycles; c++) b_tail<NT>(D, sm, 0);
+    b_add_correction<NT>(fine64(D), level_g(D.lv[0], H));
     return;
   }
+  for (int l = 0; l < ts; l++)
+    b_restrict<NT, true>(level_g(D.lv[l], H), level_g(D.lv[l + 1], H), D.lv[l].k, D.bc, D.lv[l + 1].fcm);
+  b_tail<NT>(D, sm, 1);
   for (int f = ts - 1; f >= 1; f--) {
-    b_prolong<NT>(level_g(D.lv[f + 1], H), level_g(D.lv[f], H), D.bc, D.lv[f + 1].fcm);
+    b_prolong<NT, CHQ_P_ASSIGN>(level_g(D.lv[f + 1], H), level_g(D.lv[f], H), D.bc, D.lv[f + 1].fcm);
     b_relax<NT>(level_g(D.lv[f], H), D.lv[f].k, D.bc, A.ramp);
   }
-  b_prolong<NT>(level_g(D.lv[1], H), level_g(D.lv[0], H), D.bc, D.lv[1].fcm);
+  b_prolong<NT, CHQ_P_ASSIGN>(level_g(D.lv[1], H), level_g(D.lv[0], H), D.bc, D.lv[1].fcm);
+  if (A.cycles <= 0) {
+    b_add_correction<NT>(fine64(D), level_g(D.lv[0], H));
+    return;
+  }
   for (int c = 0; c < A.cycles; c++) {
     for (int l = 0; l < ts; l++) {
       b_relax<NT>(level_g(D.lv[l], H), D.lv[l].k, D.bc, A.nu1);
       b_restrict<NT>(level_g(D.lv[l], H), level_g(D.lv[l + 1], H), D.lv[l].k, D.bc, D.lv[l + 1].fcm);
     }
     b_tail<NT>(D, sm, 0);
-    for (int l = ts - 1; l >= 0; l--) {
+    for (int l = ts - 1; l >= 1; l--) {
       b_prolong<NT>(level_g(D.lv[l + 1], H), level_g(D.lv[l], H), D.bc, D.lv[l + 1].fcm);
-      if (l > 0) b_relax<NT>(level_g(D.lv[l], H), D.lv[l].k, D.bc, A.nu2);
+      b_relax<NT>(level_g(D.lv[l], H), D.lv[l].k, D.bc, A.nu2);
+    }
+    if (c < A.cycles - 1) {
+      b_prolong<NT>(level_g(D.lv[1], H), level_g(D.lv[0], H), D.bc, D.lv[1].fcm);
+    } else {
+      const ChqX X{D.x, D.xs, D.ys};
+      if (D.vec) b_prolong<NT, CHQ_P_X64V>(level_g(D.lv[1], H), level_g(D.lv[0], H), D.bc, D.lv[1].fcm, X);
+      else b_prolong<NT, CHQ_P_X64>(level_g(D.lv[1], H), level_g(D.lv[0], H), D.bc, D.lv[1].fcm, X);
     }
   }
 }
@@ -317,8 +325,7 @@ __global__ void __launch_bounds__(NT, MINB) k_pens_solve(const __grid_constant__
       l2 = sqrt(b_residual<NT>(fine64(D), D.oc, g0, red) * D.inv_n);
       if (l2 <= tol) { conv = 1; break; }
       if (corr >= A.max_outer || !(l2 == l2)) break;
-      b_correction<NT>(D, H, sm, A);
-      b_add_correction<NT>(fine64(D), g0);
+      b_correction<NT>(D, H, sm, A);  // x += e included
       corr++;
     }
     if (threadIdx.x == 0) {
