@@ -145,12 +145,22 @@ void ProjectSolver::set_stream(cudaStream_t s) {
 static double round_t(ocu_dtype dt, double x) { return dt == OCU_F64 ? x : (double)(float)x; }
 
 NSSolver::~NSSolver() {
+  drop_tail_graphs();
   for (ocu_grid *g : {u, v, w, t, du, dv, dw, dt, ldu, ldv, ldw, ldt}) {
     if (g) { cudaFree(g->buf); delete g; }
   }
   if (scratch) cudaFree(scratch);
   if (d_red) cudaFree(d_red);
   if (h_red) cudaFreeHost(h_red);
+  if (d_coef) cudaFree(d_coef);
+}
+
+void NSSolver::drop_tail_graphs() {
+  for (int q = 0; q < 4; q++) {
+    if (tail_exec[q]) cudaGraphExecDestroy(tail_exec[q]);
+    tail_exec[q] = nullptr;
+    tail_seen[q] = 0;
+  }
 }
 
 static ocu_status make_grid(ocu_dtype dt, const ocu_layout &L, ocu_grid **out) {
@@ -197,6 +207,7 @@ ocu_status NSSolver::set_parameters(const ocu_ns_params &p, const void *iu, cons
     return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - invalid interpolation type %d", p.advection_scheme);
   if (!bc_check_scalar(p.temp_bc) || !bc_check_mac(p.flow_bc))
     return fail(OCU_ERR_INVALID_VALUE, "[ERROR] Eqn_IncompressibleNS3D::set_parameters - invalid boundary condition types");
+  if (!stream) set_stream(nullptr);
   prm = p;
   T_gravity = round_t(dtype, p.gravity);
   T_bouyancy = round_t(dtype, p.bouyancy);
@@ -204,6 +215,8 @@ ocu_status NSSolver::set_parameters(const ocu_ns_params &p, const void *iu, cons
   T_nu = round_t(dtype, p.viscosity);
   lastdt = 0;
   num_steps = 0;
+  swaps = 0;
+  drop_tail_graphs();
   ocu_layout Lu, Lv, Lw, Lt;
   ns_init_layout(p.nx, p.ny, p.nz, 'u', &Lu);
   ns_init_layout(p.nx, p.ny, p.nz, 'v', &Lv);
@@ -237,6 +250,7 @@ ocu_status NSSolver::set_parameters(const ocu_ns_params &p, const void *iu, cons
     OCU_TRY(check_cuda(cudaMalloc(&d_red, 4 * sizeof(double)), "cudaMalloc"));
     OCU_TRY(check_cuda(cudaMemset(d_red, 0, 4 * sizeof(double)), "cudaMemset"));
     OCU_TRY(check_cuda(cudaMallocHost(&h_red, 4 * sizeof(double)), "cudaMallocHost"));
+    OCU_TRY(check_cuda(cudaMalloc(&d_coef, 4 * sizeof(double)), "cudaMalloc(step coefficients)"));
   }
   initialized = true;
   return check_cuda(cudaStreamSynchronize(stream), "set_parameters");
@@ -277,7 +291,7 @@ ocu_status NSSolver::get_max_stable_timestep(double *out) {
 }
 
 template <typename T>
-ocu_status NSSolver::step_t(double dtv) {
+ocu_status NSSolver::enqueue_tail(double dtv, T ab, bool ab2, const T *dcoef) {
   const int nx = prm.nx, ny = prm.ny, nz = prm.nz;
   const int vd = prm.vertical_direction;
   const ocu_layout &Lu = u->L;
@@ -285,9 +299,10 @@ ocu_status NSSolver::step_t(double dtv) {
   const T coef = dm * (T)T_gravity * (T)T_bouyancy;
   ocu_grid *vert = (vd & OCU_DIR_XAXIS_FLAG) ? du : (vd & OCU_DIR_YAXIS_FLAG) ? dv : dw;
   const int nbr = (vd & OCU_DIR_XAXIS_FLAG) ? t->L.xstride : (vd & OCU_DIR_YAXIS_FLAG) ? t->L.ystride : 1;
-  const T ab = (T)(-dtv * dtv / (2 * lastdt));
-  const bool ab2 = prm.time_step == OCU_TS_ADAMS_BASHFORD2 && lastdt > 0;
-  num_steps++;
+  // the step's coefficients: values, or slots 0, 1, 2 of dcoef (read when the kernels run)
+  const Coef<T> c_dt = dcoef ? Coef<T>((T)dtv, dcoef + 0) : Coef<T>((T)dtv);
+  const Coef<T> c_dab = dcoef ? Coef<T>((T)(dtv - ab), dcoef + 1) : Coef<T>((T)(dtv - ab));
+  const Coef<T> c_ab = dcoef ? Coef<T>(ab, dcoef + 2) : Coef<T>(ab);
   // FP32 on a large grid: the TMA-fed form (bit-identical), its timeout word in d_red[3]
   ocu_status adv = OCU_ERR_UNSUPPORTED;
   if constexpr (sizeof(T) == 4) {
@@ -332,10 +347,10 @@ ocu_status NSSolver::step_t(double dtv) {
     OCU_TRY(launch_laplacian<T>(origin<T>(t), origin<T>(dt), t->L, nx, ny, nz, prm.hx, prm.hy, prm.hz, (T)T_kappa, stream));
   T *tb = (T *)t->buf;
   if (ab2) {
-    OCU_TRY(launch_lincomb2<T>(tb, t->L, (T)1.0, tb, (T)(dtv - ab), (const T *)dt->buf, stream));
-    OCU_TRY(launch_lincomb2<T>(tb, t->L, (T)1.0, tb, ab, (const T *)ldt->buf, stream));
+    OCU_TRY(launch_lincomb2<T>(tb, t->L, (T)1.0, tb, c_dab, (const T *)dt->buf, stream));
+    OCU_TRY(launch_lincomb2<T>(tb, t->L, (T)1.0, tb, c_ab, (const T *)ldt->buf, stream));
   } else {
-    OCU_TRY(launch_lincomb2<T>(tb, t->L, (T)1.0, tb, (T)dtv, (const T *)dt->buf, stream));
+    OCU_TRY(launch_lincomb2<T>(tb, t->L, (T)1.0, tb, c_dt, (const T *)dt->buf, stream));
   }
   OCU_TRY(launch_bc_nocorners_dev<T>(origin<T>(t), t->L, prm.temp_bc, prm.hx, prm.hy, prm.hz, stream));
   ocu_grid *st[3] = {u, v, w}, *ds[3] = {du, dv, dw}, *ls[3] = {ldu, ldv, ldw};
@@ -344,21 +359,94 @@ ocu_status NSSolver::step_t(double dtv) {
     T *x3[3] = {(T *)u->buf, (T *)v->buf, (T *)w->buf};
     const T *d3[3] = {(const T *)du->buf, (const T *)dv->buf, (const T *)dw->buf};
     const T *l3[3] = {(const T *)ldu->buf, (const T *)ldv->buf, (const T *)ldw->buf};
-    const ocu_status us = ab2 ? launch_update3<T>(x3, d3, l3, Lu, (T)(dtv - ab), ab, stream)
-                              : launch_update3<T>(x3, d3, nullptr, Lu, (T)dtv, (T)0, stream);
-    if (us == OCU_OK) goto updated;
+    const ocu_status us = ab2 ? launch_update3<T>(x3, d3, l3, Lu, c_dab, c_ab, stream)
+                              : launch_update3<T>(x3, d3, nullptr, Lu, c_dt, Coef<T>((T)0), stream);
+    if (us == OCU_OK) return OCU_OK;
     if (us != OCU_ERR_UNSUPPORTED) return us;
   }
   for (int c = 0; c < 3; c++) {
     T *x = (T *)st[c]->buf;
     if (ab2) {
-      OCU_TRY(launch_lincomb2<T>(x, st[c]->L, (T)1.0, x, (T)(dtv - ab), (const T *)ds[c]->buf, stream));
-      OCU_TRY(launch_lincomb2<T>(x, st[c]->L, (T)1.0, x, ab, (const T *)ls[c]->buf, stream));
+      OCU_TRY(launch_lincomb2<T>(x, st[c]->L, (T)1.0, x, c_dab, (const T *)ds[c]->buf, stream));
+      OCU_TRY(launch_lincomb2<T>(x, st[c]->L, (T)1.0, x, c_ab, (const T *)ls[c]->buf, stream));
     } else {
-      OCU_TRY(launch_lincomb2<T>(x, st[c]->L, (T)1.0, x, (T)dtv, (const T *)ds[c]->buf, stream));
+      OCU_TRY(launch_lincomb2<T>(x, st[c]->L, (T)1.0, x, c_dt, (const T *)ds[c]->buf, stream));
     }
   }
-updated:
+  return OCU_OK;
+}
+
+static __global__ void k_set_coef(double *c, double a, double b, double d) {
+  c[0] = a; c[1] = b; c[2] = d;
+}
+static __global__ void k_set_coef(float *c, float a, float b, float d) {
+  c[0] = a; c[1] = b; c[2] = d;
+}
+
+// Environment read by the tail's launchers (the TMA advection's mode and its timeout test): a
+// graph captured under one setting is not replayed under another.
+static std::string tail_env_signature() {
+  std::string sig;
+  for (const char *k : {"OCU_B200_ADVECT_TMA", "OCU_B200_TMA_STALL_TEST"}) {
+    const char *v = std::getenv(k);
+    sig += v ? v : "-";
+    sig += ';';
+  }
+  return sig;
+}
+
+// The step's coefficients into d_coef, then the state's graph (captured on first use).
+template <typename T>
+ocu_status NSSolver::replay_tail(int key, double dtv, T ab, bool ab2) {
+  T *c = reinterpret_cast<T *>(d_coef);
+  k_set_coef<<<1, 1, 0, stream>>>(c, (T)dtv, (T)(dtv - ab), ab);
+  OCU_TRY(check_launch("k_set_coef"));
+  if (!tail_exec[key]) {
+    OCU_TRY(check_cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture"));
+    set_capturing(true);
+    const unsigned long long n0 = launch_count_captured();
+    const ocu_status st = enqueue_tail<T>(dtv, ab, ab2, c);
+    tail_kernels[key] = (int)(launch_count_captured() - n0);
+    set_capturing(false);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    if (st != OCU_OK || e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return st != OCU_OK ? st : check_cuda(e, "cudaStreamEndCapture");
+    }
+    e = cudaGraphInstantiate(&tail_exec[key], g, 0);
+    cudaGraphDestroy(g);
+    OCU_TRY(check_cuda(e, "cudaGraphInstantiate"));
+  }
+  OCU_TRY(check_cuda(cudaGraphLaunch(tail_exec[key], stream), "cudaGraphLaunch"));
+  count_launch(tail_kernels[key]);
+  return OCU_OK;
+}
+
+// advance_one_step (eqn_incompressns3d.cu:331-399): the tail (advection, diffusion, buoyancy,
+// updates, temperature ghosts) as plain launches or one graph replay, then the projection.
+template <typename T>
+ocu_status NSSolver::step_t(double dtv) {
+  const T ab = (T)(-dtv * dtv / (2 * lastdt));
+  const bool ab2 = prm.time_step == OCU_TS_ADAMS_BASHFORD2 && lastdt > 0;
+  num_steps++;
+  const char *ge = std::getenv("OCU_B200_NS_GRAPH"), *ga = std::getenv("OCU_B200_GRAPHS");
+  bool graphed = false;
+  if (!(ge && ge[0] == '0') && !(ga && ga[0] == '0')) {
+    const std::string sig = tail_env_signature();
+    if (sig != tail_env) {
+      drop_tail_graphs();
+      tail_env = sig;
+    }
+    const int key = (ab2 ? 2 : 0) + (swaps & 1);
+    if (stream && (tail_exec[key] || tail_seen[key] > 0)) {
+      OCU_TRY(replay_tail<T>(key, dtv, ab, ab2));
+      graphed = true;
+    }
+    tail_seen[key]++;
+  }
+  if (!graphed) OCU_TRY(enqueue_tail<T>(dtv, ab, ab2, nullptr));
+
   if (prm.time_step == OCU_TS_ADAMS_BASHFORD2) {
     // this step's derivatives become the previous ones by exchanging the buffers, where the
     // reference copies them (eqn_incompressns3d.cu:390-396).  The derivative kernels overwrite
@@ -366,6 +454,7 @@ updated:
     // only the viscous term adds to; those faces of the velocity are set by the boundary
     // conditions after the update, so the velocity and temperature are the reference's.
     lastdt = dtv;
+    swaps++;
     std::swap(dt, ldt);
     std::swap(du, ldu);
     std::swap(dv, ldv);
@@ -397,6 +486,10 @@ ocu_status NSSolver::advance(double dtv) {
 }
 
 void NSSolver::set_stream(cudaStream_t s) {
+  if (!s) {
+    if (!own.s) cudaStreamCreate(&own.s);
+    s = own.s;
+  }
   stream = s;
   proj.set_stream(s);
 }

@@ -290,16 +290,18 @@ __global__ void k_lincomb1(T *res, T a1, const T *g1, long long n) {
 }
 
 template <typename T>
-__global__ void k_lincomb2_1d(T *res, T a1, const T *g1, T a2, const T *g2, long long n) {
+__global__ void k_lincomb2_1d(T *res, T a1, const T *g1, Coef<T> a2c, const T *g2, long long n) {
   pdl_entry();
+  const T a2 = a2c.get();
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     res[i] = g1[i] * a1 + g2[i] * a2;
 }
 
 template <typename T>
-__global__ void k_lincomb2_3d(T *res, T a1, const T *g1, T a2, const T *g2, long long xs, long long ys,
+__global__ void k_lincomb2_3d(T *res, T a1, const T *g1, Coef<T> a2c, const T *g2, long long xs, long long ys,
                               int nx, int ny, int nz) {
   pdl_entry();
+  const T a2 = a2c.get();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   const int j = blockIdx.y;
   const int i = blockIdx.z;
@@ -311,9 +313,10 @@ __global__ void k_lincomb2_3d(T *res, T a1, const T *g1, T a2, const T *g2, long
 // The same sum over 16-byte groups of a row: k = 0 of every row is 16-byte aligned (checked by
 // the launcher), a row's last group may be partial.  Per element the arithmetic is unchanged.
 template <typename T>
-__global__ void k_lincomb2_3dv(T *res, T a1, const T *g1, T a2, const T *g2, long long xs, long long ys, int ny,
-                               int nz, int cpr, long long nchunks) {
+__global__ void k_lincomb2_3dv(T *res, T a1, const T *g1, Coef<T> a2c, const T *g2, long long xs, long long ys,
+                               int ny, int nz, int cpr, long long nchunks) {
   pdl_entry();
+  const T a2 = a2c.get();
   constexpr int V = 16 / (int)sizeof(T);
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < nchunks;
        c += (long long)gridDim.x * blockDim.x) {
@@ -350,9 +353,10 @@ struct UpdateSet {
 };
 
 template <typename T, bool AB2>
-__global__ void k_update3_3dv(const __grid_constant__ UpdateSet<T> S, T a2, T a3, long long xs, long long ys, int ny,
-                              int nz, int cpr, long long nchunks) {
+__global__ void k_update3_3dv(const __grid_constant__ UpdateSet<T> S, Coef<T> a2c, Coef<T> a3c, long long xs,
+                              long long ys, int ny, int nz, int cpr, long long nchunks) {
   pdl_entry();
+  const T a2 = a2c.get(), a3 = a3c.get();
   constexpr int V = 16 / (int)sizeof(T);
   using Vec = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
   for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < 3 * nchunks;
@@ -418,8 +422,8 @@ ocu_status launch_lincomb1(T *res, T a1, const T *g1, long long n, cudaStream_t 
 // OCU_ERR_UNSUPPORTED when the interior-only 16-byte form would not be the one the separate
 // linear combinations take (the caller then launches those).
 template <typename T>
-ocu_status launch_update3(T *const *x, const T *const *d, const T *const *l, const ocu_layout &L, T a2, T a3,
-                          cudaStream_t s) {
+ocu_status launch_update3(T *const *x, const T *const *d, const T *const *l, const ocu_layout &L, Coef<T> a2,
+                          Coef<T> a3, cudaStream_t s) {
   const long long waste = L.allocated - (long long)L.nx * L.ny * L.nz;
   const auto a16 = [](const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
   bool ok = (double)waste > 0.03 * (double)L.allocated && (L.ystride * sizeof(T)) % 16 == 0 &&
@@ -448,7 +452,7 @@ ocu_status launch_update3(T *const *x, const T *const *d, const T *const *l, con
 // The reference switches to the interior-only kernel when more than 3% of the buffer is
 // padding (grid3ddev.cu:312); otherwise it sweeps the whole buffer, ghosts included.
 template <typename T>
-ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, T a2, const T *g2,
+ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, Coef<T> a2, const T *g2,
                            cudaStream_t s) {
   const long long waste = L.allocated - (long long)L.nx * L.ny * L.nz;
   if ((double)waste > 0.03 * (double)L.allocated) {
@@ -890,9 +894,10 @@ ocu_status launch_dot(const T *a, const T *b, const ocu_layout &L, void *d_scrat
                                               const ocu_bc_set &, cudaStream_t);                              \
   template ocu_status launch_clear<T>(T *, long long, T, cudaStream_t);                                        \
   template ocu_status launch_lincomb1<T>(T *, T, const T *, long long, cudaStream_t);                          \
-  template ocu_status launch_lincomb2<T>(T *, const ocu_layout &, T, const T *, T, const T *, cudaStream_t);   \
+  template ocu_status launch_lincomb2<T>(T *, const ocu_layout &, T, const T *, Coef<T>, const T *, cudaStream_t); \
   template ocu_status launch_reduce<T>(const T *, const ocu_layout &, int, void *, double *, cudaStream_t);    \
-  template ocu_status launch_update3<T>(T *const *, const T *const *, const T *const *, const ocu_layout &, T, T, \
+  template ocu_status launch_update3<T>(T *const *, const T *const *, const T *const *, const ocu_layout &, Coef<T>, \
+                                        Coef<T>, \
                                         cudaStream_t);                                                        \
   template ocu_status launch_dot<T>(const T *, const T *, const ocu_layout &, void *, double *, cudaStream_t);  \
   template ocu_status launch_minmax<T>(const T *const *, const ocu_layout *const *, int, int, void *, double *,  \

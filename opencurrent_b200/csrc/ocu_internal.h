@@ -126,8 +126,21 @@ template <typename T, typename S>
 ocu_status launch_convert(T *dst, const S *src, long long n, cudaStream_t s);
 template <typename T>
 ocu_status launch_lincomb1(T *res, T a1, const T *g1, long long n, cudaStream_t s);
+// A coefficient of a linear-combination kernel: the value itself, or (p set) the value the
+// kernel reads from device memory after its programmatic-dependency wait -- so a launch captured
+// once in a CUDA graph takes a new time step at every replay.
 template <typename T>
-ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, T a2, const T *g2,
+struct Coef {
+  T v;
+  const T *p;
+  __host__ __device__ Coef(T value) : v(value), p(nullptr) {}
+  __host__ __device__ Coef(T value, const T *ptr) : v(value), p(ptr) {}
+#ifdef __CUDACC__
+  __device__ __forceinline__ T get() const { return p ? *p : v; }
+#endif
+};
+template <typename T>
+ocu_status launch_lincomb2(T *res, const ocu_layout &L, T a1, const T *g1, Coef<T> a2, const T *g2,
                            cudaStream_t s);
 
 // Reduction in the reference fold order over the interior of a grid; the T result is stored
@@ -192,8 +205,8 @@ ocu_status launch_gradient_p64(float *u, float *v, float *w, const double *phi, 
                               int nz, double hx, double hy, double hz, double coefficient, cudaStream_t s);
 // u, v, w (one layout) += a2 d [then += a3 l]: one launch, or OCU_ERR_UNSUPPORTED
 template <typename T>
-ocu_status launch_update3(T *const *x, const T *const *d, const T *const *l, const ocu_layout &L, T a2, T a3,
-                          cudaStream_t s);
+ocu_status launch_update3(T *const *x, const T *const *d, const T *const *l, const ocu_layout &L, Coef<T> a2,
+                          Coef<T> a3, cudaStream_t s);
 // diffusion + buoyancy of the vertical velocity in one pass (FP32), or OCU_ERR_UNSUPPORTED
 ocu_status launch_laplacian_thermal(const float *phi, float *dphidt, const ocu_layout &L, int nx, int ny, int nz,
                                     double hx, double hy, double hz, float coefficient, const float *temp, float ct,
