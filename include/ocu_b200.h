@@ -532,7 +532,11 @@ ocu_status ocu_ns_set_parameters(ocu_ns *ns, const ocu_ns_params *params, const 
                                  const void *init_temp);
 /* get_max_stable_timestep (:301-328); blocks the host for three maxabs reductions. */
 ocu_status ocu_ns_get_max_stable_timestep(ocu_ns *ns, double *dt);
-ocu_status ocu_ns_advance_one_step(ocu_ns *ns, double dt);                  /* :331-399 */
+/* advance_one_step (:331-399).  The step's work before the projection is replayed as one CUDA
+ * graph from the second step of each time-stepping state on (dt is read from device memory, so
+ * any dt replays); OCU_B200_NS_GRAPH=0 or OCU_B200_GRAPHS=0 issues it as plain launches.  With
+ * the NULL stream the solver works on a private blocking stream (NULL orders against it). */
+ocu_status ocu_ns_advance_one_step(ocu_ns *ns, double dt);
 ocu_status ocu_ns_advance(ocu_ns *ns, double dt);       /* Equation::advance, equation.cpp:31-56 */
 /* get_u/v/w/temperature (:171-174) and the time derivatives 'U','V','W','T', pressure 'p'. */
 ocu_grid *ocu_ns_grid(ocu_ns *ns, char which);
