@@ -79,6 +79,27 @@ def test_ir_split_inner_reaches_1e10(case):
     assert e <= 1e-7
 
 
+@pytest.mark.parametrize("shape", [(8, 8, 8), (16, 16, 16), (16, 8, 32)])
+def test_ir_small_grids_through_the_tail(shape):
+    """Grids whose split hierarchy lies wholly (8^3: 512 cells) or from level 1 on in the
+    single-CTA tail: the correction then ends with x += e as its own pass (wholly in the tail)
+    or in the last prolongation out of the tail; both reach 1e-10 and the FP64 solution."""
+    L, rhs, rms = problem(shape, 800)
+    bc = bc_from(SCALAR_BCS["neumann"])
+    h = tuple(1.0 / n for n in shape)
+    om = O.OracleMG("d", mg_params(bc), *shape, *h, rhs.copy(), L)
+    ok_o, res_o = om.solve(1e-13 * rms, 60)
+    assert res_o <= 2e-11 * rms
+    dm = ocu.Sol_MultigridPressureMixed3DDeviceD("ir")
+    dm.bc = to_ocu_bc(bc)
+    dm.initialize_storage(*shape, *h, dev_grid(rhs, F64, L))
+    ok, res = dm.solve(1e-10 * rms, 20)
+    e = rel_l2(dm.pressure().copy_to_host(), om.grid("u", 0)[0], L, True)
+    print(f"IRCHQ small {shape} rel_res={res / rms:.3e} outer={dm.stats.outer_iterations} err={e:.3e}")
+    assert ok and res <= 1e-10 * rms
+    assert e <= 1e-7
+
+
 def test_ir_split_inner_second_solve_repeats_first():
     """A second solve from a zero guess replays the captured step and gives the same result."""
     shape, h, bcname = CASES[0]
